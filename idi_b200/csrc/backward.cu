@@ -1,0 +1,530 @@
+// Adjoint (backward) emitter-wavefield direct sum for sm_100a, split precision.
+//
+// For I_p = |E_p|^2 and an upstream gradient g_p = dL/dI_p the adjoint is a
+// second direct sum, reduced over pixels for every emitter j:
+//   G_p    = 2 g_p conj(E_p)                      (per pixel, prep kernel)
+//   z_pj   = G_p exp(i phi_pj)
+//   dL/da_j   =  sum_p w_pj Re z_pj
+//   dL/dpsi_j = -a_j sum_p w_pj Im z_pj
+//   dL/dr_j   = -a_j sum_p w_pj Im z_pj grad_r phi_pj
+// with grad_r phi = -q_p + kappa_p (r_j - s_pj dhat_p) in the near field
+// (q_p = k (dhat_p - zhat), kappa_p = k/|d_p|, s_pj = dhat_p . r_j; the next
+// order is k r^2/|d|^2, ~1e-10 relative), -q_p in the far field, plus
+// kappa_p (x, y, 0) for the far-field second-order term.  The 1/r factor's own
+// gradient (relative size 1/(k |d| theta) ~ 1e-9) is not included.
+//
+// The phase is formed exactly as in the forward split kernel (FP64 turns in a
+// magic binade -> 32-bit fixed point -> FP32 angle, MUFU sincos).  Here each
+// thread owns a few emitters in registers and pixel tiles stream through
+// shared memory (bulk async copies, double-buffered, bounded waits); packed
+// f32x2 arithmetic processes two emitters per instruction.  Work units are
+// (image, emitter block, pixel chunk); each unit writes FP32 partial sums of
+// its chunk, and a reduction kernel adds the chunks in a fixed order in FP64,
+// so results are deterministic.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "idiwf_internal.cuh"
+
+namespace idiwf {
+
+constexpr int kBwdThreads = 128;
+constexpr int kBwdPE = 4;                        // emitters per thread
+constexpr int kBwdEB = kBwdThreads * kBwdPE;     // emitters per block (512)
+constexpr int kBwdTP = 128;                      // pixels per shared-memory tile
+constexpr int kBwdChunk = 2048;                  // pixels per work unit
+constexpr int kBwdNAcc = 9;                      // partial sums per emitter
+
+// pixel record (geometry part, shared by all images):
+//   P64  double4 {cpm, -q'x, -q'y, -q'z}                           32 B
+//   PF   float4 x4  {dx,dx,dy,dy} {dz,dz,h,h} {qx,qx,qy,qy} {qz,qz,kap,kap}   64 B
+//   PS   float4 {iD,iD,iD2,iD2}   (scale only, stored always)       16 B
+// per image:
+//   PG   float4 {Gr,Gr,Gi,Gi}                                      16 B
+constexpr int kPixGeomBytes = 32 + 64 + 16;
+constexpr int kPixRecBytes = kPixGeomBytes + 16;
+
+struct BwdLayout {
+    int npix_pad;          // pixels rounded up to the chunk size
+    int n_chunks;
+    int64_t nrec;          // emitter records (images padded to kBwdEB)
+    size_t off_p64, off_pf, off_pg, off_erec64, off_erecf, off_part, total;
+};
+
+static BwdLayout bwd_layout(const idiwf_geom *g, const idiwf_batch *b) {
+    BwdLayout L;
+    const int64_t npix = (int64_t)g->nx * g->ny;
+    L.npix_pad = (int)((npix + kBwdChunk - 1) / kBwdChunk * kBwdChunk);
+    L.n_chunks = L.npix_pad / kBwdChunk;
+    L.nrec = 0;
+    for (int i = 0; i < b->n_images; ++i) {
+        const int64_t n = b->offsets[i + 1] - b->offsets[i];
+        L.nrec += (n + kBwdEB - 1) / kBwdEB * kBwdEB;
+    }
+    L.nrec = std::max<int64_t>(L.nrec, kBwdEB);
+    size_t o = kWsDataOffset;
+    L.off_p64 = o; o += align256((size_t)L.npix_pad * 32);
+    L.off_pf = o;  o += align256((size_t)L.npix_pad * 80);
+    L.off_pg = o;  o += align256((size_t)L.npix_pad * 16 * b->n_images);
+    L.off_erec64 = o; o += align256((size_t)L.nrec * 32);
+    L.off_erecf = o;  o += align256((size_t)L.nrec * 16);
+    L.off_part = o;   o += align256((size_t)L.n_chunks * L.nrec * kBwdNAcc * 4);
+    L.total = o;
+    return L;
+}
+
+struct BwdImage {
+    int64_t src, rec;
+    int32_t n, nblocks;
+};
+struct BwdParams {
+    int32_t n_images, n_chunks, npix, npix_pad, total_units, units_per_image_block;
+    BwdImage img[kMaxImagesPerLaunch];
+    int32_t unit_img[kMaxImagesPerLaunch];   // images by descending emitter count
+};
+
+// ---- pixel prep: geometry (image independent) ------------------------------
+template <bool NF>
+__global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad, double4 *__restrict__ p64,
+                                      float4 *__restrict__ pf) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix_pad; p += gridDim.x * blockDim.x) {
+        const int pc = min(p, npix - 1);
+        const int ix = pc / g.ny, iy = pc - ix * g.ny;
+        double dx, dy, dz;
+        pixel_cpu(g, ix, iy, dx, dy, dz);
+        const double rho2 = dx * dx + dy * dy;
+        const double D = sqrt(rho2 + dz * dz);
+        const double invD = 1.0 / D;
+        const double dzm1 = dz > 0 ? -rho2 / (D * (D + dz)) : dz * invD - 1.0;
+        double cp = 0.0;
+        if (NF) {
+            const double dmz = dz > 0 ? rho2 / (D + dz) : D - dz;
+            const double c = g.kp * dmz;
+            cp = c - rint(c);
+        }
+        p64[p] = make_double4((kTurnMagic + 0.5 + 0x1p-24) + cp, -g.kp * (dx * invD), -g.kp * (dy * invD),
+                              -g.kp * dzm1);
+        const float fdx = (float)(dx * invD), fdy = (float)(dy * invD), fdz = (float)(dz * invD);
+        const float fh = (float)(g.k * 0.5 * invD);
+        const float qx = (float)(g.k * dx * invD), qy = (float)(g.k * dy * invD), qz = (float)(g.k * dzm1);
+        const float kap = (float)(g.k * invD);
+        const float fi = (float)invD, fi2 = (float)(invD * invD);
+        float4 *r = pf + (size_t)p * 5;
+        r[0] = make_float4(fdx, fdx, fdy, fdy);
+        r[1] = make_float4(fdz, fdz, fh, fh);
+        r[2] = make_float4(qx, qx, qy, qy);
+        r[3] = make_float4(qz, qz, kap, kap);
+        r[4] = make_float4(fi, fi, fi2, fi2);
+    }
+}
+
+// ---- pixel prep: G_p = 2 g_p conj(E_p) per image ---------------------------
+__global__ void bwd_pixel_g_kernel(const double2 *__restrict__ field, const double *__restrict__ gI, int npix,
+                                   int npix_pad, int n_images, float4 *__restrict__ pg) {
+    const int64_t total = (int64_t)npix_pad * n_images;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t / npix_pad);
+        const int p = (int)(t - (int64_t)b * npix_pad);
+        float gr = 0.f, gi = 0.f;
+        if (p < npix) {
+            const double2 e = field[(int64_t)b * npix + p];
+            const double gg = 2.0 * gI[(int64_t)b * npix + p];
+            gr = (float)(gg * e.x);
+            gi = (float)(-gg * e.y);
+        }
+        pg[t] = make_float4(gr, gr, gi, gi);
+    }
+}
+
+// ---- emitter prep: records padded per image to the emitter block ------------
+__global__ void bwd_emitter_prep_kernel(const __grid_constant__ BwdParams bp, const double *__restrict__ atoms,
+                                        double4 *__restrict__ e64, float4 *__restrict__ ef, int w_mode) {
+    const int b = blockIdx.y;
+    const BwdImage d = bp.img[b];
+    const int64_t nrec = (int64_t)d.nblocks * kBwdEB;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nrec; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = d.rec + j;
+        if (j < d.n) {
+            const double4 a = reinterpret_cast<const double4 *>(atoms)[d.src + j];
+            double psi = a.w * kInvTwoPi;
+            psi = psi - rint(psi);
+            const double w = w_mode == 1 ? (a.x * a.x + a.y * a.y) + a.z * a.z
+                                         : (w_mode == 2 ? a.x * a.x + a.y * a.y : 0.0);
+            e64[r] = make_double4(a.x, a.y, a.z, psi);
+            ef[r] = make_float4((float)a.x, (float)a.y, (float)a.z, (float)w);
+        } else {
+            e64[r] = make_double4(0, 0, 0, 0);
+            ef[r] = make_float4(0, 0, 0, 0);
+        }
+    }
+}
+
+__device__ __forceinline__ float2 g2(float a, float b) { return make_float2(a, b); }
+
+// ---- the adjoint direct sum --------------------------------------------------
+template <bool NF, bool SCALE, bool SECOND>
+__global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
+    const __grid_constant__ BwdParams bp, const double4 *__restrict__ e64, const float4 *__restrict__ ef,
+    const double4 *__restrict__ p64, const float4 *__restrict__ pf, const float4 *__restrict__ pg,
+    float *__restrict__ part, int64_t nrec, WsHeader *__restrict__ hdr) {
+    constexpr int PH = kBwdPE / 2;
+    constexpr uint32_t kStage = kBwdTP * kPixRecBytes;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_unit, s_abort;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        s_abort = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+    uint32_t issued = 0, consumed = 0;
+    bool aborted = false;
+    const float2 TWO_PI2 = g2(6.28318548f, 6.28318548f);
+    const float2 NEG_3PI2 = g2(-9.42477796f, -9.42477796f);
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_unit = (int)atomicAdd(&hdr->work_counter, 1u);
+        __syncthreads();
+        const int unit = s_unit;
+        if (unit >= bp.total_units) break;
+        // unit -> (image-block, chunk); image-blocks are enumerated image by
+        // image in descending emitter count
+        const int chunk = unit % bp.n_chunks;
+        int ib = unit / bp.n_chunks;
+        int img = 0;
+        for (int k = 0; k < bp.n_images; ++k) {
+            const int b = bp.unit_img[k];
+            if (ib < bp.img[b].nblocks) { img = b; break; }
+            ib -= bp.img[b].nblocks;
+        }
+        const BwdImage d = bp.img[img];
+        const int64_t rec0 = d.rec + (int64_t)ib * kBwdEB + tid * kBwdPE;
+
+        // emitter registers
+        double ex[kBwdPE], ey[kBwdPE], ez[kBwdPE], epsi[kBwdPE];
+        float2 fx[PH], fy[PH], fz[PH], fw[PH];
+#pragma unroll
+        for (int e = 0; e < kBwdPE; ++e) {
+            const double4 r = e64[rec0 + e];
+            ex[e] = r.x; ey[e] = r.y; ez[e] = r.z; epsi[e] = r.w;
+            const float4 f = ef[rec0 + e];
+            if (e & 1) { fx[e / 2].y = f.x; fy[e / 2].y = f.y; fz[e / 2].y = f.z; fw[e / 2].y = f.w; }
+            else       { fx[e / 2].x = f.x; fy[e / 2].x = f.y; fz[e / 2].x = f.z; fw[e / 2].x = f.w; }
+        }
+        // chunk sums (FP32) of the 9 accumulators
+        float2 cs[kBwdNAcc][PH];
+#pragma unroll
+        for (int a = 0; a < kBwdNAcc; ++a)
+#pragma unroll
+            for (int q = 0; q < PH; ++q) cs[a][q] = g2(0.f, 0.f);
+
+        const int p_begin = chunk * kBwdChunk;
+        constexpr int nt = kBwdChunk / kBwdTP;
+        auto issue = [&](int t) {
+            const uint32_t slot = issued & 1;
+            unsigned char *st = smem + slot * kStage;
+            const int p0 = p_begin + t * kBwdTP;
+            mbar_arrive_expect_tx(&bar[slot], kStage);
+            bulk_g2s(st, p64 + p0, kBwdTP * 32, &bar[slot]);
+            bulk_g2s(st + kBwdTP * 32, pf + (size_t)p0 * 5, kBwdTP * 80, &bar[slot]);
+            bulk_g2s(st + kBwdTP * 112, pg + (size_t)img * bp.npix_pad + p0, kBwdTP * 16, &bar[slot]);
+            ++issued;
+        };
+        if (tid == 0) {
+            issue(0);
+            issue(1);
+        }
+        for (int it = 0; it < nt; ++it) {
+            const uint32_t slot = consumed & 1;
+            if (!mbar_wait_bounded(&bar[slot], (consumed >> 1) & 1)) {
+                record_error(&hdr->error, kErrTimeout);
+                s_abort = 1;
+            }
+            const unsigned char *st = smem + slot * kStage;
+            const double4 *s64 = reinterpret_cast<const double4 *>(st);
+            const float4 *sf = reinterpret_cast<const float4 *>(st + kBwdTP * 32);
+            const float4 *sg = reinterpret_cast<const float4 *>(st + kBwdTP * 112);
+            float2 ac[kBwdNAcc][PH];
+#pragma unroll
+            for (int a = 0; a < kBwdNAcc; ++a)
+#pragma unroll
+                for (int q = 0; q < PH; ++q) ac[a][q] = g2(0.f, 0.f);
+#pragma unroll 2
+            for (int j = 0; j < kBwdTP; ++j) {
+                const double4 P = s64[j];
+                const float4 F0 = sf[5 * j + 0];   // dx dx dy dy
+                const float4 F1 = sf[5 * j + 1];   // dz dz h h
+                const float4 F2 = sf[5 * j + 2];   // qx qx qy qy
+                const float4 F3 = sf[5 * j + 3];   // qz qz kap kap
+                const float4 GG = sg[j];           // Gr Gr Gi Gi
+#pragma unroll
+                for (int q = 0; q < PH; ++q) {
+                    uint32_t lo[2];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int i = 2 * q + e;
+                        double t = __dadd_rn(P.x, epsi[i]);
+                        t = __fma_rn(P.y, ex[i], t);
+                        t = __fma_rn(P.z, ey[i], t);
+                        t = __fma_rn(P.w, ez[i], t);
+                        lo[e] = (uint32_t)__double2loint(t);
+                    }
+                    const float2 u = g2(__uint_as_float((lo[0] >> 9) | 0x3F800000u),
+                                        __uint_as_float((lo[1] >> 9) | 0x3F800000u));
+                    float2 arg = __ffma2_rn(u, TWO_PI2, NEG_3PI2);
+                    float2 s = g2(0.f, 0.f);
+                    if (NF) {
+                        s = __fmul2_rn(g2(F0.x, F0.y), fx[q]);
+                        s = __ffma2_rn(g2(F0.z, F0.w), fy[q], s);
+                        s = __ffma2_rn(g2(F1.x, F1.y), fz[q], s);
+                        const float2 w2 = __ffma2_rn(g2(-s.x, -s.y), s, fw[q]);
+                        arg = __ffma2_rn(g2(F1.z, F1.w), w2, arg);
+                    } else if (SECOND) {
+                        arg = __ffma2_rn(g2(F1.z, F1.w), fw[q], arg);
+                    }
+                    float s0, c0, s1, c1;
+                    __sincosf(arg.x, &s0, &c0);
+                    __sincosf(arg.y, &s1, &c1);
+                    const float2 cc = g2(c0, c1), ss = g2(s0, s1);
+                    // z = G e^{i phi}
+                    float2 zr = __fmul2_rn(g2(GG.x, GG.y), cc);
+                    zr = __ffma2_rn(g2(-GG.z, -GG.w), ss, zr);
+                    float2 zi = __fmul2_rn(g2(GG.x, GG.y), ss);
+                    zi = __ffma2_rn(g2(GG.z, GG.w), cc, zi);
+                    if (NF && SCALE) {
+                        const float4 F4 = sf[5 * j + 4];  // iD iD iD2 iD2
+                        const float2 w = __ffma2_rn(s, g2(F4.z, F4.w), g2(F4.x, F4.y));
+                        zr = __fmul2_rn(zr, w);
+                        zi = __fmul2_rn(zi, w);
+                    } else if (SCALE) {
+                        const float4 F4 = sf[5 * j + 4];
+                        zr = __fmul2_rn(zr, g2(F4.x, F4.y));
+                        zi = __fmul2_rn(zi, g2(F4.x, F4.y));
+                    }
+                    ac[0][q] = __fadd2_rn(ac[0][q], zr);
+                    ac[1][q] = __fadd2_rn(ac[1][q], zi);
+                    ac[2][q] = __ffma2_rn(zi, g2(F2.x, F2.y), ac[2][q]);
+                    ac[3][q] = __ffma2_rn(zi, g2(F2.z, F2.w), ac[3][q]);
+                    ac[4][q] = __ffma2_rn(zi, g2(F3.x, F3.y), ac[4][q]);
+                    if (NF || SECOND) {
+                        const float2 ki = __fmul2_rn(zi, g2(F3.z, F3.w));
+                        ac[5][q] = __fadd2_rn(ac[5][q], ki);
+                        if (NF) {
+                            const float2 ks = __fmul2_rn(ki, s);
+                            ac[6][q] = __ffma2_rn(ks, g2(F0.x, F0.y), ac[6][q]);
+                            ac[7][q] = __ffma2_rn(ks, g2(F0.z, F0.w), ac[7][q]);
+                            ac[8][q] = __ffma2_rn(ks, g2(F1.x, F1.y), ac[8][q]);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < kBwdNAcc; ++a)
+#pragma unroll
+                for (int q = 0; q < PH; ++q) cs[a][q] = __fadd2_rn(cs[a][q], ac[a][q]);
+            ++consumed;
+            __syncthreads();
+            if (s_abort) {
+                aborted = true;
+                break;
+            }
+            if (tid == 0 && it + 2 < nt) issue(it + 2);
+        }
+        if (aborted) break;
+        // partials: part[chunk][rec][acc]
+        float *dst = part + ((size_t)chunk * nrec + rec0) * kBwdNAcc;
+#pragma unroll
+        for (int q = 0; q < PH; ++q)
+#pragma unroll
+            for (int a = 0; a < kBwdNAcc; ++a) {
+                dst[(2 * q) * kBwdNAcc + a] = cs[a][q].x;
+                dst[(2 * q + 1) * kBwdNAcc + a] = cs[a][q].y;
+            }
+    }
+    if (aborted && tid == 0)
+        while (consumed < issued) {
+            mbar_wait_bounded(&bar[consumed & 1], (consumed >> 1) & 1);
+            ++consumed;
+        }
+}
+
+// ---- chunk reduction + final gradients -------------------------------------
+template <bool NF, bool SECOND>
+__global__ void bwd_reduce_kernel(const __grid_constant__ BwdParams bp, const float *__restrict__ part,
+                                  int64_t nrec, const double *__restrict__ atoms, const void *__restrict__ amps,
+                                  int amp_dtype, double *__restrict__ grad_atoms, double *__restrict__ grad_amp) {
+    const int b = blockIdx.y;
+    const BwdImage d = bp.img[b];
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < d.n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = d.rec + j;
+        double acc[kBwdNAcc];
+#pragma unroll
+        for (int a = 0; a < kBwdNAcc; ++a) acc[a] = 0.0;
+        for (int c = 0; c < bp.n_chunks; ++c) {
+            const float *src = part + ((size_t)c * nrec + r) * kBwdNAcc;
+#pragma unroll
+            for (int a = 0; a < kBwdNAcc; ++a) acc[a] += (double)src[a];
+        }
+        const int64_t s = d.src + j;
+        const double4 at = reinterpret_cast<const double4 *>(atoms)[s];
+        double aj = 1.0;
+        if (amps) aj = amp_dtype == IDIWF_F32 ? (double)static_cast<const float *>(amps)[s]
+                                             : static_cast<const double *>(amps)[s];
+        // dL/dr = -a sum w Im z grad(phi), grad(phi) = -q + kap (r - s dhat) [nf]
+        double gx = acc[2], gy = acc[3], gz = acc[4];
+        if (NF) {
+            gx += -acc[5] * at.x + acc[6];
+            gy += -acc[5] * at.y + acc[7];
+            gz += -acc[5] * at.z + acc[8];
+        } else if (SECOND) {
+            gx += -acc[5] * at.x;
+            gy += -acc[5] * at.y;
+        }
+        reinterpret_cast<double4 *>(grad_atoms)[s] = make_double4(aj * gx, aj * gy, aj * gz, -aj * acc[1]);
+        if (grad_amp) grad_amp[s] = acc[0];
+    }
+}
+
+template <bool NF, bool SCALE, bool SECOND>
+static void *bwd_kernel_ptr() {
+    return (void *)bwd_split_kernel<NF, SCALE, SECOND>;
+}
+
+}  // namespace idiwf
+
+using namespace idiwf;
+
+static idiwf_status bwd_validate(const idiwf_geom *g, const idiwf_batch *b) {
+    if (!g || !b || !b->offsets || b->n_images <= 0)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "geom/batch missing or empty");
+    if (g->nx <= 0 || g->ny <= 0 || (int64_t)g->nx * g->ny >= (int64_t)1 << 30)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "bad detector size");
+    if (b->n_images > kMaxImagesPerLaunch)
+        return set_error(IDIWF_ERR_UNSUPPORTED, "backward handles at most 512 images per call");
+    if (b->offsets[0] != 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "offsets[0] must be 0");
+    for (int i = 0; i < b->n_images; ++i)
+        if (b->offsets[i + 1] < b->offsets[i]) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
+    if (b->atoms && (reinterpret_cast<uintptr_t>(b->atoms) & 31))
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "atoms must be 32-byte aligned");
+    if (g->flags & ~(IDIWF_NF | IDIWF_SCALE | IDIWF_SECONDORDER))
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "unknown geometry flag");
+    return IDIWF_OK;
+}
+
+extern "C" size_t idiwf_backward_workspace_size(const idiwf_geom *geom, const idiwf_batch *batch,
+                                                const idiwf_config *cfg) {
+    (void)cfg;
+    if (bwd_validate(geom, batch) != IDIWF_OK) return 0;
+    return bwd_layout(geom, batch).total;
+}
+
+extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch *batch, const void *field,
+                                       const double *grad_intensity, double *grad_atoms, double *grad_amp,
+                                       void *workspace, size_t workspace_bytes, const idiwf_config *cfg,
+                                       cudaStream_t stream) {
+    (void)cfg;
+    idiwf_status st = bwd_validate(geom, batch);
+    if (st != IDIWF_OK) return st;
+    if (!field || !grad_intensity || !grad_atoms)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "field, grad_intensity and grad_atoms are required");
+    const BwdLayout L = bwd_layout(geom, batch);
+    if (!workspace || workspace_bytes < L.total)
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_backward_workspace_size()");
+    if (reinterpret_cast<uintptr_t>(workspace) & 255)
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    const int64_t ntot = batch->offsets[batch->n_images];
+    if (ntot == 0) return IDIWF_OK;
+
+    char *ws = static_cast<char *>(workspace);
+    WsHeader *hdr = reinterpret_cast<WsHeader *>(ws);
+    double4 *p64 = reinterpret_cast<double4 *>(ws + L.off_p64);
+    float4 *pf = reinterpret_cast<float4 *>(ws + L.off_pf);
+    float4 *pg = reinterpret_cast<float4 *>(ws + L.off_pg);
+    double4 *e64 = reinterpret_cast<double4 *>(ws + L.off_erec64);
+    float4 *ef = reinterpret_cast<float4 *>(ws + L.off_erecf);
+    float *part = reinterpret_cast<float *>(ws + L.off_part);
+
+    const GeomParams g = make_geom(geom);
+    const int npix = geom->nx * geom->ny;
+    const bool nf = geom->flags & IDIWF_NF, sc = geom->flags & IDIWF_SCALE, so = geom->flags & IDIWF_SECONDORDER;
+
+    static thread_local BwdParams bp;
+    std::memset(&bp, 0, sizeof(bp));
+    bp.n_images = batch->n_images;
+    bp.n_chunks = L.n_chunks;
+    bp.npix = npix;
+    bp.npix_pad = L.npix_pad;
+    int64_t rec = 0;
+    int total_blocks = 0, max_blocks = 0;
+    std::vector<int> ord(batch->n_images);
+    for (int i = 0; i < batch->n_images; ++i) {
+        const int64_t n = batch->offsets[i + 1] - batch->offsets[i];
+        bp.img[i].src = batch->offsets[i];
+        bp.img[i].rec = rec;
+        bp.img[i].n = (int32_t)n;
+        bp.img[i].nblocks = (int32_t)((n + kBwdEB - 1) / kBwdEB);
+        rec += (int64_t)bp.img[i].nblocks * kBwdEB;
+        total_blocks += bp.img[i].nblocks;
+        max_blocks = std::max(max_blocks, bp.img[i].nblocks);
+        ord[i] = i;
+    }
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int c) { return bp.img[a].n > bp.img[c].n; });
+    for (int i = 0; i < batch->n_images; ++i) bp.unit_img[i] = ord[i];
+    bp.total_units = total_blocks * L.n_chunks;
+
+    const int pthreads = 256;
+    if (nf)
+        bwd_pixel_geom_kernel<true><<<(L.npix_pad + pthreads - 1) / pthreads, pthreads, 0, stream>>>(g, npix, L.npix_pad, p64, pf);
+    else
+        bwd_pixel_geom_kernel<false><<<(L.npix_pad + pthreads - 1) / pthreads, pthreads, 0, stream>>>(g, npix, L.npix_pad, p64, pf);
+    IDIWF_CUDA_CHECK(cudaGetLastError());
+    {
+        const int64_t tot = (int64_t)L.npix_pad * batch->n_images;
+        const int blocks = (int)std::min<int64_t>((tot + pthreads - 1) / pthreads, 65535);
+        bwd_pixel_g_kernel<<<blocks, pthreads, 0, stream>>>(static_cast<const double2 *>(field), grad_intensity, npix,
+                                                            L.npix_pad, batch->n_images, pg);
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+    }
+    {
+        const int w_mode = nf ? 1 : (so ? 2 : 0);
+        dim3 grid((unsigned)std::max(1, (max_blocks * kBwdEB + 255) / 256), batch->n_images);
+        bwd_emitter_prep_kernel<<<grid, 256, 0, stream>>>(bp, batch->atoms, e64, ef, w_mode);
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+    }
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 2 * sizeof(uint32_t), stream));  // counter + error word
+    void *fn;
+    if (nf) fn = sc ? bwd_kernel_ptr<true, true, false>() : bwd_kernel_ptr<true, false, false>();
+    else if (so) fn = sc ? bwd_kernel_ptr<false, true, true>() : bwd_kernel_ptr<false, false, true>();
+    else fn = sc ? bwd_kernel_ptr<false, true, false>() : bwd_kernel_ptr<false, false, false>();
+    const size_t smem = 2 * (size_t)kBwdTP * kPixRecBytes;
+    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    IDIWF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBwdThreads, smem));
+    const int grid = (int)std::min<int64_t>(bp.total_units, (int64_t)sms * std::max(occ, 1));
+    int64_t nrec = L.nrec;
+    void *args[] = {&bp, &e64, &ef, &p64, &pf, &pg, &part, &nrec, &hdr};
+    IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(kBwdThreads), args, smem, stream));
+    {
+        dim3 rgrid((unsigned)std::max<int64_t>(1, (max_blocks * kBwdEB + 255) / 256), batch->n_images);
+        if (nf)
+            bwd_reduce_kernel<true, false><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
+                                                                      batch->amp_dtype, grad_atoms, grad_amp);
+        else if (so)
+            bwd_reduce_kernel<false, true><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
+                                                                      batch->amp_dtype, grad_atoms, grad_amp);
+        else
+            bwd_reduce_kernel<false, false><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
+                                                                       batch->amp_dtype, grad_atoms, grad_amp);
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+    }
+    return IDIWF_OK;
+}

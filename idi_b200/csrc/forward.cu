@@ -1,0 +1,928 @@
+// Forward emitter-wavefield direct sum for sm_100a.
+//
+// Two kernels share one persistent work-queue skeleton:
+//
+//  * fwd_split_kernel (IDIWF_SPLIT) — the throughput kernel.  The phase of
+//    each emitter/pixel pair is formed in FP64 *in turns* with the per-pixel
+//    constant part pre-folded into a magic number, so the last DFMA leaves
+//    the fractional turn as 32-bit fixed point in the low word of the double
+//    (phase mod 2pi for free).  The top 23 bits become an FP32 angle in
+//    [-pi, pi); the near-field second-order term, sincos (MUFU), the 1/r
+//    factor and the field accumulation run in FP32, two pixels per
+//    instruction with Blackwell's packed f32x2 FMA.  Field sums are FP32
+//    partials over 64-emitter blocks folded into Kahan-compensated totals.
+//
+//  * fwd_double_kernel (IDIWF_DOUBLE) — all-FP64, and op-for-op the
+//    rounding sequence of the reference CPU kernel
+//    (idi/simulation/cpu.py:42-107 as numba/LLVM contracts it), so its
+//    fields match the reference to the last bits of sin/cos.
+//
+// Both stage emitter tiles from HBM to shared memory with bulk asynchronous
+// copies (cp.async.bulk, mbarrier completion, double-buffered, bounded
+// waits) and broadcast them to all warps; each thread owns a run of
+// consecutive pixels along a detector row, so loads of the tile are
+// broadcasts and the output stores are contiguous per warp.
+//
+// Work units are (image, pixel tile); a CTA takes units from an atomic
+// counter in the workspace, images ordered by descending emitter count, so
+// one launch balances a batch of images with uneven emitter counts.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "idiwf_internal.cuh"
+
+namespace idiwf {
+
+// ---------------------------------------------------------------------------
+// record layouts
+// ---------------------------------------------------------------------------
+// split:  r64 double4 {x, y, z, psi/2pi - rint}   (32 B)
+//         rA  float4  {x, x, y, y}                (16 B)  duplicated for f32x2
+//         rB  float4  {z, z, w, w}                (16 B)  w = |r|^2 (nf) or x^2+y^2
+//         rC  float2  {a, a}                      ( 8 B)
+// double: r64 double4 {x, y, z, psi}, ra double a
+constexpr int kSplitRecBytes = 72;
+constexpr int kDoubleRecBytes = 40;
+constexpr int kFold = 64;  // emitters per FP32 partial before the Kahan fold
+
+struct SplitRecs {
+    double4 *r64;
+    float4 *rA;
+    float4 *rB;
+    float2 *rC;
+};
+struct DoubleRecs {
+    double4 *r64;
+    double *ra;
+};
+
+static inline SplitRecs split_recs(void *ws, int64_t nrec) {
+    char *base = static_cast<char *>(ws) + kWsDataOffset;
+    SplitRecs r;
+    r.r64 = reinterpret_cast<double4 *>(base);
+    base += align256(nrec * 32);
+    r.rA = reinterpret_cast<float4 *>(base);
+    base += align256(nrec * 16);
+    r.rB = reinterpret_cast<float4 *>(base);
+    base += align256(nrec * 16);
+    r.rC = reinterpret_cast<float2 *>(base);
+    return r;
+}
+static inline size_t split_recs_bytes(int64_t nrec) {
+    return align256(nrec * 32) + 2 * align256(nrec * 16) + align256(nrec * 8);
+}
+static inline DoubleRecs double_recs(void *ws, int64_t nrec) {
+    char *base = static_cast<char *>(ws) + kWsDataOffset;
+    DoubleRecs r;
+    r.r64 = reinterpret_cast<double4 *>(base);
+    base += align256(nrec * 32);
+    r.ra = reinterpret_cast<double *>(base);
+    return r;
+}
+static inline size_t double_recs_bytes(int64_t nrec) {
+    return align256(nrec * 32) + align256(nrec * 8);
+}
+
+// ---------------------------------------------------------------------------
+// prep kernels: caller layout (N,4) f64 [+ amplitudes] -> padded tile records
+// ---------------------------------------------------------------------------
+__global__ void prep_split_kernel(const __grid_constant__ BatchParams bp, const double *__restrict__ atoms,
+                                  const void *__restrict__ amps, int amp_dtype, int w_mode,
+                                  double max_abs, SplitRecs rec, uint32_t *err) {
+    const int b = blockIdx.y;
+    const ImageDesc d = bp.img[b];
+    const int64_t nrec = (int64_t)d.ntiles * bp.te;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nrec;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = d.rec + j;
+        if (j < d.n) {
+            const int64_t s = d.src + j;
+            const double4 a = reinterpret_cast<const double4 *>(atoms)[s];
+            double psi = a.w * kInvTwoPi;
+            psi = psi - rint(psi);
+            float amp = 1.0f;
+            if (amps) amp = amp_dtype == IDIWF_F32 ? static_cast<const float *>(amps)[s]
+                                                  : (float)static_cast<const double *>(amps)[s];
+            if (!(fabs(a.x) <= max_abs && fabs(a.y) <= max_abs && fabs(a.z) <= max_abs))
+                record_error(err, kErrRange);
+            const double w = w_mode == 1 ? (a.x * a.x + a.y * a.y) + a.z * a.z
+                                         : (w_mode == 2 ? a.x * a.x + a.y * a.y : 0.0);
+            const float fx = (float)a.x, fy = (float)a.y, fz = (float)a.z, fw = (float)w;
+            rec.r64[r] = make_double4(a.x, a.y, a.z, psi);
+            rec.rA[r] = make_float4(fx, fx, fy, fy);
+            rec.rB[r] = make_float4(fz, fz, fw, fw);
+            rec.rC[r] = make_float2(amp, amp);
+        } else {
+            rec.r64[r] = make_double4(0, 0, 0, 0);
+            rec.rA[r] = make_float4(0, 0, 0, 0);
+            rec.rB[r] = make_float4(0, 0, 0, 0);
+            rec.rC[r] = make_float2(0, 0);
+        }
+    }
+}
+
+__global__ void prep_double_kernel(const __grid_constant__ BatchParams bp, const double *__restrict__ atoms,
+                                   const void *__restrict__ amps, int amp_dtype, DoubleRecs rec) {
+    const int b = blockIdx.y;
+    const ImageDesc d = bp.img[b];
+    const int64_t nrec = (int64_t)d.ntiles * bp.te;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nrec;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = d.rec + j;
+        if (j < d.n) {
+            const int64_t s = d.src + j;
+            rec.r64[r] = reinterpret_cast<const double4 *>(atoms)[s];
+            double amp = 1.0;
+            if (amps) amp = amp_dtype == IDIWF_F32 ? (double)static_cast<const float *>(amps)[s]
+                                                  : static_cast<const double *>(amps)[s];
+            rec.ra[r] = amp;
+        } else {
+            rec.r64[r] = make_double4(0, 0, 0, 0);
+            rec.ra[r] = 0.0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// output
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void store_pixel(void *out, int out_kind, int64_t idx, double re,
+                                            double im) {
+    switch (out_kind) {
+        case IDIWF_OUT_C128:
+            reinterpret_cast<double2 *>(out)[idx] = make_double2(re, im);
+            break;
+        case IDIWF_OUT_C64:
+            reinterpret_cast<float2 *>(out)[idx] = make_float2((float)re, (float)im);
+            break;
+        case IDIWF_OUT_I64:
+            reinterpret_cast<double *>(out)[idx] = re * re + im * im;
+            break;
+        default:
+            reinterpret_cast<float *>(out)[idx] = (float)(re * re + im * im);
+            break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// split-precision kernel
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+template <int PPT, bool NF, bool SCALE, bool SECOND>
+__global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ BatchParams bp,
+                                                        const GeomParams g, SplitRecs rec,
+                                                        void *__restrict__ out, int out_kind,
+                                                        WsHeader *__restrict__ hdr,
+                                                        uint64_t *__restrict__ cta_ns) {
+    static_assert(PPT % 2 == 0, "pixels are processed in f32x2 pairs");
+    constexpr int PH = PPT / 2;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_unit, s_abort;
+
+    const int tid = threadIdx.x;
+    const int TE = bp.te;
+    const uint32_t stage_bytes = (uint32_t)TE * kSplitRecBytes;
+    const uint64_t t_start = globaltimer_ns();
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        s_abort = 0;
+        mbar_fence_init();
+        if (blockIdx.x == 0) hdr->n_ctas = gridDim.x;
+    }
+    __syncthreads();
+
+    const int npix = g.nx * g.ny;
+    const int tile_px = blockDim.x * PPT;
+    uint32_t issued = 0, consumed = 0;
+    bool aborted = false;
+
+    const float2 TWO_PI2 = f2(6.28318548f, 6.28318548f);
+    const float2 NEG_3PI2 = f2(-9.42477796f, -9.42477796f);
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_unit = (int)atomicAdd(&hdr->work_counter, 1u);
+        __syncthreads();
+        const int unit = s_unit;
+        if (unit >= bp.total_units) break;
+        const int img = bp.order[unit / bp.tiles_per_image];
+        const int ptile = unit % bp.tiles_per_image;
+        const ImageDesc d = bp.img[img];
+        const int p0 = ptile * tile_px + tid * PPT;
+
+        // ---- per-pixel constants (FP64 geometry) ----
+        double cpm[PPT], nqx[PPT], nqy[PPT], nqz[PPT];
+        float2 dhx[PH], dhy[PH], dhz[PH], hh[PH], iD[PH], iD2[PH];
+        float rd[PPT];
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) {
+            const int p = min(p0 + i, npix - 1);
+            const int ix = p / g.ny, iy = p - ix * g.ny;
+            double dx, dy, dz;
+            pixel_cpu(g, ix, iy, dx, dy, dz);
+            const double rho2 = dx * dx + dy * dy;
+            const double D = sqrt(rho2 + dz * dz);
+            const double invD = 1.0 / D;
+            const double dzm1 = dz > 0 ? -rho2 / (D * (D + dz)) : dz * invD - 1.0;
+            nqx[i] = -g.kp * (dx * invD);
+            nqy[i] = -g.kp * (dy * invD);
+            nqz[i] = -g.kp * dzm1;
+            double cp = 0.0;
+            if (NF) {
+                const double dmz = dz > 0 ? rho2 / (D + dz) : D - dz;
+                const double c = g.kp * dmz;
+                cp = c - rint(c);
+            }
+            // +0.5 turn: the FP32 angle is built as 2pi*(u - 1.5), u in [1,2);
+            // +2^-24 turn: rounds (instead of truncating) to the 23 kept bits.
+            cpm[i] = (kTurnMagic + 0.5 + 0x1p-24) + cp;
+            const float fh = (float)(g.k * 0.5 * invD);
+            const float fdx = (float)(dx * invD), fdy = (float)(dy * invD), fdz = (float)(dz * invD);
+            const float fi = (float)invD, fi2 = (float)(invD * invD);
+            rd[i] = fi;
+            if (i & 1) {
+                dhx[i / 2].y = fdx; dhy[i / 2].y = fdy; dhz[i / 2].y = fdz;
+                hh[i / 2].y = fh; iD[i / 2].y = fi; iD2[i / 2].y = fi2;
+            } else {
+                dhx[i / 2].x = fdx; dhy[i / 2].x = fdy; dhz[i / 2].x = fdz;
+                hh[i / 2].x = fh; iD[i / 2].x = fi; iD2[i / 2].x = fi2;
+            }
+        }
+
+        float sre[PPT], cre[PPT], sim[PPT], cim[PPT];
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) sre[i] = cre[i] = sim[i] = cim[i] = 0.0f;
+
+        const int nt = d.ntiles;
+        if (tid == 0) {
+            for (int s = 0; s < 2 && s < nt; ++s) {
+                const uint32_t slot = issued & 1;
+                unsigned char *st = smem + slot * stage_bytes;
+                const int64_t r0 = d.rec + (int64_t)s * TE;
+                mbar_arrive_expect_tx(&bar[slot], stage_bytes);
+                bulk_g2s(st, rec.r64 + r0, TE * 32, &bar[slot]);
+                bulk_g2s(st + TE * 32, rec.rA + r0, TE * 16, &bar[slot]);
+                bulk_g2s(st + TE * 48, rec.rB + r0, TE * 16, &bar[slot]);
+                bulk_g2s(st + TE * 64, rec.rC + r0, TE * 8, &bar[slot]);
+                ++issued;
+            }
+        }
+        for (int it = 0; it < nt; ++it) {
+            const uint32_t slot = consumed & 1;
+            if (!mbar_wait_bounded(&bar[slot], (consumed >> 1) & 1)) {
+                record_error(&hdr->error, kErrTimeout);
+                s_abort = 1;
+            }
+            const unsigned char *st = smem + slot * stage_bytes;
+            const double4 *s64 = reinterpret_cast<const double4 *>(st);
+            const float4 *sA = reinterpret_cast<const float4 *>(st + TE * 32);
+            const float4 *sB = reinterpret_cast<const float4 *>(st + TE * 48);
+            const float2 *sC = reinterpret_cast<const float2 *>(st + TE * 64);
+
+            for (int jb = 0; jb < TE; jb += kFold) {
+                float2 are[PH], aim[PH];
+#pragma unroll
+                for (int q = 0; q < PH; ++q) are[q] = aim[q] = f2(0.f, 0.f);
+#pragma unroll 2
+                for (int j = jb; j < jb + kFold; ++j) {
+                    const double4 r = s64[j];
+                    const float4 A = sA[j];
+                    const float4 B = sB[j];
+                    const float2 a2 = sC[j];
+#pragma unroll
+                    for (int q = 0; q < PH; ++q) {
+                        uint32_t lo[2];
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const int i = 2 * q + e;
+                            double t = __dadd_rn(cpm[i], r.w);
+                            t = __fma_rn(nqx[i], r.x, t);
+                            t = __fma_rn(nqy[i], r.y, t);
+                            t = __fma_rn(nqz[i], r.z, t);
+                            lo[e] = (uint32_t)__double2loint(t);
+                        }
+                        const float2 u = f2(__uint_as_float((lo[0] >> 9) | 0x3F800000u),
+                                            __uint_as_float((lo[1] >> 9) | 0x3F800000u));
+                        float2 arg = __ffma2_rn(u, TWO_PI2, NEG_3PI2);
+                        float2 amp = a2;
+                        if (NF) {
+                            float2 s = __fmul2_rn(dhx[q], f2(A.x, A.y));
+                            s = __ffma2_rn(dhy[q], f2(A.z, A.w), s);
+                            s = __ffma2_rn(dhz[q], f2(B.x, B.y), s);
+                            const float2 w2 = __ffma2_rn(f2(-s.x, -s.y), s, f2(B.z, B.w));
+                            arg = __ffma2_rn(hh[q], w2, arg);
+                            if (SCALE) amp = __fmul2_rn(a2, __ffma2_rn(s, iD2[q], iD[q]));
+                        } else if (SECOND) {
+                            arg = __ffma2_rn(hh[q], f2(B.z, B.w), arg);
+                        }
+                        float s0, c0, s1, c1;
+                        __sincosf(arg.x, &s0, &c0);
+                        __sincosf(arg.y, &s1, &c1);
+                        are[q] = __ffma2_rn(amp, f2(c0, c1), are[q]);
+                        aim[q] = __ffma2_rn(amp, f2(s0, s1), aim[q]);
+                    }
+                }
+                // Kahan fold of the block partials
+#pragma unroll
+                for (int q = 0; q < PH; ++q) {
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int i = 2 * q + e;
+                        const float pr = e ? are[q].y : are[q].x;
+                        const float pi = e ? aim[q].y : aim[q].x;
+                        float y = pr - cre[i];
+                        float t = sre[i] + y;
+                        cre[i] = (t - sre[i]) - y;
+                        sre[i] = t;
+                        y = pi - cim[i];
+                        t = sim[i] + y;
+                        cim[i] = (t - sim[i]) - y;
+                        sim[i] = t;
+                    }
+                }
+            }
+            ++consumed;
+            __syncthreads();
+            if (s_abort) {
+                aborted = true;
+                break;
+            }
+            if (tid == 0 && it + 2 < nt) {
+                const uint32_t slot2 = issued & 1;
+                unsigned char *st2 = smem + slot2 * stage_bytes;
+                const int64_t r0 = d.rec + (int64_t)(it + 2) * TE;
+                mbar_arrive_expect_tx(&bar[slot2], stage_bytes);
+                bulk_g2s(st2, rec.r64 + r0, TE * 32, &bar[slot2]);
+                bulk_g2s(st2 + TE * 32, rec.rA + r0, TE * 16, &bar[slot2]);
+                bulk_g2s(st2 + TE * 48, rec.rB + r0, TE * 16, &bar[slot2]);
+                bulk_g2s(st2 + TE * 64, rec.rC + r0, TE * 8, &bar[slot2]);
+                ++issued;
+            }
+        }
+        if (aborted) break;
+
+        const int64_t obase = (int64_t)img * npix;
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) {
+            const int p = p0 + i;
+            if (p < npix) {
+                double re = (double)sre[i] - (double)cre[i];
+                double im = (double)sim[i] - (double)cim[i];
+                if (!NF && SCALE) {
+                    re *= rd[i];
+                    im *= rd[i];
+                }
+                store_pixel(out, out_kind, obase + p, re, im);
+            }
+        }
+    }
+    if (aborted) {
+        // wait (bounded) for copies still in flight into this CTA's shared memory
+        if (tid == 0)
+            while (consumed < issued) {
+                mbar_wait_bounded(&bar[consumed & 1], (consumed >> 1) & 1);
+                ++consumed;
+            }
+        return;
+    }
+    if (tid == 0) cta_ns[blockIdx.x] = globaltimer_ns() - t_start;
+}
+
+// ---------------------------------------------------------------------------
+// all-FP64 kernel (reference rounding sequence)
+// ---------------------------------------------------------------------------
+template <int PPT, bool NF, bool SCALE, bool SECOND>
+__global__ void __launch_bounds__(256) fwd_double_kernel(const __grid_constant__ BatchParams bp,
+                                                         const GeomParams g, DoubleRecs rec,
+                                                         void *__restrict__ out, int out_kind,
+                                                         WsHeader *__restrict__ hdr,
+                                                         uint64_t *__restrict__ cta_ns) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_unit, s_abort;
+
+    const int tid = threadIdx.x;
+    const int TE = bp.te;
+    const uint32_t stage_bytes = (uint32_t)TE * kDoubleRecBytes;
+    const uint64_t t_start = globaltimer_ns();
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        s_abort = 0;
+        mbar_fence_init();
+        if (blockIdx.x == 0) hdr->n_ctas = gridDim.x;
+    }
+    __syncthreads();
+    const int npix = g.nx * g.ny;
+    const int tile_px = blockDim.x * PPT;
+    uint32_t issued = 0, consumed = 0;
+    bool aborted = false;
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_unit = (int)atomicAdd(&hdr->work_counter, 1u);
+        __syncthreads();
+        const int unit = s_unit;
+        if (unit >= bp.total_units) break;
+        const int img = bp.order[unit / bp.tiles_per_image];
+        const int ptile = unit % bp.tiles_per_image;
+        const ImageDesc d = bp.img[img];
+        const int p0 = ptile * tile_px + tid * PPT;
+
+        double px[PPT], py[PPT], pz[PPT], qx[PPT], qy[PPT], qz[PPT], rdist[PPT], c2[PPT];
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) {
+            const int p = min(p0 + i, npix - 1);
+            const int ix = p / g.ny, iy = p - ix * g.ny;
+            pixel_cpu(g, ix, iy, px[i], py[i], pz[i]);
+            // cpu.py:86-89
+            rdist[i] = __drcp_rn(__dsqrt_rn(
+                __dadd_rn(__dadd_rn(__dmul_rn(px[i], px[i]), __dmul_rn(py[i], py[i])), __dmul_rn(pz[i], pz[i]))));
+            qz[i] = __dmul_rn(g.k, __dsub_rn(__dmul_rn(pz[i], rdist[i]), 1.0));
+            qx[i] = __dmul_rn(g.k, __dmul_rn(px[i], rdist[i]));
+            qy[i] = __dmul_rn(g.k, __dmul_rn(py[i], rdist[i]));
+            c2[i] = __dmul_rn(g.k, rdist[i]) * 0.5;
+        }
+        double ax[PPT], ay[PPT], cx[PPT], cy[PPT];
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) ax[i] = ay[i] = cx[i] = cy[i] = 0.0;
+
+        const int nt = d.ntiles;
+        if (tid == 0) {
+            for (int s = 0; s < 2 && s < nt; ++s) {
+                const uint32_t slot = issued & 1;
+                unsigned char *st = smem + slot * stage_bytes;
+                const int64_t r0 = d.rec + (int64_t)s * TE;
+                mbar_arrive_expect_tx(&bar[slot], stage_bytes);
+                bulk_g2s(st, rec.r64 + r0, TE * 32, &bar[slot]);
+                bulk_g2s(st + TE * 32, rec.ra + r0, TE * 8, &bar[slot]);
+                ++issued;
+            }
+        }
+        for (int it = 0; it < nt; ++it) {
+            const uint32_t slot = consumed & 1;
+            if (!mbar_wait_bounded(&bar[slot], (consumed >> 1) & 1)) {
+                record_error(&hdr->error, kErrTimeout);
+                s_abort = 1;
+            }
+            const unsigned char *st = smem + slot * stage_bytes;
+            const double4 *s64 = reinterpret_cast<const double4 *>(st);
+            const double *sa = reinterpret_cast<const double *>(st + TE * 32);
+            const int jend = min(TE, d.n - it * TE);
+            for (int j = 0; j < jend; ++j) {
+                const double4 r = s64[j];
+                const double aj = sa[j];
+#pragma unroll
+                for (int i = 0; i < PPT; ++i) {
+                    double phase, w = 1.0;
+                    if (NF) {
+                        // cpu.py:44-47 with numba's contraction
+                        const double a = __dsub_rn(px[i], r.x), b = __dsub_rn(py[i], r.y),
+                                     c = __dsub_rn(pz[i], r.z);
+                        const double dist = __dsqrt_rn(__fma_rn(c, c, __fma_rn(a, a, __dmul_rn(b, b))));
+                        phase = __fma_rn(__dadd_rn(__dsub_rn(dist, pz[i]), r.z), g.k, r.w);
+                        if (SCALE) w = __drcp_rn(dist);
+                    } else {
+                        // cpu.py:59
+                        phase = __dadd_rn(-__fma_rn(r.z, qz[i], __fma_rn(r.x, qx[i], __dmul_rn(r.y, qy[i]))), r.w);
+                        if (SECOND)  // sim.cu:88
+                            phase = __dadd_rn(phase, __dmul_rn(c2[i], __dadd_rn(__dmul_rn(r.x, r.x), __dmul_rn(r.y, r.y))));
+                        if (SCALE) w = rdist[i];
+                    }
+                    w = __dmul_rn(w, aj);
+                    double sn, cs;
+                    sincos(phase, &sn, &cs);
+                    const double vx = __dmul_rn(w, cs), vy = __dmul_rn(w, sn);
+                    // Kahan, cpu.py:97-105
+                    const double yx = __dsub_rn(vx, cx[i]), yy = __dsub_rn(vy, cy[i]);
+                    const double tx = __dadd_rn(ax[i], yx), ty = __dadd_rn(ay[i], yy);
+                    cx[i] = __dsub_rn(__dsub_rn(tx, ax[i]), yx);
+                    cy[i] = __dsub_rn(__dsub_rn(ty, ay[i]), yy);
+                    ax[i] = tx;
+                    ay[i] = ty;
+                }
+            }
+            ++consumed;
+            __syncthreads();
+            if (s_abort) {
+                aborted = true;
+                break;
+            }
+            if (tid == 0 && it + 2 < nt) {
+                const uint32_t slot2 = issued & 1;
+                unsigned char *st2 = smem + slot2 * stage_bytes;
+                const int64_t r0 = d.rec + (int64_t)(it + 2) * TE;
+                mbar_arrive_expect_tx(&bar[slot2], stage_bytes);
+                bulk_g2s(st2, rec.r64 + r0, TE * 32, &bar[slot2]);
+                bulk_g2s(st2 + TE * 32, rec.ra + r0, TE * 8, &bar[slot2]);
+                ++issued;
+            }
+        }
+        if (aborted) break;
+        const int64_t obase = (int64_t)img * npix;
+#pragma unroll
+        for (int i = 0; i < PPT; ++i) {
+            const int p = p0 + i;
+            if (p < npix) store_pixel(out, out_kind, obase + p, ax[i], ay[i]);
+        }
+    }
+    if (aborted) {
+        if (tid == 0)
+            while (consumed < issued) {
+                mbar_wait_bounded(&bar[consumed & 1], (consumed >> 1) & 1);
+                ++consumed;
+            }
+        return;
+    }
+    if (tid == 0) cta_ns[blockIdx.x] = globaltimer_ns() - t_start;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+typedef void (*KernelFn)(BatchParams, GeomParams, SplitRecs, void *, int, WsHeader *, uint64_t *);
+
+struct LaunchShape {
+    int threads, ppt, te, ctas_per_sm;
+};
+
+static int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cached[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = n > 0 ? n : 148;
+    }
+    return cached[dev];
+}
+
+GeomParams make_geom(const idiwf_geom *g) {
+    GeomParams p;
+    p.nx = g->nx;
+    p.ny = g->ny;
+    p.flags = g->flags;
+    p.has_rot = g->has_rot;
+    p.pixelsize = g->pixelsize;
+    p.detz = g->detz;
+    p.k = g->k;
+    p.kp = g->k * kInvTwoPi;
+    p.offx = g->offset[0];
+    p.offy = g->offset[1];
+    for (int i = 0; i < 9; ++i) p.rot[i] = g->has_rot ? g->rot[i] : (i % 4 == 0 ? 1.0 : 0.0);
+    return p;
+}
+
+static idiwf_status validate_geom(const idiwf_geom *g) {
+    if (!g) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "geom is NULL");
+    if (g->nx <= 0 || g->ny <= 0)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "detector size must be positive");
+    if ((int64_t)g->nx * g->ny >= (int64_t)1 << 31)
+        return set_error(IDIWF_ERR_UNSUPPORTED, "detector has 2^31 or more pixels");
+    if (!(g->k > 0) || !std::isfinite(g->k))
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "k must be positive and finite");
+    if (!std::isfinite(g->pixelsize) || !std::isfinite(g->detz))
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "pixelsize/detz must be finite");
+    if (g->flags & ~(IDIWF_NF | IDIWF_SCALE | IDIWF_SECONDORDER))
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "unknown geometry flag");
+    return IDIWF_OK;
+}
+
+static idiwf_status validate_batch(const idiwf_batch *b) {
+    if (!b) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "batch is NULL");
+    if (b->n_images <= 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "batch has no images");
+    if (!b->offsets) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "batch offsets are NULL");
+    if (b->offsets[0] != 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "offsets[0] must be 0");
+    for (int i = 0; i < b->n_images; ++i) {
+        const int64_t n = b->offsets[i + 1] - b->offsets[i];
+        if (n < 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
+        if (n >= ((int64_t)1 << 30)) return set_error(IDIWF_ERR_UNSUPPORTED, "image with 2^30 or more emitters");
+    }
+    if (b->offsets[b->n_images] > 0 && !b->atoms)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "atoms pointer is NULL");
+    if (b->atoms && (reinterpret_cast<uintptr_t>(b->atoms) & 31))
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "atoms must be 32-byte aligned");
+    if (b->amplitudes && b->amp_dtype != IDIWF_F64 && b->amp_dtype != IDIWF_F32)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "amp_dtype must be IDIWF_F64 or IDIWF_F32");
+    return IDIWF_OK;
+}
+
+// --- tuned shape cache ------------------------------------------------------
+struct TuneKey {
+    int precision, flags, nx, ny, nbucket;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(precision, flags, nx, ny, nbucket) < std::tie(o.precision, o.flags, o.nx, o.ny, o.nbucket);
+    }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, LaunchShape> g_tune_cache;
+
+static int n_bucket(const idiwf_batch *b) {
+    const double mean = (double)b->offsets[b->n_images] / b->n_images;
+    return mean <= 0 ? 0 : (int)std::floor(std::log2(mean));
+}
+
+static LaunchShape default_shape(int precision) {
+    if (precision == IDIWF_SPLIT) return LaunchShape{256, 8, 256, 1};
+    return LaunchShape{128, 2, 128, 2};
+}
+
+static idiwf_status resolve_shape(const idiwf_geom *g, const idiwf_batch *b, int precision,
+                                  const idiwf_config *cfg, LaunchShape &s) {
+    s = default_shape(precision);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(TuneKey{precision, g->flags, g->nx, g->ny, n_bucket(b)});
+        if (it != g_tune_cache.end()) s = it->second;
+    }
+    if (cfg) {
+        if (cfg->threads) s.threads = cfg->threads;
+        if (cfg->pixels_per_thread) s.ppt = cfg->pixels_per_thread;
+        if (cfg->emitters_per_tile) s.te = cfg->emitters_per_tile;
+        if (cfg->ctas_per_sm) s.ctas_per_sm = cfg->ctas_per_sm;
+    }
+    if (s.threads != 64 && s.threads != 128 && s.threads != 256)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "threads must be 64, 128 or 256");
+    if (precision == IDIWF_SPLIT) {
+        if (s.ppt != 2 && s.ppt != 4 && s.ppt != 8)
+            return set_error(IDIWF_ERR_INVALID_ARGUMENT, "split pixels_per_thread must be 2, 4 or 8");
+        if (s.te < kFold || s.te > 1024 || s.te % kFold)
+            return set_error(IDIWF_ERR_INVALID_ARGUMENT, "split emitters_per_tile must be a multiple of 64 in [64,1024]");
+    } else {
+        if (s.ppt != 1 && s.ppt != 2 && s.ppt != 4)
+            return set_error(IDIWF_ERR_INVALID_ARGUMENT, "double pixels_per_thread must be 1, 2 or 4");
+        if (s.te < 16 || s.te > 1024 || s.te % 16)
+            return set_error(IDIWF_ERR_INVALID_ARGUMENT, "double emitters_per_tile must be a multiple of 16 in [16,1024]");
+    }
+    if (s.ctas_per_sm < 1 || s.ctas_per_sm > 8)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "ctas_per_sm must be in [1,8]");
+    return IDIWF_OK;
+}
+
+static int64_t total_records(const idiwf_batch *b, int te) {
+    int64_t t = 0;
+    for (int i = 0; i < b->n_images; ++i) {
+        const int64_t n = b->offsets[i + 1] - b->offsets[i];
+        t += (n + te - 1) / te * te;
+    }
+    return t;
+}
+
+static size_t forward_ws_bytes(const idiwf_batch *b, int precision, const LaunchShape &s) {
+    const int64_t nrec = std::max<int64_t>(total_records(b, s.te), 1);
+    return kWsDataOffset + (precision == IDIWF_SPLIT ? split_recs_bytes(nrec) : double_recs_bytes(nrec));
+}
+
+// kernel table ---------------------------------------------------------------
+template <int PPT>
+static void *split_kernel_for(int flags) {
+    const bool nf = flags & IDIWF_NF, sc = flags & IDIWF_SCALE, so = flags & IDIWF_SECONDORDER;
+    if (nf) return sc ? (void *)fwd_split_kernel<PPT, true, true, false> : (void *)fwd_split_kernel<PPT, true, false, false>;
+    if (so) return sc ? (void *)fwd_split_kernel<PPT, false, true, true> : (void *)fwd_split_kernel<PPT, false, false, true>;
+    return sc ? (void *)fwd_split_kernel<PPT, false, true, false> : (void *)fwd_split_kernel<PPT, false, false, false>;
+}
+template <int PPT>
+static void *double_kernel_for(int flags) {
+    const bool nf = flags & IDIWF_NF, sc = flags & IDIWF_SCALE, so = flags & IDIWF_SECONDORDER;
+    if (nf) return sc ? (void *)fwd_double_kernel<PPT, true, true, false> : (void *)fwd_double_kernel<PPT, true, false, false>;
+    if (so) return sc ? (void *)fwd_double_kernel<PPT, false, true, true> : (void *)fwd_double_kernel<PPT, false, false, true>;
+    return sc ? (void *)fwd_double_kernel<PPT, false, true, false> : (void *)fwd_double_kernel<PPT, false, false, false>;
+}
+static void *kernel_for(int precision, int ppt, int flags) {
+    if (precision == IDIWF_SPLIT) {
+        if (ppt == 2) return split_kernel_for<2>(flags);
+        if (ppt == 4) return split_kernel_for<4>(flags);
+        return split_kernel_for<8>(flags);
+    }
+    if (ppt == 1) return double_kernel_for<1>(flags);
+    if (ppt == 2) return double_kernel_for<2>(flags);
+    return double_kernel_for<4>(flags);
+}
+
+static idiwf_status ensure_smem(void *fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<void *, int>, size_t> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair(fn, dev);
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return IDIWF_OK;
+    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done[key] = bytes;
+    return IDIWF_OK;
+}
+
+// Launch the forward for images [i0, i1) of the batch (records of the whole
+// batch are laid out by `rec_base`).
+static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, int precision,
+                                 int out_kind, void *out, void *ws, const LaunchShape &s,
+                                 int i0, int i1, const std::vector<int64_t> &rec_base, int64_t nrec,
+                                 cudaStream_t stream) {
+    const GeomParams g = make_geom(geom);
+    const int npix = geom->nx * geom->ny;
+    const int tile_px = s.threads * s.ppt;
+    static thread_local BatchParams bp;  // ~13 KB: keep off the stack
+    std::memset(&bp, 0, sizeof(bp));
+    bp.n_images = i1 - i0;
+    bp.tiles_per_image = (npix + tile_px - 1) / tile_px;
+    bp.te = s.te;
+    bp.total_units = bp.n_images * bp.tiles_per_image;
+    int max_tiles = 0;
+    std::vector<int> ord(bp.n_images);
+    for (int i = 0; i < bp.n_images; ++i) {
+        const int64_t n = b->offsets[i0 + i + 1] - b->offsets[i0 + i];
+        bp.img[i].src = b->offsets[i0 + i];
+        bp.img[i].rec = rec_base[i0 + i];
+        bp.img[i].n = (int32_t)n;
+        bp.img[i].ntiles = (int32_t)((n + s.te - 1) / s.te);
+        max_tiles = std::max(max_tiles, bp.img[i].ntiles);
+        ord[i] = i;
+    }
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int c) { return bp.img[a].n > bp.img[c].n; });
+    for (int i = 0; i < bp.n_images; ++i) bp.order[i] = (uint16_t)ord[i];
+
+    WsHeader *hdr = static_cast<WsHeader *>(ws);
+    uint64_t *cta_ns = reinterpret_cast<uint64_t *>(static_cast<char *>(ws) + kWsTimingOffset);
+    void *out_chunk = static_cast<char *>(out) +
+                      (size_t)i0 * npix * (out_kind == IDIWF_OUT_C128 ? 16 : (out_kind == IDIWF_OUT_I32 ? 4 : 8));
+
+    // prep
+    if (max_tiles > 0) {
+        dim3 pgrid((unsigned)std::min<int64_t>(((int64_t)max_tiles * s.te + 255) / 256, 1024), bp.n_images);
+        if (precision == IDIWF_SPLIT) {
+            const int w_mode = (geom->flags & IDIWF_NF) ? 1 : ((geom->flags & IDIWF_SECONDORDER) ? 2 : 0);
+            // emitter coordinates must keep |q.r| inside the magic binade
+            const double max_abs = kMaxTurns / (3.0 * 2.0 * geom->k * kInvTwoPi);
+            prep_split_kernel<<<pgrid, 256, 0, stream>>>(bp, b->atoms, b->amplitudes, b->amp_dtype, w_mode,
+                                                         max_abs, split_recs(ws, nrec), &hdr->error);
+        } else {
+            prep_double_kernel<<<pgrid, 256, 0, stream>>>(bp, b->atoms, b->amplitudes, b->amp_dtype,
+                                                          double_recs(ws, nrec));
+        }
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+    }
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(&hdr->work_counter, 0, sizeof(uint32_t), stream));
+
+    void *fn = kernel_for(precision, s.ppt, geom->flags);
+    const size_t smem = 2 * (size_t)s.te * (precision == IDIWF_SPLIT ? kSplitRecBytes : kDoubleRecBytes);
+    idiwf_status st = ensure_smem(fn, smem);
+    if (st != IDIWF_OK) return st;
+    const int grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * s.ctas_per_sm), kMaxCtas);
+    if (precision == IDIWF_SPLIT) {
+        SplitRecs rec = split_recs(ws, nrec);
+        void *args[] = {&bp, (void *)&g, &rec, &out_chunk, &out_kind, &hdr, &cta_ns};
+        IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
+    } else {
+        DoubleRecs rec = double_recs(ws, nrec);
+        void *args[] = {&bp, (void *)&g, &rec, &out_chunk, &out_kind, &hdr, &cta_ns};
+        IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
+    }
+    return IDIWF_OK;
+}
+
+static idiwf_status forward_impl(const idiwf_geom *geom, const idiwf_batch *b, int precision,
+                                 int out_kind, void *out, void *ws, size_t ws_bytes,
+                                 const LaunchShape &s, cudaStream_t stream) {
+    const size_t need = forward_ws_bytes(b, precision, s);
+    if (!ws || ws_bytes < need)
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_forward_workspace_size()");
+    if (reinterpret_cast<uintptr_t>(ws) & 255) return set_error(IDIWF_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    std::vector<int64_t> rec_base(b->n_images + 1, 0);
+    for (int i = 0; i < b->n_images; ++i) {
+        const int64_t n = b->offsets[i + 1] - b->offsets[i];
+        rec_base[i + 1] = rec_base[i] + (n + s.te - 1) / s.te * s.te;
+    }
+    const int64_t nrec = std::max<int64_t>(rec_base[b->n_images], 1);
+    // reset the work counter and the error word: errors reported by
+    // idiwf_workspace_error() are those of the most recent call
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(ws, 0, 2 * sizeof(uint32_t), stream));
+    for (int i0 = 0; i0 < b->n_images; i0 += kMaxImagesPerLaunch) {
+        const int i1 = std::min(b->n_images, i0 + kMaxImagesPerLaunch);
+        idiwf_status st = launch_chunk(geom, b, precision, out_kind, out, ws, s, i0, i1, rec_base, nrec, stream);
+        if (st != IDIWF_OK) return st;
+    }
+    return IDIWF_OK;
+}
+
+}  // namespace idiwf
+
+using namespace idiwf;
+
+extern "C" size_t idiwf_forward_workspace_size(const idiwf_geom *geom, const idiwf_batch *batch,
+                                               int32_t precision, const idiwf_config *cfg) {
+    if (validate_geom(geom) != IDIWF_OK || validate_batch(batch) != IDIWF_OK) return 0;
+    if (precision != IDIWF_SPLIT && precision != IDIWF_DOUBLE) return 0;
+    // size for the largest tile any shape may use, so a tuned shape always fits
+    LaunchShape s;
+    if (resolve_shape(geom, batch, precision, cfg, s) != IDIWF_OK) return 0;
+    LaunchShape big = s;
+    big.te = 1024;
+    return std::max(forward_ws_bytes(batch, precision, s), forward_ws_bytes(batch, precision, big));
+}
+
+extern "C" idiwf_status idiwf_forward(const idiwf_geom *geom, const idiwf_batch *batch, int32_t precision,
+                                      int32_t out_kind, void *out, void *workspace, size_t workspace_bytes,
+                                      const idiwf_config *cfg, cudaStream_t stream) {
+    idiwf_status st = validate_geom(geom);
+    if (st != IDIWF_OK) return st;
+    if ((st = validate_batch(batch)) != IDIWF_OK) return st;
+    if (precision != IDIWF_SPLIT && precision != IDIWF_DOUBLE)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "precision must be IDIWF_SPLIT or IDIWF_DOUBLE");
+    if (out_kind < IDIWF_OUT_C128 || out_kind > IDIWF_OUT_I32)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "unknown out_kind");
+    if (!out) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "out is NULL");
+    LaunchShape s;
+    if ((st = resolve_shape(geom, batch, precision, cfg, s)) != IDIWF_OK) return st;
+    return forward_impl(geom, batch, precision, out_kind, out, workspace, workspace_bytes, s, stream);
+}
+
+extern "C" idiwf_status idiwf_forward_cta_times(const void *workspace, uint64_t *host_ns, int32_t cap,
+                                                int32_t *n, cudaStream_t stream) {
+    if (!workspace || !host_ns || !n || cap <= 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "bad arguments");
+    WsHeader h;
+    IDIWF_CUDA_CHECK(cudaMemcpyAsync(&h, workspace, sizeof(h), cudaMemcpyDeviceToHost, stream));
+    IDIWF_CUDA_CHECK(cudaStreamSynchronize(stream));
+    const int cnt = std::min<int>((int)h.n_ctas, std::min(cap, kMaxCtas));
+    if (cnt > 0)
+        IDIWF_CUDA_CHECK(cudaMemcpyAsync(host_ns, static_cast<const char *>(workspace) + kWsTimingOffset,
+                                         sizeof(uint64_t) * cnt, cudaMemcpyDeviceToHost, stream));
+    IDIWF_CUDA_CHECK(cudaStreamSynchronize(stream));
+    *n = cnt;
+    return IDIWF_OK;
+}
+
+extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *batch, int32_t precision,
+                                   int32_t out_kind, void *out, void *workspace, size_t workspace_bytes,
+                                   cudaStream_t stream, idiwf_config *best) {
+    idiwf_status st = validate_geom(geom);
+    if (st != IDIWF_OK) return st;
+    if ((st = validate_batch(batch)) != IDIWF_OK) return st;
+    if (precision != IDIWF_SPLIT && precision != IDIWF_DOUBLE)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "precision must be IDIWF_SPLIT or IDIWF_DOUBLE");
+    std::vector<LaunchShape> cands;
+    if (precision == IDIWF_SPLIT) {
+        for (int th : {128, 256})
+            for (int ppt : {4, 8})
+                for (int te : {128, 256, 512})
+                    for (int c : {1, 2}) cands.push_back(LaunchShape{th, ppt, te, c});
+    } else {
+        for (int th : {128, 256})
+            for (int ppt : {1, 2})
+                for (int te : {64, 128}) cands.push_back(LaunchShape{th, ppt, te, 2});
+    }
+    // Time each shape on the whole batch (the caller sizes the batch it tunes
+    // on; one warm-up + best of two timed runs per shape).
+    cudaEvent_t e0, e1;
+    IDIWF_CUDA_CHECK(cudaEventCreate(&e0));
+    IDIWF_CUDA_CHECK(cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    LaunchShape best_s = default_shape(precision);
+    for (const LaunchShape &s : cands) {
+        if (forward_ws_bytes(batch, precision, s) > workspace_bytes) continue;
+        st = forward_impl(geom, batch, precision, out_kind, out, workspace, workspace_bytes, s, stream);
+        if (st != IDIWF_OK) break;
+        float ms_best = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {
+            cudaEventRecord(e0, stream);
+            st = forward_impl(geom, batch, precision, out_kind, out, workspace, workspace_bytes, s, stream);
+            cudaEventRecord(e1, stream);
+            if (st != IDIWF_OK) break;
+            cudaEventSynchronize(e1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms_best = std::min(ms_best, ms);
+        }
+        if (st != IDIWF_OK) break;
+        if (ms_best < best_ms) {
+            best_ms = ms_best;
+            best_s = s;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != IDIWF_OK) return st;
+    IDIWF_CUDA_CHECK(cudaGetLastError());
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[TuneKey{precision, geom->flags, geom->nx, geom->ny, n_bucket(batch)}] = best_s;
+    }
+    if (best) {
+        best->threads = best_s.threads;
+        best->pixels_per_thread = best_s.ppt;
+        best->emitters_per_tile = best_s.te;
+        best->ctas_per_sm = best_s.ctas_per_sm;
+    }
+    return IDIWF_OK;
+}

@@ -1,0 +1,189 @@
+// Internal declarations shared by the idiwf CUDA sources (sm_100a only).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "idiwf.h"
+
+namespace idiwf {
+
+// ---------------------------------------------------------------------------
+// host-side error state
+// ---------------------------------------------------------------------------
+idiwf_status set_error(idiwf_status st, const std::string &msg);
+idiwf_status cuda_error(cudaError_t e, const char *where);
+
+#define IDIWF_CUDA_CHECK(expr)                                         \
+    do {                                                               \
+        cudaError_t _e = (expr);                                       \
+        if (_e != cudaSuccess) return ::idiwf::cuda_error(_e, #expr);  \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// constants
+// ---------------------------------------------------------------------------
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double kInvTwoPi = 0.15915494309189533576888376337251;
+// Adding 1.5*2^20 to a phase measured in turns puts it in the binade
+// [2^20, 2^21) whose ulp is 2^-32: the low 32 bits of the double are then
+// the fractional turn as an unsigned fixed-point number (phase mod 1).
+constexpr double kTurnMagic = 1572864.0;
+// Largest |phase| in turns the magic binade holds with margin.
+constexpr double kMaxTurns = 262144.0;
+
+// Workspace header (first 256 bytes of every workspace).
+struct WsHeader {
+    uint32_t work_counter;  // persistent-kernel work queue
+    uint32_t error;         // device error word (IDIWF_ERR_* bit set)
+    uint32_t n_ctas;        // CTAs of the last forward launch
+    uint32_t pad0;
+    uint64_t pad[30];
+};
+static_assert(sizeof(WsHeader) == 256, "workspace header is 256 bytes");
+constexpr int kMaxCtas = 4096;                       // per-CTA timing slots
+constexpr size_t kWsTimingOffset = 256;
+constexpr size_t kWsDataOffset = 256 + 8 * kMaxCtas; // 256-aligned
+constexpr uint32_t kErrTimeout = 1u;
+constexpr uint32_t kErrRange = 2u;
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Maximum images per launch (descriptors travel as kernel parameters).
+constexpr int kMaxImagesPerLaunch = 512;
+
+struct GeomParams {
+    int32_t nx, ny, flags, has_rot;
+    double pixelsize, detz, k, kp;  // kp = k / 2pi
+    double offx, offy;
+    double rot[9];
+};
+
+struct ImageDesc {
+    int64_t src;    // first emitter row of the image in the caller's atoms
+    int64_t rec;    // first record of the image in the padded record arrays
+    int32_t n;      // emitters
+    int32_t ntiles; // record tiles (n rounded up to the tile size)
+};
+
+struct BatchParams {
+    int32_t n_images;
+    int32_t tiles_per_image;  // pixel tiles per image
+    int32_t te;               // emitters per tile
+    int32_t total_units;      // n_images * tiles_per_image
+    ImageDesc img[kMaxImagesPerLaunch];
+    uint16_t order[kMaxImagesPerLaunch];  // images by descending emitter count
+};
+
+GeomParams make_geom(const idiwf_geom *g);
+
+// ---------------------------------------------------------------------------
+// device helpers: mbarrier + bulk async copy (TMA, no multicast)
+// ---------------------------------------------------------------------------
+#if defined(__CUDACC__)
+
+// try_wait suspends for a hardware time window per call; this cap bounds a
+// wait to a few seconds, after which the caller records kErrTimeout.
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: true when the phase completed, false when the cap ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    for (uint32_t it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// Global -> shared bulk copy (size and both addresses 16-byte aligned),
+// completion signalled on `bar` as transaction bytes.
+__device__ __forceinline__ void bulk_g2s(void *sdst, const void *gsrc, uint32_t bytes,
+                                         uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(sdst)),
+        "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Detector pixel position, idi/simulation/cpu.py:76-80 rounding sequence
+// (float nx/2, separate multiply and add, numba's contracted mat-vec).
+__device__ __forceinline__ void pixel_cpu(const GeomParams &g, int ix, int iy, double &x,
+                                          double &y, double &z) {
+    const double px = __dadd_rn(__dmul_rn(__dsub_rn((double)ix, g.nx * 0.5), g.pixelsize), g.offx);
+    const double py = __dadd_rn(__dmul_rn(__dsub_rn((double)iy, g.ny * 0.5), g.pixelsize), g.offy);
+    const double pz = g.detz;
+    if (g.has_rot) {
+        const double *M = g.rot;
+        x = __fma_rn(M[2], pz, __fma_rn(M[0], px, __dmul_rn(M[1], py)));
+        y = __fma_rn(M[5], pz, __fma_rn(M[3], px, __dmul_rn(M[4], py)));
+        z = __fma_rn(M[8], pz, __fma_rn(M[6], px, __dmul_rn(M[7], py)));
+    } else {
+        x = px;
+        y = py;
+        z = pz;
+    }
+}
+
+// Detector pixel position, idi/simulation/time.py:77-81 (meshgrid, dets @ M.T
+// as OpenBLAS evaluates it: fma(M[i,2], z, fma(M[i,1], y, M[i,0]*x))).
+__device__ __forceinline__ void pixel_time(const GeomParams &g, int ix, int iy, double &x,
+                                           double &y, double &z) {
+    const double px = __dmul_rn(g.pixelsize, __dsub_rn((double)ix, g.nx * 0.5));
+    const double py = __dmul_rn(g.pixelsize, __dsub_rn((double)iy, g.ny * 0.5));
+    const double pz = g.detz;
+    if (g.has_rot) {
+        const double *M = g.rot;
+        x = __fma_rn(M[2], pz, __fma_rn(M[1], py, __dmul_rn(M[0], px)));
+        y = __fma_rn(M[5], pz, __fma_rn(M[4], py, __dmul_rn(M[3], px)));
+        z = __fma_rn(M[8], pz, __fma_rn(M[7], py, __dmul_rn(M[6], px)));
+    } else {
+        x = px;
+        y = py;
+        z = pz;
+    }
+}
+
+__device__ __forceinline__ void record_error(uint32_t *err, uint32_t bit) { atomicOr(err, bit); }
+
+#endif  // __CUDACC__
+
+}  // namespace idiwf

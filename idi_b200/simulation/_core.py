@@ -1,0 +1,367 @@
+"""Host-side core: geometry, settings, workspaces and the tensor-level calls
+into the CUDA library.  Everything here takes and returns torch tensors on a
+CUDA device; the reference-compatible entry points in :mod:`.cuda`,
+:mod:`.cutime` and :mod:`.autograd` are built on these functions.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import threading
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from .. import _native as nat
+
+__all__ = [
+    "rotation",
+    "parse_settings",
+    "make_geom",
+    "forward",
+    "backward",
+    "time_forward",
+    "time_order",
+    "tune",
+    "microbench",
+    "workspace_error",
+]
+
+
+def rotation(alpha, beta, gamma):
+    """Yaw-pitch-roll rotation matrix, as ``idi/util/__init__.py:348-372``
+    (same expression order, so the detector positions agree bit for bit)."""
+    cosa, cosb, cosg = math.cos(alpha), math.cos(beta), math.cos(gamma)
+    sina, sinb, sing = math.sin(alpha), math.sin(beta), math.sin(gamma)
+    return np.array(
+        [
+            [cosb * cosg, sina * sinb * cosg - cosa * sing, cosa * sinb * cosg + sina * sing],
+            [cosb * sing, sina * sinb * sing + cosa * cosg, cosa * sinb * sing - sina * cosg],
+            [-sinb, sina * cosb, cosa * cosb],
+        ]
+    )
+
+
+def parse_settings(settings: str, default_precision: str = "double"):
+    """Map the reference's ``settings`` substrings (``idi/simulation/cuda.py:51-65``)
+    to (geometry flags, precision, complex64 output).
+
+    ``single`` -> split-precision kernel with complex64 output; ``split`` ->
+    split-precision kernel with complex128 output; ``double`` (or neither) ->
+    all-FP64 kernel.  ``nf``, ``scale``, ``secondorder`` select the geometry.
+    ``nofast`` and unknown substrings are ignored, as in the reference.
+    """
+    s = settings or ""
+    flags = 0
+    if "nf" in s:
+        flags |= nat.NF
+    if "scale" in s:
+        flags |= nat.SCALE
+    if "secondorder" in s:
+        flags |= nat.SECONDORDER
+    if "split" in s:
+        return flags, nat.SPLIT, False
+    if "single" in s:
+        return flags, nat.SPLIT, True
+    if "double" in s:
+        return flags, nat.DOUBLE, False
+    return flags, (nat.SPLIT if default_precision == "split" else nat.DOUBLE), False
+
+
+def ndet_pair(Ndet):
+    if np.size(Ndet) == 1:
+        n = int(np.ravel([Ndet])[0])
+        return [n, n]
+    return [int(Ndet[0]), int(Ndet[1])]
+
+
+def make_geom(Ndet, pixelsize, detz, k, detangles=(0, 0), detoffset=(0, 0), flags=0) -> nat.Geom:
+    nx, ny = ndet_pair(Ndet)
+    g = nat.Geom()
+    g.nx, g.ny = nx, ny
+    g.flags = int(flags)
+    g.pixelsize, g.detz, g.k = float(pixelsize), float(detz), float(k)
+    g.offset[0], g.offset[1] = float(detoffset[0]), float(detoffset[1])
+    if np.any(detangles):
+        M = rotation(float(detangles[0]), float(detangles[1]), 0.0)
+        g.has_rot = 1
+        for i, v in enumerate(M.ravel()):
+            g.rot[i] = float(v)
+    else:
+        g.has_rot = 0
+        for i in range(9):
+            g.rot[i] = 1.0 if i % 4 == 0 else 0.0
+    return g
+
+
+# ---------------------------------------------------------------------------
+# workspaces
+# ---------------------------------------------------------------------------
+class _Workspaces:
+    """One growing uint8 buffer per (device, role); released with :func:`release`."""
+
+    def __init__(self):
+        self._bufs = {}
+        self._lock = threading.Lock()
+
+    def get(self, nbytes: int, device: torch.device, role: str = "main") -> torch.Tensor:
+        key = (device.index if device.index is not None else torch.cuda.current_device(), role)
+        with self._lock:
+            buf = self._bufs.get(key)
+            if buf is None or buf.numel() < nbytes:
+                self._bufs.pop(key, None)
+                buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+                self._bufs[key] = buf
+            return buf
+
+    def drop(self, device: torch.device, role: str):
+        key = (device.index if device.index is not None else torch.cuda.current_device(), role)
+        with self._lock:
+            self._bufs.pop(key, None)
+
+    def release(self):
+        with self._lock:
+            self._bufs.clear()
+
+
+WORKSPACES = _Workspaces()
+
+
+def release():
+    """Free the cached workspaces (the reference's ``idiwf_release``)."""
+    WORKSPACES.release()
+
+
+def _stream(device: torch.device) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _require_cuda(t: torch.Tensor, name: str, dtype=None):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if dtype is not None and t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+def _offsets_array(offsets, n_atoms: int) -> np.ndarray:
+    off = np.ascontiguousarray(np.asarray(offsets, dtype=np.int64))
+    if off.ndim != 1 or off.size < 2 or off[0] != 0 or off[-1] != n_atoms or np.any(np.diff(off) < 0):
+        raise ValueError("offsets must be non-decreasing, start at 0 and end at the emitter count")
+    return off
+
+
+def _batch(atoms: torch.Tensor, off: np.ndarray, amplitudes: Optional[torch.Tensor]) -> nat.Batch:
+    b = nat.Batch()
+    b.n_images = int(off.size - 1)
+    b.offsets = off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    b.atoms = ctypes.c_void_p(atoms.data_ptr() if atoms.numel() else 0)
+    if amplitudes is None:
+        b.amplitudes = None
+        b.amp_dtype = nat.F64
+    else:
+        b.amplitudes = ctypes.c_void_p(amplitudes.data_ptr())
+        b.amp_dtype = nat.F32 if amplitudes.dtype == torch.float32 else nat.F64
+    return b
+
+
+_OUT_DTYPES = {
+    nat.OUT_C128: torch.complex128,
+    nat.OUT_C64: torch.complex64,
+    nat.OUT_I64: torch.float64,
+    nat.OUT_I32: torch.float32,
+}
+
+
+def _config(config) -> Optional[nat.Config]:
+    if config is None:
+        return None
+    if isinstance(config, nat.Config):
+        return config
+    c = nat.Config()
+    c.threads = int(config.get("threads", 0))
+    c.pixels_per_thread = int(config.get("pixels_per_thread", 0))
+    c.emitters_per_tile = int(config.get("emitters_per_tile", 0))
+    c.ctas_per_sm = int(config.get("ctas_per_sm", 0))
+    return c
+
+
+def _check_amplitudes(amplitudes, atoms):
+    if amplitudes is None:
+        return None
+    _require_cuda(amplitudes, "amplitudes")
+    if amplitudes.dtype not in (torch.float32, torch.float64):
+        raise ValueError("amplitudes must be float32 or float64")
+    if amplitudes.numel() != atoms.shape[0]:
+        raise ValueError("amplitudes must have one entry per emitter")
+    return amplitudes
+
+
+def forward(
+    atoms: torch.Tensor,
+    offsets: Sequence[int],
+    geom: nat.Geom,
+    precision: int = nat.SPLIT,
+    out_kind: int = nat.OUT_C128,
+    amplitudes: Optional[torch.Tensor] = None,
+    out: Optional[torch.Tensor] = None,
+    config=None,
+    role: str = "main",
+) -> torch.Tensor:
+    """Direct sum of a batch of images: ``atoms`` (N,4) float64 on the GPU,
+    image b = rows ``offsets[b]:offsets[b+1]``.  Returns (B, nx, ny)."""
+    lib = nat.load()
+    _require_cuda(atoms, "atoms", torch.float64)
+    if atoms.ndim != 2 or atoms.shape[1] != 4:
+        raise ValueError("atoms must have shape (N, 4): x, y, z, phase")
+    amplitudes = _check_amplitudes(amplitudes, atoms)
+    off = _offsets_array(offsets, atoms.shape[0])
+    B = off.size - 1
+    dev = atoms.device
+    if out is None:
+        out = torch.empty((B, geom.nx, geom.ny), dtype=_OUT_DTYPES[out_kind], device=dev)
+    else:
+        _require_cuda(out, "out", _OUT_DTYPES[out_kind])
+        if tuple(out.shape) != (B, geom.nx, geom.ny):
+            raise ValueError("out has the wrong shape")
+    batch = _batch(atoms, off, amplitudes)
+    cfg = _config(config)
+    cfg_p = ctypes.byref(cfg) if cfg is not None else None
+    nbytes = lib.idiwf_forward_workspace_size(ctypes.byref(geom), ctypes.byref(batch), precision, cfg_p)
+    if nbytes == 0:
+        nat.check(nat.ERR_INVALID_ARGUMENT)
+    ws = WORKSPACES.get(nbytes, dev, role)
+    nat.check(lib.idiwf_forward(ctypes.byref(geom), ctypes.byref(batch), precision, out_kind,
+                                ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                                cfg_p, _stream(dev)))
+    return out
+
+
+def tune(atoms, offsets, geom, precision=nat.SPLIT, out_kind=nat.OUT_I32, amplitudes=None, role="main") -> dict:
+    """Autotune the forward kernel shape on this batch (synchronises)."""
+    lib = nat.load()
+    _require_cuda(atoms, "atoms", torch.float64)
+    amplitudes = _check_amplitudes(amplitudes, atoms)
+    off = _offsets_array(offsets, atoms.shape[0])
+    out = torch.empty((off.size - 1, geom.nx, geom.ny), dtype=_OUT_DTYPES[out_kind], device=atoms.device)
+    batch = _batch(atoms, off, amplitudes)
+    nbytes = lib.idiwf_forward_workspace_size(ctypes.byref(geom), ctypes.byref(batch), precision, None)
+    ws = WORKSPACES.get(nbytes, atoms.device, role)
+    best = nat.Config()
+    nat.check(lib.idiwf_tune(ctypes.byref(geom), ctypes.byref(batch), precision, out_kind,
+                             ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                             _stream(atoms.device), ctypes.byref(best)))
+    return {"threads": best.threads, "pixels_per_thread": best.pixels_per_thread,
+            "emitters_per_tile": best.emitters_per_tile, "ctas_per_sm": best.ctas_per_sm}
+
+
+def cta_times(device=None, role="main") -> np.ndarray:
+    """Per-CTA busy time (ns) of the last forward launch on ``device``."""
+    lib = nat.load()
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    ws = WORKSPACES.get(256, dev, role)
+    buf = (ctypes.c_uint64 * 4096)()
+    n = ctypes.c_int32(0)
+    nat.check(lib.idiwf_forward_cta_times(ctypes.c_void_p(ws.data_ptr()), buf, 4096, ctypes.byref(n), _stream(dev)))
+    return np.frombuffer(buf, dtype=np.uint64, count=n.value).copy()
+
+
+def workspace_error(device=None, role="main"):
+    """Raise if a kernel recorded a device-side error in the workspace (synchronises)."""
+    lib = nat.load()
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    ws = WORKSPACES.get(256, dev, role)
+    nat.check(lib.idiwf_workspace_error(ctypes.c_void_p(ws.data_ptr()), _stream(dev)))
+
+
+def backward(
+    atoms: torch.Tensor,
+    offsets: Sequence[int],
+    geom: nat.Geom,
+    field: torch.Tensor,
+    grad_intensity: torch.Tensor,
+    amplitudes: Optional[torch.Tensor] = None,
+    want_amp: bool = True,
+):
+    """Adjoint of I = |E|^2: returns (grad_atoms (N,4) [dx,dy,dz,dphase], grad_amp (N) or None)."""
+    lib = nat.load()
+    _require_cuda(atoms, "atoms", torch.float64)
+    _require_cuda(field, "field", torch.complex128)
+    _require_cuda(grad_intensity, "grad_intensity", torch.float64)
+    amplitudes = _check_amplitudes(amplitudes, atoms)
+    off = _offsets_array(offsets, atoms.shape[0])
+    B = off.size - 1
+    if tuple(field.shape) != (B, geom.nx, geom.ny) or tuple(grad_intensity.shape) != (B, geom.nx, geom.ny):
+        raise ValueError("field and grad_intensity must be (B, nx, ny)")
+    batch = _batch(atoms, off, amplitudes)
+    dev = atoms.device
+    grad_atoms = torch.empty((atoms.shape[0], 4), dtype=torch.float64, device=dev)
+    grad_amp = torch.empty((atoms.shape[0],), dtype=torch.float64, device=dev) if want_amp else None
+    nbytes = lib.idiwf_backward_workspace_size(ctypes.byref(geom), ctypes.byref(batch), None)
+    if nbytes == 0:
+        nat.check(nat.ERR_INVALID_ARGUMENT)
+    ws = WORKSPACES.get(nbytes, dev, "backward")
+    nat.check(lib.idiwf_backward(ctypes.byref(geom), ctypes.byref(batch), ctypes.c_void_p(field.data_ptr()),
+                                 ctypes.c_void_p(grad_intensity.data_ptr()), ctypes.c_void_p(grad_atoms.data_ptr()),
+                                 ctypes.c_void_p(grad_amp.data_ptr()) if grad_amp is not None else None,
+                                 ctypes.c_void_p(ws.data_ptr()), ws.numel(), None, _stream(dev)))
+    return grad_atoms, grad_amp
+
+
+def time_max_emitters() -> int:
+    return int(nat.load().idiwf_time_max_emitters())
+
+
+def time_forward(atoms: torch.Tensor, times: torch.Tensor, geom: nat.Geom, c: float, tau: float,
+                 out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Time-dependent intensity (nx, ny) float64 of one image."""
+    lib = nat.load()
+    _require_cuda(atoms, "atoms", torch.float64)
+    _require_cuda(times, "times", torch.float64)
+    if times.numel() != atoms.shape[0]:
+        raise ValueError("one emission time per emitter")
+    dev = atoms.device
+    if out is None:
+        out = torch.empty((geom.nx, geom.ny), dtype=torch.float64, device=dev)
+    nbytes = lib.idiwf_time_workspace_size(ctypes.byref(geom), atoms.shape[0])
+    ws = WORKSPACES.get(nbytes, dev, "time")
+    nat.check(lib.idiwf_time_forward(ctypes.byref(geom), ctypes.c_void_p(atoms.data_ptr()),
+                                     ctypes.c_void_p(times.data_ptr()), atoms.shape[0], float(c), float(tau),
+                                     ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                                     _stream(dev)))
+    return out
+
+
+def time_order(atoms: torch.Tensor, times: torch.Tensor, geom: nat.Geom, c: float, ix: int, iy: int):
+    """Sorted emitter order and arrival times of pixel (ix, iy), as the time path sorts them."""
+    lib = nat.load()
+    _require_cuda(atoms, "atoms", torch.float64)
+    _require_cuda(times, "times", torch.float64)
+    dev = atoms.device
+    n = atoms.shape[0]
+    order = torch.empty(n, dtype=torch.int32, device=dev)
+    keys = torch.empty(n, dtype=torch.float64, device=dev)
+    nbytes = lib.idiwf_time_workspace_size(ctypes.byref(geom), n)
+    ws = WORKSPACES.get(nbytes, dev, "time")
+    nat.check(lib.idiwf_time_order(ctypes.byref(geom), ctypes.c_void_p(atoms.data_ptr()),
+                                   ctypes.c_void_p(times.data_ptr()), n, float(c), int(ix), int(iy),
+                                   ctypes.c_void_p(order.data_ptr()), ctypes.c_void_p(keys.data_ptr()),
+                                   ctypes.c_void_p(ws.data_ptr()), ws.numel(), _stream(dev)))
+    return order, keys
+
+
+MICROBENCH_KINDS = {"mufu_sincos": 0, "fp64_fma": 1, "fp32_fma": 2, "fp32x2_fma": 3}
+
+
+def microbench(kind: str, device=None) -> float:
+    """Measured pipe throughput: MUFU ops/s, or flop/s for the FMA pipes."""
+    lib = nat.load()
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    scratch = torch.empty(4 << 20, dtype=torch.uint8, device=dev)
+    rate = ctypes.c_double(0)
+    nat.check(lib.idiwf_microbench(MICROBENCH_KINDS[kind], ctypes.c_void_p(scratch.data_ptr()), _stream(dev),
+                                   ctypes.byref(rate)))
+    return rate.value

@@ -1,0 +1,218 @@
+/*
+ * idiwf — B200 (sm_100a) emitter-wavefield direct sum, C ABI.
+ *
+ * The library computes, for every detector pixel p and image b,
+ *     E_bp = sum_j a_j w_pj exp(i phi_pj),   I_bp = |E_bp|^2
+ * over the emitters j of image b, in the geometry and phase conventions of
+ * fzimmermann89/idi (idi/simulation/cpu.py, idi/simulation/sim.cu), plus the
+ * time-dependent variant of idi/simulation/time.py and simtime.cu.
+ *
+ * Conventions shared by every entry point
+ *  - Lengths in the caller's unit (the reference uses micrometres), k in 1/length.
+ *  - Emitters use the reference's (N,4) float64 layout [x, y, z, phase]
+ *    (idi/simulation/cuda.py:85, cpu.py:69), row-major, on the DEVICE.
+ *  - Detector arrays are (nx, ny) row-major, pixel (ix, iy) at
+ *    ((ix - nx/2) * pixelsize + offset[0], (iy - ny/2) * pixelsize + offset[1], detz),
+ *    optionally rotated by rot (idi/simulation/cpu.py:76-80).
+ *  - Every device buffer is allocated by the caller.  Scratch space is a
+ *    caller-provided workspace whose size the *_workspace_size functions report;
+ *    no entry point allocates device or pinned memory.
+ *  - Work is enqueued on `stream` and is asynchronous: no entry point
+ *    synchronises the device, so all of them can be captured in a CUDA graph.
+ *  - Errors are returned as idiwf_status, never by aborting.  Asynchronous
+ *    device-side failures (a bounded wait that ran out) are recorded in the
+ *    workspace and reported by idiwf_workspace_error().
+ *  - The library holds no global mutable state except the autotune cache
+ *    (mutex-protected) and a thread-local last-error string.
+ */
+#ifndef IDIWF_H
+#define IDIWF_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t idiwf_status;
+#define IDIWF_OK 0
+#define IDIWF_ERR_INVALID_ARGUMENT 1
+#define IDIWF_ERR_CUDA 2
+#define IDIWF_ERR_WORKSPACE 3   /* workspace missing, too small or misaligned */
+#define IDIWF_ERR_TIMEOUT 4     /* a bounded device-side wait gave up */
+#define IDIWF_ERR_UNSUPPORTED 5 /* size or mode outside what the kernels implement */
+
+/* geometry flags: the reference's `settings` substrings (cuda.py:51-65) */
+#define IDIWF_NF 1          /* "nf": exact spherical path |d - r| (else far field) */
+#define IDIWF_SCALE 2       /* "scale": 1/r amplitude factor */
+#define IDIWF_SECONDORDER 4 /* "secondorder": Fresnel term of sim.cu:88 (far field) */
+
+/* precision */
+#define IDIWF_DOUBLE 0 /* all-FP64, reproduces the reference CPU rounding sequence */
+#define IDIWF_SPLIT 1  /* FP64 path difference + phase reduction, FP32 sincos/accumulation */
+
+/* output kinds */
+#define IDIWF_OUT_C128 0 /* complex128 field, interleaved (re, im) doubles */
+#define IDIWF_OUT_C64 1  /* complex64 field */
+#define IDIWF_OUT_I64 2  /* float64 intensity |E|^2 */
+#define IDIWF_OUT_I32 3  /* float32 intensity */
+
+/* amplitude / real-array element types */
+#define IDIWF_F64 0
+#define IDIWF_F32 1
+
+typedef struct idiwf_geom {
+    int32_t nx, ny;   /* detector pixels: Ndet[0] (rows), Ndet[1] (columns) */
+    int32_t flags;    /* IDIWF_NF | IDIWF_SCALE | IDIWF_SECONDORDER */
+    int32_t has_rot;  /* nonzero: apply rot to every pixel position */
+    double pixelsize; /* pixel pitch */
+    double detz;      /* detector distance */
+    double k;         /* angular wavenumber 2 pi / lambda */
+    double offset[2]; /* detoffset (x, y) */
+    double rot[9];    /* row-major rotation from detangles (idi/util rotation(theta, phi, 0)) */
+} idiwf_geom;
+
+/* Kernel shape; zero fields select the tuned (or default) value. */
+typedef struct idiwf_config {
+    int32_t threads;            /* threads per CTA (split: 128 or 256) */
+    int32_t pixels_per_thread;  /* split forward: 4 or 8; double forward: 2 */
+    int32_t emitters_per_tile;  /* emitters staged per shared-memory tile: 64..512 */
+    int32_t ctas_per_sm;        /* persistent grid = SMs * ctas_per_sm */
+} idiwf_config;
+
+/* Batch of images with uneven emitter counts.  Image b owns emitter rows
+ * [offsets[b], offsets[b+1]) of `atoms` (and of `amplitudes`). */
+typedef struct idiwf_batch {
+    int32_t n_images;
+    int32_t amp_dtype;        /* IDIWF_F64 or IDIWF_F32; ignored when amplitudes == NULL */
+    const int64_t *offsets;   /* HOST array, n_images + 1 entries, offsets[0] == 0 */
+    const double *atoms;      /* DEVICE (offsets[n_images], 4) float64 [x, y, z, phase] */
+    const void *amplitudes;   /* DEVICE (offsets[n_images]) or NULL for unit amplitudes */
+} idiwf_batch;
+
+/* ------------------------------------------------------------------------ */
+/* forward direct sum                                                        */
+/* ------------------------------------------------------------------------ */
+
+/* Bytes of workspace idiwf_forward needs for this batch (256-byte aligned base). */
+size_t idiwf_forward_workspace_size(const idiwf_geom *geom, const idiwf_batch *batch,
+                                    int32_t precision, const idiwf_config *cfg);
+
+/*
+ * Forward direct sum of every image of `batch` into `out`
+ * ((n_images, nx, ny) of `out_kind`), in one persistent launch whose work
+ * units (image, pixel tile) are taken from an atomic queue in descending
+ * emitter count.
+ *
+ * Replaces the reference kernels wfkernelf / wfkerneld
+ * (idi/simulation/sim.cu:141-149) and their per-image launch loop in
+ * idi/simulation/cuda.py:88-136; IDIWF_DOUBLE follows the FP64 CPU kernel
+ * idi/simulation/cpu.py:68-107.  Amplitudes (per-emitter a_j) and batching
+ * have no reference counterpart.
+ */
+idiwf_status idiwf_forward(const idiwf_geom *geom, const idiwf_batch *batch, int32_t precision,
+                           int32_t out_kind, void *out, void *workspace, size_t workspace_bytes,
+                           const idiwf_config *cfg, cudaStream_t stream);
+
+/* Per-CTA busy time of the last forward launch that used `workspace`
+ * (nanoseconds, DEVICE->host copy + stream sync).  Fills up to `cap` entries,
+ * returns the count in *n.  Used to report load imbalance. */
+idiwf_status idiwf_forward_cta_times(const void *workspace, uint64_t *host_ns, int32_t cap,
+                                     int32_t *n, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* adjoint                                                                   */
+/* ------------------------------------------------------------------------ */
+
+size_t idiwf_backward_workspace_size(const idiwf_geom *geom, const idiwf_batch *batch,
+                                     const idiwf_config *cfg);
+
+/*
+ * Adjoint direct sum (split precision) of I = |E|^2: given the forward field
+ * `field` (complex128, (n_images, nx, ny), from idiwf_forward) and the
+ * upstream gradient `grad_intensity` = dL/dI ((n_images, nx, ny) float64),
+ * writes
+ *   grad_atoms (offsets[n], 4) float64: dL/dx, dL/dy, dL/dz, dL/dphase
+ *   grad_amp   (offsets[n])    float64: dL/da (may be NULL)
+ * No reference counterpart (the reference has no gradients).
+ */
+idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch *batch,
+                            const void *field, const double *grad_intensity, double *grad_atoms,
+                            double *grad_amp, void *workspace, size_t workspace_bytes,
+                            const idiwf_config *cfg, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* time-dependent path                                                       */
+/* ------------------------------------------------------------------------ */
+
+/* Largest emitter count the on-chip per-pixel sort handles. */
+int64_t idiwf_time_max_emitters(void);
+
+size_t idiwf_time_workspace_size(const idiwf_geom *geom, int64_t n);
+
+/*
+ * Time-dependent intensity (FP64): per pixel, arrival times t_j + path/c,
+ * an on-chip sort by arrival time, the decaying coherent scan and the
+ * analytic interval integral; out is (nx, ny) float64.
+ * geom->offset must be zero (the reference time path has no detector offset).
+ * Replaces simulated / simulatef / simulatedf and tempsize*
+ * (idi/simulation/simtime.cu:170-278) driven by idi/simulation/cutime.py:9-139,
+ * with the FP64 CPU semantics of idi/simulation/time.py:48-98.
+ */
+idiwf_status idiwf_time_forward(const idiwf_geom *geom, const double *atoms, const double *times,
+                                int64_t n, double c, double tau, double *out, void *workspace,
+                                size_t workspace_bytes, cudaStream_t stream);
+
+/*
+ * Sorted emitter order of one pixel, as the time path computes it
+ * (order[m] = emitter of the m-th earliest arrival; sorted_keys[m] its
+ * arrival time).  Verification helper for bit-exact ordering; device outputs.
+ * Mirrors the argsort of idi/simulation/time.py:19-29.
+ */
+idiwf_status idiwf_time_order(const idiwf_geom *geom, const double *atoms, const double *times,
+                              int64_t n, double c, int32_t ix, int32_t iy, int32_t *order,
+                              double *sorted_keys, void *workspace, size_t workspace_bytes,
+                              cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* tuning, diagnostics                                                       */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Autotune the forward kernel shape for this geometry/batch/precision: times
+ * each candidate idiwf_config on a subsample of the work with CUDA events and
+ * caches the fastest under a key of (precision, flags, nx, ny, emitter-count
+ * bucket).  Later idiwf_forward calls with cfg == NULL use the cached shape.
+ * Synchronises `stream`.  Writes the chosen shape to *best when non-NULL.
+ */
+idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *batch, int32_t precision,
+                        int32_t out_kind, void *out, void *workspace, size_t workspace_bytes,
+                        cudaStream_t stream, idiwf_config *best);
+
+/* Reads the device error word of `workspace` (synchronises `stream`): the
+ * errors of the most recent call that used this workspace (every call clears
+ * the word when it starts).  Returns IDIWF_OK, IDIWF_ERR_TIMEOUT when a
+ * bounded wait gave up, or IDIWF_ERR_UNSUPPORTED when emitter coordinates
+ * were outside the split-precision phase range. */
+idiwf_status idiwf_workspace_error(const void *workspace, cudaStream_t stream);
+
+/*
+ * Pipe-throughput microbenchmark used to measure the roofline denominators:
+ * kind 0 = MUFU sin+cos (ops/s), 1 = FP64 FMA (flop/s counted as 2 per FMA),
+ * 2 = FP32 FMA, 3 = packed FP32x2 FMA.  Runs on `stream`, synchronises it and
+ * returns the measured rate in *rate.  scratch: DEVICE, >= 4 MiB.
+ */
+idiwf_status idiwf_microbench(int32_t kind, void *scratch, cudaStream_t stream, double *rate);
+
+/* Human-readable description of the last error on the calling thread. */
+const char *idiwf_last_error_string(void);
+
+/* Library version, ABI version in the high 16 bits. */
+int32_t idiwf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IDIWF_H */

@@ -1,0 +1,208 @@
+"""ORACLE — test infrastructure only.
+
+CPU restatement of the reference's emitter-wavefield direct sum (plain C in
+``wavefield_oracle.c``, built into ``liboracle.so`` by ``oracle/Makefile``) with a
+numpy/ctypes front end.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` use it, and only as the checker or as the
+timed CPU baseline; the ``idi_b200`` package never imports it.
+
+Parity of this restatement with the reference itself is pinned by
+``tests/test_oracle.py`` (executes the reference's numba code through
+``oracle/refshim.py`` where the reference tree is present) and by the committed
+fixtures in ``tests/golden/`` (produced by ``tests/golden/make_golden.py`` from
+the reference's own ``cpu.simulate`` / ``time.simulate``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+NF = 1
+SCALE = 2
+SECONDORDER = 4
+ACCURATE = 8
+
+
+class OrcGeom(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32),
+        ("ny", ctypes.c_int32),
+        ("pixelsize", ctypes.c_double),
+        ("detz", ctypes.c_double),
+        ("k", ctypes.c_double),
+        ("offx", ctypes.c_double),
+        ("offy", ctypes.c_double),
+        ("rot", ctypes.c_double * 9),
+        ("has_rot", ctypes.c_int32),
+    ]
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(_HERE, "wavefield_oracle.c")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.POINTER
+        d = ctypes.c_double
+        vp = ctypes.c_void_p
+        L.orc_wavefield.argtypes = [P(OrcGeom), ctypes.c_int, vp, vp, ctypes.c_int64, vp]
+        L.orc_wavefield.restype = None
+        L.orc_adjoint.argtypes = [P(OrcGeom), ctypes.c_int, vp, vp, ctypes.c_int64, vp, vp, vp, vp, vp]
+        L.orc_adjoint.restype = d
+        L.orc_time_image.argtypes = [P(OrcGeom), ctypes.c_int, vp, vp, ctypes.c_int64, d, d, vp]
+        L.orc_time_image.restype = None
+        L.orc_time_order.argtypes = [P(OrcGeom), ctypes.c_int, vp, vp, ctypes.c_int64, d,
+                                     ctypes.c_int, ctypes.c_int, vp]
+        L.orc_time_order.restype = None
+        L.orc_time_keys.argtypes = [P(OrcGeom), ctypes.c_int, vp, vp, ctypes.c_int64, d,
+                                    ctypes.c_int, ctypes.c_int, vp, vp, vp]
+        L.orc_time_keys.restype = None
+        _lib = L
+    return _lib
+
+
+def rotation(alpha, beta, gamma):
+    """Restatement of ``idi/util/__init__.py:348-372`` (yaw-pitch-roll matrix)."""
+    cosa, cosb, cosg = math.cos(alpha), math.cos(beta), math.cos(gamma)
+    sina, sinb, sing = math.sin(alpha), math.sin(beta), math.sin(gamma)
+    return np.array(
+        [
+            [cosb * cosg, sina * sinb * cosg - cosa * sing, cosa * sinb * cosg + sina * sing],
+            [cosb * sing, sina * sinb * sing + cosa * cosg, cosa * sinb * sing - sina * cosg],
+            [-sinb, sina * cosb, cosa * cosb],
+        ]
+    )
+
+
+def flags_from_settings(settings: str) -> int:
+    f = 0
+    if "nf" in settings:
+        f |= NF
+    if "scale" in settings:
+        f |= SCALE
+    if "secondorder" in settings:
+        f |= SECONDORDER
+    return f
+
+
+def geometry(Ndet, pixelsize, detz, k, detangles=(0, 0), detoffset=(0, 0)) -> OrcGeom:
+    if np.size(Ndet) == 1:
+        Ndet = [int(np.ravel([Ndet])[0])] * 2
+    g = OrcGeom()
+    g.nx, g.ny = int(Ndet[0]), int(Ndet[1])
+    g.pixelsize, g.detz, g.k = float(pixelsize), float(detz), float(k)
+    g.offx, g.offy = float(detoffset[0]), float(detoffset[1])
+    if np.any(detangles):
+        M = rotation(detangles[0], detangles[1], 0)
+        g.has_rot = 1
+    else:
+        M = np.eye(3)
+        g.has_rot = 0
+    for i, v in enumerate(M.ravel()):
+        g.rot[i] = float(v)
+    return g
+
+
+def _c(a, dtype=np.float64):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def wavefield(g: OrcGeom, flags: int, atoms, amp=None) -> np.ndarray:
+    """One image: complex128 (nx, ny) field, following ``cpu.py:73-107``."""
+    atoms = _c(atoms)
+    assert atoms.ndim == 2 and atoms.shape[1] == 4
+    out = np.empty((g.nx, g.ny), np.complex128)
+    a = None if amp is None else _c(amp)
+    lib().orc_wavefield(ctypes.byref(g), int(flags), atoms.ctypes.data,
+                        None if a is None else a.ctypes.data, atoms.shape[0], out.ctypes.data)
+    return out
+
+
+def adjoint(g: OrcGeom, flags: int, atoms, amp, E, target):
+    """FP64 gradients of L = sum (|E|^2 - target)^2; returns (loss, dpos, dpsi, damp)."""
+    atoms = _c(atoms)
+    n = atoms.shape[0]
+    E = np.ascontiguousarray(E, np.complex128)
+    T = _c(target)
+    a = None if amp is None else _c(amp)
+    gpos = np.zeros((n, 3))
+    gpsi = np.zeros(n)
+    gamp = np.zeros(n)
+    loss = lib().orc_adjoint(ctypes.byref(g), int(flags), atoms.ctypes.data,
+                             None if a is None else a.ctypes.data, n, E.ctypes.data, T.ctypes.data,
+                             gpos.ctypes.data, gpsi.ctypes.data, gamp.ctypes.data)
+    return loss, gpos, gpsi, gamp
+
+
+def time_image(g: OrcGeom, flags: int, atoms, times, c, tau) -> np.ndarray:
+    """Time-dependent intensity (nx, ny), following ``time.py:48-98``."""
+    atoms = _c(atoms)
+    times = _c(times)
+    out = np.empty((g.nx, g.ny), np.float64)
+    lib().orc_time_image(ctypes.byref(g), int(flags), atoms.ctypes.data, times.ctypes.data,
+                         atoms.shape[0], float(c), float(tau), out.ctypes.data)
+    return out
+
+
+def time_order(g: OrcGeom, flags: int, atoms, times, c, ix, iy) -> np.ndarray:
+    atoms = _c(atoms)
+    times = _c(times)
+    order = np.empty(atoms.shape[0], np.int64)
+    lib().orc_time_order(ctypes.byref(g), int(flags), atoms.ctypes.data, times.ctypes.data,
+                         atoms.shape[0], float(c), int(ix), int(iy), order.ctypes.data)
+    return order
+
+
+def time_keys(g: OrcGeom, flags: int, atoms, times, c, ix, iy):
+    atoms = _c(atoms)
+    times = _c(times)
+    n = atoms.shape[0]
+    t = np.empty(n)
+    er = np.empty(n)
+    ei = np.empty(n)
+    lib().orc_time_keys(ctypes.byref(g), int(flags), atoms.ctypes.data, times.ctypes.data, n,
+                        float(c), int(ix), int(iy), t.ctypes.data, er.ctypes.data, ei.ctypes.data)
+    return t, er + 1j * ei
+
+
+def intensity_metrics(I, I_ref, floor=1e-3):
+    """Error statistics used by every parity test and by the bench record.
+
+    Per-pixel relative error is ill-conditioned at speckle minima, so two
+    figures are reported: the max of |dI|/I_ref over pixels with
+    I_ref >= floor * mean(I_ref), and the max of |dI|/mean(I_ref) over all
+    pixels; plus the 50/99/99.99 percentiles of |dI|/I_ref over the masked set.
+    """
+    I = np.asarray(I, np.float64)
+    I_ref = np.asarray(I_ref, np.float64)
+    mean = float(np.mean(I_ref))
+    d = np.abs(I - I_ref)
+    mask = I_ref >= floor * mean
+    rel = d[mask] / I_ref[mask]
+    return {
+        "max_rel_masked": float(rel.max()) if rel.size else 0.0,
+        "max_rel_to_mean": float(d.max() / mean) if mean > 0 else float(d.max()),
+        "p50": float(np.percentile(rel, 50)) if rel.size else 0.0,
+        "p99": float(np.percentile(rel, 99)) if rel.size else 0.0,
+        "p9999": float(np.percentile(rel, 99.99)) if rel.size else 0.0,
+        "masked_fraction": float(mask.mean()),
+        "floor": floor,
+    }

@@ -1,0 +1,49 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built CUDA library")
+
+
+def pytest_collection_modifyitems(config, items):
+    try:
+        import torch
+
+        has_gpu = torch.cuda.is_available()
+    except Exception:  # pragma: no cover
+        has_gpu = False
+    if has_gpu:
+        return
+    skip = pytest.mark.skip(reason="no CUDA GPU")
+    for item in items:
+        if "gpu" in item.keywords:
+            item.add_marker(skip)
+
+
+@pytest.fixture(scope="session")
+def golden_forward():
+    return np.load(os.path.join(GOLDEN, "forward_ref.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_time():
+    return np.load(os.path.join(GOLDEN, "time_ref.npz"))
+
+
+@pytest.fixture(scope="session")
+def reference():
+    from oracle import refshim
+
+    if not refshim.available():
+        pytest.skip("reference tree not available")
+    return refshim.load()

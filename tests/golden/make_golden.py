@@ -1,0 +1,122 @@
+"""Generate the golden fixtures in this directory from the reference itself.
+
+    python tests/golden/make_golden.py
+
+Runs the reference's own CPU implementations -- ``idi/simulation/cpu.py``
+``simulate`` and ``idi/simulation/time.py`` ``simulate`` -- unmodified, through
+``oracle/refshim.py``, on seeded inputs (numpy Philox), and stores inputs and
+outputs.  For the time path it also records, per pixel, the arrival-time keys
+the reference computes and the order its ``_psort`` puts them in, by wrapping
+the module's ``_integral`` (the reference calls it once per pixel block with
+the keys; the wrapper copies them before and after the in-place sort and then
+calls the original).
+
+Needs the reference tree (``IDI_REFERENCE``, default /root/reference).
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import refshim  # noqa: E402
+
+E_EV = 6400.0
+K = 2 * np.pi / (1.24 / E_EV)
+
+FWD_CASES = [
+    # name, settings, Ndet, pixelsize, detz, detangles, detoffset
+    ("ff", "", (24, 16), 75.0, 1e5, (0, 0), (0, 0)),
+    ("nf", "nf", (24, 16), 75.0, 1e5, (0, 0), (0, 0)),
+    ("ff_scale", "scale", (24, 16), 75.0, 1e5, (0, 0), (0, 0)),
+    ("nf_scale", "nf scale", (24, 16), 75.0, 1e5, (0, 0), (0, 0)),
+    ("nf_rot_off", "nf", (17, 12), 60.5, 8e4, (0.1, 0.2), (30.0, -20.0)),
+    ("ff_rot_off", "", (17, 12), 60.5, 8e4, (0.1, 0.2), (30.0, -20.0)),
+]
+
+TIME_CASES = [
+    # name, settings, Ndet, pixelsize, detz, detangles, c, tau, pulsewidth
+    ("time_ff", "", (4, 4), 75.0, 1e5, (0, 0), 0.3, 2.0, 5.0),
+    ("time_ff_scale_rot", "scale", (4, 4), 75.0, 1e5, (0.05, 0.1), 0.3, 2.0, 5.0),
+]
+
+
+def sphere(rng, n, r):
+    t = rng.uniform(-1, 1, n)
+    p = rng.uniform(0, 2 * np.pi, n)
+    u = r * rng.uniform(0, 1, n) ** (1 / 3)
+    s = np.sqrt(1 - t ** 2)
+    return np.stack([u * t, u * s * np.sin(p), u * s * np.cos(p)], -1)
+
+
+def make_forward(ref):
+    out = {}
+    for i, (name, settings, ndet, ps, dz, ang, off) in enumerate(FWD_CASES):
+        rng = np.random.Generator(np.random.Philox(1000 + i))
+        n = 400
+        pos = sphere(rng, n, 0.01)
+        ph = rng.uniform(0, 2 * np.pi, (2, n))
+        obj = refshim.InjectedObject(E_EV, pos, ph)
+        res = ref.cpu.simulate(2, obj, list(ndet), ps, dz, K, settings=settings, detangles=ang, detoffset=off)
+        out[f"{name}__pos"] = pos
+        out[f"{name}__phases"] = ph
+        out[f"{name}__field"] = res
+        out[f"{name}__meta"] = np.array([ndet[0], ndet[1], ps, dz, ang[0], ang[1], off[0], off[1], K])
+        out[f"{name}__settings"] = np.array(settings)
+    return out
+
+
+def make_time(ref):
+    out = {}
+    tmod = ref.time
+    for i, (name, settings, ndet, ps, dz, ang, c, tau, pw) in enumerate(TIME_CASES):
+        rng = np.random.Generator(np.random.Philox(2000 + i))
+        n = 200
+        pos = sphere(rng, n, 0.01)
+        ph = rng.uniform(0, 2 * np.pi, (1, n))
+        obj = refshim.InjectedObject(E_EV, pos, ph)
+        keys, sorted_keys = [], []
+        orig = tmod._integral
+
+        def spy(amp, t0, tau_):
+            t2 = np.atleast_2d(t0)
+            keys.append(t2.copy())
+            r = orig(amp, t0, tau_)
+            sorted_keys.append(np.atleast_2d(t0).copy())
+            return r
+
+        tmod._integral = spy
+        try:
+            np.random.seed(3000 + i)  # the reference draws emission times from the global RNG
+            img = tmod.simulate(obj, list(ndet), ps, dz, K, c, tau, pw, detangles=ang, settings=settings)
+        finally:
+            tmod._integral = orig
+        np.random.seed(3000 + i)
+        times = np.random.randn(n) * (pw / 2.35)
+        out[f"{name}__pos"] = pos
+        out[f"{name}__phases"] = ph
+        out[f"{name}__times"] = times
+        out[f"{name}__image"] = img
+        out[f"{name}__keys"] = np.concatenate(keys, 0)          # (npix, n) unsorted, emitter order
+        out[f"{name}__sorted_keys"] = np.concatenate(sorted_keys, 0)
+        out[f"{name}__meta"] = np.array([ndet[0], ndet[1], ps, dz, ang[0], ang[1], c, tau, pw, K])
+        out[f"{name}__settings"] = np.array(settings)
+    return out
+
+
+def main():
+    if not refshim.available():
+        raise SystemExit("reference tree not available")
+    ref = refshim.load()
+    np.savez_compressed(os.path.join(HERE, "forward_ref.npz"), **make_forward(ref))
+    np.savez_compressed(os.path.join(HERE, "time_ref.npz"), **make_time(ref))
+    print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
+
+
+if __name__ == "__main__":
+    main()

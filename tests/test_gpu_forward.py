@@ -1,0 +1,205 @@
+"""Forward direct sum on the GPU against the reference (golden fixtures made
+by the reference's own cpu.simulate) and against the oracle."""
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from idi_b200 import _native as nat
+from idi_b200.simulation import _core, cuda, simobj
+from tests.helpers import E_EV, K64, atoms, rel_field_err, rng, sphere
+
+pytestmark = pytest.mark.gpu
+
+# split precision: <= 1e-4 relative intensity over pixels with I >= 1e-3 <I>,
+# and the field error relative to the rms field
+SPLIT_REL_MASKED = 1e-4
+SPLIT_FIELD = 2e-5
+# FP64 mode: <= 1e-5 relative intensity per pixel (it reproduces the
+# reference's rounding; sin/cos differ by at most an ulp)
+DOUBLE_REL = 1e-5
+
+
+def _gpu(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _run(at, offsets, geom, precision, out_kind=nat.OUT_C128, amps=None, config=None):
+    E = _core.forward(_gpu(at), offsets, geom, precision, out_kind,
+                      amplitudes=None if amps is None else _gpu(amps), config=config)
+    torch.cuda.synchronize()
+    _core.workspace_error()
+    return E.cpu().numpy()
+
+
+def _golden_cases(golden_forward):
+    names = sorted({k.split("__")[0] for k in golden_forward.files})
+    for name in names:
+        nx, ny, ps, dz, a0, a1, o0, o1, k = golden_forward[f"{name}__meta"]
+        settings = str(golden_forward[f"{name}__settings"])
+        flags, _, _ = _core.parse_settings(settings)
+        geom = _core.make_geom([int(nx), int(ny)], ps, dz, k, (a0, a1), (o0, o1), flags)
+        pos = golden_forward[f"{name}__pos"]
+        ph = golden_forward[f"{name}__phases"]
+        at = np.concatenate([atoms(pos, p) for p in ph])
+        offsets = np.arange(ph.shape[0] + 1) * pos.shape[0]
+        yield name, geom, at, offsets, golden_forward[f"{name}__field"]
+
+
+def test_double_matches_reference_golden(golden_forward):
+    for name, geom, at, off, ref in _golden_cases(golden_forward):
+        E = _run(at, off, geom, nat.DOUBLE)
+        assert rel_field_err(E, ref) < 1e-12, name
+        m = oracle.intensity_metrics(np.abs(E) ** 2, np.abs(ref) ** 2, floor=0.0)
+        assert m["max_rel_masked"] < DOUBLE_REL, (name, m)
+
+
+def test_split_matches_reference_golden(golden_forward):
+    for name, geom, at, off, ref in _golden_cases(golden_forward):
+        E = _run(at, off, geom, nat.SPLIT)
+        assert rel_field_err(E, ref) < SPLIT_FIELD, name
+        m = oracle.intensity_metrics(np.abs(E) ** 2, np.abs(ref) ** 2)
+        assert m["max_rel_masked"] < SPLIT_REL_MASKED, (name, m)
+
+
+@pytest.mark.parametrize("settings", ["", "nf", "scale", "nf scale", "secondorder", "secondorder scale"])
+@pytest.mark.parametrize("precision", [nat.DOUBLE, nat.SPLIT])
+def test_modes_amplitudes_vs_oracle(settings, precision):
+    g0 = rng(11)
+    n = 1500
+    pos = sphere(g0, n, 0.015)
+    ph = g0.uniform(0, 2 * np.pi, n)
+    amp = g0.uniform(0.5, 1.5, n).astype(np.float32)
+    flags, _, _ = _core.parse_settings(settings)
+    geom = _core.make_geom([33, 20], 75.0, 1e5, K64, (0.02, -0.03), (40.0, 10.0), flags)
+    ref = oracle.wavefield(oracle.geometry([33, 20], 75.0, 1e5, K64, (0.02, -0.03), (40.0, 10.0)),
+                           oracle.flags_from_settings(settings), atoms(pos, ph), amp.astype(np.float64))
+    E = _run(atoms(pos, ph), [0, n], geom, precision, amps=amp)[0]
+    if precision == nat.DOUBLE:
+        assert rel_field_err(E, ref) < 1e-12
+    else:
+        assert rel_field_err(E, ref) < SPLIT_FIELD
+        m = oracle.intensity_metrics(np.abs(E) ** 2, np.abs(ref) ** 2)
+        assert m["max_rel_masked"] < SPLIT_REL_MASKED, m
+
+
+@pytest.mark.parametrize("precision", [nat.DOUBLE, nat.SPLIT])
+def test_batched_uneven_and_edge_sizes(precision):
+    """Ragged batch incl. an empty image, a single emitter and non-tile sizes;
+    odd detector sizes exercise the pixel tail."""
+    g0 = rng(21)
+    counts = [0, 1, 7, 64, 65, 300, 1000, 2500]
+    imgs = [atoms(sphere(g0, c, 0.01), g0.uniform(0, 2 * np.pi, c)) for c in counts]
+    at = np.concatenate(imgs)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    for ndet in ([13, 7], [1, 1], [5, 129]):
+        geom = _core.make_geom(ndet, 75.0, 1e5, K64, flags=nat.NF)
+        og = oracle.geometry(ndet, 75.0, 1e5, K64)
+        E = _run(at, off, geom, precision)
+        assert E.shape == (len(counts), ndet[0], ndet[1])
+        for b, a in enumerate(imgs):
+            ref = oracle.wavefield(og, oracle.NF, a) if len(a) else np.zeros((ndet[0], ndet[1]), complex)
+            if len(a) == 0:
+                assert np.all(E[b] == 0)
+                continue
+            tol = 1e-12 if precision == nat.DOUBLE else 1e-5
+            assert np.abs(E[b] - ref).max() <= tol * max(np.sqrt(len(a)), 1.0), (ndet, counts[b])
+
+
+def test_output_kinds():
+    g0 = rng(5)
+    n = 700
+    at = atoms(sphere(g0, n, 0.01), g0.uniform(0, 2 * np.pi, n))
+    geom = _core.make_geom([40, 24], 75.0, 1e5, K64, flags=nat.NF)
+    E = _run(at, [0, n], geom, nat.SPLIT, nat.OUT_C128)[0]
+    E64 = _run(at, [0, n], geom, nat.SPLIT, nat.OUT_C64)[0]
+    I64 = _run(at, [0, n], geom, nat.SPLIT, nat.OUT_I64)[0]
+    I32 = _run(at, [0, n], geom, nat.SPLIT, nat.OUT_I32)[0]
+    assert E64.dtype == np.complex64 and I32.dtype == np.float32
+    assert np.allclose(E64, E, rtol=0, atol=1e-5 * np.abs(E).max())
+    assert np.allclose(I64, np.abs(E) ** 2, rtol=1e-12)
+    assert np.allclose(I32, np.abs(E) ** 2, rtol=1e-6)
+
+
+def test_kernel_shapes_agree():
+    """Every tile/thread shape gives identical sums (the summation order per
+    pixel does not depend on the shape)."""
+    g0 = rng(8)
+    n = 2100
+    at = atoms(sphere(g0, n, 0.012), g0.uniform(0, 2 * np.pi, n))
+    geom = _core.make_geom([37, 29], 75.0, 1e5, K64, flags=nat.NF)
+    base = _run(at, [0, n], geom, nat.SPLIT)
+    for cfg in ({"threads": 128, "pixels_per_thread": 4, "emitters_per_tile": 128},
+                {"threads": 256, "pixels_per_thread": 2, "emitters_per_tile": 512, "ctas_per_sm": 2},
+                {"threads": 64, "pixels_per_thread": 8, "emitters_per_tile": 64}):
+        assert np.array_equal(_run(at, [0, n], geom, nat.SPLIT, config=cfg), base), cfg
+    dbase = _run(at, [0, n], geom, nat.DOUBLE)
+    for cfg in ({"threads": 256, "pixels_per_thread": 1, "emitters_per_tile": 64},
+                {"threads": 64, "pixels_per_thread": 4, "emitters_per_tile": 32}):
+        assert np.array_equal(_run(at, [0, n], geom, nat.DOUBLE, config=cfg), dbase), cfg
+
+
+def test_split_accuracy_against_accurate_fp64():
+    """Split precision against the cancellation-free FP64 oracle (error floor
+    ~1e-9 rad), on a window of the 8 keV, 0.2 m, 50 um precision geometry:
+    50,000 fcc emitters, detector corner (largest angles)."""
+    g0 = rng(99)
+    a = 3.6e-4
+    m = int(np.ceil(0.012 / a))
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    cells = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 1, 3)
+    sites = ((cells + base[None]) * a).reshape(-1, 3) - 0.006
+    pos = sites[g0.choice(len(sites), 50000, replace=False)] + g0.normal(0, 1e-5, (50000, 3))
+    ph = g0.uniform(0, 2 * np.pi, 50000)
+    k8 = 2 * np.pi / (1.24 / 8000.0)
+    off = (448 * 50.0, 448 * 50.0)
+    geom = _core.make_geom([64, 64], 50.0, 2e5, k8, (0, 0), off, nat.NF)
+    truth = oracle.wavefield(oracle.geometry([64, 64], 50.0, 2e5, k8, (0, 0), off), oracle.NF | oracle.ACCURATE,
+                             atoms(pos, ph))
+    E = _run(atoms(pos, ph), [0, 50000], geom, nat.SPLIT)[0]
+    m_split = oracle.intensity_metrics(np.abs(E) ** 2, np.abs(truth) ** 2)
+    assert m_split["max_rel_masked"] < SPLIT_REL_MASKED, m_split
+    assert m_split["max_rel_to_mean"] < 1e-5, m_split
+
+
+def test_reference_api_shapes():
+    """Mirrors the reference's tests/test_sim.py:124-135 (cuda.simulate shape)."""
+    obj = simobj.sphere(100, 100, 10, rng=np.random.default_rng(0))
+    res = cuda.simulate(2, obj, 4, 10, 1000, obj.k, verbose=False)
+    assert res.shape == (2, 4, 4) and res.dtype == np.complex128
+    gen = cuda.simulate_gen(obj, [4, 6], 10, 1000, obj.k, settings="single", maximg=3)
+    imgs = list(gen)
+    assert len(imgs) == 3 and imgs[0].shape == (4, 6) and imgs[0].dtype == np.complex64
+    g = cuda.simulate(2, obj, 8, 10, 1000, settings="nf split", returngpu=True, verbose=False)
+    assert isinstance(g, torch.Tensor) and g.is_cuda and tuple(g.shape) == (2, 8, 8)
+
+
+def test_simulate_matches_reference_simulate(reference):
+    """The drop-in simulate() against the reference's cpu.simulate on the same
+    injected simobject sequence (two images, near field)."""
+    from oracle import refshim
+
+    g0 = rng(31)
+    n = 600
+    pos = sphere(g0, n, 0.01)
+    ph = g0.uniform(0, 2 * np.pi, (2, n))
+    ref = reference.cpu.simulate(2, refshim.InjectedObject(E_EV, pos, ph), 20, 75.0, 1e5, K64, settings="nf")
+    ours = cuda.simulate(2, refshim.InjectedObject(E_EV, pos, ph), 20, 75.0, 1e5, K64, settings="nf double",
+                         verbose=False)
+    assert rel_field_err(ours, ref) < 1e-12
+
+
+def test_range_check_reports_error():
+    """Emitters too far out for the split phase range are reported, not wrapped."""
+    at = np.zeros((4, 4))
+    at[0, 0] = 1e4
+    geom = _core.make_geom([8, 8], 75.0, 1e5, K64)
+    _core.forward(_gpu(at), [0, 4], geom, nat.SPLIT)
+    with pytest.raises(nat.IdiwfError) as ei:
+        _core.workspace_error()
+    assert ei.value.status == nat.ERR_UNSUPPORTED
+    # the next call clears the error word
+    at[0, 0] = 0.0
+    _core.forward(_gpu(at), [0, 4], geom, nat.SPLIT)
+    _core.workspace_error()
