@@ -1,0 +1,425 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the emitter-wavefield direct sum on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the precision configuration of the direct sum): 50,000 emitters on
+an fcc lattice (a = 0.36 nm) filling a 12 nm cube with 0.01 nm Gaussian
+jitter, uniform phases, 8.0 keV, 1024 x 1024 detector with 50 um pixels at
+0.2 m, 32 images with independent phase draws, near-field geometry, split
+precision.  Inputs are synthetic (seeded Philox).  One step = one batched
+forward of the 32 images (1.68e12 emitter-pixel pairs).
+
+The JSON line carries the headline value (pairs/s with inputs resident in
+HBM), the end-to-end figure through the public API (host emitters in, host
+fields out), the forward+adjoint cost on the differentiation configuration,
+the all-FP64 comparator, split-vs-FP64 error statistics, the MUFU roofline
+and the CPU baseline (the oracle's C restatement on the host cores).
+
+Multi-GPU (torchrun): images are independent, so every rank runs its own 32
+images (weak scaling) with no data-path collective; timing is the max over
+ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+E_EV = 8000.0
+NDET = 1024
+PIXEL = 50.0
+DETZ = 2e5
+N_EMIT = 50000
+N_IMG = 32
+SETTINGS = "nf split"
+WORKLOAD = "fcc 50k emitters, 12 nm cube, 8 keV, 1024x1024 @ 50 um, 0.2 m, 32 images, near field, split precision"
+
+
+def k_of(E):
+    return 2 * np.pi / (1.24 / E)
+
+
+def fcc_emitters(seed=1):
+    g = np.random.Generator(np.random.Philox(seed))
+    a = 3.6e-4
+    m = int(np.ceil(0.012 / a))
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    cells = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 1, 3)
+    sites = ((cells + base[None]) * a).reshape(-1, 3)
+    sites = sites[np.all(sites < 0.012, axis=1)] - 0.006
+    pos = sites[g.choice(len(sites), N_EMIT, replace=False)] + g.normal(0, 1e-5, (N_EMIT, 3))
+    return pos
+
+
+def phases(seed, n_img=N_IMG):
+    g = np.random.Generator(np.random.Philox(seed))
+    return g.uniform(0, 2 * np.pi, (n_img, N_EMIT))
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (the oracle's C restatement, all host cores)
+# ---------------------------------------------------------------------------
+def cpu_baseline(pos, ph, rows_target_s=12.0):
+    import oracle
+
+    k = k_of(E_EV)
+    at = np.ascontiguousarray(np.concatenate([pos, ph[0][:, None]], 1))
+    # calibrate on 2 detector rows, then size the sample to ~rows_target_s
+    def run(rows):
+        g = oracle.geometry([rows, NDET], PIXEL, DETZ, k, (0, 0), ((rows / 2 - NDET / 2) * PIXEL, 0.0))
+        t0 = time.perf_counter()
+        oracle.wavefield(g, oracle.NF, at)
+        return time.perf_counter() - t0
+
+    t_cal = run(2)
+    rows = int(max(2, min(NDET, round(2 * rows_target_s / max(t_cal, 1e-3)))))
+    dt = run(rows)
+    pairs = rows * NDET * N_EMIT
+    return {"value": pairs / dt, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{rows} detector rows x {NDET} px x {N_EMIT} emitters of image 0 "
+                      f"({pairs:.3g} pairs, {dt:.1f} s), FP64 near field, OpenMP over rows"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+
+    pos = fcc_emitters()
+    ph = phases(2, 1)
+    k = k_of(E_EV)
+    at = np.ascontiguousarray(np.concatenate([pos, ph[0][:, None]], 1))
+    rows = 8
+    g = oracle.geometry([rows, NDET], PIXEL, DETZ, k, (0, 0), ((rows / 2 - NDET / 2) * PIXEL, 0.0))
+    for _ in range(args.warmup):
+        oracle.wavefield(g, oracle.NF, at)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.wavefield(g, oracle.NF, at)
+    dt = (time.perf_counter() - t0) / args.steps
+    pairs = rows * NDET * N_EMIT
+    v = pairs / dt
+    line = {
+        "impl": "reference", "metric": "emitter-pixel pairs/s", "value": v, "unit": "pairs/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded Philox)", "config": {"workload": WORKLOAD},
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"per step: {rows} rows x {NDET} px x {N_EMIT} emitters of image 0, "
+                                   "FP64 near field (the oracle's C restatement of idi/simulation/cpu.py)"},
+        "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e/fwd+bwd/fp64/accuracy legs")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    if args.warmup < 3:
+        args.warmup = 3
+
+    import torch
+
+    rank, world, local = dist_init()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from idi_b200 import _native as nat
+    from idi_b200.simulation import _core, cuda, simobj
+
+    k = k_of(E_EV)
+    pos = fcc_emitters()
+    ph = phases(1000 + rank)
+    atoms_h = np.concatenate([np.concatenate([pos, p[:, None]], 1) for p in ph])
+    atoms = torch.from_numpy(np.ascontiguousarray(atoms_h)).to(dev)
+    offsets = np.arange(N_IMG + 1, dtype=np.int64) * N_EMIT
+    flags, precision, _ = _core.parse_settings(SETTINGS)
+    geom = _core.make_geom(NDET, PIXEL, DETZ, k, flags=flags)
+    out = torch.empty((N_IMG, NDET, NDET), dtype=torch.complex128, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    pairs_per_step = N_IMG * N_EMIT * NDET * NDET
+
+    cfg = _core.tune(atoms[: 4 * N_EMIT], offsets[:5], geom, precision, nat.OUT_C128)
+
+    def step():
+        _core.forward(atoms, offsets, geom, precision, nat.OUT_C128, out=out, config=cfg)
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        step()
+    barrier(world)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        barrier(world)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for i in range(args.steps):
+            flush.fill_(1)
+            ev[i][0].record()
+            step()
+            ev[i][1].record()
+        t1.record()
+        barrier(world)
+    total_ms = t0.elapsed_time(t1)
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = max_over_ranks(total_ms, world)
+    _core.workspace_error(dev)
+    ms_per_step = total_ms / args.steps
+    value = pairs_per_step * world / (ms_per_step * 1e-3)
+    kern_avg = sum(kern_ms) / len(kern_ms)
+
+    # MUFU roofline: the split kernel issues one sin and one cos per pair
+    mufu = _core.microbench("mufu_sincos", dev)
+    achieved_mufu = 2.0 * pairs_per_step / (kern_avg * 1e-3)
+    clocks = clk.summary()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    nominal_mufu = sms * 16 * (clocks["sm_max_mhz"] or 1965.0) * 1e6
+
+    line = {
+        "metric": "emitter-pixel pairs/s (split-precision forward)",
+        "value": value,
+        "unit": "pairs/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 phase / f32 sincos+sum",
+        "data": "synthetic (seeded Philox)",
+        "config": {"workload": WORKLOAD, "images": N_IMG, "emitters": N_EMIT, "detector": [NDET, NDET],
+                   "settings": SETTINGS, "parallelism": f"images per rank, {world} rank(s)",
+                   "l2": "flushed between steps (256 MiB write)", "kernel_shape": cfg},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+        "roofline": {"bound": "sfu", "achieved": achieved_mufu / 1e9, "peak": mufu / 1e9, "unit": "Gop/s (MUFU)",
+                     "frac": achieved_mufu / mufu, "frac_of_nominal": achieved_mufu / nominal_mufu,
+                     "peak_source": "measured: in-repo MUFU sin/cos microbenchmark (idiwf_microbench kind 0)",
+                     "ops_per_pair": 2, "kernel_ms": kern_avg, "traffic": None},
+    }
+    if not args.no_extras and rank == 0:
+        line.update(extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, offsets, cfg))
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        try:
+            line["cpu_baseline"] = cpu_baseline(pos, ph)
+        except Exception as e:  # the oracle library may be missing on a stripped box
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, offsets, cfg):
+    res = {}
+    # --- end to end through the public API: host emitters in, host fields out
+    obj = simobj.fixed(E_EV, pos, phases=ph)
+    cuda.simulate(2, obj, NDET, PIXEL, DETZ, k, settings=SETTINGS, verbose=False)  # warm
+    n_e2e = min(args.steps, 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        cuda.simulate(N_IMG, obj, NDET, PIXEL, DETZ, k, settings=SETTINGS, verbose=False)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / n_e2e
+    pairs = N_IMG * N_EMIT * NDET * NDET
+    res["e2e"] = {"value": pairs / dt, "unit": "pairs/s", "h2d_bytes_per_step": N_IMG * N_EMIT * 32,
+                  "d2h_bytes_per_step": N_IMG * NDET * NDET * 16,
+                  "call": "idi_b200.simulation.cuda.simulate(32, simobject, 1024, 50, 2e5, k, settings='nf split')"}
+
+    # --- all-FP64 comparator on 2 images of the same batch
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = 1e30
+        for _ in range(reps):
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b))
+        return best
+
+    at2 = atoms[: 2 * N_EMIT]
+    off2 = offsets[:3]
+    ms64 = timed(lambda: _core.forward(at2, off2, geom, nat.DOUBLE, nat.OUT_C128), reps=2)
+    v64 = 2 * N_EMIT * NDET * NDET / (ms64 * 1e-3)
+    res["fp64"] = {"value": v64, "unit": "pairs/s", "images": 2, "ms": ms64}
+
+    # --- split vs FP64 accuracy on 2 full images
+    Es = _core.forward(at2, off2, geom, nat.SPLIT, nat.OUT_C128, config=cfg)
+    Ed = _core.forward(at2, off2, geom, nat.DOUBLE, nat.OUT_C128)
+    Is = (Es.real ** 2 + Es.imag ** 2).cpu().numpy()
+    Id = (Ed.real ** 2 + Ed.imag ** 2).cpu().numpy()
+    mean = Id.mean()
+    d = np.abs(Is - Id)
+    mask = Id >= 1e-3 * mean
+    rel = d[mask] / Id[mask]
+    hist, edges = np.histogram(np.log10(np.maximum(rel, 1e-12)), bins=np.arange(-12, 0.5, 1.0))
+    res["accuracy_split_vs_fp64"] = {
+        "pixels": int(Id.size), "max_rel_masked": float(rel.max()), "max_rel_to_mean": float(d.max() / mean),
+        "p50": float(np.percentile(rel, 50)), "p99": float(np.percentile(rel, 99)),
+        "p9999": float(np.percentile(rel, 99.99)), "mask": "I_fp64 >= 1e-3 mean",
+        "log10_rel_hist": {f"{int(e)}": int(h) for e, h in zip(edges[:-1], hist)}}
+    del Es, Ed
+
+    # --- forward + adjoint on the differentiation configuration
+    g = np.random.Generator(np.random.Philox(7))
+    n4 = 10000
+    t = g.uniform(-1, 1, n4)
+    p = g.uniform(0, 2 * np.pi, n4)
+    u = 0.015 * g.uniform(0, 1, n4) ** (1 / 3)
+    s = np.sqrt(1 - t ** 2)
+    pos4 = np.stack([u * t, u * s * np.sin(p), u * s * np.cos(p)], -1)
+    ph4 = g.uniform(0, 2 * np.pi, n4)
+    k4 = k_of(6400.0)
+    geom4 = _core.make_geom(512, 75.0, 1e5, k4, flags=nat.NF)
+    a4 = torch.from_numpy(np.concatenate([pos4, ph4[:, None]], 1)).to(dev)
+    T4 = _core.forward(torch.from_numpy(np.concatenate([pos4 + g.normal(0, 5e-5, pos4.shape), ph4[:, None]], 1)).to(dev),
+                       [0, n4], geom4, nat.SPLIT, nat.OUT_I64)
+    off4 = [0, n4]
+
+    def fwd():
+        return _core.forward(a4, off4, geom4, nat.SPLIT, nat.OUT_C128)
+
+    def fwd_bwd():
+        E = fwd()
+        I = E.real ** 2 + E.imag ** 2
+        return _core.backward(a4, off4, geom4, E, (2 * (I - T4)).contiguous())
+
+    ms_f = timed(fwd, reps=5)
+    ms_fb = timed(fwd_bwd, reps=5)
+    pairs4 = n4 * 512 * 512
+    res["fwd_bwd"] = {"workload": "10k emitters, 15 nm sphere, 512x512 @ 75 um, 0.1 m, 6.4 keV, near field",
+                      "fwd_ms": ms_f, "fwd_bwd_ms": ms_fb, "ratio": ms_fb / ms_f,
+                      "fwd_pairs_per_s": pairs4 / (ms_f * 1e-3), "fwd_bwd_pairs_per_s": pairs4 / (ms_fb * 1e-3)}
+    return res
+
+
+if __name__ == "__main__":
+    sys.exit(main())

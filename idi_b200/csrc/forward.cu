@@ -6,8 +6,9 @@
 //    each emitter/pixel pair is formed in FP64 *in turns* with the per-pixel
 //    constant part pre-folded into a magic number, so the last DFMA leaves
 //    the fractional turn as 32-bit fixed point in the low word of the double
-//    (phase mod 2pi for free).  The top 23 bits become an FP32 angle in
-//    [-pi, pi); the near-field second-order term, sincos (MUFU), the 1/r
+//    (phase mod 2pi for free).  Its top bit selects the half turn (folded
+//    into the sign of the amplitude) and the next 23 bits become an FP32
+//    angle in [-pi/2, pi/2); the near-field second-order term, sincos (MUFU), the 1/r
 //    factor and the field accumulation run in FP32, two pixels per
 //    instruction with Blackwell's packed f32x2 FMA.  Field sums are FP32
 //    partials over 64-emitter blocks folded into Kahan-compensated totals.
@@ -205,8 +206,8 @@ __global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ 
     uint32_t issued = 0, consumed = 0;
     bool aborted = false;
 
-    const float2 TWO_PI2 = f2(6.28318548f, 6.28318548f);
-    const float2 NEG_3PI2 = f2(-9.42477796f, -9.42477796f);
+    const float2 PI2 = f2(3.14159274f, 3.14159274f);
+    const float2 NEG_15PI2 = f2(-4.71238898f, -4.71238898f);
 
     for (;;) {
         __syncthreads();
@@ -242,9 +243,11 @@ __global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ 
                 const double c = g.kp * dmz;
                 cp = c - rint(c);
             }
-            // +0.5 turn: the FP32 angle is built as 2pi*(u - 1.5), u in [1,2);
-            // +2^-24 turn: rounds (instead of truncating) to the 23 kept bits.
-            cpm[i] = (kTurnMagic + 0.5 + 0x1p-24) + cp;
+            // +1/4 turn: bit 31 of the fixed-point phase then marks the half
+            // turn centred on pi, and bits 30..8 the angle within it (see the
+            // inner loop); +2^-25 turn rounds (instead of truncating) to the
+            // 23 kept bits.
+            cpm[i] = (kTurnMagic + 0.25 + 0x1p-25) + cp;
             const float fh = (float)(g.k * 0.5 * invD);
             const float fdx = (float)(dx * invD), fdy = (float)(dy * invD), fdz = (float)(dz * invD);
             const float fi = (float)invD, fi2 = (float)(invD * invD);
@@ -310,9 +313,15 @@ __global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ 
                             t = __fma_rn(nqz[i], r.z, t);
                             lo[e] = (uint32_t)__double2loint(t);
                         }
-                        const float2 u = f2(__uint_as_float((lo[0] >> 9) | 0x3F800000u),
-                                            __uint_as_float((lo[1] >> 9) | 0x3F800000u));
-                        float2 arg = __ffma2_rn(u, TWO_PI2, NEG_3PI2);
+                        // phase = n*pi + x, x = pi*(u - 1.5) in [-pi/2, pi/2): u from
+                        // bits 30..8; odd n (bit 31) negates the term, folded into
+                        // the amplitude's sign.  Mapping both halves of the circle
+                        // onto one half and flipping the sign makes the mean error
+                        // of the hardware cosine cancel over the circle instead of
+                        // adding up coherently over emitters.
+                        const float2 u = f2(__uint_as_float(((lo[0] >> 8) & 0x007FFFFFu) | 0x3F800000u),
+                                            __uint_as_float(((lo[1] >> 8) & 0x007FFFFFu) | 0x3F800000u));
+                        float2 arg = __ffma2_rn(u, PI2, NEG_15PI2);
                         float2 amp = a2;
                         if (NF) {
                             float2 s = __fmul2_rn(dhx[q], f2(A.x, A.y));
@@ -324,6 +333,8 @@ __global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ 
                         } else if (SECOND) {
                             arg = __ffma2_rn(hh[q], f2(B.z, B.w), arg);
                         }
+                        amp.x = __uint_as_float(__float_as_uint(amp.x) ^ (lo[0] & 0x80000000u));
+                        amp.y = __uint_as_float(__float_as_uint(amp.y) ^ (lo[1] & 0x80000000u));
                         float s0, c0, s1, c1;
                         __sincosf(arg.x, &s0, &c0);
                         __sincosf(arg.y, &s1, &c1);
