@@ -45,6 +45,7 @@ EXPORTED = (
     "idiwf_forward_workspace_size",
     "idiwf_forward",
     "idiwf_forward_cta_times",
+    "idiwf_forward_noalloc",
     "idiwf_backward_workspace_size",
     "idiwf_backward",
     "idiwf_time_max_emitters",
@@ -124,6 +125,8 @@ def load():
     L.idiwf_forward.argtypes = [P(Geom), P(Batch), ctypes.c_int32, ctypes.c_int32, vp, vp, ctypes.c_size_t,
                                 P(Config), vp]
     L.idiwf_forward.restype = st
+    L.idiwf_forward_noalloc.argtypes = [P(Geom), P(Batch), ctypes.c_int32, vp, vp]
+    L.idiwf_forward_noalloc.restype = st
     L.idiwf_forward_cta_times.argtypes = [vp, P(ctypes.c_uint64), ctypes.c_int32, P(ctypes.c_int32), vp]
     L.idiwf_forward_cta_times.restype = st
     L.idiwf_backward_workspace_size.argtypes = [P(Geom), P(Batch), P(Config)]

@@ -937,3 +937,119 @@ extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *ba
     }
     return IDIWF_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Split-precision forward for callers that cannot allocate device memory.
+//
+// Some hosts of this library cannot call cudaMalloc at all: code that runs
+// inside another framework's memory pool or allocator hooks, inside a stream
+// capture they do not own, or in plug-ins whose host forbids device
+// allocation.  For them this entry point keeps its scratch (work counter,
+// error word, per-CTA timing, emitter tile records) in one file-scope device
+// array of fixed size, so the caller passes only inputs and outputs and
+// nothing is allocated -- neither device memory nor host heap memory.
+// ---------------------------------------------------------------------------
+namespace idiwf {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[IDIWF_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[kNoAllocMaxDevices];
+
+// Device address of the scratch array on the current device.  The name
+// g_noalloc_scratch in host code is only a host-side stand-in, so the
+// address is looked up once per device (with that device current) and
+// cached.
+static idiwf_status noalloc_scratch(void **ptr) {
+    int dev = 0;
+    IDIWF_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return set_error(IDIWF_ERR_UNSUPPORTED, "idiwf_forward_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_ptr[dev] = p;
+    }
+    *ptr = g_noalloc_ptr[dev];
+    return IDIWF_OK;
+}
+
+}  // namespace idiwf
+
+extern "C" idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiwf_batch *batch, int32_t out_kind,
+                                              void *out, cudaStream_t stream) {
+    idiwf_status st = validate_geom(geom);
+    if (st != IDIWF_OK) return st;
+    if ((st = validate_batch(batch)) != IDIWF_OK) return st;
+    if (out_kind < IDIWF_OUT_C128 || out_kind > IDIWF_OUT_I32)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "unknown out_kind");
+    if (!out) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "out is NULL");
+    if (batch->n_images > kMaxImagesPerLaunch)
+        return set_error(IDIWF_ERR_UNSUPPORTED, "idiwf_forward_noalloc: at most 512 images per call");
+
+    const LaunchShape s{256, 4, 256, 2};
+    static thread_local BatchParams bp;
+    std::memset(&bp, 0, sizeof(bp));
+    const int npix = geom->nx * geom->ny;
+    const int tile_px = s.threads * s.ppt;
+    bp.n_images = batch->n_images;
+    bp.tiles_per_image = (npix + tile_px - 1) / tile_px;
+    bp.te = s.te;
+    bp.total_units = bp.n_images * bp.tiles_per_image;
+    int64_t nrec = 0;
+    int max_tiles = 0;
+    for (int i = 0; i < bp.n_images; ++i) {
+        const int64_t n = batch->offsets[i + 1] - batch->offsets[i];
+        bp.img[i].src = batch->offsets[i];
+        bp.img[i].rec = nrec;
+        bp.img[i].n = (int32_t)n;
+        bp.img[i].ntiles = (int32_t)((n + s.te - 1) / s.te);
+        nrec += (int64_t)bp.img[i].ntiles * s.te;
+        max_tiles = std::max(max_tiles, bp.img[i].ntiles);
+    }
+    nrec = std::max<int64_t>(nrec, 1);
+    if (kWsDataOffset + split_recs_bytes(nrec) > (size_t)IDIWF_NOALLOC_SCRATCH_BYTES)
+        return set_error(IDIWF_ERR_UNSUPPORTED,
+                         "idiwf_forward_noalloc: batch needs more than the 16 MiB static scratch "
+                         "(at most 232448 emitters in total after padding every image to a multiple of 256); "
+                         "use idiwf_forward with a caller workspace");
+    // images by descending emitter count (stable insertion sort, no heap)
+    for (int i = 0; i < bp.n_images; ++i) {
+        int j = i;
+        while (j > 0 && bp.img[bp.order[j - 1]].n < bp.img[i].n) {
+            bp.order[j] = bp.order[j - 1];
+            --j;
+        }
+        bp.order[j] = (uint16_t)i;
+    }
+
+    void *ws = nullptr;
+    if ((st = noalloc_scratch(&ws)) != IDIWF_OK) return st;
+    WsHeader *hdr = static_cast<WsHeader *>(ws);
+    uint64_t *cta_ns = reinterpret_cast<uint64_t *>(static_cast<char *>(ws) + kWsTimingOffset);
+    SplitRecs rec = split_recs(ws, nrec);
+    const GeomParams g = make_geom(geom);
+
+    // every call starts from a zero work counter and error word; the records
+    // are rewritten in full by the prep kernel
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(ws, 0, 2 * sizeof(uint32_t), stream));
+    if (max_tiles > 0) {
+        const int w_mode = (geom->flags & IDIWF_NF) ? 1 : ((geom->flags & IDIWF_SECONDORDER) ? 2 : 0);
+        const double max_abs = kMaxTurns / (3.0 * 2.0 * geom->k * kInvTwoPi);
+        dim3 pgrid((unsigned)std::min<int64_t>(((int64_t)max_tiles * s.te + 255) / 256, 1024), bp.n_images);
+        prep_split_kernel<<<pgrid, 256, 0, stream>>>(bp, batch->atoms, batch->amplitudes, batch->amp_dtype, w_mode,
+                                                     max_abs, rec, &hdr->error);
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+    }
+    void *fn = split_kernel_for<4>(geom->flags);
+    const size_t smem = 2 * (size_t)s.te * kSplitRecBytes;
+    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * s.ctas_per_sm),
+                                            kMaxCtas);
+    void *args[] = {&bp, (void *)&g, &rec, &out, &out_kind, &hdr, &cta_ns};
+    IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
+    return IDIWF_OK;
+}

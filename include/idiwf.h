@@ -122,6 +122,33 @@ idiwf_status idiwf_forward(const idiwf_geom *geom, const idiwf_batch *batch, int
 idiwf_status idiwf_forward_cta_times(const void *workspace, uint64_t *host_ns, int32_t cap,
                                      int32_t *n, cudaStream_t stream);
 
+/*
+ * Split-precision forward that allocates nothing: no device memory, no
+ * workspace argument, no host heap.  It has no counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc or hand the library a workspace
+ * (code running inside another framework's memory pool or allocator hooks,
+ * or plug-ins whose host forbids device allocation).  Its scratch is a
+ * static device array of IDIWF_NOALLOC_SCRATCH_BYTES (16 MiB) that every
+ * GPU which loads this library holds until the process exits.
+ *
+ * Limits: at most 512 images per call, and the emitters of all images, each
+ * image padded to a multiple of 256, must fit the scratch at 72 bytes each:
+ * 232,448 emitters in total.  Larger batches are rejected with
+ * IDIWF_ERR_UNSUPPORTED before anything is enqueued.
+ *
+ * The first call on a device looks up the array's device address (with that
+ * device current); make that first call before any stream capture.  All
+ * calls share the one array and it keeps the last call's contents; each call
+ * clears what must start at zero.  Calls whose work overlaps on the GPU
+ * (other streams, other threads, other graph branches) race on the scratch:
+ * serialise them.  Same semantics and results as idiwf_forward with
+ * precision IDIWF_SPLIT; idiwf_workspace_error() does not apply.
+ */
+#define IDIWF_NOALLOC_SCRATCH_BYTES (16u << 20)
+idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiwf_batch *batch, int32_t out_kind,
+                                   void *out, cudaStream_t stream);
+
 /* ------------------------------------------------------------------------ */
 /* adjoint                                                                   */
 /* ------------------------------------------------------------------------ */
