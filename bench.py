@@ -232,7 +232,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e/fwd+bwd/fp64/accuracy legs")
+    ap.add_argument("--case", default="full", choices=["full", "small"],
+                    help="small: 2 images on a 256x256 detector (profiling-sized capture of the same kernel)")
+    ap.add_argument("--no-tune", action="store_true", help="use the default kernel shape instead of autotuning")
+    ap.add_argument("--config", default=None, help='kernel shape as JSON, e.g. {"threads":256,"pixels_per_thread":4}')
     args = ap.parse_args()
+    global N_IMG, NDET
+    global WORKLOAD
+    if args.case == "small":
+        N_IMG, NDET = 2, 256
+        WORKLOAD = WORKLOAD.replace("1024x1024", "256x256").replace("32 images", "2 images")
     if args.impl == "reference":
         return reference_arm(args)
     if args.warmup < 3:
@@ -248,7 +257,7 @@ def main():
 
     k = k_of(E_EV)
     pos = fcc_emitters()
-    ph = phases(1000 + rank)
+    ph = phases(1000 + rank, N_IMG)
     atoms_h = np.concatenate([np.concatenate([pos, p[:, None]], 1) for p in ph])
     atoms = torch.from_numpy(np.ascontiguousarray(atoms_h)).to(dev)
     offsets = np.arange(N_IMG + 1, dtype=np.int64) * N_EMIT
@@ -258,7 +267,13 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
     pairs_per_step = N_IMG * N_EMIT * NDET * NDET
 
-    cfg = _core.tune(atoms[: 4 * N_EMIT], offsets[:5], geom, precision, nat.OUT_C128)
+    if args.config:
+        cfg = json.loads(args.config)
+    elif args.no_tune:
+        cfg = None
+    else:
+        nt = min(4, N_IMG)
+        cfg = _core.tune(atoms[: nt * N_EMIT], offsets[: nt + 1], geom, precision, nat.OUT_C128)
 
     def step():
         _core.forward(atoms, offsets, geom, precision, nat.OUT_C128, out=out, config=cfg)
