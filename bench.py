@@ -233,15 +233,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e/fwd+bwd/fp64/accuracy legs")
     ap.add_argument("--case", default="full", choices=["full", "small"],
-                    help="small: 2 images on a 256x256 detector (profiling-sized capture of the same kernel)")
+                    help="small: 8 images on a 512x512 detector (profiling-sized capture of the same kernel)")
     ap.add_argument("--no-tune", action="store_true", help="use the default kernel shape instead of autotuning")
     ap.add_argument("--config", default=None, help='kernel shape as JSON, e.g. {"threads":256,"pixels_per_thread":4}')
     args = ap.parse_args()
     global N_IMG, NDET
     global WORKLOAD
     if args.case == "small":
-        N_IMG, NDET = 2, 256
-        WORKLOAD = WORKLOAD.replace("1024x1024", "256x256").replace("32 images", "2 images")
+        N_IMG, NDET = 8, 512
+        WORKLOAD = WORKLOAD.replace("1024x1024", "512x512").replace("32 images", "8 images")
     if args.impl == "reference":
         return reference_arm(args)
     if args.warmup < 3:

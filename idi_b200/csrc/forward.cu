@@ -43,7 +43,7 @@ namespace idiwf {
 // ---------------------------------------------------------------------------
 // record layouts
 // ---------------------------------------------------------------------------
-// split:  r64 double4 {x, y, z, psi/2pi - rint}   (32 B)
+// split:  r64 double4 {x, y, z, Psi}              (32 B)  Psi = magic + 1/4 + psi/2pi mod 1
 //         rA  float4  {x, x, y, y}                (16 B)  duplicated for f32x2
 //         rB  float4  {z, z, w, w}                (16 B)  w = |r|^2 (nf) or x^2+y^2
 //         rC  float2  {a, a}                      ( 8 B)
@@ -107,6 +107,11 @@ __global__ void prep_split_kernel(const __grid_constant__ BatchParams bp, const 
             const double4 a = reinterpret_cast<const double4 *>(atoms)[s];
             double psi = a.w * kInvTwoPi;
             psi = psi - rint(psi);
+            // the DFMA chain of the kernel starts from this value: the magic
+            // binade, +1/4 turn (bit 31 of the fixed-point phase then marks
+            // the half turn centred on pi) and +2^-25 turn (rounds instead of
+            // truncating to the 23 angle bits the kernel keeps)
+            psi = (kTurnMagic + 0.25 + 0x1p-25) + psi;
             float amp = 1.0f;
             if (amps) amp = amp_dtype == IDIWF_F32 ? static_cast<const float *>(amps)[s]
                                                   : (float)static_cast<const double *>(amps)[s];
@@ -221,7 +226,7 @@ __global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ 
         const int p0 = ptile * tile_px + tid * PPT;
 
         // ---- per-pixel constants (FP64 geometry) ----
-        double cpm[PPT], nqx[PPT], nqy[PPT], nqz[PPT];
+        double nqx[PPT], nqy[PPT], nqz[PPT];
         float2 dhx[PH], dhy[PH], dhz[PH], hh[PH], iD[PH], iD2[PH];
         float rd[PPT];
 #pragma unroll
@@ -237,17 +242,6 @@ __global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ 
             nqx[i] = -g.kp * (dx * invD);
             nqy[i] = -g.kp * (dy * invD);
             nqz[i] = -g.kp * dzm1;
-            double cp = 0.0;
-            if (NF) {
-                const double dmz = dz > 0 ? rho2 / (D + dz) : D - dz;
-                const double c = g.kp * dmz;
-                cp = c - rint(c);
-            }
-            // +1/4 turn: bit 31 of the fixed-point phase then marks the half
-            // turn centred on pi, and bits 30..8 the angle within it (see the
-            // inner loop); +2^-25 turn rounds (instead of truncating) to the
-            // 23 kept bits.
-            cpm[i] = (kTurnMagic + 0.25 + 0x1p-25) + cp;
             const float fh = (float)(g.k * 0.5 * invD);
             const float fdx = (float)(dx * invD), fdy = (float)(dy * invD), fdz = (float)(dz * invD);
             const float fi = (float)invD, fi2 = (float)(invD * invD);
@@ -307,8 +301,7 @@ __global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ 
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
                             const int i = 2 * q + e;
-                            double t = __dadd_rn(cpm[i], r.w);
-                            t = __fma_rn(nqx[i], r.x, t);
+                            double t = __fma_rn(nqx[i], r.x, r.w);
                             t = __fma_rn(nqy[i], r.y, t);
                             t = __fma_rn(nqz[i], r.z, t);
                             lo[e] = (uint32_t)__double2loint(t);
@@ -391,6 +384,21 @@ __global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ 
                 if (!NF && SCALE) {
                     re *= rd[i];
                     im *= rd[i];
+                }
+                if (NF && out_kind <= IDIWF_OUT_C64) {
+                    // the pixel's constant phase k (|d| - d_z), left out of the
+                    // per-pair sum, applied once here in FP64
+                    const int ix = p / g.ny, iy = p - ix * g.ny;
+                    double dx, dy, dz;
+                    pixel_cpu(g, ix, iy, dx, dy, dz);
+                    const double rho2 = dx * dx + dy * dy;
+                    const double D = sqrt(rho2 + dz * dz);
+                    const double c = g.kp * (dz > 0 ? rho2 / (D + dz) : D - dz);
+                    double sn, cs;
+                    sincospi(2.0 * (c - rint(c)), &sn, &cs);
+                    const double r2 = re * cs - im * sn;
+                    im = re * sn + im * cs;
+                    re = r2;
                 }
                 store_pixel(out, out_kind, obase + p, re, im);
             }
@@ -885,9 +893,12 @@ extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *ba
     std::vector<LaunchShape> cands;
     if (precision == IDIWF_SPLIT) {
         for (int th : {128, 256})
-            for (int ppt : {4, 8})
-                for (int te : {128, 256, 512})
-                    for (int c : {1, 2}) cands.push_back(LaunchShape{th, ppt, te, c});
+            for (int ppt : {2, 4, 8})
+                for (int te : {256, 512})
+                    for (int c : {1, 2, 3, 4}) {
+                        if (ppt == 8 && c > 2) continue;
+                        cands.push_back(LaunchShape{th, ppt, te, c});
+                    }
     } else {
         for (int th : {128, 256})
             for (int ppt : {1, 2})
