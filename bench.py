@@ -272,7 +272,7 @@ def main():
     elif args.no_tune:
         cfg = None
     else:
-        nt = min(4, N_IMG)
+        nt = min(2, N_IMG)
         cfg = _core.tune(atoms[: nt * N_EMIT], offsets[: nt + 1], geom, precision, nat.OUT_C128)
 
     def step():
@@ -433,7 +433,96 @@ def extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, 
     res["fwd_bwd"] = {"workload": "10k emitters, 15 nm sphere, 512x512 @ 75 um, 0.1 m, 6.4 keV, near field",
                       "fwd_ms": ms_f, "fwd_bwd_ms": ms_fb, "ratio": ms_fb / ms_f,
                       "fwd_pairs_per_s": pairs4 / (ms_f * 1e-3), "fwd_bwd_pairs_per_s": pairs4 / (ms_fb * 1e-3)}
+    del a4, T4
+    res["batched_uneven"] = batched_leg(torch, dev, _core, nat)
+    res["time_path"] = time_leg(torch, dev, _core, nat, args)
     return res
+
+
+def sphere_points(g, n, r):
+    t = g.uniform(-1, 1, n)
+    p = g.uniform(0, 2 * np.pi, n)
+    u = r * g.uniform(0, 1, n) ** (1 / 3)
+    s = np.sqrt(1 - t ** 2)
+    return np.stack([u * t, u * s * np.sin(p), u * s * np.cos(p)], -1)
+
+
+def batched_leg(torch, dev, _core, nat):
+    """256 images, emitter counts log-uniform in [1e3, 1e5], sphere radii
+    uniform in [5, 25] nm, amplitudes uniform in [0.5, 1.5] (float32),
+    512x512 @ 75 um, 0.1 m, 6.4 keV, near field, split precision: one
+    persistent launch per batch, captured in a CUDA graph, shape autotuned."""
+    from idi_b200.simulation.batch import BatchPlan
+
+    g = np.random.Generator(np.random.Philox(33))
+    counts = np.floor(np.exp(g.uniform(np.log(1e3), np.log(1e5), 256))).astype(np.int64)
+    radii = g.uniform(0.005, 0.025, 256)
+    at = np.concatenate([np.concatenate([sphere_points(g, int(c), r), g.uniform(0, 2 * np.pi, (int(c), 1))], 1)
+                         for c, r in zip(counts, radii)])
+    amp = g.uniform(0.5, 1.5, at.shape[0]).astype(np.float32)
+    geom = _core.make_geom(512, 75.0, 1e5, k_of(6400.0), flags=nat.NF)
+    plan = BatchPlan(counts, geom, nat.SPLIT, nat.OUT_I64, amplitudes="float32", device=dev)
+    d_at = torch.from_numpy(at).to(dev)
+    d_amp = torch.from_numpy(amp).to(dev)
+    plan.run(d_at, d_amp)  # autotune + capture
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 2
+    a.record()
+    for _ in range(reps):
+        plan.run()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    plan.check()
+    busy = plan.cta_times().astype(np.float64)
+    pairs = int(counts.sum()) * 512 * 512
+    out = {"workload": "256 images, N log-uniform [1e3, 1e5], r in [5, 25] nm, a in [0.5, 1.5] f32, "
+                       "512x512 @ 75 um, 0.1 m, 6.4 keV, near field, split, CUDA graph",
+           "emitters": int(counts.sum()), "pairs_per_step": pairs, "ms": ms, "pairs_per_s": pairs / (ms * 1e-3),
+           "kernel_shape": plan.config,
+           "load_imbalance_max_over_mean_cta_busy": float(busy.max() / busy.mean()) if busy.size else None,
+           "ctas": int(busy.size)}
+    plan.close()
+    return out
+
+
+def time_leg(torch, dev, _core, nat, args):
+    """20,000 emitters in a 10 nm sphere, emission times Gaussian (5 fs FWHM),
+    tau = 2 fs, c = 0.3 um/fs, 256x256 @ 75 um, 0.1 m, 6.4 keV, 4 images."""
+    import oracle
+
+    g = np.random.Generator(np.random.Philox(44))
+    n, nimg = 20000, 4
+    geom = _core.make_geom(256, 75.0, 1e5, k_of(6400.0))
+    pos = sphere_points(g, n, 0.01)
+    imgs = []
+    for _ in range(nimg):
+        at = np.concatenate([pos, g.uniform(0, 2 * np.pi, (n, 1))], 1)
+        t = g.normal(0, 5.0 / 2.35, n)
+        imgs.append((torch.from_numpy(at).to(dev), torch.from_numpy(t).to(dev), at, t))
+    _core.time_forward(imgs[0][0], imgs[0][1], geom, 0.3, 2.0)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for d_at, d_t, _, _ in imgs:
+        _core.time_forward(d_at, d_t, geom, 0.3, 2.0)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    pairs = nimg * n * 256 * 256
+    out = {"workload": "20k emitters, 10 nm sphere, 5 fs FWHM emission, tau 2 fs, 256x256 @ 75 um, 0.1 m, 4 images",
+           "ms": ms, "pairs_per_s": pairs / (ms * 1e-3)}
+    if not args.no_cpu_baseline:
+        # CPU: the oracle's C restatement of time.py on a row-block sample of image 0
+        rows = 2
+        og = oracle.geometry([rows, 256], 75.0, 1e5, k_of(6400.0))
+        t0 = time.perf_counter()
+        oracle.time_image(og, 0, imgs[0][2], imgs[0][3], 0.3, 2.0)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": rows * 256 * n / dt, "unit": "pairs/s", "cores": os.cpu_count(),
+                               "kind": "port", "sample": f"{rows} rows x 256 px x {n} emitters of image 0"}
+    return out
 
 
 if __name__ == "__main__":

@@ -182,7 +182,7 @@ __device__ __forceinline__ void store_pixel(void *out, int out_kind, int64_t idx
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 template <int PPT, bool NF, bool SCALE, bool SECOND>
-__global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ BatchParams bp,
+__global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(const __grid_constant__ BatchParams bp,
                                                         const GeomParams g, SplitRecs rec,
                                                         void *__restrict__ out, int out_kind,
                                                         WsHeader *__restrict__ hdr,
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(256) fwd_split_kernel(const __grid_constant__ 
                 float2 are[PH], aim[PH];
 #pragma unroll
                 for (int q = 0; q < PH; ++q) are[q] = aim[q] = f2(0.f, 0.f);
-#pragma unroll 2
+#pragma unroll(PPT <= 4 ? 4 : 2)
                 for (int j = jb; j < jb + kFold; ++j) {
                     const double4 r = s64[j];
                     const float4 A = sA[j];

@@ -59,8 +59,17 @@ class BatchPlan:
 
     def _prepare(self):
         if self._autotune:
-            self.config = _core.tune(self.atoms, self.offsets, self.geom, self.precision, self.out_kind,
-                                     amplitudes=self.amplitudes, role=self._role)
+            # tune on up to 8 images spread over the sorted emitter counts
+            order = np.argsort(self.counts)
+            pick = np.unique(order[np.linspace(0, len(order) - 1, min(8, len(order))).astype(int)])
+            rows = [self.atoms[self.offsets[i]:self.offsets[i + 1]] for i in pick]
+            sub = torch.cat(rows).contiguous()
+            sub_off = np.concatenate([[0], np.cumsum(self.counts[pick])]).astype(np.int64)
+            sub_amp = None
+            if self.amplitudes is not None:
+                sub_amp = torch.cat([self.amplitudes[self.offsets[i]:self.offsets[i + 1]] for i in pick]).contiguous()
+            self.config = _core.tune(sub, sub_off, self.geom, self.precision, self.out_kind, amplitudes=sub_amp,
+                                     role=self._role)
             self._autotune = False
         if self._use_graph and self._graph is None:
             s = torch.cuda.Stream(self.device)
