@@ -7,20 +7,25 @@
 //   dL/da_j   =  sum_p w_pj Re z_pj
 //   dL/dpsi_j = -a_j sum_p w_pj Im z_pj
 //   dL/dr_j   = -a_j sum_p w_pj Im z_pj grad_r phi_pj
-// with grad_r phi = -q_p + kappa_p (r_j - s_pj dhat_p) in the near field
-// (q_p = k (dhat_p - zhat), kappa_p = k/|d_p|, s_pj = dhat_p . r_j; the next
-// order is k r^2/|d|^2, ~1e-10 relative), -q_p in the far field, plus
-// kappa_p (x, y, 0) for the far-field second-order term.  The 1/r factor's own
-// gradient (relative size 1/(k |d| theta) ~ 1e-9) is not included.
+// with grad_r phi = -q_p + kappa_p P_p r_j in the near field (q_p = k (dhat_p -
+// zhat), kappa_p = k/|d_p|, P_p = I - dhat_p dhat_p^T; the next order is
+// k r^2/|d|^2, ~1e-10 relative), -q_p in the far field, plus kappa_p (x, y, 0)
+// for the far-field second-order term.  The near-field projector is taken
+// paraxially, P ~ diag(1, 1, 0): the kappa term is itself r / (|d| theta) of
+// the main term and the neglected part is theta times that, below 1e-7 of
+// the gradient.  The 1/r factor's own gradient (relative size
+// 1/(k |d| theta) ~ 1e-9) is not included.
 //
-// The phase is formed exactly as in the forward split kernel (FP64 turns in a
-// magic binade -> 32-bit fixed point -> FP32 angle, MUFU sincos).  Here each
+// The phase is formed as in the forward split kernel (FP64 turns in a magic
+// binade -> 32-bit fixed point -> FP32 angle, MUFU sincos), with the
+// pixel's constant near-field phase folded into G instead of the per-pair
+// chain.  Here each
 // thread owns a few emitters in registers and pixel tiles stream through
 // shared memory (bulk async copies, double-buffered, bounded waits); packed
 // f32x2 arithmetic processes two emitters per instruction.  Work units are
 // (image, emitter block, pixel chunk); each unit writes FP32 partial sums of
-// its chunk, and a reduction kernel adds the chunks in a fixed order in FP64,
-// so results are deterministic.
+// its 2048-pixel chunk, and a reduction kernel adds the chunks in a fixed
+// order in FP64, so results are deterministic.
 
 #include <algorithm>
 #include <cmath>
@@ -32,39 +37,40 @@
 namespace idiwf {
 
 constexpr int kBwdThreads = 128;
-constexpr int kBwdPE = 4;                        // emitters per thread
-constexpr int kBwdEB = kBwdThreads * kBwdPE;     // emitters per block (512)
 constexpr int kBwdTP = 128;                      // pixels per shared-memory tile
 constexpr int kBwdChunk = 2048;                  // pixels per work unit
-constexpr int kBwdNAcc = 9;                      // partial sums per emitter
+constexpr int kBwdNAcc = 6;                      // partial sums per emitter
+constexpr int kBwdMaxPE = 8;                     // largest emitters-per-thread instantiation
 
 // pixel record (geometry part, shared by all images):
-//   P64  double4 {cpm, -q'x, -q'y, -q'z}                           32 B
-//   PF   float4 x4  {dx,dx,dy,dy} {dz,dz,h,h} {qx,qx,qy,qy} {qz,qz,kap,kap}   64 B
-//   PS   float4 {iD,iD,iD2,iD2}   (scale only, stored always)       16 B
+//   P64  double4 {-q'x, -q'y, -q'z, 0}   q' = k (dhat - zhat) / 2pi      32 B
+//   PF   float4 x5  {dx,dx,dy,dy} {dz,dz,h,h} {qx,qx,qy,qy} {qz,qz,kap,kap}
+//                   {iD,iD,iD2,iD2}   (the last one read in "scale" mode) 80 B
 // per image:
-//   PG   float4 {Gr,Gr,Gi,Gi}                                      16 B
-constexpr int kPixGeomBytes = 32 + 64 + 16;
-constexpr int kPixRecBytes = kPixGeomBytes + 16;
+//   PG   float4 {G'r,G'r,G'i,G'i}   G' = 2 g conj(E) exp(2 pi i C')      16 B
+// Values are duplicated in pairs because f32x2 instructions process two
+// emitters of a thread against the same pixel.
+constexpr int kPixRecBytes = 32 + 80 + 16;
 
 struct BwdLayout {
     int npix_pad;          // pixels rounded up to the chunk size
     int n_chunks;
-    int64_t nrec;          // emitter records (images padded to kBwdEB)
+    int64_t nrec;          // emitter records (images padded to the emitter block)
     size_t off_p64, off_pf, off_pg, off_erec64, off_erecf, off_part, total;
 };
 
 static BwdLayout bwd_layout(const idiwf_geom *g, const idiwf_batch *b) {
     BwdLayout L;
     const int64_t npix = (int64_t)g->nx * g->ny;
+    const int eb = kBwdThreads * kBwdMaxPE;
     L.npix_pad = (int)((npix + kBwdChunk - 1) / kBwdChunk * kBwdChunk);
     L.n_chunks = L.npix_pad / kBwdChunk;
     L.nrec = 0;
     for (int i = 0; i < b->n_images; ++i) {
         const int64_t n = b->offsets[i + 1] - b->offsets[i];
-        L.nrec += (n + kBwdEB - 1) / kBwdEB * kBwdEB;
+        L.nrec += (n + eb - 1) / eb * eb;
     }
-    L.nrec = std::max<int64_t>(L.nrec, kBwdEB);
+    L.nrec = std::max<int64_t>(L.nrec, eb);
     size_t o = kWsDataOffset;
     L.off_p64 = o; o += align256((size_t)L.npix_pad * 32);
     L.off_pf = o;  o += align256((size_t)L.npix_pad * 80);
@@ -81,13 +87,20 @@ struct BwdImage {
     int32_t n, nblocks;
 };
 struct BwdParams {
-    int32_t n_images, n_chunks, npix, npix_pad, total_units, units_per_image_block;
+    int32_t n_images, n_chunks, npix, npix_pad, total_units, eb;
     BwdImage img[kMaxImagesPerLaunch];
     int32_t unit_img[kMaxImagesPerLaunch];   // images by descending emitter count
 };
 
+__device__ __forceinline__ double nf_constant_turns(const GeomParams &g, double dx, double dy, double dz) {
+    // k (|d| - d_z) / 2pi mod 1, without cancellation
+    const double rho2 = dx * dx + dy * dy;
+    const double D = sqrt(rho2 + dz * dz);
+    const double c = g.kp * (dz > 0 ? rho2 / (D + dz) : D - dz);
+    return c - rint(c);
+}
+
 // ---- pixel prep: geometry (image independent) ------------------------------
-template <bool NF>
 __global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad, double4 *__restrict__ p64,
                                       float4 *__restrict__ pf) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix_pad; p += gridDim.x * blockDim.x) {
@@ -99,14 +112,7 @@ __global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad
         const double D = sqrt(rho2 + dz * dz);
         const double invD = 1.0 / D;
         const double dzm1 = dz > 0 ? -rho2 / (D * (D + dz)) : dz * invD - 1.0;
-        double cp = 0.0;
-        if (NF) {
-            const double dmz = dz > 0 ? rho2 / (D + dz) : D - dz;
-            const double c = g.kp * dmz;
-            cp = c - rint(c);
-        }
-        p64[p] = make_double4((kTurnMagic + 0.5 + 0x1p-24) + cp, -g.kp * (dx * invD), -g.kp * (dy * invD),
-                              -g.kp * dzm1);
+        p64[p] = make_double4(-g.kp * (dx * invD), -g.kp * (dy * invD), -g.kp * dzm1, 0.0);
         const float fdx = (float)(dx * invD), fdy = (float)(dy * invD), fdz = (float)(dz * invD);
         const float fh = (float)(g.k * 0.5 * invD);
         const float qx = (float)(g.k * dx * invD), qy = (float)(g.k * dy * invD), qz = (float)(g.k * dzm1);
@@ -121,9 +127,14 @@ __global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad
     }
 }
 
-// ---- pixel prep: G_p = 2 g_p conj(E_p) per image ---------------------------
-__global__ void bwd_pixel_g_kernel(const double2 *__restrict__ field, const double *__restrict__ gI, int npix,
-                                   int npix_pad, int n_images, float4 *__restrict__ pg) {
+// ---- pixel prep: G'_p = 2 g_p conj(E_p) exp(2 pi i C'_p) per image --------
+// C'_p is the near-field constant phase k (|d| - d_z) that the per-pair
+// phase leaves out; folding it into G keeps the per-pair FP64 chain at three
+// DFMA.
+template <bool NF>
+__global__ void bwd_pixel_g_kernel(const GeomParams g, const double2 *__restrict__ field,
+                                   const double *__restrict__ gI, int npix, int npix_pad, int n_images,
+                                   float4 *__restrict__ pg) {
     const int64_t total = (int64_t)npix_pad * n_images;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int b = (int)(t / npix_pad);
@@ -132,8 +143,19 @@ __global__ void bwd_pixel_g_kernel(const double2 *__restrict__ field, const doub
         if (p < npix) {
             const double2 e = field[(int64_t)b * npix + p];
             const double gg = 2.0 * gI[(int64_t)b * npix + p];
-            gr = (float)(gg * e.x);
-            gi = (float)(-gg * e.y);
+            double r = gg * e.x, i = -gg * e.y;
+            if (NF) {
+                const int ix = p / g.ny, iy = p - ix * g.ny;
+                double dx, dy, dz;
+                pixel_cpu(g, ix, iy, dx, dy, dz);
+                double sn, cs;
+                sincospi(2.0 * nf_constant_turns(g, dx, dy, dz), &sn, &cs);
+                const double r2 = r * cs - i * sn;
+                i = r * sn + i * cs;
+                r = r2;
+            }
+            gr = (float)r;
+            gi = (float)i;
         }
         pg[t] = make_float4(gr, gr, gi, gi);
     }
@@ -144,19 +166,21 @@ __global__ void bwd_emitter_prep_kernel(const __grid_constant__ BwdParams bp, co
                                         double4 *__restrict__ e64, float4 *__restrict__ ef, int w_mode) {
     const int b = blockIdx.y;
     const BwdImage d = bp.img[b];
-    const int64_t nrec = (int64_t)d.nblocks * kBwdEB;
+    const int64_t nrec = (int64_t)d.nblocks * bp.eb;
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nrec; j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t r = d.rec + j;
         if (j < d.n) {
             const double4 a = reinterpret_cast<const double4 *>(atoms)[d.src + j];
             double psi = a.w * kInvTwoPi;
             psi = psi - rint(psi);
+            // magic binade + 1/2 turn (angle = 2pi (u - 1.5)) + 2^-24 turn rounding bias
+            psi = (kTurnMagic + 0.5 + 0x1p-24) + psi;
             const double w = w_mode == 1 ? (a.x * a.x + a.y * a.y) + a.z * a.z
                                          : (w_mode == 2 ? a.x * a.x + a.y * a.y : 0.0);
             e64[r] = make_double4(a.x, a.y, a.z, psi);
             ef[r] = make_float4((float)a.x, (float)a.y, (float)a.z, (float)w);
         } else {
-            e64[r] = make_double4(0, 0, 0, 0);
+            e64[r] = make_double4(0, 0, 0, kTurnMagic);
             ef[r] = make_float4(0, 0, 0, 0);
         }
     }
@@ -165,12 +189,21 @@ __global__ void bwd_emitter_prep_kernel(const __grid_constant__ BwdParams bp, co
 __device__ __forceinline__ float2 g2(float a, float b) { return make_float2(a, b); }
 
 // ---- the adjoint direct sum --------------------------------------------------
-template <bool NF, bool SCALE, bool SECOND>
+// Accumulators per emitter (FP32 over a 2048-pixel chunk):
+//   0  sum w Re z        -> dL/da
+//   1  sum w Im z        -> dL/dpsi = -a * acc1
+//   2-4 sum w Im z q     -> dL/dr main term
+//   5  sum w Im z kappa  -> near-field / second-order correction -kappa (x, y, 0)
+// The near-field correction uses the paraxial projector: grad phi =
+// -q + kappa P r with P = I - dhat dhat^T ~ diag(1, 1, 0); the neglected part
+// is of relative size theta (the pixel angle) times the correction, which is
+// itself r / (|d| theta) of the main term: below 1e-7 of the gradient.
+template <bool NF, bool SCALE, bool SECOND, int PE>
 __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
     const __grid_constant__ BwdParams bp, const double4 *__restrict__ e64, const float4 *__restrict__ ef,
     const double4 *__restrict__ p64, const float4 *__restrict__ pf, const float4 *__restrict__ pg,
     float *__restrict__ part, int64_t nrec, WsHeader *__restrict__ hdr) {
-    constexpr int PH = kBwdPE / 2;
+    constexpr int PH = PE / 2;
     constexpr uint32_t kStage = kBwdTP * kPixRecBytes;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar[2];
@@ -187,6 +220,7 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
     bool aborted = false;
     const float2 TWO_PI2 = g2(6.28318548f, 6.28318548f);
     const float2 NEG_3PI2 = g2(-9.42477796f, -9.42477796f);
+    const int eb = kBwdThreads * PE;
 
     for (;;) {
         __syncthreads();
@@ -194,8 +228,6 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
         __syncthreads();
         const int unit = s_unit;
         if (unit >= bp.total_units) break;
-        // unit -> (image-block, chunk); image-blocks are enumerated image by
-        // image in descending emitter count
         const int chunk = unit % bp.n_chunks;
         int ib = unit / bp.n_chunks;
         int img = 0;
@@ -205,25 +237,23 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
             ib -= bp.img[b].nblocks;
         }
         const BwdImage d = bp.img[img];
-        const int64_t rec0 = d.rec + (int64_t)ib * kBwdEB + tid * kBwdPE;
+        const int64_t rec0 = d.rec + (int64_t)ib * eb + tid * PE;
 
-        // emitter registers
-        double ex[kBwdPE], ey[kBwdPE], ez[kBwdPE], epsi[kBwdPE];
+        double ex[PE], ey[PE], ez[PE], epsi[PE];
         float2 fx[PH], fy[PH], fz[PH], fw[PH];
 #pragma unroll
-        for (int e = 0; e < kBwdPE; ++e) {
+        for (int e = 0; e < PE; ++e) {
             const double4 r = e64[rec0 + e];
             ex[e] = r.x; ey[e] = r.y; ez[e] = r.z; epsi[e] = r.w;
             const float4 f = ef[rec0 + e];
             if (e & 1) { fx[e / 2].y = f.x; fy[e / 2].y = f.y; fz[e / 2].y = f.z; fw[e / 2].y = f.w; }
             else       { fx[e / 2].x = f.x; fy[e / 2].x = f.y; fz[e / 2].x = f.z; fw[e / 2].x = f.w; }
         }
-        // chunk sums (FP32) of the 9 accumulators
-        float2 cs[kBwdNAcc][PH];
+        float2 ac[kBwdNAcc][PH];
 #pragma unroll
         for (int a = 0; a < kBwdNAcc; ++a)
 #pragma unroll
-            for (int q = 0; q < PH; ++q) cs[a][q] = g2(0.f, 0.f);
+            for (int q = 0; q < PH; ++q) ac[a][q] = g2(0.f, 0.f);
 
         const int p_begin = chunk * kBwdChunk;
         constexpr int nt = kBwdChunk / kBwdTP;
@@ -251,11 +281,6 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
             const double4 *s64 = reinterpret_cast<const double4 *>(st);
             const float4 *sf = reinterpret_cast<const float4 *>(st + kBwdTP * 32);
             const float4 *sg = reinterpret_cast<const float4 *>(st + kBwdTP * 112);
-            float2 ac[kBwdNAcc][PH];
-#pragma unroll
-            for (int a = 0; a < kBwdNAcc; ++a)
-#pragma unroll
-                for (int q = 0; q < PH; ++q) ac[a][q] = g2(0.f, 0.f);
 #pragma unroll 2
             for (int j = 0; j < kBwdTP; ++j) {
                 const double4 P = s64[j];
@@ -263,17 +288,16 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
                 const float4 F1 = sf[5 * j + 1];   // dz dz h h
                 const float4 F2 = sf[5 * j + 2];   // qx qx qy qy
                 const float4 F3 = sf[5 * j + 3];   // qz qz kap kap
-                const float4 GG = sg[j];           // Gr Gr Gi Gi
+                const float4 GG = sg[j];           // G'r G'r G'i G'i
 #pragma unroll
                 for (int q = 0; q < PH; ++q) {
                     uint32_t lo[2];
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
                         const int i = 2 * q + e;
-                        double t = __dadd_rn(P.x, epsi[i]);
-                        t = __fma_rn(P.y, ex[i], t);
-                        t = __fma_rn(P.z, ey[i], t);
-                        t = __fma_rn(P.w, ez[i], t);
+                        double t = __fma_rn(P.x, ex[i], epsi[i]);
+                        t = __fma_rn(P.y, ey[i], t);
+                        t = __fma_rn(P.z, ez[i], t);
                         lo[e] = (uint32_t)__double2loint(t);
                     }
                     const float2 u = g2(__uint_as_float((lo[0] >> 9) | 0x3F800000u),
@@ -293,42 +317,27 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
                     __sincosf(arg.x, &s0, &c0);
                     __sincosf(arg.y, &s1, &c1);
                     const float2 cc = g2(c0, c1), ss = g2(s0, s1);
-                    // z = G e^{i phi}
-                    float2 zr = __fmul2_rn(g2(GG.x, GG.y), cc);
-                    zr = __ffma2_rn(g2(-GG.z, -GG.w), ss, zr);
+                    // z = G' e^{i phi'}: Im z = Gr s + Gi c, Re z = Gr c - Gi s
                     float2 zi = __fmul2_rn(g2(GG.x, GG.y), ss);
                     zi = __ffma2_rn(g2(GG.z, GG.w), cc, zi);
-                    if (NF && SCALE) {
+                    if (SCALE) {
                         const float4 F4 = sf[5 * j + 4];  // iD iD iD2 iD2
-                        const float2 w = __ffma2_rn(s, g2(F4.z, F4.w), g2(F4.x, F4.y));
-                        zr = __fmul2_rn(zr, w);
+                        const float2 w = NF ? __ffma2_rn(s, g2(F4.z, F4.w), g2(F4.x, F4.y)) : g2(F4.x, F4.y);
+                        float2 zr = __fmul2_rn(g2(GG.x, GG.y), cc);
+                        zr = __ffma2_rn(g2(-GG.z, -GG.w), ss, zr);
                         zi = __fmul2_rn(zi, w);
-                    } else if (SCALE) {
-                        const float4 F4 = sf[5 * j + 4];
-                        zr = __fmul2_rn(zr, g2(F4.x, F4.y));
-                        zi = __fmul2_rn(zi, g2(F4.x, F4.y));
+                        ac[0][q] = __ffma2_rn(zr, w, ac[0][q]);
+                    } else {
+                        ac[0][q] = __ffma2_rn(g2(GG.x, GG.y), cc, ac[0][q]);
+                        ac[0][q] = __ffma2_rn(g2(-GG.z, -GG.w), ss, ac[0][q]);
                     }
-                    ac[0][q] = __fadd2_rn(ac[0][q], zr);
                     ac[1][q] = __fadd2_rn(ac[1][q], zi);
                     ac[2][q] = __ffma2_rn(zi, g2(F2.x, F2.y), ac[2][q]);
                     ac[3][q] = __ffma2_rn(zi, g2(F2.z, F2.w), ac[3][q]);
                     ac[4][q] = __ffma2_rn(zi, g2(F3.x, F3.y), ac[4][q]);
-                    if (NF || SECOND) {
-                        const float2 ki = __fmul2_rn(zi, g2(F3.z, F3.w));
-                        ac[5][q] = __fadd2_rn(ac[5][q], ki);
-                        if (NF) {
-                            const float2 ks = __fmul2_rn(ki, s);
-                            ac[6][q] = __ffma2_rn(ks, g2(F0.x, F0.y), ac[6][q]);
-                            ac[7][q] = __ffma2_rn(ks, g2(F0.z, F0.w), ac[7][q]);
-                            ac[8][q] = __ffma2_rn(ks, g2(F1.x, F1.y), ac[8][q]);
-                        }
-                    }
+                    if (NF || SECOND) ac[5][q] = __ffma2_rn(zi, g2(F3.z, F3.w), ac[5][q]);
                 }
             }
-#pragma unroll
-            for (int a = 0; a < kBwdNAcc; ++a)
-#pragma unroll
-                for (int q = 0; q < PH; ++q) cs[a][q] = __fadd2_rn(cs[a][q], ac[a][q]);
             ++consumed;
             __syncthreads();
             if (s_abort) {
@@ -344,8 +353,8 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
         for (int q = 0; q < PH; ++q)
 #pragma unroll
             for (int a = 0; a < kBwdNAcc; ++a) {
-                dst[(2 * q) * kBwdNAcc + a] = cs[a][q].x;
-                dst[(2 * q + 1) * kBwdNAcc + a] = cs[a][q].y;
+                dst[(2 * q) * kBwdNAcc + a] = ac[a][q].x;
+                dst[(2 * q + 1) * kBwdNAcc + a] = ac[a][q].y;
             }
     }
     if (aborted && tid == 0)
@@ -356,7 +365,7 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
 }
 
 // ---- chunk reduction + final gradients -------------------------------------
-template <bool NF, bool SECOND>
+template <bool KAPPA>
 __global__ void bwd_reduce_kernel(const __grid_constant__ BwdParams bp, const float *__restrict__ part,
                                   int64_t nrec, const double *__restrict__ atoms, const void *__restrict__ amps,
                                   int amp_dtype, double *__restrict__ grad_atoms, double *__restrict__ grad_amp) {
@@ -377,24 +386,22 @@ __global__ void bwd_reduce_kernel(const __grid_constant__ BwdParams bp, const fl
         double aj = 1.0;
         if (amps) aj = amp_dtype == IDIWF_F32 ? (double)static_cast<const float *>(amps)[s]
                                              : static_cast<const double *>(amps)[s];
-        // dL/dr = -a sum w Im z grad(phi), grad(phi) = -q + kap (r - s dhat) [nf]
-        double gx = acc[2], gy = acc[3], gz = acc[4];
-        if (NF) {
-            gx += -acc[5] * at.x + acc[6];
-            gy += -acc[5] * at.y + acc[7];
-            gz += -acc[5] * at.z + acc[8];
-        } else if (SECOND) {
-            gx += -acc[5] * at.x;
-            gy += -acc[5] * at.y;
+        // dL/dr = -a sum w Im z grad(phi) = a (Q - K (x, y, 0))
+        double gx = acc[2], gy = acc[3];
+        if (KAPPA) {
+            gx -= acc[5] * at.x;
+            gy -= acc[5] * at.y;
         }
-        reinterpret_cast<double4 *>(grad_atoms)[s] = make_double4(aj * gx, aj * gy, aj * gz, -aj * acc[1]);
+        reinterpret_cast<double4 *>(grad_atoms)[s] = make_double4(aj * gx, aj * gy, aj * acc[4], -aj * acc[1]);
         if (grad_amp) grad_amp[s] = acc[0];
     }
 }
 
-template <bool NF, bool SCALE, bool SECOND>
-static void *bwd_kernel_ptr() {
-    return (void *)bwd_split_kernel<NF, SCALE, SECOND>;
+template <int PE>
+static void *bwd_kernel_for(bool nf, bool sc, bool so) {
+    if (nf) return sc ? (void *)bwd_split_kernel<true, true, false, PE> : (void *)bwd_split_kernel<true, false, false, PE>;
+    if (so) return sc ? (void *)bwd_split_kernel<false, true, true, PE> : (void *)bwd_split_kernel<false, false, true, PE>;
+    return sc ? (void *)bwd_split_kernel<false, true, false, PE> : (void *)bwd_split_kernel<false, false, false, PE>;
 }
 
 }  // namespace idiwf
@@ -455,12 +462,17 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
     const int npix = geom->nx * geom->ny;
     const bool nf = geom->flags & IDIWF_NF, sc = geom->flags & IDIWF_SCALE, so = geom->flags & IDIWF_SECONDORDER;
 
+    // emitters per thread: 4 (default) or 8, from cfg->pixels_per_thread
+    const int pe = (cfg && cfg->pixels_per_thread) ? cfg->pixels_per_thread : 4;
+    if (pe != 4 && pe != 8) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "backward emitters per thread must be 4 or 8");
+    const int eb = kBwdThreads * pe;
     static thread_local BwdParams bp;
     std::memset(&bp, 0, sizeof(bp));
     bp.n_images = batch->n_images;
     bp.n_chunks = L.n_chunks;
     bp.npix = npix;
     bp.npix_pad = L.npix_pad;
+    bp.eb = eb;
     int64_t rec = 0;
     int total_blocks = 0, max_blocks = 0;
     std::vector<int> ord(batch->n_images);
@@ -469,8 +481,8 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
         bp.img[i].src = batch->offsets[i];
         bp.img[i].rec = rec;
         bp.img[i].n = (int32_t)n;
-        bp.img[i].nblocks = (int32_t)((n + kBwdEB - 1) / kBwdEB);
-        rec += (int64_t)bp.img[i].nblocks * kBwdEB;
+        bp.img[i].nblocks = (int32_t)((n + eb - 1) / eb);
+        rec += (int64_t)bp.img[i].nblocks * eb;
         total_blocks += bp.img[i].nblocks;
         max_blocks = std::max(max_blocks, bp.img[i].nblocks);
         ord[i] = i;
@@ -480,29 +492,29 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
     bp.total_units = total_blocks * L.n_chunks;
 
     const int pthreads = 256;
-    if (nf)
-        bwd_pixel_geom_kernel<true><<<(L.npix_pad + pthreads - 1) / pthreads, pthreads, 0, stream>>>(g, npix, L.npix_pad, p64, pf);
-    else
-        bwd_pixel_geom_kernel<false><<<(L.npix_pad + pthreads - 1) / pthreads, pthreads, 0, stream>>>(g, npix, L.npix_pad, p64, pf);
+    bwd_pixel_geom_kernel<<<(L.npix_pad + pthreads - 1) / pthreads, pthreads, 0, stream>>>(g, npix, L.npix_pad, p64, pf);
     IDIWF_CUDA_CHECK(cudaGetLastError());
     {
         const int64_t tot = (int64_t)L.npix_pad * batch->n_images;
         const int blocks = (int)std::min<int64_t>((tot + pthreads - 1) / pthreads, 65535);
-        bwd_pixel_g_kernel<<<blocks, pthreads, 0, stream>>>(static_cast<const double2 *>(field), grad_intensity, npix,
-                                                            L.npix_pad, batch->n_images, pg);
+        if (nf)
+            bwd_pixel_g_kernel<true><<<blocks, pthreads, 0, stream>>>(g, static_cast<const double2 *>(field),
+                                                                      grad_intensity, npix, L.npix_pad,
+                                                                      batch->n_images, pg);
+        else
+            bwd_pixel_g_kernel<false><<<blocks, pthreads, 0, stream>>>(g, static_cast<const double2 *>(field),
+                                                                       grad_intensity, npix, L.npix_pad,
+                                                                       batch->n_images, pg);
         IDIWF_CUDA_CHECK(cudaGetLastError());
     }
     {
         const int w_mode = nf ? 1 : (so ? 2 : 0);
-        dim3 grid((unsigned)std::max(1, (max_blocks * kBwdEB + 255) / 256), batch->n_images);
+        dim3 grid((unsigned)std::max(1, (max_blocks * eb + 255) / 256), batch->n_images);
         bwd_emitter_prep_kernel<<<grid, 256, 0, stream>>>(bp, batch->atoms, e64, ef, w_mode);
         IDIWF_CUDA_CHECK(cudaGetLastError());
     }
     IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 2 * sizeof(uint32_t), stream));  // counter + error word
-    void *fn;
-    if (nf) fn = sc ? bwd_kernel_ptr<true, true, false>() : bwd_kernel_ptr<true, false, false>();
-    else if (so) fn = sc ? bwd_kernel_ptr<false, true, true>() : bwd_kernel_ptr<false, false, true>();
-    else fn = sc ? bwd_kernel_ptr<false, true, false>() : bwd_kernel_ptr<false, false, false>();
+    void *fn = pe == 8 ? bwd_kernel_for<8>(nf, sc, so) : bwd_kernel_for<4>(nf, sc, so);
     const size_t smem = 2 * (size_t)kBwdTP * kPixRecBytes;
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev = 0, sms = 148, occ = 1;
@@ -514,16 +526,13 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
     void *args[] = {&bp, &e64, &ef, &p64, &pf, &pg, &part, &nrec, &hdr};
     IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(kBwdThreads), args, smem, stream));
     {
-        dim3 rgrid((unsigned)std::max<int64_t>(1, (max_blocks * kBwdEB + 255) / 256), batch->n_images);
-        if (nf)
-            bwd_reduce_kernel<true, false><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
-                                                                      batch->amp_dtype, grad_atoms, grad_amp);
-        else if (so)
-            bwd_reduce_kernel<false, true><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
-                                                                      batch->amp_dtype, grad_atoms, grad_amp);
+        dim3 rgrid((unsigned)std::max<int64_t>(1, (max_blocks * eb + 255) / 256), batch->n_images);
+        if (nf || so)
+            bwd_reduce_kernel<true><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
+                                                                batch->amp_dtype, grad_atoms, grad_amp);
         else
-            bwd_reduce_kernel<false, false><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
-                                                                       batch->amp_dtype, grad_atoms, grad_amp);
+            bwd_reduce_kernel<false><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
+                                                                 batch->amp_dtype, grad_atoms, grad_amp);
         IDIWF_CUDA_CHECK(cudaGetLastError());
     }
     return IDIWF_OK;
