@@ -236,6 +236,8 @@ def main():
                     help="small: 8 images on a 512x512 detector (profiling-sized capture of the same kernel)")
     ap.add_argument("--no-tune", action="store_true", help="use the default kernel shape instead of autotuning")
     ap.add_argument("--config", default=None, help='kernel shape as JSON, e.g. {"threads":256,"pixels_per_thread":4}')
+    ap.add_argument("--leg", default="main", choices=["main", "fwd_bwd", "time", "batched"],
+                    help="run one secondary leg alone (for profiling) instead of the headline measurement")
     args = ap.parse_args()
     global N_IMG, NDET
     global WORKLOAD
@@ -244,6 +246,8 @@ def main():
         WORKLOAD = WORKLOAD.replace("1024x1024", "512x512").replace("32 images", "8 images")
     if args.impl == "reference":
         return reference_arm(args)
+    if args.leg != "main":
+        return single_leg(args)
     if args.warmup < 3:
         args.warmup = 3
 
@@ -367,18 +371,7 @@ def extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, 
                   "call": "idi_b200.simulation.cuda.simulate(32, simobject, 1024, 50, 2e5, k, settings='nf split')"}
 
     # --- all-FP64 comparator on 2 images of the same batch
-    def timed(fn, reps=3):
-        fn()
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        best = 1e30
-        for _ in range(reps):
-            a.record()
-            fn()
-            b.record()
-            torch.cuda.synchronize()
-            best = min(best, a.elapsed_time(b))
-        return best
+    timed = timed_fn(torch)
 
     at2 = atoms[: 2 * N_EMIT]
     off2 = offsets[:3]
@@ -403,7 +396,32 @@ def extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, 
         "log10_rel_hist": {f"{int(e)}": int(h) for e, h in zip(edges[:-1], hist)}}
     del Es, Ed
 
-    # --- forward + adjoint on the differentiation configuration
+    res["fwd_bwd"] = fwd_bwd_leg(torch, dev, _core, nat, timed)
+    res["batched_uneven"] = batched_leg(torch, dev, _core, nat)
+    res["time_path"] = time_leg(torch, dev, _core, nat, args)
+    return res
+
+
+def timed_fn(torch):
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = 1e30
+        for _ in range(reps):
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b))
+        return best
+    return timed
+
+
+def fwd_bwd_leg(torch, dev, _core, nat, timed):
+    """Forward + adjoint on the differentiation configuration: 10,000 emitters
+    in a 15 nm sphere, 512x512 @ 75 um, 0.1 m, 6.4 keV, near field; target =
+    intensities after a 0.05 nm Gaussian displacement; L = sum (I - T)^2."""
     g = np.random.Generator(np.random.Philox(7))
     n4 = 10000
     t = g.uniform(-1, 1, n4)
@@ -430,13 +448,27 @@ def extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, 
     ms_f = timed(fwd, reps=5)
     ms_fb = timed(fwd_bwd, reps=5)
     pairs4 = n4 * 512 * 512
-    res["fwd_bwd"] = {"workload": "10k emitters, 15 nm sphere, 512x512 @ 75 um, 0.1 m, 6.4 keV, near field",
-                      "fwd_ms": ms_f, "fwd_bwd_ms": ms_fb, "ratio": ms_fb / ms_f,
-                      "fwd_pairs_per_s": pairs4 / (ms_f * 1e-3), "fwd_bwd_pairs_per_s": pairs4 / (ms_fb * 1e-3)}
-    del a4, T4
-    res["batched_uneven"] = batched_leg(torch, dev, _core, nat)
-    res["time_path"] = time_leg(torch, dev, _core, nat, args)
-    return res
+    return {"workload": "10k emitters, 15 nm sphere, 512x512 @ 75 um, 0.1 m, 6.4 keV, near field",
+            "fwd_ms": ms_f, "fwd_bwd_ms": ms_fb, "ratio": ms_fb / ms_f,
+            "fwd_pairs_per_s": pairs4 / (ms_f * 1e-3), "fwd_bwd_pairs_per_s": pairs4 / (ms_fb * 1e-3)}
+
+
+def single_leg(args):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    from idi_b200 import _native as nat
+    from idi_b200.simulation import _core
+
+    if args.leg == "fwd_bwd":
+        out = fwd_bwd_leg(torch, dev, _core, nat, timed_fn(torch))
+    elif args.leg == "time":
+        out = time_leg(torch, dev, _core, nat, args)
+    else:
+        out = batched_leg(torch, dev, _core, nat)
+    print(json.dumps({"leg": args.leg, **out}), flush=True)
+    return 0
 
 
 def sphere_points(g, n, r):
