@@ -143,14 +143,9 @@ def dist_init():
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from idi_b200.simulation.shard import max_over_ranks as _max
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return _max(x) if world > 1 else x
 
 
 def barrier(world):
@@ -311,6 +306,14 @@ def main():
     mufu = _core.microbench("mufu_sincos", dev)
     achieved_mufu = 2.0 * pairs_per_step / (kern_avg * 1e-3)
     clocks = clk.summary()
+    traffic = None
+    try:  # DRAM bytes per launch from the committed ncu capture, scaled to this launch
+        with open(os.path.join(ROOT, "profiles", "fwd_split_traffic.json")) as f:
+            cap = json.load(f)
+        traffic = (cap["dram_bytes_read"] + cap["dram_bytes_write"]) * (N_IMG * N_EMIT) / (
+            cap["images"] * cap["emitters_per_image"])
+    except (OSError, KeyError, ValueError):
+        pass
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     nominal_mufu = sms * 16 * (clocks["sm_max_mhz"] or 1965.0) * 1e6
 
@@ -335,7 +338,8 @@ def main():
         "roofline": {"bound": "sfu", "achieved": achieved_mufu / 1e9, "peak": mufu / 1e9, "unit": "Gop/s (MUFU)",
                      "frac": achieved_mufu / mufu, "frac_of_nominal": achieved_mufu / nominal_mufu,
                      "peak_source": "measured: in-repo MUFU sin/cos microbenchmark (idiwf_microbench kind 0)",
-                     "ops_per_pair": 2, "kernel_ms": kern_avg, "traffic": None},
+                     "ops_per_pair": 2, "kernel_ms": kern_avg, "traffic": traffic,
+                     "traffic_unit": "bytes per launch (ncu capture of 8 images, scaled by emitter records)"},
     }
     if not args.no_extras and rank == 0:
         line.update(extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, offsets, cfg))
