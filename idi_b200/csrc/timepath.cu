@@ -11,14 +11,15 @@
 // pixel queue).  Arrival times are computed in FP64 with the exact rounding
 // sequence of the reference (np.inner as fma(q2,z,fma(q1,y,q0*x)), IEEE
 // division by c), so the keys -- and therefore the sorted order -- are bit
-// for bit those of the reference.  The sort is an on-chip LSD radix sort
-// (8 passes of 8 bits over the order-preserving 64-bit image of the double
-// keys) that moves only 16-bit emitter indices: keys stay in a shared-memory
-// table indexed by emitter, so N <= 20480 fits in 200 KB of shared memory.
-// Ranking is per warp with __match_any_sync, which keeps the sort stable
-// (ties, which the reference breaks arbitrarily, keep emitter order).  The
-// decaying scan is a block-wide scan of affine maps x -> D x + B; the
-// interval integral is a block reduction.
+// for bit those of the reference.  The keys stay in a shared-memory table
+// indexed by emitter (N <= 20480 in 160 KB) and only 16-bit emitter indices
+// move.  The sort is exact and stable: 8192 buckets by a monotone FP64 map of
+// the key (so bucket order is key order), then insertion sort inside each
+// bucket by (key, emitter index); if a bucket overflows, an on-chip LSD radix
+// sort (8 passes of 8 bits, per-warp ranking with __match_any_sync) takes
+// over.  The decaying scan is one pass: each thread keeps its run as an
+// affine map x -> D x + B plus three sums from which the run's share of the
+// interval integral follows once the block scan delivers the entering x.
 
 #include <algorithm>
 #include <cmath>
@@ -72,6 +73,22 @@ __device__ __forceinline__ void arrival(const GeomParams &g, double dx, double d
     }
 }
 
+// Path difference s (and the 1/r distance) of one emitter, as arrival() but
+// without forming the arrival time (the scan reads times from the key table).
+template <bool NF>
+__device__ __forceinline__ void path_only(double dx, double dy, double dz, double dn, double q0, double q1,
+                                          double q2, const double4 &a, double &s_out, double &dist_out) {
+    if (!NF) {
+        s_out = __fma_rn(q2, a.z, __fma_rn(q1, a.y, __dmul_rn(q0, a.x)));
+        dist_out = dn;
+    } else {
+        const double ax = __dsub_rn(dx, a.x), ay = __dsub_rn(dy, a.y), az = __dsub_rn(dz, a.z);
+        const double dist = __dsqrt_rn(__fma_rn(az, az, __fma_rn(ax, ax, __dmul_rn(ay, ay))));
+        s_out = __dadd_rn(__dsub_rn(dist, dn), a.z);
+        dist_out = dist;
+    }
+}
+
 template <bool NF, bool SCALE>
 __device__ __forceinline__ void amplitude(double k, double s, double psi, double dist, double &re, double &im) {
     double th;
@@ -87,6 +104,198 @@ __device__ __forceinline__ void amplitude(double k, double s, double psi, double
     im = sn;
 }
 
+// Block-wide min / max of the keys; result broadcast through smem (2 doubles).
+__device__ __forceinline__ void block_minmax(double &lo, double &hi, double *sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    __syncthreads();
+    if (lane == 0) {
+        sm[2 * warp] = lo;
+        sm[2 * warp + 1] = hi;
+    }
+    __syncthreads();
+    lo = sm[0];
+    hi = sm[1];
+    for (int w = 1; w < kTimeWarps; ++w) {
+        lo = fmin(lo, sm[2 * w]);
+        hi = fmax(hi, sm[2 * w + 1]);
+    }
+    __syncthreads();
+}
+
+// Exact sort of emitter indices by key, by buckets.  The bucket of a key is
+// floor((t - kmin) * NB / (kmax - kmin)), a non-decreasing function of t in
+// IEEE arithmetic, so bucket order is key order; each bucket is then
+// insertion-sorted by (key, emitter index).  Returns false (perm undefined)
+// when a bucket holds more than kMaxBucket keys; the caller then runs the
+// radix sort.  cnt: kBuckets/2 words of packed 16-bit counters.
+constexpr int kBuckets = 8192;
+constexpr int kMaxBucket = 128;
+constexpr int kBucketsPerThread = kBuckets / kTimeThreads;  // 16
+
+__device__ __forceinline__ uint32_t bucket_of(double t, double kmin, double scale) {
+    const int b = __double2int_rz(__dmul_rn(__dsub_rn(t, kmin), scale));
+    return (uint32_t)min(max(b, 0), kBuckets - 1);
+}
+__device__ __forceinline__ uint32_t cnt_get(const uint32_t *cnt, uint32_t b) {
+    const uint32_t w = cnt[b >> 1];
+    return (b & 1) ? (w >> 16) : (w & 0xFFFFu);
+}
+
+__device__ bool bucket_sort(const double *keytab, uint16_t *perm, uint32_t *cnt, int n, double kmin, double kmax,
+                            double *scratch, int *s_flag) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (!(kmax > kmin)) {
+        // all keys equal (or one key): stable order is emitter order
+        for (int m = tid; m < n; m += kTimeThreads) perm[m] = (uint16_t)m;
+        __syncthreads();
+        return true;
+    }
+    const double scale = (double)kBuckets / (kmax - kmin);
+    for (int w = tid; w < kBuckets / 2; w += kTimeThreads) cnt[w] = 0u;
+    if (tid == 0) *s_flag = 0;
+    __syncthreads();
+    for (int j = tid; j < n; j += kTimeThreads) {
+        const uint32_t b = bucket_of(keytab[j], kmin, scale);
+        atomicAdd(&cnt[b >> 1], (b & 1) ? 0x10000u : 1u);
+    }
+    __syncthreads();
+    // exclusive scan of the counters: thread t owns buckets [16t, 16t+16)
+    uint32_t loc[kBucketsPerThread];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < kBucketsPerThread; ++i) {
+        loc[i] = cnt_get(cnt, tid * kBucketsPerThread + i);
+        sum += loc[i];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    uint32_t *wsum = reinterpret_cast<uint32_t *>(scratch);  // 16 words
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t run = incl - sum;
+    for (int w = 0; w < warp; ++w) run += wsum[w];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kBucketsPerThread; i += 2) {
+        const uint32_t s0 = run, s1 = run + loc[i];
+        cnt[(tid * kBucketsPerThread + i) >> 1] = s0 | (s1 << 16);
+        if (loc[i] > kMaxBucket || loc[i + 1] > kMaxBucket) *s_flag = 1;
+        run = s1 + loc[i + 1];
+    }
+    __syncthreads();
+    if (*s_flag) return false;  // uniform: every thread read the same flag after the barrier
+    // scatter: afterwards cnt holds the end (= next start) of every bucket
+    for (int j = tid; j < n; j += kTimeThreads) {
+        const uint32_t b = bucket_of(keytab[j], kmin, scale);
+        const uint32_t old = atomicAdd(&cnt[b >> 1], (b & 1) ? 0x10000u : 1u);
+        perm[(b & 1) ? (old >> 16) : (old & 0xFFFFu)] = (uint16_t)j;
+    }
+    __syncthreads();
+    // insertion sort inside each bucket by (key, emitter index)
+    for (int i = 0; i < kBucketsPerThread; ++i) {
+        const uint32_t b = tid * kBucketsPerThread + i;
+        const int start = b == 0 ? 0 : (int)cnt_get(cnt, b - 1);
+        const int end = (int)cnt_get(cnt, b);
+        for (int m = start + 1; m < end; ++m) {
+            const uint16_t v = perm[m];
+            const double kv = keytab[v];
+            int q = m - 1;
+            while (q >= start) {
+                const uint16_t u = perm[q];
+                const double ku = keytab[u];
+                if (ku < kv || (ku == kv && u < v)) break;
+                perm[q + 1] = u;
+                --q;
+            }
+            perm[q + 1] = v;
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
+// Stable LSD radix sort (8 passes of 8 bits) of emitter indices by the
+// order-preserving 64-bit image of their keys; the fallback of bucket_sort.
+// Keys of positions >= n are +inf and stay at the end.
+__device__ void radix_sort(const double *keytab, uint16_t *perm, uint32_t *H, uint32_t *base) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int S = 32 * kTimeIPT;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint16_t idx[kTimeIPT];
+#pragma unroll
+    for (int i = 0; i < kTimeIPT; ++i) idx[i] = (uint16_t)(warp * S + i * 32 + lane);
+    __syncthreads();
+    for (int pass = 0; pass < 8; ++pass) {
+        const int shift = pass * 8;
+        uint32_t *Hw = H + warp * 256;
+        for (int k = lane; k < 256; k += 32) Hw[k] = 0;
+        __syncwarp();
+        for (int i = 0; i < kTimeIPT; ++i) {
+            const uint32_t dg = (uint32_t)(sortable(keytab[idx[i]]) >> shift) & 255u;
+            const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+            if ((peers & lt_mask) == 0) Hw[dg] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        if (tid < 256) {
+            uint32_t run = 0;
+            for (int w = 0; w < kTimeWarps; ++w) {
+                const uint32_t h = H[w * 256 + tid];
+                H[w * 256 + tid] = run;
+                run += h;
+            }
+            base[tid] = run;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t v[8], sum = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                v[k] = base[lane * 8 + k];
+                sum += v[k];
+            }
+            uint32_t incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            uint32_t run = incl - sum;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                base[lane * 8 + k] = run;
+                run += v[k];
+            }
+        }
+        __syncthreads();
+        for (int k = lane; k < 256; k += 32) Hw[k] += base[k];
+        __syncwarp();
+        for (int i = 0; i < kTimeIPT; ++i) {
+            const uint32_t dg = (uint32_t)(sortable(keytab[idx[i]]) >> shift) & 255u;
+            const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+            const uint32_t b0 = Hw[dg];
+            const uint32_t rank = b0 + __popc(peers & lt_mask);
+            __syncwarp();
+            if ((peers & lt_mask) == 0) Hw[dg] = b0 + __popc(peers);
+            __syncwarp();
+            perm[rank] = idx[i];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kTimeIPT; ++i) idx[i] = perm[warp * S + i * 32 + lane];
+        __syncthreads();
+    }
+}
+
 template <bool NF, bool SCALE>
 __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams g, const double *__restrict__ atoms,
                                                                 const double *__restrict__ times, int n, double c,
@@ -100,12 +309,10 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
     uint32_t *H = reinterpret_cast<uint32_t *>(smem + (size_t)kTimeMaxN * 10);
     uint32_t *base = H + kTimeWarps * 256;
     double *scratch = reinterpret_cast<double *>(base + 256);  // 128 doubles
-    __shared__ int s_pix;
+    __shared__ int s_pix, s_flag;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int npix = g.nx * g.ny;
-    const int S = 32 * kTimeIPT;  // elements per warp segment
-    const uint32_t lt_mask = (1u << lane) - 1u;
 
     // order_pixel >= 0: process that one pixel only, record its sorted order
     // and write its intensity to out[0]
@@ -124,89 +331,26 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
         // time.py:89-91 (np.linalg.norm = sqrt((x*x + y*y) + z*z); q = det/d; q_z -= 1)
         const double dn = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
         const double q0 = __ddiv_rn(dx, dn), q1 = __ddiv_rn(dy, dn), q2 = __dsub_rn(__ddiv_rn(dz, dn), 1.0);
+        // the scan's exponents use a multiply by 1/tau (1 ulp from the reference's
+        // division, ~1e-16 relative in the decay); only the sort keys must match bit for bit
+        const double inv_tau = 1.0 / tau;
 
         // ---- keys: table by emitter index, +inf padding ----
+        double kmin = __longlong_as_double(0x7FF0000000000000ll), kmax = -kmin;
         for (int j = tid; j < kTimeMaxN; j += kTimeThreads) {
             double t = __longlong_as_double(0x7FF0000000000000ll);  // +inf
             if (j < n) {
                 const double4 a = reinterpret_cast<const double4 *>(atoms)[j];
                 double s, dist;
                 arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, t, s, dist);
+                kmin = fmin(kmin, t);
+                kmax = fmax(kmax, t);
             }
             keytab[j] = t;
         }
-        // initial order: warp segment layout, element (i, lane) of warp w at
-        // position w*S + i*32 + lane holds emitter w*S + i*32 + lane
-        uint16_t idx[kTimeIPT];
-#pragma unroll
-        for (int i = 0; i < kTimeIPT; ++i) idx[i] = (uint16_t)(warp * S + i * 32 + lane);
-        __syncthreads();
-
-        for (int pass = 0; pass < 8; ++pass) {
-            const int shift = pass * 8;
-            uint32_t *Hw = H + warp * 256;
-            for (int k = lane; k < 256; k += 32) Hw[k] = 0;
-            __syncwarp();
-            // phase 1: per-warp digit histogram
-#pragma unroll 4
-            for (int i = 0; i < kTimeIPT; ++i) {
-                const uint32_t dg = (uint32_t)(sortable(keytab[idx[i]]) >> shift) & 255u;
-                const uint32_t peers = __match_any_sync(0xffffffffu, dg);
-                if ((peers & lt_mask) == 0) Hw[dg] += __popc(peers);
-                __syncwarp();
-            }
-            __syncthreads();
-            // digit totals and exclusive prefix over warps, then over digits
-            if (tid < 256) {
-                uint32_t run = 0;
-                for (int w = 0; w < kTimeWarps; ++w) {
-                    const uint32_t h = H[w * 256 + tid];
-                    H[w * 256 + tid] = run;
-                    run += h;
-                }
-                base[tid] = run;
-            }
-            __syncthreads();
-            if (warp == 0) {
-                // exclusive scan of 256 digit totals, 8 per lane
-                uint32_t v[8], sum = 0;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    v[k] = base[lane * 8 + k];
-                    sum += v[k];
-                }
-                uint32_t incl = sum;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += y;
-                }
-                uint32_t run = incl - sum;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    base[lane * 8 + k] = run;
-                    run += v[k];
-                }
-            }
-            __syncthreads();
-            for (int k = lane; k < 256; k += 32) Hw[k] += base[k];
-            __syncwarp();
-            // phase 2: stable scatter of indices
-#pragma unroll 4
-            for (int i = 0; i < kTimeIPT; ++i) {
-                const uint32_t dg = (uint32_t)(sortable(keytab[idx[i]]) >> shift) & 255u;
-                const uint32_t peers = __match_any_sync(0xffffffffu, dg);
-                const uint32_t b0 = Hw[dg];
-                const uint32_t rank = b0 + __popc(peers & lt_mask);
-                __syncwarp();
-                if ((peers & lt_mask) == 0) Hw[dg] = b0 + __popc(peers);
-                __syncwarp();
-                perm[rank] = idx[i];
-            }
-            __syncthreads();
-#pragma unroll
-            for (int i = 0; i < kTimeIPT; ++i) idx[i] = perm[warp * S + i * 32 + lane];
-            __syncthreads();
+        block_minmax(kmin, kmax, scratch + 96);
+        if (!bucket_sort(keytab, perm, reinterpret_cast<uint32_t *>(H), n, kmin, kmax, scratch, &s_flag)) {
+            radix_sort(keytab, perm, H, base);
         }
         // perm[m] = emitter at sorted position m (positions >= n hold padding)
 
@@ -217,23 +361,41 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
             }
         }
 
-        // ---- decaying scan over the sorted sequence (blocked: thread owns
-        //      positions [tid*IPT, tid*IPT + IPT)) ----
+        // ---- decaying scan over the sorted sequence, one pass ----
+        // Thread t owns positions [40t, 40t+40).  Inside its run
+        //   x_m = D_m X + B_m,  D_m = prod of the run's decays up to m,
+        // with X the value entering the run (known only after the block scan),
+        // so sum_m w_m |x_m|^2 = |X|^2 S1 + 2 Re(X conj(S2)) + S3 with
+        //   S1 = sum w D^2, S2 = sum w D B, S3 = sum w |B|^2
+        // and w_m = -tau/2 expm1(-2 (t_{m+1} - t_m)/tau), w_{n-1} = tau/2
+        // (the interval integral of time.py:36-45).
         const int m0 = tid * kTimeIPT;
-        Affine agg = {1.0, 0.0, 0.0};
+        double Dm = 1.0, Br = 0.0, Bi = 0.0;
+        double S1 = 0.0, S2r = 0.0, S2i = 0.0, S3 = 0.0;
         for (int i = 0; i < kTimeIPT; ++i) {
             const int m = m0 + i;
             if (m >= n) break;
             const int j = perm[m];
+            const double tj = keytab[j];
             const double4 a = reinterpret_cast<const double4 *>(atoms)[j];
-            double t, s, dist, re, im;
-            arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, t, s, dist);
+            double s, dist, re, im;
+            path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
             amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
-            const double dec = m == 0 ? 0.0 : exp(__ddiv_rn(-__dsub_rn(keytab[j], keytab[perm[m - 1]]), tau));
-            const Affine e = {dec, re, im};
-            agg = compose(agg, e);
+            const double dec = m == 0 ? 0.0 : exp(-__dsub_rn(tj, keytab[perm[m - 1]]) * inv_tau);
+            Dm *= dec;
+            Br = fma(dec, Br, re);
+            Bi = fma(dec, Bi, im);
+            const double w = m < n - 1
+                                 ? (-tau / 2) * expm1(-2 * __dsub_rn(keytab[perm[m + 1]], tj) * inv_tau)
+                                 : tau / 2;
+            const double wD = w * Dm;
+            S1 = fma(wD, Dm, S1);
+            S2r = fma(wD, Br, S2r);
+            S2i = fma(wD, Bi, S2i);
+            S3 = fma(w, fma(Br, Br, Bi * Bi), S3);
         }
-        // block exclusive scan of aggregates
+        const Affine agg = {Dm, Br, Bi};
+        // block exclusive scan of the run maps
         Affine incl = agg;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -260,33 +422,9 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
         excl.bi = __shfl_up_sync(0xffffffffu, incl.bi, 1);
         if (lane == 0) excl = Affine{1.0, 0.0, 0.0};
         excl = compose(wpre, excl);
-        // x entering this thread's run = excl applied to x_{-1} = 0
-        double xr = excl.br, xi = excl.bi;
-        double part = 0.0;
-        for (int i = 0; i < kTimeIPT; ++i) {
-            const int m = m0 + i;
-            if (m >= n) break;
-            const int j = perm[m];
-            const double4 a = reinterpret_cast<const double4 *>(atoms)[j];
-            double t, s, dist, re, im;
-            arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, t, s, dist);
-            amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
-            if (m == 0) {
-                xr = re;
-                xi = im;
-            } else {
-                const double dec = exp(__ddiv_rn(-__dsub_rn(keytab[j], keytab[perm[m - 1]]), tau));
-                xr = __dadd_rn(re, __dmul_rn(dec, xr));
-                xi = __dadd_rn(im, __dmul_rn(dec, xi));
-            }
-            const double I = __dadd_rn(__dmul_rn(xi, xi), __dmul_rn(xr, xr));
-            if (m < n - 1) {
-                const double td = __dsub_rn(keytab[perm[m + 1]], keytab[j]);
-                part += __dmul_rn(__dmul_rn(-tau / 2, I), expm1(__ddiv_rn(-2 * td, tau)));
-            } else {
-                part += tau / 2 * I;
-            }
-        }
+        // X entering this thread's run = excl applied to x_{-1} = 0
+        const double Xr = excl.br, Xi = excl.bi;
+        double part = fma(fma(Xr, Xr, Xi * Xi), S1, fma(2.0, fma(Xr, S2r, Xi * S2i), S3));
         // block sum
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);

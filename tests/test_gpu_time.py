@@ -102,3 +102,26 @@ def test_cutime_reference_api_shape():
     assert res.shape == (4, 4) and res.dtype == np.float64
     gen = cutime.simulate_gen(obj, 4, 10, 1000, obj.k, 1.0, 1.0, 1.0, maximg=2)
     assert len(list(gen)) == 2
+
+
+def test_time_sort_fallback_and_degenerate_keys():
+    """Keys that defeat the bucket sort (one far outlier puts every other key
+    in one bucket -> radix fallback) and all-equal keys keep the exact order."""
+    g0 = rng(101)
+    n = 5000
+    at = atoms(sphere(g0, n, 0.01), g0.uniform(0, 2 * np.pi, n))
+    geom = _core.make_geom([3, 2], 75.0, 1e5, K64)
+    og = oracle.geometry([3, 2], 75.0, 1e5, K64)
+    times = np.zeros(n)
+    times[1234] = 1e6
+    for tt in (times, np.zeros(n)):
+        for ix, iy in [(0, 0), (2, 1)]:
+            order, keys = _core.time_order(_gpu(at), _gpu(tt), geom, 0.3, ix, iy)
+            assert np.array_equal(order.cpu().numpy(), oracle.time_order(og, 0, at, tt, 0.3, ix, iy))
+        img = _core.time_forward(_gpu(at), _gpu(tt), geom, 0.3, 2.0).cpu().numpy()
+        ref = oracle.time_image(og, 0, at, tt, 0.3, 2.0)
+        assert np.max(np.abs(img - ref) / np.abs(ref)) < 1e-10
+    # a single emitter
+    one = at[:1]
+    img = _core.time_forward(_gpu(one), _gpu(np.zeros(1)), geom, 0.3, 2.0).cpu().numpy()
+    assert np.allclose(img, oracle.time_image(og, 0, one, np.zeros(1), 0.3, 2.0), rtol=1e-12)
