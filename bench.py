@@ -383,22 +383,32 @@ def extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, 
     v64 = 2 * N_EMIT * NDET * NDET / (ms64 * 1e-3)
     res["fp64"] = {"value": v64, "unit": "pairs/s", "images": 2, "ms": ms64}
 
-    # --- split vs FP64 accuracy on 2 full images
+    # --- accuracy on 2 full images: split and the reference-sequence FP64
+    #     kernel, both against the cancellation-free FP64 kernel ("truth")
     Es = _core.forward(at2, off2, geom, nat.SPLIT, nat.OUT_C128, config=cfg)
     Ed = _core.forward(at2, off2, geom, nat.DOUBLE, nat.OUT_C128)
+    geom_acc = _core.make_geom(NDET, PIXEL, DETZ, k, flags=nat.NF | nat.ACCURATE)
+    Ea = _core.forward(at2, off2, geom_acc, nat.DOUBLE, nat.OUT_C128)
     Is = (Es.real ** 2 + Es.imag ** 2).cpu().numpy()
     Id = (Ed.real ** 2 + Ed.imag ** 2).cpu().numpy()
-    mean = Id.mean()
-    d = np.abs(Is - Id)
-    mask = Id >= 1e-3 * mean
-    rel = d[mask] / Id[mask]
-    hist, edges = np.histogram(np.log10(np.maximum(rel, 1e-12)), bins=np.arange(-12, 0.5, 1.0))
-    res["accuracy_split_vs_fp64"] = {
-        "pixels": int(Id.size), "max_rel_masked": float(rel.max()), "max_rel_to_mean": float(d.max() / mean),
-        "p50": float(np.percentile(rel, 50)), "p99": float(np.percentile(rel, 99)),
-        "p9999": float(np.percentile(rel, 99.99)), "mask": "I_fp64 >= 1e-3 mean",
-        "log10_rel_hist": {f"{int(e)}": int(h) for e, h in zip(edges[:-1], hist)}}
-    del Es, Ed
+    Ia = (Ea.real ** 2 + Ea.imag ** 2).cpu().numpy()
+
+    def stats(I, Iref, name):
+        mean = Iref.mean()
+        d = np.abs(I - Iref)
+        mask = Iref >= 1e-3 * mean
+        rel = d[mask] / Iref[mask]
+        hist, edges = np.histogram(np.log10(np.maximum(rel, 1e-12)), bins=np.arange(-12, 0.5, 1.0))
+        return {"compare": name, "pixels": int(Iref.size), "max_rel_masked": float(rel.max()),
+                "max_rel_to_mean": float(d.max() / mean), "p50": float(np.percentile(rel, 50)),
+                "p99": float(np.percentile(rel, 99)), "p9999": float(np.percentile(rel, 99.99)),
+                "mask": "I_ref >= 1e-3 mean",
+                "log10_rel_hist": {f"{int(e)}": int(h) for e, h in zip(edges[:-1], hist)}}
+
+    res["accuracy_split_vs_fp64"] = stats(Is, Id, "split vs FP64 (reference rounding sequence)")
+    res["accuracy_vs_truth"] = {"split": stats(Is, Ia, "split vs cancellation-free FP64"),
+                                "fp64_reference_sequence": stats(Id, Ia, "FP64 reference sequence vs cancellation-free FP64")}
+    del Es, Ed, Ea
 
     res["fwd_bwd"] = fwd_bwd_leg(torch, dev, _core, nat, timed)
     res["batched_uneven"] = batched_leg(torch, dev, _core, nat)

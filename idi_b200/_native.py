@@ -28,6 +28,7 @@ ERR_UNSUPPORTED = 5
 NF = 1
 SCALE = 2
 SECONDORDER = 4
+ACCURATE = 8
 
 DOUBLE = 0
 SPLIT = 1

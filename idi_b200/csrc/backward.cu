@@ -420,7 +420,7 @@ static idiwf_status bwd_validate(const idiwf_geom *g, const idiwf_batch *b) {
         if (b->offsets[i + 1] < b->offsets[i]) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
     if (b->atoms && (reinterpret_cast<uintptr_t>(b->atoms) & 31))
         return set_error(IDIWF_ERR_INVALID_ARGUMENT, "atoms must be 32-byte aligned");
-    if (g->flags & ~(IDIWF_NF | IDIWF_SCALE | IDIWF_SECONDORDER))
+    if (g->flags & ~(IDIWF_NF | IDIWF_SCALE | IDIWF_SECONDORDER | IDIWF_ACCURATE))
         return set_error(IDIWF_ERR_INVALID_ARGUMENT, "unknown geometry flag");
     return IDIWF_OK;
 }

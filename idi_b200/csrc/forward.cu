@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
 // ---------------------------------------------------------------------------
 // all-FP64 kernel (reference rounding sequence)
 // ---------------------------------------------------------------------------
-template <int PPT, bool NF, bool SCALE, bool SECOND>
+template <int PPT, bool NF, bool SCALE, bool SECOND, bool ACC = false>
 __global__ void __launch_bounds__(256) fwd_double_kernel(const __grid_constant__ BatchParams bp,
                                                          const GeomParams g, DoubleRecs rec,
                                                          void *__restrict__ out, int out_kind,
@@ -470,6 +470,15 @@ __global__ void __launch_bounds__(256) fwd_double_kernel(const __grid_constant__
             qx[i] = __dmul_rn(g.k, __dmul_rn(px[i], rdist[i]));
             qy[i] = __dmul_rn(g.k, __dmul_rn(py[i], rdist[i]));
             c2[i] = __dmul_rn(g.k, rdist[i]) * 0.5;
+            if (ACC) {
+                // accurate near field: the pixel constant k (|d| - d_z) in
+                // turns, without cancellation (reuses the far-field slots)
+                const double rho2 = px[i] * px[i] + py[i] * py[i];
+                const double D = sqrt(rho2 + pz[i] * pz[i]);
+                const double cc = g.kp * (pz[i] > 0 ? rho2 / (D + pz[i]) : D - pz[i]);
+                qx[i] = D;
+                qy[i] = cc - rint(cc);
+            }
         }
         double ax[PPT], ay[PPT], cx[PPT], cy[PPT];
 #pragma unroll
@@ -508,7 +517,15 @@ __global__ void __launch_bounds__(256) fwd_double_kernel(const __grid_constant__
                         const double a = __dsub_rn(px[i], r.x), b = __dsub_rn(py[i], r.y),
                                      c = __dsub_rn(pz[i], r.z);
                         const double dist = __dsqrt_rn(__fma_rn(c, c, __fma_rn(a, a, __dmul_rn(b, b))));
-                        phase = __fma_rn(__dadd_rn(__dsub_rn(dist, pz[i]), r.z), g.k, r.w);
+                        if (ACC) {
+                            // |d-r| - |d| = (|r|^2 - 2 d.r) / (|d-r| + |d|): no cancellation
+                            const double rr = fma(r.z, r.z, fma(r.x, r.x, r.y * r.y));
+                            const double dr = fma(pz[i], r.z, fma(px[i], r.x, py[i] * r.y));
+                            const double delta = (rr - 2.0 * dr) / (dist + qx[i]);
+                            phase = fma(kTwoPi, qy[i], fma(g.k, delta + r.z, r.w));
+                        } else {
+                            phase = __fma_rn(__dadd_rn(__dsub_rn(dist, pz[i]), r.z), g.k, r.w);
+                        }
                         if (SCALE) w = __drcp_rn(dist);
                     } else {
                         // cpu.py:59
@@ -613,7 +630,7 @@ static idiwf_status validate_geom(const idiwf_geom *g) {
         return set_error(IDIWF_ERR_INVALID_ARGUMENT, "k must be positive and finite");
     if (!std::isfinite(g->pixelsize) || !std::isfinite(g->detz))
         return set_error(IDIWF_ERR_INVALID_ARGUMENT, "pixelsize/detz must be finite");
-    if (g->flags & ~(IDIWF_NF | IDIWF_SCALE | IDIWF_SECONDORDER))
+    if (g->flags & ~(IDIWF_NF | IDIWF_SCALE | IDIWF_SECONDORDER | IDIWF_ACCURATE))
         return set_error(IDIWF_ERR_INVALID_ARGUMENT, "unknown geometry flag");
     return IDIWF_OK;
 }
@@ -714,6 +731,9 @@ static void *split_kernel_for(int flags) {
 template <int PPT>
 static void *double_kernel_for(int flags) {
     const bool nf = flags & IDIWF_NF, sc = flags & IDIWF_SCALE, so = flags & IDIWF_SECONDORDER;
+    if (nf && (flags & IDIWF_ACCURATE))
+        return sc ? (void *)fwd_double_kernel<PPT, true, true, false, true>
+                  : (void *)fwd_double_kernel<PPT, true, false, false, true>;
     if (nf) return sc ? (void *)fwd_double_kernel<PPT, true, true, false> : (void *)fwd_double_kernel<PPT, true, false, false>;
     if (so) return sc ? (void *)fwd_double_kernel<PPT, false, true, true> : (void *)fwd_double_kernel<PPT, false, false, true>;
     return sc ? (void *)fwd_double_kernel<PPT, false, true, false> : (void *)fwd_double_kernel<PPT, false, false, false>;

@@ -50,7 +50,8 @@ def parse_settings(settings: str, default_precision: str = "double"):
 
     ``single`` -> split-precision kernel with complex64 output; ``split`` ->
     split-precision kernel with complex128 output; ``double`` (or neither) ->
-    all-FP64 kernel.  ``nf``, ``scale``, ``secondorder`` select the geometry.
+    all-FP64 kernel; ``accurate`` -> all-FP64 kernel with the cancellation-free
+    near-field path difference.  ``nf``, ``scale``, ``secondorder`` select the geometry.
     ``nofast`` and unknown substrings are ignored, as in the reference.
     """
     s = settings or ""
@@ -61,6 +62,9 @@ def parse_settings(settings: str, default_precision: str = "double"):
         flags |= nat.SCALE
     if "secondorder" in s:
         flags |= nat.SECONDORDER
+    if "accurate" in s:
+        # FP64 near field without the reference's |d-r| - d_z cancellation
+        return flags | nat.ACCURATE, nat.DOUBLE, False
     if "split" in s:
         return flags, nat.SPLIT, False
     if "single" in s:

@@ -48,6 +48,8 @@ typedef int32_t idiwf_status;
 #define IDIWF_NF 1          /* "nf": exact spherical path |d - r| (else far field) */
 #define IDIWF_SCALE 2       /* "scale": 1/r amplitude factor */
 #define IDIWF_SECONDORDER 4 /* "secondorder": Fresnel term of sim.cu:88 (far field) */
+#define IDIWF_ACCURATE 8    /* IDIWF_DOUBLE near field: cancellation-free |d-r|-|d| instead of
+                               the reference's rounding sequence (ignored elsewhere) */
 
 /* precision */
 #define IDIWF_DOUBLE 0 /* all-FP64, reproduces the reference CPU rounding sequence */
