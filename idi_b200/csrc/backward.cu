@@ -44,7 +44,7 @@ constexpr int kBwdMaxPE = 8;                     // largest emitters-per-thread 
 
 // pixel record (geometry part, shared by all images):
 //   P64  double4 {-q'x, -q'y, -q'z, 0}   q' = k (dhat - zhat) / 2pi      32 B
-//   PF   float4 x5  {dx,dx,dy,dy} {dz,dz,h,h} {qx,qx,qy,qy} {qz,qz,kap,kap}
+//   PF   float4 x5  {dx,dx,dy,dy} {dz,dz,-h,-h} {qx,qx,qy,qy} {qz,qz,kap,kap}
 //                   {iD,iD,iD2,iD2}   (the last one read in "scale" mode) 80 B
 // per image:
 //   PG   float4 {G'r,G'r,G'i,G'i}   G' = 2 g conj(E) exp(2 pi i C')      16 B
@@ -114,7 +114,7 @@ __global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad
         const double dzm1 = dz > 0 ? -rho2 / (D * (D + dz)) : dz * invD - 1.0;
         p64[p] = make_double4(-g.kp * (dx * invD), -g.kp * (dy * invD), -g.kp * dzm1, 0.0);
         const float fdx = (float)(dx * invD), fdy = (float)(dy * invD), fdz = (float)(dz * invD);
-        const float fh = (float)(g.k * 0.5 * invD);
+        const float fh = (float)(-g.k * 0.5 * invD);  // -h, pairs with the negated w
         const float qx = (float)(g.k * dx * invD), qy = (float)(g.k * dy * invD), qz = (float)(g.k * dzm1);
         const float kap = (float)(g.k * invD);
         const float fi = (float)invD, fi2 = (float)(invD * invD);
@@ -178,7 +178,7 @@ __global__ void bwd_emitter_prep_kernel(const __grid_constant__ BwdParams bp, co
             const double w = w_mode == 1 ? (a.x * a.x + a.y * a.y) + a.z * a.z
                                          : (w_mode == 2 ? a.x * a.x + a.y * a.y : 0.0);
             e64[r] = make_double4(a.x, a.y, a.z, psi);
-            ef[r] = make_float4((float)a.x, (float)a.y, (float)a.z, (float)w);
+            ef[r] = make_float4((float)a.x, (float)a.y, (float)a.z, (float)(-w));  // w negated
         } else {
             e64[r] = make_double4(0, 0, 0, kTurnMagic);
             ef[r] = make_float4(0, 0, 0, 0);
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
                         s = __fmul2_rn(g2(F0.x, F0.y), fx[q]);
                         s = __ffma2_rn(g2(F0.z, F0.w), fy[q], s);
                         s = __ffma2_rn(g2(F1.x, F1.y), fz[q], s);
-                        const float2 w2 = __ffma2_rn(g2(-s.x, -s.y), s, fw[q]);
+                        const float2 w2 = __ffma2_rn(s, s, fw[q]);  // s^2 - |r|^2
                         arg = __ffma2_rn(g2(F1.z, F1.w), w2, arg);
                     } else if (SECOND) {
                         arg = __ffma2_rn(g2(F1.z, F1.w), fw[q], arg);

@@ -45,7 +45,7 @@ namespace idiwf {
 // ---------------------------------------------------------------------------
 // split:  r64 double4 {x, y, z, Psi}              (32 B)  Psi = magic + 1/4 + psi/2pi mod 1
 //         rA  float4  {x, x, y, y}                (16 B)  duplicated for f32x2
-//         rB  float4  {z, z, w, w}                (16 B)  w = |r|^2 (nf) or x^2+y^2
+//         rB  float4  {z, z, -w, -w}              (16 B)  w = |r|^2 (nf) or x^2+y^2
 //         rC  float2  {a, a}                      ( 8 B)
 // double: r64 double4 {x, y, z, psi}, ra double a
 constexpr int kSplitRecBytes = 72;
@@ -119,7 +119,8 @@ __global__ void prep_split_kernel(const __grid_constant__ BatchParams bp, const 
                 record_error(err, kErrRange);
             const double w = w_mode == 1 ? (a.x * a.x + a.y * a.y) + a.z * a.z
                                          : (w_mode == 2 ? a.x * a.x + a.y * a.y : 0.0);
-            const float fx = (float)a.x, fy = (float)a.y, fz = (float)a.z, fw = (float)w;
+            // w is stored negated: the kernel forms s^2 - w and subtracts h times it
+            const float fx = (float)a.x, fy = (float)a.y, fz = (float)a.z, fw = (float)(-w);
             rec.r64[r] = make_double4(a.x, a.y, a.z, psi);
             rec.rA[r] = make_float4(fx, fx, fy, fy);
             rec.rB[r] = make_float4(fz, fz, fw, fw);
@@ -242,7 +243,7 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
             nqx[i] = -g.kp * (dx * invD);
             nqy[i] = -g.kp * (dy * invD);
             nqz[i] = -g.kp * dzm1;
-            const float fh = (float)(g.k * 0.5 * invD);
+            const float fh = (float)(-g.k * 0.5 * invD);  // -h, pairs with the negated w
             const float fdx = (float)(dx * invD), fdy = (float)(dy * invD), fdz = (float)(dz * invD);
             const float fi = (float)invD, fi2 = (float)(invD * invD);
             rd[i] = fi;
@@ -320,11 +321,12 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
                             float2 s = __fmul2_rn(dhx[q], f2(A.x, A.y));
                             s = __ffma2_rn(dhy[q], f2(A.z, A.w), s);
                             s = __ffma2_rn(dhz[q], f2(B.x, B.y), s);
-                            const float2 w2 = __ffma2_rn(f2(-s.x, -s.y), s, f2(B.z, B.w));
+                            // -h (s^2 - |r|^2) = h (|r|^2 - s^2)
+                            const float2 w2 = __ffma2_rn(s, s, f2(B.z, B.w));
                             arg = __ffma2_rn(hh[q], w2, arg);
                             if (SCALE) amp = __fmul2_rn(a2, __ffma2_rn(s, iD2[q], iD[q]));
                         } else if (SECOND) {
-                            arg = __ffma2_rn(hh[q], f2(B.z, B.w), arg);
+                            arg = __ffma2_rn(hh[q], f2(B.z, B.w), arg);  // (-h)(-(x^2+y^2))
                         }
                         amp.x = __uint_as_float(__float_as_uint(amp.x) ^ (lo[0] & 0x80000000u));
                         amp.y = __uint_as_float(__float_as_uint(amp.y) ^ (lo[1] & 0x80000000u));

@@ -94,9 +94,11 @@ void orc_wavefield(const orc_geom *g, int flags, const double *atoms, const doub
                 qy = k * (dety * rdist);
                 c2 = k * rdist / 2.0; /* sim.cu:83 */
             } else if (accurate) {
-                /* |d| - d_z without cancellation: (dx^2+dy^2)/(|d|+d_z) */
+                /* k (|d| - d_z) without cancellation, (dx^2+dy^2)/(|d|+d_z), and
+                 * reduced mod 2pi in turns before it meets the per-emitter phase */
                 D = sqrt((detx * detx + dety * dety) + detz * detz);
-                pconst = k * ((detx * detx + dety * dety) / (D + detz));
+                const double c = k / (2.0 * M_PI) * ((detx * detx + dety * dety) / (D + detz));
+                pconst = 2.0 * M_PI * (c - rint(c));
             }
             double ax = 0, ay = 0, cx = 0, cy = 0;
             for (int64_t j = 0; j < n; j++) {

@@ -217,7 +217,7 @@ def test_accurate_fp64_mode_vs_oracle():
     og = oracle.geometry([40, 30], 50.0, 2e5, K64, (0.01, 0.02), (2e4, -1e4))
     E = _run(at, [0, n], geom, nat.DOUBLE)[0]
     truth = oracle.wavefield(og, oracle.NF | oracle.SCALE | oracle.ACCURATE, at)
-    assert rel_field_err(E, truth) < 1e-11
+    assert rel_field_err(E, truth) < 1e-10
     # the reference-sequence FP64 kernel differs from the truth by its own rounding noise
     E_ref = _run(at, [0, n], _core.make_geom([40, 30], 50.0, 2e5, K64, (0.01, 0.02), (2e4, -1e4),
                                              nat.NF | nat.SCALE), nat.DOUBLE)[0]
