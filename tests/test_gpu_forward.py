@@ -217,7 +217,10 @@ def test_accurate_fp64_mode_vs_oracle():
     og = oracle.geometry([40, 30], 50.0, 2e5, K64, (0.01, 0.02), (2e4, -1e4))
     E = _run(at, [0, n], geom, nat.DOUBLE)[0]
     truth = oracle.wavefield(og, oracle.NF | oracle.SCALE | oracle.ACCURATE, at)
-    assert rel_field_err(E, truth) < 1e-10
+    # with a 2e4 um detector offset the pixel constant k (|d| - d_z) is ~5e7 rad,
+    # so two FP64 evaluations of it differ by ~1e-8 rad (a per-pixel phase)
+    assert rel_field_err(E, truth) < 2e-7
+    assert oracle.intensity_metrics(np.abs(E) ** 2, np.abs(truth) ** 2, floor=0.0)["max_rel_masked"] < 1e-9
     # the reference-sequence FP64 kernel differs from the truth by its own rounding noise
     E_ref = _run(at, [0, n], _core.make_geom([40, 30], 50.0, 2e5, K64, (0.01, 0.02), (2e4, -1e4),
                                              nat.NF | nat.SCALE), nat.DOUBLE)[0]
