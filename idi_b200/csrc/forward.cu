@@ -177,6 +177,53 @@ __device__ __forceinline__ void store_pixel(void *out, int out_kind, int64_t idx
     }
 }
 
+// Final per-pixel step of the split forward: the far-field 1/|d| factor, the
+// near-field constant phase k (|d| - d_z) (left out of the per-pair sum,
+// applied here in FP64 for field outputs), then the store.
+template <bool NF, bool SCALE>
+__device__ __forceinline__ void finish_pixel(const GeomParams &g, int p, double re, double im, void *out,
+                                             int out_kind, int64_t idx) {
+    if ((!NF && SCALE) || (NF && out_kind <= IDIWF_OUT_C64)) {
+        const int ix = p / g.ny, iy = p - ix * g.ny;
+        double dx, dy, dz;
+        pixel_cpu(g, ix, iy, dx, dy, dz);
+        const double rho2 = dx * dx + dy * dy;
+        const double D = sqrt(rho2 + dz * dz);
+        if (!NF && SCALE) {
+            re /= D;
+            im /= D;
+        }
+        if (NF && out_kind <= IDIWF_OUT_C64) {
+            const double c = g.kp * (dz > 0 ? rho2 / (D + dz) : D - dz);
+            double sn, cs;
+            sincospi(2.0 * (c - rint(c)), &sn, &cs);
+            const double r2 = re * cs - im * sn;
+            im = re * sn + im * cs;
+            re = r2;
+        }
+    }
+    store_pixel(out, out_kind, idx, re, im);
+}
+
+// Sum of the emitter-chunk partials of every pixel, in chunk order, then the
+// final per-pixel step.  partials: [ksplit][n_images][npix] double2.
+template <bool NF, bool SCALE>
+__global__ void fwd_finish_kernel(const GeomParams g, const double2 *__restrict__ partials, int ksplit,
+                                  int n_images, void *__restrict__ out, int out_kind) {
+    const int npix = g.nx * g.ny;
+    const int64_t total = (int64_t)n_images * npix;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        double re = 0.0, im = 0.0;
+        for (int c = 0; c < ksplit; ++c) {
+            const double2 v = partials[(int64_t)c * total + t];
+            re += v.x;
+            im += v.y;
+        }
+        finish_pixel<NF, SCALE>(g, (int)(t % npix), re, im, out, out_kind, t);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // split-precision kernel
 // ---------------------------------------------------------------------------
@@ -187,7 +234,8 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
                                                         const GeomParams g, SplitRecs rec,
                                                         void *__restrict__ out, int out_kind,
                                                         WsHeader *__restrict__ hdr,
-                                                        uint64_t *__restrict__ cta_ns) {
+                                                        uint64_t *__restrict__ cta_ns,
+                                                        double2 *__restrict__ partials) {
     static_assert(PPT % 2 == 0, "pixels are processed in f32x2 pairs");
     constexpr int PH = PPT / 2;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -221,15 +269,20 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
         __syncthreads();
         const int unit = s_unit;
         if (unit >= bp.total_units) break;
-        const int img = bp.order[unit / bp.tiles_per_image];
-        const int ptile = unit % bp.tiles_per_image;
+        const int ks = bp.ksplit > 1 ? bp.ksplit : 1;
+        const int chunk = unit % ks;
+        const int pu = unit / ks;
+        const int img = bp.order[pu / bp.tiles_per_image];
+        const int ptile = pu % bp.tiles_per_image;
         const ImageDesc d = bp.img[img];
         const int p0 = ptile * tile_px + tid * PPT;
+        // emitter tiles of this unit: the whole image, or one chunk of it
+        const int tbeg = ks > 1 ? min(chunk * d.tpc, d.ntiles) : 0;
+        const int tend = ks > 1 ? min(tbeg + d.tpc, d.ntiles) : d.ntiles;
 
         // ---- per-pixel constants (FP64 geometry) ----
         double nqx[PPT], nqy[PPT], nqz[PPT];
         float2 dhx[PH], dhy[PH], dhz[PH], hh[PH], iD[PH], iD2[PH];
-        float rd[PPT];
 #pragma unroll
         for (int i = 0; i < PPT; ++i) {
             const int p = min(p0 + i, npix - 1);
@@ -246,7 +299,6 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
             const float fh = (float)(-g.k * 0.5 * invD);  // -h, pairs with the negated w
             const float fdx = (float)(dx * invD), fdy = (float)(dy * invD), fdz = (float)(dz * invD);
             const float fi = (float)invD, fi2 = (float)(invD * invD);
-            rd[i] = fi;
             if (i & 1) {
                 dhx[i / 2].y = fdx; dhy[i / 2].y = fdy; dhz[i / 2].y = fdz;
                 hh[i / 2].y = fh; iD[i / 2].y = fi; iD2[i / 2].y = fi2;
@@ -260,12 +312,12 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
 #pragma unroll
         for (int i = 0; i < PPT; ++i) sre[i] = cre[i] = sim[i] = cim[i] = 0.0f;
 
-        const int nt = d.ntiles;
+        const int nt = tend - tbeg;
         if (tid == 0) {
             for (int s = 0; s < 2 && s < nt; ++s) {
                 const uint32_t slot = issued & 1;
                 unsigned char *st = smem + slot * stage_bytes;
-                const int64_t r0 = d.rec + (int64_t)s * TE;
+                const int64_t r0 = d.rec + (int64_t)(tbeg + s) * TE;
                 mbar_arrive_expect_tx(&bar[slot], stage_bytes);
                 bulk_g2s(st, rec.r64 + r0, TE * 32, &bar[slot]);
                 bulk_g2s(st + TE * 32, rec.rA + r0, TE * 16, &bar[slot]);
@@ -365,7 +417,7 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
             if (tid == 0 && it + 2 < nt) {
                 const uint32_t slot2 = issued & 1;
                 unsigned char *st2 = smem + slot2 * stage_bytes;
-                const int64_t r0 = d.rec + (int64_t)(it + 2) * TE;
+                const int64_t r0 = d.rec + (int64_t)(tbeg + it + 2) * TE;
                 mbar_arrive_expect_tx(&bar[slot2], stage_bytes);
                 bulk_g2s(st2, rec.r64 + r0, TE * 32, &bar[slot2]);
                 bulk_g2s(st2 + TE * 32, rec.rA + r0, TE * 16, &bar[slot2]);
@@ -381,28 +433,12 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
         for (int i = 0; i < PPT; ++i) {
             const int p = p0 + i;
             if (p < npix) {
-                double re = (double)sre[i] - (double)cre[i];
-                double im = (double)sim[i] - (double)cim[i];
-                if (!NF && SCALE) {
-                    re *= rd[i];
-                    im *= rd[i];
-                }
-                if (NF && out_kind <= IDIWF_OUT_C64) {
-                    // the pixel's constant phase k (|d| - d_z), left out of the
-                    // per-pair sum, applied once here in FP64
-                    const int ix = p / g.ny, iy = p - ix * g.ny;
-                    double dx, dy, dz;
-                    pixel_cpu(g, ix, iy, dx, dy, dz);
-                    const double rho2 = dx * dx + dy * dy;
-                    const double D = sqrt(rho2 + dz * dz);
-                    const double c = g.kp * (dz > 0 ? rho2 / (D + dz) : D - dz);
-                    double sn, cs;
-                    sincospi(2.0 * (c - rint(c)), &sn, &cs);
-                    const double r2 = re * cs - im * sn;
-                    im = re * sn + im * cs;
-                    re = r2;
-                }
-                store_pixel(out, out_kind, obase + p, re, im);
+                const double re = (double)sre[i] - (double)cre[i];
+                const double im = (double)sim[i] - (double)cim[i];
+                if (ks > 1)
+                    partials[((int64_t)chunk * bp.n_images + img) * npix + p] = make_double2(re, im);
+                else
+                    finish_pixel<NF, SCALE>(g, p, re, im, out, out_kind, obase + p);
             }
         }
     }
@@ -587,7 +623,6 @@ __global__ void __launch_bounds__(256) fwd_double_kernel(const __grid_constant__
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-typedef void (*KernelFn)(BatchParams, GeomParams, SplitRecs, void *, int, WsHeader *, uint64_t *);
 
 struct LaunchShape {
     int threads, ppt, te, ctas_per_sm;
@@ -695,8 +730,8 @@ static idiwf_status resolve_shape(const idiwf_geom *g, const idiwf_batch *b, int
     if (precision == IDIWF_SPLIT) {
         if (s.ppt != 2 && s.ppt != 4 && s.ppt != 8)
             return set_error(IDIWF_ERR_INVALID_ARGUMENT, "split pixels_per_thread must be 2, 4 or 8");
-        if (s.te < kFold || s.te > 1024 || s.te % kFold)
-            return set_error(IDIWF_ERR_INVALID_ARGUMENT, "split emitters_per_tile must be a multiple of 64 in [64,1024]");
+        if (s.te < kFold || s.te > kChunkEmitters || (s.te & (s.te - 1)))
+            return set_error(IDIWF_ERR_INVALID_ARGUMENT, "split emitters_per_tile must be a power of two in [64,1024]");
     } else {
         if (s.ppt != 1 && s.ppt != 2 && s.ppt != 4)
             return set_error(IDIWF_ERR_INVALID_ARGUMENT, "double pixels_per_thread must be 1, 2 or 4");
@@ -717,9 +752,32 @@ static int64_t total_records(const idiwf_batch *b, int te) {
     return t;
 }
 
-static size_t forward_ws_bytes(const idiwf_batch *b, int precision, const LaunchShape &s) {
+// Emitter chunks per (image, pixel tile) for the split kernel: 1 when the
+// batch has pixel tiles for at least 3/4 of one wave of CTA slots (two per
+// SM), else about two waves' worth of units.  Depends only on the problem and
+// the SM count (not on the kernel shape), so the summation order is the same
+// for every shape.
+static int choose_ksplit(const idiwf_geom *g, const idiwf_batch *b) {
+    const int npix = g->nx * g->ny;
+    const int64_t base = (int64_t)std::min(b->n_images, kMaxImagesPerLaunch) * ((npix + 1023) / 1024);
+    const int64_t slots = 2 * (int64_t)sm_count();
+    if (4 * base >= 3 * slots) return 1;
+    int64_t nmax = 0;
+    for (int i = 0; i < b->n_images; ++i) nmax = std::max<int64_t>(nmax, b->offsets[i + 1] - b->offsets[i]);
+    int64_t k = (2 * slots + base / 2) / base;
+    k = std::min<int64_t>(k, (nmax + kChunkEmitters - 1) / kChunkEmitters);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(k, 64));
+}
+
+static size_t partials_bytes(const idiwf_geom *g, const idiwf_batch *b, int ksplit) {
+    if (ksplit <= 1) return 0;
+    return align256((size_t)ksplit * std::min(b->n_images, kMaxImagesPerLaunch) * g->nx * g->ny * 16);
+}
+
+static size_t forward_ws_bytes(const idiwf_geom *g, const idiwf_batch *b, int precision, const LaunchShape &s) {
     const int64_t nrec = std::max<int64_t>(total_records(b, s.te), 1);
-    return kWsDataOffset + (precision == IDIWF_SPLIT ? split_recs_bytes(nrec) : double_recs_bytes(nrec));
+    if (precision != IDIWF_SPLIT) return kWsDataOffset + double_recs_bytes(nrec);
+    return kWsDataOffset + split_recs_bytes(nrec) + partials_bytes(g, b, choose_ksplit(g, b));
 }
 
 // kernel table ---------------------------------------------------------------
@@ -770,7 +828,7 @@ static idiwf_status ensure_smem(void *fn, size_t bytes) {
 static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, int precision,
                                  int out_kind, void *out, void *ws, const LaunchShape &s,
                                  int i0, int i1, const std::vector<int64_t> &rec_base, int64_t nrec,
-                                 cudaStream_t stream) {
+                                 int ksplit, cudaStream_t stream) {
     const GeomParams g = make_geom(geom);
     const int npix = geom->nx * geom->ny;
     const int tile_px = s.threads * s.ppt;
@@ -779,7 +837,9 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
     bp.n_images = i1 - i0;
     bp.tiles_per_image = (npix + tile_px - 1) / tile_px;
     bp.te = s.te;
-    bp.total_units = bp.n_images * bp.tiles_per_image;
+    if (precision != IDIWF_SPLIT) ksplit = 1;
+    bp.ksplit = ksplit;
+    bp.total_units = bp.n_images * bp.tiles_per_image * ksplit;
     int max_tiles = 0;
     std::vector<int> ord(bp.n_images);
     for (int i = 0; i < bp.n_images; ++i) {
@@ -788,6 +848,8 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
         bp.img[i].rec = rec_base[i0 + i];
         bp.img[i].n = (int32_t)n;
         bp.img[i].ntiles = (int32_t)((n + s.te - 1) / s.te);
+        const int64_t nblk = (n + kChunkEmitters - 1) / kChunkEmitters;
+        bp.img[i].tpc = (int32_t)((nblk + ksplit - 1) / ksplit * (kChunkEmitters / s.te));
         max_tiles = std::max(max_tiles, bp.img[i].ntiles);
         ord[i] = i;
     }
@@ -823,8 +885,26 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
     const int grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * s.ctas_per_sm), kMaxCtas);
     if (precision == IDIWF_SPLIT) {
         SplitRecs rec = split_recs(ws, nrec);
-        void *args[] = {&bp, (void *)&g, &rec, &out_chunk, &out_kind, &hdr, &cta_ns};
+        double2 *partials = ksplit > 1 ? reinterpret_cast<double2 *>(static_cast<char *>(ws) + kWsDataOffset +
+                                                                     split_recs_bytes(nrec))
+                                       : nullptr;
+        void *args[] = {&bp, (void *)&g, &rec, &out_chunk, &out_kind, &hdr, &cta_ns, &partials};
         IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
+        if (ksplit > 1) {
+            const int64_t total = (int64_t)bp.n_images * npix;
+            const int blocks = (int)std::min<int64_t>((total + 255) / 256, 8 * (int64_t)sm_count());
+            const bool nf = geom->flags & IDIWF_NF, sc = geom->flags & IDIWF_SCALE;
+            if (nf)
+                fwd_finish_kernel<true, false><<<blocks, 256, 0, stream>>>(g, partials, ksplit, bp.n_images,
+                                                                           out_chunk, out_kind);
+            else if (sc)
+                fwd_finish_kernel<false, true><<<blocks, 256, 0, stream>>>(g, partials, ksplit, bp.n_images,
+                                                                           out_chunk, out_kind);
+            else
+                fwd_finish_kernel<false, false><<<blocks, 256, 0, stream>>>(g, partials, ksplit, bp.n_images,
+                                                                            out_chunk, out_kind);
+            IDIWF_CUDA_CHECK(cudaGetLastError());
+        }
     } else {
         DoubleRecs rec = double_recs(ws, nrec);
         void *args[] = {&bp, (void *)&g, &rec, &out_chunk, &out_kind, &hdr, &cta_ns};
@@ -836,7 +916,7 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
 static idiwf_status forward_impl(const idiwf_geom *geom, const idiwf_batch *b, int precision,
                                  int out_kind, void *out, void *ws, size_t ws_bytes,
                                  const LaunchShape &s, cudaStream_t stream) {
-    const size_t need = forward_ws_bytes(b, precision, s);
+    const size_t need = forward_ws_bytes(geom, b, precision, s);
     if (!ws || ws_bytes < need)
         return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_forward_workspace_size()");
     if (reinterpret_cast<uintptr_t>(ws) & 255) return set_error(IDIWF_ERR_WORKSPACE, "workspace must be 256-byte aligned");
@@ -849,9 +929,11 @@ static idiwf_status forward_impl(const idiwf_geom *geom, const idiwf_batch *b, i
     // reset the work counter and the error word: errors reported by
     // idiwf_workspace_error() are those of the most recent call
     IDIWF_CUDA_CHECK(cudaMemsetAsync(ws, 0, 2 * sizeof(uint32_t), stream));
+    const int ksplit = precision == IDIWF_SPLIT ? choose_ksplit(geom, b) : 1;
     for (int i0 = 0; i0 < b->n_images; i0 += kMaxImagesPerLaunch) {
         const int i1 = std::min(b->n_images, i0 + kMaxImagesPerLaunch);
-        idiwf_status st = launch_chunk(geom, b, precision, out_kind, out, ws, s, i0, i1, rec_base, nrec, stream);
+        idiwf_status st =
+            launch_chunk(geom, b, precision, out_kind, out, ws, s, i0, i1, rec_base, nrec, ksplit, stream);
         if (st != IDIWF_OK) return st;
     }
     return IDIWF_OK;
@@ -870,7 +952,7 @@ extern "C" size_t idiwf_forward_workspace_size(const idiwf_geom *geom, const idi
     if (resolve_shape(geom, batch, precision, cfg, s) != IDIWF_OK) return 0;
     LaunchShape big = s;
     big.te = 1024;
-    return std::max(forward_ws_bytes(batch, precision, s), forward_ws_bytes(batch, precision, big));
+    return std::max(forward_ws_bytes(geom, batch, precision, s), forward_ws_bytes(geom, batch, precision, big));
 }
 
 extern "C" idiwf_status idiwf_forward(const idiwf_geom *geom, const idiwf_batch *batch, int32_t precision,
@@ -934,7 +1016,7 @@ extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *ba
     float best_ms = 1e30f;
     LaunchShape best_s = default_shape(precision);
     for (const LaunchShape &s : cands) {
-        if (forward_ws_bytes(batch, precision, s) > workspace_bytes) continue;
+        if (forward_ws_bytes(geom, batch, precision, s) > workspace_bytes) continue;
         st = forward_impl(geom, batch, precision, out_kind, out, workspace, workspace_bytes, s, stream);
         if (st != IDIWF_OK) break;
         float ms_best = 1e30f;
@@ -1082,7 +1164,8 @@ extern "C" idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiw
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * s.ctas_per_sm),
                                             kMaxCtas);
-    void *args[] = {&bp, (void *)&g, &rec, &out, &out_kind, &hdr, &cta_ns};
+    double2 *no_partials = nullptr;  // bp.ksplit == 0: the kernel writes the outputs itself
+    void *args[] = {&bp, (void *)&g, &rec, &out, &out_kind, &hdr, &cta_ns, &no_partials};
     IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
     return IDIWF_OK;
 }

@@ -66,16 +66,24 @@ struct ImageDesc {
     int64_t rec;    // first record of the image in the padded record arrays
     int32_t n;      // emitters
     int32_t ntiles; // record tiles (n rounded up to the tile size)
+    int32_t tpc;    // record tiles per emitter chunk (split over emitters)
+    int32_t pad;
 };
 
 struct BatchParams {
     int32_t n_images;
     int32_t tiles_per_image;  // pixel tiles per image
     int32_t te;               // emitters per tile
-    int32_t total_units;      // n_images * tiles_per_image
+    int32_t total_units;      // n_images * tiles_per_image * ksplit
+    int32_t ksplit;           // emitter chunks per (image, pixel tile); 0 or 1 = none
+    int32_t pad;
     ImageDesc img[kMaxImagesPerLaunch];
     uint16_t order[kMaxImagesPerLaunch];  // images by descending emitter count
 };
+
+// Emitters per chunk are a multiple of this, so chunk boundaries -- and with
+// them the summation order -- do not depend on the kernel shape.
+constexpr int kChunkEmitters = 1024;
 
 GeomParams make_geom(const idiwf_geom *g);
 
