@@ -53,13 +53,30 @@ def _amplitude_rows(amplitudes, n_img, N, start):
     return a[start:start + n_img].reshape(-1)
 
 
-class _Stager:
-    """Pinned host staging of emitter blocks and their upload."""
+_PINNED = {}
 
-    def __init__(self, N, max_imgs, device):
+
+def _pinned(key, nbytes):
+    """Cached pinned host buffer (grow-only), reused across calls."""
+    buf = _PINNED.get(key)
+    if buf is None or buf.numel() < nbytes:
+        buf = torch.empty(int(nbytes), dtype=torch.uint8, pin_memory=True)
+        _PINNED[key] = buf
+    return buf
+
+
+class _Stager:
+    """Pinned host staging of emitter blocks and their upload.  With a `key`,
+    the pinned buffer comes from a cache reused across calls."""
+
+    def __init__(self, N, max_imgs, device, key=None):
         self.N = N
         self.device = device
-        self.host = torch.empty((max_imgs * N, 4), dtype=torch.float64, pin_memory=True)
+        if key is None:
+            self.host = torch.empty((max_imgs * N, 4), dtype=torch.float64, pin_memory=True)
+        else:
+            raw = _pinned(key, max_imgs * N * 32)
+            self.host = raw[: max_imgs * N * 32].view(torch.float64).view(max_imgs * N, 4)
         self.hnp = self.host.numpy()
 
     def fill(self, simobject, n_img):
@@ -149,40 +166,93 @@ def simulate(
     """``Nimg`` simulated wavefields, complex128 array (Nimg, Nx, Ny).
 
     Mirrors ``idi/simulation/cuda.py:141-202``: images are drawn from
-    ``simobject.get2()`` in order; all images of a chunk run in one
-    persistent GPU launch.  Ctrl-C returns the images finished so far.
+    ``simobject.get2()`` in order and run in batched persistent launches.
+    With host output, the images are processed in up to four chunks whose
+    device-to-host copies (into pinned staging, on a second stream) overlap
+    the next chunk's kernel.  Ctrl-C returns the images finished so far.
     """
     Ndet, geom, precision, out_kind = _setup(simobject, Ndet, pixelsize, detz, k, settings, detangles, detoffset)
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     N = int(simobject.N)
     Nimg = int(Nimg)
-    per_img = Ndet[0] * Ndet[1] * 16
-    chunk = int(max(1, min(Nimg, _MAX_OUT_BYTES // max(per_img, 1))))
-    stager = _Stager(N, chunk, dev)
+    npix = Ndet[0] * Ndet[1]
+    elem = 8 if out_kind == nat.OUT_C64 else 16
+    per_img = npix * elem
+    cap = int(max(1, _MAX_OUT_BYTES // max(per_img, 1)))
+    # enough chunks to overlap copies with compute when the output is large
+    nchunks = 4 if (per_img * Nimg >= (64 << 20) and Nimg >= 4) else 1
+    chunk = int(max(1, min(cap, -(-Nimg // nchunks))))
+    done = 0
     if returngpu:
         result = torch.empty((Nimg, Ndet[0], Ndet[1]), dtype=torch.complex128, device=dev)
-    else:
-        result = np.empty((Nimg, Ndet[0], Ndet[1]), np.complex128)
-    done = 0
+        stager = _Stager(N, chunk, dev)
+        try:
+            while done < Nimg:
+                nb = min(chunk, Nimg - done)
+                d_atoms = stager.fill(simobject, nb)
+                amps = _upload_amps(_amplitude_rows(amplitudes, nb, N, done), dev)
+                offsets = np.arange(nb + 1, dtype=np.int64) * N
+                result[done:done + nb] = _core.forward(d_atoms, offsets, geom, precision, out_kind, amplitudes=amps)
+                done += nb
+                if verbose:
+                    print(done, end=". ", flush=True)
+            return result
+        except KeyboardInterrupt:
+            if verbose:
+                print("Interrupted")
+            return result[:done]
+
+    result = np.empty((Nimg, Ndet[0], Ndet[1]), np.complex128)
+    compute = torch.cuda.current_stream(dev)
+    copy = torch.cuda.Stream(dev)
+    dtype = torch.complex64 if out_kind == nat.OUT_C64 else torch.complex128
+    stagers = [_Stager(N, chunk, dev, ("sim_in", dev.index, i)) for i in range(2)]
+    d_out = [torch.empty((chunk, Ndet[0], Ndet[1]), dtype=dtype, device=dev) for _ in range(2)]
+    h_raw = [_pinned(("sim_out", dev.index, i), chunk * per_img) for i in range(2)]
+    h_out = [h[: chunk * per_img].view(dtype).view(chunk, Ndet[0], Ndet[1]) for h in h_raw]
+    ev_done = [torch.cuda.Event(), torch.cuda.Event()]
+    ev_copied = [torch.cuda.Event(), torch.cuda.Event()]
+    ev_h2d = [None, None]
+    pending = None  # (slot, start, count) of the chunk whose copy is in flight
     try:
+        i = 0
         while done < Nimg:
+            slot = i & 1
             nb = min(chunk, Nimg - done)
-            d_atoms = stager.fill(simobject, nb)
+            if ev_h2d[slot] is not None:
+                ev_h2d[slot].synchronize()  # staging buffer free again
+            d_atoms = stagers[slot].fill(simobject, nb)
+            ev_h2d[slot] = torch.cuda.Event()
+            ev_h2d[slot].record(compute)
             amps = _upload_amps(_amplitude_rows(amplitudes, nb, N, done), dev)
             offsets = np.arange(nb + 1, dtype=np.int64) * N
-            E = _core.forward(d_atoms, offsets, geom, precision, out_kind, amplitudes=amps)
-            if returngpu:
-                result[done:done + nb] = E
-            else:
-                result[done:done + nb] = E.cpu().numpy()
+            compute.wait_event(ev_copied[slot])  # device output buffer copied out
+            _core.forward(d_atoms, offsets, geom, precision, out_kind, amplitudes=amps, out=d_out[slot][:nb])
+            ev_done[slot].record(compute)
+            copy.wait_event(ev_done[slot])
+            with torch.cuda.stream(copy):
+                h_out[slot][:nb].copy_(d_out[slot][:nb], non_blocking=True)
+            ev_copied[slot].record(copy)
+            if pending is not None:
+                ps, pstart, pn = pending
+                ev_copied[ps].synchronize()
+                result[pstart:pstart + pn] = h_out[ps][:pn].numpy()
+                if verbose:
+                    print(pstart + pn, end=". ", flush=True)
+            pending = (slot, done, nb)
             done += nb
-            if verbose:
-                print(done, end=". ", flush=True)
+            i += 1
+        ps, pstart, pn = pending
+        ev_copied[ps].synchronize()
+        result[pstart:pstart + pn] = h_out[ps][:pn].numpy()
+        if verbose:
+            print(pstart + pn, end=". ", flush=True)
         return result
     except KeyboardInterrupt:
         if verbose:
             print("Interrupted")
-        return result[:done]
+        torch.cuda.synchronize(dev)
+        return result[: pending[1] if pending else 0]
 
 
 def simulate_batch(
