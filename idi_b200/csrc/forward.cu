@@ -229,7 +229,7 @@ __global__ void fwd_finish_kernel(const GeomParams g, const double2 *__restrict_
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
-template <int PPT, bool NF, bool SCALE, bool SECOND>
+template <int PPT, bool NF, bool SCALE, bool SECOND, bool CHUNKED>
 __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(const __grid_constant__ BatchParams bp,
                                                         const GeomParams g, SplitRecs rec,
                                                         void *__restrict__ out, int out_kind,
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
         __syncthreads();
         const int unit = s_unit;
         if (unit >= bp.total_units) break;
-        const int ks = bp.ksplit > 1 ? bp.ksplit : 1;
+        const int ks = CHUNKED ? bp.ksplit : 1;
         const int chunk = unit % ks;
         const int pu = unit / ks;
         const int img = bp.order[pu / bp.tiles_per_image];
@@ -277,8 +277,8 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
         const ImageDesc d = bp.img[img];
         const int p0 = ptile * tile_px + tid * PPT;
         // emitter tiles of this unit: the whole image, or one chunk of it
-        const int tbeg = ks > 1 ? min(chunk * d.tpc, d.ntiles) : 0;
-        const int tend = ks > 1 ? min(tbeg + d.tpc, d.ntiles) : d.ntiles;
+        const int tbeg = CHUNKED ? min(chunk * d.tpc, d.ntiles) : 0;
+        const int tend = CHUNKED ? min(tbeg + d.tpc, d.ntiles) : d.ntiles;
 
         // ---- per-pixel constants (FP64 geometry) ----
         double nqx[PPT], nqy[PPT], nqz[PPT];
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
             if (p < npix) {
                 const double re = (double)sre[i] - (double)cre[i];
                 const double im = (double)sim[i] - (double)cim[i];
-                if (ks > 1)
+                if (CHUNKED)
                     partials[((int64_t)chunk * bp.n_images + img) * npix + p] = make_double2(re, im);
                 else
                     finish_pixel<NF, SCALE>(g, p, re, im, out, out_kind, obase + p);
@@ -781,12 +781,18 @@ static size_t forward_ws_bytes(const idiwf_geom *g, const idiwf_batch *b, int pr
 }
 
 // kernel table ---------------------------------------------------------------
-template <int PPT>
-static void *split_kernel_for(int flags) {
+template <int PPT, bool CH>
+static void *split_kernel_for2(int flags) {
     const bool nf = flags & IDIWF_NF, sc = flags & IDIWF_SCALE, so = flags & IDIWF_SECONDORDER;
-    if (nf) return sc ? (void *)fwd_split_kernel<PPT, true, true, false> : (void *)fwd_split_kernel<PPT, true, false, false>;
-    if (so) return sc ? (void *)fwd_split_kernel<PPT, false, true, true> : (void *)fwd_split_kernel<PPT, false, false, true>;
-    return sc ? (void *)fwd_split_kernel<PPT, false, true, false> : (void *)fwd_split_kernel<PPT, false, false, false>;
+    if (nf) return sc ? (void *)fwd_split_kernel<PPT, true, true, false, CH>
+                      : (void *)fwd_split_kernel<PPT, true, false, false, CH>;
+    if (so) return sc ? (void *)fwd_split_kernel<PPT, false, true, true, CH>
+                      : (void *)fwd_split_kernel<PPT, false, false, true, CH>;
+    return sc ? (void *)fwd_split_kernel<PPT, false, true, false, CH> : (void *)fwd_split_kernel<PPT, false, false, false, CH>;
+}
+template <int PPT>
+static void *split_kernel_for(int flags, bool chunked = false) {
+    return chunked ? split_kernel_for2<PPT, true>(flags) : split_kernel_for2<PPT, false>(flags);
 }
 template <int PPT>
 static void *double_kernel_for(int flags) {
@@ -798,11 +804,11 @@ static void *double_kernel_for(int flags) {
     if (so) return sc ? (void *)fwd_double_kernel<PPT, false, true, true> : (void *)fwd_double_kernel<PPT, false, false, true>;
     return sc ? (void *)fwd_double_kernel<PPT, false, true, false> : (void *)fwd_double_kernel<PPT, false, false, false>;
 }
-static void *kernel_for(int precision, int ppt, int flags) {
+static void *kernel_for(int precision, int ppt, int flags, bool chunked) {
     if (precision == IDIWF_SPLIT) {
-        if (ppt == 2) return split_kernel_for<2>(flags);
-        if (ppt == 4) return split_kernel_for<4>(flags);
-        return split_kernel_for<8>(flags);
+        if (ppt == 2) return split_kernel_for<2>(flags, chunked);
+        if (ppt == 4) return split_kernel_for<4>(flags, chunked);
+        return split_kernel_for<8>(flags, chunked);
     }
     if (ppt == 1) return double_kernel_for<1>(flags);
     if (ppt == 2) return double_kernel_for<2>(flags);
@@ -878,7 +884,7 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
     }
     IDIWF_CUDA_CHECK(cudaMemsetAsync(&hdr->work_counter, 0, sizeof(uint32_t), stream));
 
-    void *fn = kernel_for(precision, s.ppt, geom->flags);
+    void *fn = kernel_for(precision, s.ppt, geom->flags, ksplit > 1);
     const size_t smem = 2 * (size_t)s.te * (precision == IDIWF_SPLIT ? kSplitRecBytes : kDoubleRecBytes);
     idiwf_status st = ensure_smem(fn, smem);
     if (st != IDIWF_OK) return st;
