@@ -40,6 +40,9 @@ OUT_I32 = 3
 
 F64 = 0
 F32 = 1
+I32 = 2
+U32 = 3
+I64 = 4
 
 # every symbol include/idiwf.h declares
 EXPORTED = (
@@ -53,6 +56,10 @@ EXPORTED = (
     "idiwf_time_workspace_size",
     "idiwf_time_forward",
     "idiwf_time_order",
+    "idiwf_photons_workspace_size",
+    "idiwf_photons",
+    "idiwf_chargesharing_workspace_size",
+    "idiwf_chargesharing",
     "idiwf_tune",
     "idiwf_workspace_error",
     "idiwf_microbench",
@@ -104,6 +111,14 @@ class Batch(ctypes.Structure):
     ]
 
 
+class Rng(ctypes.Structure):
+    _fields_ = [
+        ("key", ctypes.c_uint64 * 2),
+        ("stream", ctypes.c_uint64),
+        ("first_image", ctypes.c_uint64),
+    ]
+
+
 _lib = None
 
 
@@ -144,6 +159,17 @@ def load():
     L.idiwf_time_order.argtypes = [P(Geom), vp, vp, ctypes.c_int64, ctypes.c_double, ctypes.c_int32,
                                    ctypes.c_int32, vp, vp, vp, ctypes.c_size_t, vp]
     L.idiwf_time_order.restype = st
+    L.idiwf_photons_workspace_size.argtypes = [ctypes.c_int32, ctypes.c_int64]
+    L.idiwf_photons_workspace_size.restype = ctypes.c_size_t
+    L.idiwf_photons.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_double, P(Rng), vp,
+                                ctypes.c_int32, vp, ctypes.c_size_t, vp]
+    L.idiwf_photons.restype = st
+    L.idiwf_chargesharing_workspace_size.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+    L.idiwf_chargesharing_workspace_size.restype = ctypes.c_size_t
+    L.idiwf_chargesharing.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.c_double, ctypes.c_double, P(Rng), vp, vp, ctypes.c_int64, vp, vp,
+                                      ctypes.c_size_t, vp]
+    L.idiwf_chargesharing.restype = st
     L.idiwf_tune.argtypes = [P(Geom), P(Batch), ctypes.c_int32, ctypes.c_int32, vp, vp, ctypes.c_size_t, vp,
                              P(Config)]
     L.idiwf_tune.restype = st

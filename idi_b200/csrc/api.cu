@@ -106,6 +106,9 @@ extern "C" idiwf_status idiwf_workspace_error(const void *workspace, cudaStream_
     IDIWF_CUDA_CHECK(cudaMemcpyAsync(&h, workspace, sizeof(h), cudaMemcpyDeviceToHost, stream));
     IDIWF_CUDA_CHECK(cudaStreamSynchronize(stream));
     if (h.error & kErrTimeout) return set_error(IDIWF_ERR_TIMEOUT, "a bounded device wait gave up");
+    if (h.error & kErrValue)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT,
+                         "invalid input value (negative or NaN entry, all-zero image, or photon count mismatch)");
     if (h.error & kErrRange)
         return set_error(IDIWF_ERR_UNSUPPORTED,
                          "emitter coordinates too large for the split-precision phase range");

@@ -1,0 +1,587 @@
+// Detector stage on the device: Poisson photon counts (randomphotons,
+// idi/simulation/common.py:11-23) and charge sharing (chargesharing,
+// idi/simulation/common.py:26-67).
+//
+//  * photon_sum_kernel / photon_sample_kernel — per-image FP64 sum of the
+//    probabilities in a fixed reduction tree, then one Poisson draw per pixel
+//    from the pixel's own Philox4x64-10 stream.  HBM-bound: 2 reads of the
+//    probabilities and one write of the counts per pixel.
+//  * cs_seg_kernel / cs_seg_scan_kernel / cs_start_kernel — exclusive scan of
+//    the photon counts (injected positions only: photon g's row in the
+//    caller's arrays).
+//  * cs_gather_kernel — one thread per output pixel sums the charge of every
+//    photon within w pixels, walking source pixels in row-major order and the
+//    photons of a pixel in order: the reference's scatter loop adds to each
+//    pixel in exactly that order.
+#include <cmath>
+
+#include "idiwf_internal.cuh"
+
+namespace idiwf {
+
+// ---------------------------------------------------------------------------
+// Philox4x64-10 (Salmon et al., SC 2011), numpy.random.Philox counter
+// convention: the counter word 0 is incremented before each block.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void philox4x64(uint64_t c0, uint64_t c1, uint64_t c2, uint64_t c3, uint64_t k0,
+                                           uint64_t k1, uint64_t &r0, uint64_t &r1, uint64_t &r2, uint64_t &r3) {
+    constexpr uint64_t kM0 = 0xD2E7470EE14C6C93ull, kM1 = 0xCA5A826395121157ull;
+    constexpr uint64_t kW0 = 0x9E3779B97F4A7C15ull, kW1 = 0xBB67AE8584CAA73Bull;
+#pragma unroll
+    for (int round = 0; round < 10; ++round) {
+        const uint64_t hi0 = __umul64hi(kM0, c0), lo0 = kM0 * c0;
+        const uint64_t hi1 = __umul64hi(kM1, c2), lo1 = kM1 * c2;
+        const uint64_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += kW0;
+        k1 += kW1;
+    }
+    r0 = c0;
+    r1 = c1;
+    r2 = c2;
+    r3 = c3;
+}
+
+__device__ __forceinline__ double u01(uint64_t x) { return (double)(x >> 11) * 0x1p-53; }
+
+// Sequential stream of uniform doubles, counter (j, c1, c2, c3), j = 1, 2, ...
+struct PhiloxStream {
+    uint64_t c1, c2, c3, k0, k1, j;
+    uint64_t b0, b1, b2, b3;
+    int pos;
+    __device__ PhiloxStream(uint64_t c1_, uint64_t c2_, uint64_t c3_, uint64_t k0_, uint64_t k1_)
+        : c1(c1_), c2(c2_), c3(c3_), k0(k0_), k1(k1_), j(0), b0(0), b1(0), b2(0), b3(0), pos(4) {}
+    __device__ __forceinline__ double uniform() {
+        if (pos == 4) {
+            ++j;
+            philox4x64(j, c1, c2, c3, k0, k1, b0, b1, b2, b3);
+            pos = 0;
+        }
+        const uint64_t x = pos == 0 ? b0 : (pos == 1 ? b1 : (pos == 2 ? b2 : b3));
+        ++pos;
+        return u01(x);
+    }
+};
+
+// Box-Muller (1958): a standard normal from two uniforms in [0, 1).
+__device__ __forceinline__ double box_muller(double ua, double ub) {
+    return sqrt(-2.0 * log(1.0 - ua)) * cospi(2.0 * ub);
+}
+
+// ---------------------------------------------------------------------------
+// Poisson sampler
+// ---------------------------------------------------------------------------
+constexpr double kPtrsMinRate = 10.0;
+constexpr int kMaxRejections = 1000;  // acceptance is above 0.88 per trial
+
+// Returns -1 when the rejection loop ran out (never in practice).
+__device__ double poisson_draw(double lam, PhiloxStream &st) {
+    if (!(lam > 0.0)) return 0.0;
+    if (lam < kPtrsMinRate) {
+        // inversion: smallest k with F(k) >= u, F accumulated term by term
+        const double u = st.uniform();
+        double p = exp(-lam), F = p;
+        double k = 0.0;
+        while (u > F) {
+            k += 1.0;
+            p = p * lam / k;
+            const double Fn = F + p;
+            if (Fn == F) break;  // the tail no longer changes F: u is in the last ulp
+            F = Fn;
+        }
+        return k;
+    }
+    // PTRS, Hoermann (1993): transformed rejection with squeeze
+    const double slam = sqrt(lam), loglam = log(lam);
+    const double b = 0.931 + 2.53 * slam;
+    const double a = -0.059 + 0.02483 * b;
+    const double invalpha = 1.1239 + 1.1328 / (b - 3.4);
+    const double vr = 0.9277 - 3.6224 / (b - 2.0);
+    for (int trial = 0; trial < kMaxRejections; ++trial) {
+        const double U = st.uniform() - 0.5;
+        const double V = st.uniform();
+        const double us = 0.5 - fabs(U);
+        if (!(us > 0.0)) continue;
+        const double k = floor((2.0 * a / us + b) * U + lam + 0.43);
+        if (us >= 0.07 && V <= vr) return k;
+        if (k < 0.0 || (us < 0.013 && V > us)) continue;
+        if (log(V) + log(invalpha) - log(a / (us * us) + b) <= -lam + k * loglam - lgamma(k + 1.0)) return k;
+    }
+    return -1.0;
+}
+
+template <typename T>
+__device__ __forceinline__ double load_real(const T *p, int64_t i) {
+    return (double)p[i];
+}
+
+template <typename T>
+__device__ __forceinline__ void store_count(T *p, int64_t i, double v) {
+    p[i] = (T)v;
+}
+
+// ---------------------------------------------------------------------------
+// photon kernels
+// ---------------------------------------------------------------------------
+constexpr int kSumThreads = 256;
+constexpr int kSumMaxBlocks = 256;
+constexpr int kSumPerThread = 8;
+
+// Partial-sum blocks per image: a function of npix only, so the reduction
+// tree (and with it the sum) does not depend on the device.
+static int sum_blocks(int64_t npix) {
+    const int64_t per_block = (int64_t)kSumThreads * kSumPerThread;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(kSumMaxBlocks, (npix + per_block - 1) / per_block));
+}
+
+// Fixed-shape tree over kSumThreads values in shared memory; result in v[0].
+__device__ __forceinline__ void tree_sum(double *v) {
+#pragma unroll
+    for (int h = kSumThreads / 2; h > 0; h >>= 1) {
+        __syncthreads();
+        if ((int)threadIdx.x < h) v[threadIdx.x] += v[threadIdx.x + h];
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSumThreads) photon_sum_kernel(const T *__restrict__ probs, int64_t npix, int nblk,
+                                                                 double *__restrict__ partials,
+                                                                 uint32_t *__restrict__ err) {
+    __shared__ double v[kSumThreads];
+    const int b = blockIdx.y;
+    const T *img = probs + (int64_t)b * npix;
+    double acc = 0.0;
+    bool bad = false;
+    for (int64_t i = (int64_t)blockIdx.x * kSumThreads + threadIdx.x; i < npix; i += (int64_t)nblk * kSumThreads) {
+        const double x = load_real(img, i);
+        bad |= !(x >= 0.0);
+        acc += x;
+    }
+    if (bad) record_error(err, kErrValue);
+    v[threadIdx.x] = acc;
+    tree_sum(v);
+    if (threadIdx.x == 0) partials[(int64_t)b * nblk + blockIdx.x] = v[0];
+}
+
+template <typename TI, typename TO>
+__global__ void __launch_bounds__(kSumThreads) photon_sample_kernel(const TI *__restrict__ probs, int64_t npix,
+                                                                    int nblk, const double *__restrict__ partials,
+                                                                    double n_photons, uint64_t k0, uint64_t k1,
+                                                                    uint64_t stream, uint64_t img0,
+                                                                    TO *__restrict__ out,
+                                                                    uint32_t *__restrict__ err) {
+    __shared__ double v[kSumThreads];
+    const int b = blockIdx.y;
+    v[threadIdx.x] = (int)threadIdx.x < nblk ? partials[(int64_t)b * nblk + threadIdx.x] : 0.0;
+    tree_sum(v);
+    const double total = v[0];
+    const double scale = n_photons / total;
+    const TI *img = probs + (int64_t)b * npix;
+    TO *o = out + (int64_t)b * npix;
+    bool bad = false;
+    for (int64_t p = (int64_t)blockIdx.x * kSumThreads + threadIdx.x; p < npix; p += (int64_t)gridDim.x * kSumThreads) {
+        const double lam = load_real(img, p) * scale;
+        double k = 0.0;
+        if (lam >= 0.0 && lam < 0x1p62) {
+            PhiloxStream st((uint64_t)p, img0 + (uint64_t)b, stream, k0, k1);
+            k = poisson_draw(lam, st);
+            if (k < 0.0) {
+                bad = true;
+                k = 0.0;
+            }
+        } else if (!(lam == 0.0)) {
+            bad = true;
+        }
+        store_count(o, p, k);
+    }
+    if (bad) record_error(err, kErrValue);
+}
+
+// ---------------------------------------------------------------------------
+// charge sharing
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanPerThread = 16;
+constexpr int64_t kScanSeg = (int64_t)kScanThreads * kScanPerThread;
+
+// photons in a pixel: numpy astype(int) truncates toward zero; negative or
+// NaN counts are invalid
+template <typename T>
+__device__ __forceinline__ int64_t photon_count(const T *c, int64_t i, bool &bad) {
+    const double x = (double)c[i];
+    if (!(x >= 0.0) || x >= 0x1p62) {
+        bad = true;
+        return 0;
+    }
+    return (int64_t)x;
+}
+template <>
+__device__ __forceinline__ int64_t photon_count<int64_t>(const int64_t *c, int64_t i, bool &bad) {
+    const int64_t x = c[i];
+    if (x < 0) {
+        bad = true;
+        return 0;
+    }
+    return x;
+}
+template <>
+__device__ __forceinline__ int64_t photon_count<int32_t>(const int32_t *c, int64_t i, bool &bad) {
+    const int32_t x = c[i];
+    if (x < 0) {
+        bad = true;
+        return 0;
+    }
+    return x;
+}
+template <>
+__device__ __forceinline__ int64_t photon_count<uint32_t>(const uint32_t *c, int64_t i, bool &) {
+    return (int64_t)c[i];
+}
+
+__device__ __forceinline__ int64_t block_exclusive_scan(int64_t x, int64_t *sh, int64_t &total) {
+    // Hillis-Steele over kScanThreads values (integers: exact in any order)
+    sh[threadIdx.x] = x;
+    __syncthreads();
+#pragma unroll
+    for (int d = 1; d < kScanThreads; d <<= 1) {
+        const int64_t y = (int)threadIdx.x >= d ? sh[threadIdx.x - d] : 0;
+        __syncthreads();
+        sh[threadIdx.x] += y;
+        __syncthreads();
+    }
+    total = sh[kScanThreads - 1];
+    const int64_t incl = sh[threadIdx.x];
+    __syncthreads();
+    return incl - x;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) cs_seg_kernel(const T *__restrict__ counts, int64_t n,
+                                                              int64_t *__restrict__ seg_tot,
+                                                              uint32_t *__restrict__ err) {
+    __shared__ int64_t sh[kScanThreads];
+    const int64_t base = (int64_t)blockIdx.x * kScanSeg + (int64_t)threadIdx.x * kScanPerThread;
+    int64_t acc = 0;
+    bool bad = false;
+    for (int e = 0; e < kScanPerThread; ++e) {
+        const int64_t i = base + e;
+        if (i < n) acc += photon_count(counts, i, bad);
+    }
+    if (bad) record_error(err, kErrValue);
+    int64_t total;
+    block_exclusive_scan(acc, sh, total);
+    if (threadIdx.x == 0) seg_tot[blockIdx.x] = total;
+}
+
+// Exclusive scan of the segment totals in place (one block; exact integers).
+__global__ void __launch_bounds__(kScanThreads) cs_seg_scan_kernel(int64_t *__restrict__ seg_tot, int64_t nseg,
+                                                                   int64_t n_positions, uint32_t *__restrict__ err) {
+    __shared__ int64_t sh[kScanThreads];
+    const int64_t per = (nseg + kScanThreads - 1) / kScanThreads;
+    const int64_t lo = (int64_t)threadIdx.x * per, hi = min(lo + per, nseg);
+    int64_t acc = 0;
+    for (int64_t i = lo; i < hi; ++i) acc += seg_tot[i];
+    int64_t total;
+    int64_t run = block_exclusive_scan(acc, sh, total);
+    for (int64_t i = lo; i < hi; ++i) {
+        const int64_t t = seg_tot[i];
+        seg_tot[i] = run;
+        run += t;
+    }
+    if (threadIdx.x == 0 && total != n_positions) record_error(err, kErrValue);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) cs_start_kernel(const T *__restrict__ counts, int64_t n,
+                                                                const int64_t *__restrict__ seg_off,
+                                                                int64_t *__restrict__ start) {
+    __shared__ int64_t sh[kScanThreads];
+    const int64_t base = (int64_t)blockIdx.x * kScanSeg + (int64_t)threadIdx.x * kScanPerThread;
+    bool bad = false;
+    int64_t c[kScanPerThread];
+    int64_t acc = 0;
+#pragma unroll
+    for (int e = 0; e < kScanPerThread; ++e) {
+        const int64_t i = base + e;
+        c[e] = i < n ? photon_count(counts, i, bad) : 0;
+        acc += c[e];
+    }
+    int64_t total;
+    int64_t run = block_exclusive_scan(acc, sh, total) + seg_off[blockIdx.x];
+#pragma unroll
+    for (int e = 0; e < kScanPerThread; ++e) {
+        const int64_t i = base + e;
+        if (i < n) start[i] = run;
+        run += c[e];
+    }
+}
+
+struct CsParams {
+    int32_t n_images, nx, ny, w;
+    double c;        // 1 / (2 sqrt(2) s)
+    double rs2;      // sqrt(2) s
+    double ns;
+    uint64_t k0, k1, stream, img0;
+    int64_t n_positions;
+};
+
+// erf(c + a) + erf(c - a), a = (mu - d) / (sqrt(2) s): charge fraction (x2)
+// of a Gaussian centred mu inside the pixel at offset d (common.py:57-62)
+__device__ __forceinline__ double cs_factor(double mu, int d, const CsParams &P) {
+    const double a = (mu - (double)d) / P.rs2;
+    return erf(P.c + a) + erf(P.c - a);
+}
+
+template <typename T, bool INJ>
+__global__ void __launch_bounds__(256) cs_gather_kernel(const T *__restrict__ counts, const CsParams P,
+                                                        const double *__restrict__ positions,
+                                                        const double *__restrict__ scales,
+                                                        const int64_t *__restrict__ start,
+                                                        double *__restrict__ out, uint32_t *__restrict__ err) {
+    const int64_t npix = (int64_t)P.nx * P.ny;
+    const int64_t total = npix * P.n_images;
+    bool bad = false;
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < total; o += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(o / npix);
+        const int64_t po = o - (int64_t)b * npix;
+        const int r = (int)(po / P.ny), col = (int)(po - (int64_t)r * P.ny);
+        double acc = 0.0;
+        const int r0 = max(r - P.w, 0), r1 = min(r + P.w, P.nx - 1);
+        const int c0 = max(col - P.w, 0), c1 = min(col + P.w, P.ny - 1);
+        for (int qr = r0; qr <= r1; ++qr) {
+            const int dr = r - qr;
+            for (int qc = c0; qc <= c1; ++qc) {
+                const int dc = col - qc;
+                const int64_t q = (int64_t)qr * P.ny + qc;
+                const int64_t gq = (int64_t)b * npix + q;
+                const int64_t n = photon_count(counts, gq, bad);
+                for (int64_t i = 0; i < n; ++i) {
+                    double mux, muy, sc = 1.0;
+                    if (INJ) {
+                        const int64_t g = start[gq] + i;
+                        if (g >= P.n_positions) {
+                            bad = true;
+                            break;
+                        }
+                        mux = positions[2 * g];
+                        muy = positions[2 * g + 1];
+                        if (P.ns > 0.0 && scales) sc = scales[g];
+                    } else {
+                        uint64_t w0, w1, w2, w3;
+                        philox4x64((uint64_t)i + 1, (uint64_t)q, (P.img0 + (uint64_t)b) | (1ull << 63), P.stream,
+                                   P.k0, P.k1, w0, w1, w2, w3);
+                        mux = u01(w0) - 0.5;
+                        muy = u01(w1) - 0.5;
+                        if (P.ns > 0.0) sc = 1.0 + box_muller(u01(w2), u01(w3)) * P.ns;
+                    }
+                    // k[x, y] = (1/4 f_x) f_y, deposited at (hit_x + y - w, hit_y + x - w)
+                    const double kxy = (0.25 * cs_factor(mux, dc, P)) * cs_factor(muy, dr, P);
+                    acc += P.ns > 0.0 ? sc * kxy : kxy;
+                }
+            }
+        }
+        out[o] = acc;
+    }
+    if (bad) record_error(err, kErrValue);
+}
+
+// s <= 0: counts * (1 + ns N(0,1)) per pixel (common.py:35-39)
+template <typename T, bool INJ>
+__global__ void cs_noshare_kernel(const T *__restrict__ counts, const CsParams P, const double *__restrict__ scales,
+                                  double *__restrict__ out) {
+    const int64_t npix = (int64_t)P.nx * P.ny;
+    const int64_t total = npix * P.n_images;
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < total; o += (int64_t)gridDim.x * blockDim.x) {
+        const double x = (double)counts[o];
+        if (!(P.ns != 0.0)) {
+            out[o] = x;
+            continue;
+        }
+        double f;
+        if (INJ) {
+            f = scales[o];
+        } else {
+            const int b = (int)(o / npix);
+            const int64_t p = o - (int64_t)b * npix;
+            uint64_t w0, w1, w2, w3;
+            philox4x64(1, (uint64_t)p, (P.img0 + (uint64_t)b) | (1ull << 62), P.stream, P.k0, P.k1, w0, w1, w2,
+                       w3);
+            f = 1.0 + P.ns * box_muller(u01(w0), u01(w1));
+        }
+        out[o] = x * f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static int dev_sms() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+static size_t photons_ws_bytes(int32_t n_images, int64_t npix) {
+    return 256 + align256((size_t)n_images * sum_blocks(npix) * sizeof(double));
+}
+
+template <typename TI, typename TO>
+static idiwf_status launch_photons(const void *probs, int32_t n_images, int64_t npix, double n_photons,
+                                   const idiwf_rng *rng, void *out, void *ws, cudaStream_t stream) {
+    WsHeader *hdr = static_cast<WsHeader *>(ws);
+    double *partials = reinterpret_cast<double *>(static_cast<char *>(ws) + 256);
+    const int nblk = sum_blocks(npix);
+    photon_sum_kernel<TI><<<dim3(nblk, n_images), kSumThreads, 0, stream>>>(static_cast<const TI *>(probs), npix,
+                                                                            nblk, partials, &hdr->error);
+    IDIWF_CUDA_CHECK(cudaGetLastError());
+    const int64_t want = (npix + kSumThreads - 1) / kSumThreads;
+    const int gx = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)8 * dev_sms() / std::max(1, n_images) + 1));
+    photon_sample_kernel<TI, TO><<<dim3(gx, n_images), kSumThreads, 0, stream>>>(
+        static_cast<const TI *>(probs), npix, nblk, partials, n_photons, rng->key[0], rng->key[1], rng->stream,
+        rng->first_image, static_cast<TO *>(out), &hdr->error);
+    IDIWF_CUDA_CHECK(cudaGetLastError());
+    return IDIWF_OK;
+}
+
+template <typename TI>
+static idiwf_status photons_out(int32_t out_dtype, const void *probs, int32_t n_images, int64_t npix,
+                                double n_photons, const idiwf_rng *rng, void *out, void *ws, cudaStream_t stream) {
+    switch (out_dtype) {
+        case IDIWF_F64: return launch_photons<TI, double>(probs, n_images, npix, n_photons, rng, out, ws, stream);
+        case IDIWF_F32: return launch_photons<TI, float>(probs, n_images, npix, n_photons, rng, out, ws, stream);
+        case IDIWF_I32: return launch_photons<TI, int32_t>(probs, n_images, npix, n_photons, rng, out, ws, stream);
+        case IDIWF_U32: return launch_photons<TI, uint32_t>(probs, n_images, npix, n_photons, rng, out, ws, stream);
+        case IDIWF_I64: return launch_photons<TI, int64_t>(probs, n_images, npix, n_photons, rng, out, ws, stream);
+        default: return set_error(IDIWF_ERR_INVALID_ARGUMENT, "out_dtype must be IDIWF_F64/F32/I32/U32/I64");
+    }
+}
+
+static size_t cs_ws_bytes(int32_t n_images, int32_t nx, int32_t ny, int32_t injected) {
+    const int64_t n = (int64_t)n_images * nx * ny;
+    const int64_t nseg = (n + kScanSeg - 1) / kScanSeg;
+    size_t bytes = 256;
+    if (injected) bytes += align256((size_t)nseg * 8) + align256((size_t)n * 8);
+    return bytes;
+}
+
+template <typename T>
+static idiwf_status launch_cs(const void *counts_v, int32_t n_images, int32_t nx, int32_t ny, double s, double ns,
+                              const idiwf_rng *rng, const double *positions, const double *scales,
+                              int64_t n_positions, double *out, void *ws, cudaStream_t stream) {
+    const T *counts = static_cast<const T *>(counts_v);
+    WsHeader *hdr = static_cast<WsHeader *>(ws);
+    const int64_t n = (int64_t)n_images * nx * ny;
+    CsParams P{};
+    P.n_images = n_images;
+    P.nx = nx;
+    P.ny = ny;
+    P.ns = ns;
+    P.k0 = rng ? rng->key[0] : 0;
+    P.k1 = rng ? rng->key[1] : 0;
+    P.stream = rng ? rng->stream : 0;
+    P.img0 = rng ? rng->first_image : 0;
+    P.n_positions = n_positions;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)16 * dev_sms()));
+    if (!(s > 0.0)) {
+        if (ns != 0.0 && scales != nullptr)
+            cs_noshare_kernel<T, true><<<blocks, 256, 0, stream>>>(counts, P, scales, out);
+        else
+            cs_noshare_kernel<T, false><<<blocks, 256, 0, stream>>>(counts, P, nullptr, out);
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+        return IDIWF_OK;
+    }
+    P.w = (int)std::ceil(2.0 * s);
+    P.c = 1.0 / (2.0 * std::sqrt(2.0) * s);
+    P.rs2 = std::sqrt(2.0) * s;
+    if (positions) {
+        const int64_t nseg = (n + kScanSeg - 1) / kScanSeg;
+        int64_t *seg = reinterpret_cast<int64_t *>(static_cast<char *>(ws) + 256);
+        int64_t *start = reinterpret_cast<int64_t *>(static_cast<char *>(ws) + 256 + align256((size_t)nseg * 8));
+        cs_seg_kernel<T><<<(unsigned)nseg, kScanThreads, 0, stream>>>(counts, n, seg, &hdr->error);
+        cs_seg_scan_kernel<<<1, kScanThreads, 0, stream>>>(seg, nseg, n_positions, &hdr->error);
+        cs_start_kernel<T><<<(unsigned)nseg, kScanThreads, 0, stream>>>(counts, n, seg, start);
+        cs_gather_kernel<T, true><<<blocks, 256, 0, stream>>>(counts, P, positions, scales, start, out, &hdr->error);
+    } else {
+        cs_gather_kernel<T, false><<<blocks, 256, 0, stream>>>(counts, P, nullptr, nullptr, nullptr, out, &hdr->error);
+    }
+    IDIWF_CUDA_CHECK(cudaGetLastError());
+    return IDIWF_OK;
+}
+
+}  // namespace idiwf
+
+using namespace idiwf;
+
+extern "C" size_t idiwf_photons_workspace_size(int32_t n_images, int64_t npix) {
+    if (n_images <= 0 || npix <= 0) return 0;
+    return photons_ws_bytes(n_images, npix);
+}
+
+extern "C" idiwf_status idiwf_photons(const void *probs, int32_t probs_dtype, int32_t n_images, int64_t npix,
+                                      double n_photons, const idiwf_rng *rng, void *out, int32_t out_dtype,
+                                      void *workspace, size_t workspace_bytes, cudaStream_t stream) {
+    if (n_images <= 0 || npix <= 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "n_images and npix must be positive");
+    if (n_images > 65535) return set_error(IDIWF_ERR_UNSUPPORTED, "at most 65535 images per call");
+    if (!probs || !out || !rng) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "probs, out and rng must be non-NULL");
+    if (!std::isfinite(n_photons) || n_photons < 0)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "n_photons must be finite and >= 0");
+    if (!workspace || workspace_bytes < photons_ws_bytes(n_images, npix))
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_photons_workspace_size()");
+    if (reinterpret_cast<uintptr_t>(workspace) & 255)
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(workspace, 0, 2 * sizeof(uint32_t), stream));
+    if (probs_dtype == IDIWF_F64)
+        return photons_out<double>(out_dtype, probs, n_images, npix, n_photons, rng, out, workspace, stream);
+    if (probs_dtype == IDIWF_F32)
+        return photons_out<float>(out_dtype, probs, n_images, npix, n_photons, rng, out, workspace, stream);
+    return set_error(IDIWF_ERR_INVALID_ARGUMENT, "probs_dtype must be IDIWF_F64 or IDIWF_F32");
+}
+
+extern "C" size_t idiwf_chargesharing_workspace_size(int32_t n_images, int32_t nx, int32_t ny, int32_t injected) {
+    if (n_images <= 0 || nx <= 0 || ny <= 0) return 0;
+    return cs_ws_bytes(n_images, nx, ny, injected);
+}
+
+extern "C" idiwf_status idiwf_chargesharing(const void *counts, int32_t counts_dtype, int32_t n_images, int32_t nx,
+                                            int32_t ny, double s, double ns, const idiwf_rng *rng,
+                                            const double *positions, const double *scales, int64_t n_positions,
+                                            double *out, void *workspace, size_t workspace_bytes,
+                                            cudaStream_t stream) {
+    if (n_images <= 0 || nx <= 0 || ny <= 0)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "n_images, nx and ny must be positive");
+    if (!counts || !out) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "counts and out must be non-NULL");
+    if (!std::isfinite(s) || !std::isfinite(ns)) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "s and ns must be finite");
+    if (s > 0.0 && std::ceil(2.0 * s) > 64.0) return set_error(IDIWF_ERR_UNSUPPORTED, "s above 32 pixels");
+    const bool injected = positions != nullptr && s > 0.0;
+    // draws come from rng unless injected: positions (+ scales when ns > 0)
+    // for s > 0, per-pixel scales for s <= 0
+    const bool random = s > 0.0 ? !injected : (ns != 0.0 && scales == nullptr);
+    if (random && !rng) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "rng must be non-NULL without injected draws");
+    if (injected && n_positions < 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "n_positions must be >= 0");
+    if (injected && ns > 0.0 && !scales)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "injected positions with ns > 0 need injected scales");
+    if (!workspace || workspace_bytes < cs_ws_bytes(n_images, nx, ny, injected))
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_chargesharing_workspace_size()");
+    if (reinterpret_cast<uintptr_t>(workspace) & 255)
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(workspace, 0, 2 * sizeof(uint32_t), stream));
+    const double *pos = s > 0.0 ? positions : nullptr;
+    switch (counts_dtype) {
+        case IDIWF_F64:
+            return launch_cs<double>(counts, n_images, nx, ny, s, ns, rng, pos, scales, n_positions, out, workspace, stream);
+        case IDIWF_F32:
+            return launch_cs<float>(counts, n_images, nx, ny, s, ns, rng, pos, scales, n_positions, out, workspace, stream);
+        case IDIWF_I32:
+            return launch_cs<int32_t>(counts, n_images, nx, ny, s, ns, rng, pos, scales, n_positions, out, workspace, stream);
+        case IDIWF_U32:
+            return launch_cs<uint32_t>(counts, n_images, nx, ny, s, ns, rng, pos, scales, n_positions, out, workspace, stream);
+        case IDIWF_I64:
+            return launch_cs<int64_t>(counts, n_images, nx, ny, s, ns, rng, pos, scales, n_positions, out, workspace, stream);
+        default: return set_error(IDIWF_ERR_INVALID_ARGUMENT, "counts_dtype must be IDIWF_F64/F32/I32/U32/I64");
+    }
+}

@@ -48,6 +48,7 @@ constexpr size_t kWsTimingOffset = 256;
 constexpr size_t kWsDataOffset = 256 + 8 * kMaxCtas; // 256-aligned
 constexpr uint32_t kErrTimeout = 1u;
 constexpr uint32_t kErrRange = 2u;
+constexpr uint32_t kErrValue = 4u;  // invalid input value (negative, NaN, zero-sum, count mismatch)
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 

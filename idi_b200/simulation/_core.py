@@ -27,6 +27,8 @@ __all__ = [
     "tune",
     "microbench",
     "workspace_error",
+    "photons",
+    "chargesharing",
 ]
 
 
@@ -369,3 +371,108 @@ def microbench(kind: str, device=None) -> float:
     nat.check(lib.idiwf_microbench(MICROBENCH_KINDS[kind], ctypes.c_void_p(scratch.data_ptr()), _stream(dev),
                                    ctypes.byref(rate)))
     return rate.value
+
+
+# ---------------------------------------------------------------------------
+# detector stage
+# ---------------------------------------------------------------------------
+_ELEM_CODE = {torch.float64: nat.F64, torch.float32: nat.F32, torch.int32: nat.I32, torch.int64: nat.I64}
+if hasattr(torch, "uint32"):
+    _ELEM_CODE[torch.uint32] = nat.U32
+
+
+def make_rng(key, stream: int = 0, first_image: int = 0) -> nat.Rng:
+    r = nat.Rng()
+    r.key[0] = int(key[0]) & (2**64 - 1)
+    r.key[1] = int(key[1]) & (2**64 - 1)
+    r.stream = int(stream) & (2**64 - 1)
+    r.first_image = int(first_image) & (2**64 - 1)
+    return r
+
+
+def photons(probs: torch.Tensor, n_photons: float, key, stream: int = 0, dtype=torch.float64,
+            out: Optional[torch.Tensor] = None, first_image: int = 0, check: bool = False) -> torch.Tensor:
+    """Poisson photon counts of ``probs`` (..., nx, ny) on its CUDA device: rate
+    ``probs * (n_photons / sum over the last two axes)`` (``idi/simulation/common.py:17``).
+    ``check`` synchronises and raises ValueError on a negative/NaN probability or an all-zero image."""
+    lib = nat.load()
+    _require_cuda(probs, "probs")
+    if probs.dtype not in (torch.float64, torch.float32):
+        raise ValueError("probs must be float64 or float32")
+    if probs.dim() < 2:
+        raise ValueError("probs needs at least two (detector) axes")
+    if dtype not in _ELEM_CODE:
+        raise ValueError(f"unsupported count dtype {dtype}")
+    npix = probs.shape[-1] * probs.shape[-2]
+    B = probs.numel() // npix if npix else 0
+    if out is None:
+        out = torch.empty(probs.shape, dtype=dtype, device=probs.device)
+    elif out.shape != probs.shape or out.dtype != dtype or not out.is_contiguous():
+        raise ValueError("out must be a contiguous tensor of probs' shape and the count dtype")
+    if B == 0 or npix == 0:
+        return out
+    dev = probs.device
+    ws = WORKSPACES.get(lib.idiwf_photons_workspace_size(B, npix), dev, "photons")
+    rng = make_rng(key, stream, first_image)
+    nat.check(lib.idiwf_photons(ctypes.c_void_p(probs.data_ptr()), _ELEM_CODE[probs.dtype], B, npix,
+                                float(n_photons), ctypes.byref(rng), ctypes.c_void_p(out.data_ptr()),
+                                _ELEM_CODE[dtype], ctypes.c_void_p(ws.data_ptr()), ws.numel(), _stream(dev)))
+    if check:
+        _value_check(dev, "photons")
+    return out
+
+
+def _value_check(dev, role):
+    try:
+        workspace_error(dev, role)
+    except nat.IdiwfError as e:
+        if e.status == nat.ERR_INVALID_ARGUMENT:
+            raise ValueError(str(e)) from None
+        raise
+
+
+def chargesharing(counts: torch.Tensor, s: float, ns: float = 0.0, key=(0, 0), stream: int = 0,
+                  positions: Optional[torch.Tensor] = None, scales: Optional[torch.Tensor] = None,
+                  out: Optional[torch.Tensor] = None, first_image: int = 0, check: bool = False) -> torch.Tensor:
+    """Charge sharing (``idi/simulation/common.py:26-67``) of photon counts
+    (..., nx, ny) on their CUDA device; float64 result.  ``positions`` (P, 2)
+    and ``scales`` inject the per-photon draws in the reference's photon order."""
+    lib = nat.load()
+    _require_cuda(counts, "counts")
+    if counts.dtype not in _ELEM_CODE:
+        raise ValueError(f"unsupported counts dtype {counts.dtype}")
+    if counts.dim() < 2:
+        raise ValueError("counts needs at least two (detector) axes")
+    nx, ny = counts.shape[-2], counts.shape[-1]
+    B = counts.numel() // (nx * ny) if nx * ny else 0
+    if out is None:
+        out = torch.empty(counts.shape, dtype=torch.float64, device=counts.device)
+    if B == 0:
+        return out
+    dev = counts.device
+    npos = 0
+    if positions is not None:
+        _require_cuda(positions, "positions", torch.float64)
+        if positions.dim() != 2 or positions.shape[1] != 2:
+            raise ValueError("positions must be (photons, 2)")
+        npos = positions.shape[0]
+    if scales is not None:
+        _require_cuda(scales, "scales", torch.float64)
+        need = npos if (s > 0) else counts.numel()
+        if scales.numel() != need:
+            raise ValueError(f"scales must hold {need} values")
+    injected = int(positions is not None and s > 0)
+    pos_ptr = None
+    if positions is not None:
+        # any non-NULL pointer selects injected draws, also for zero photons
+        pos_ptr = ctypes.c_void_p(positions.data_ptr() or out.data_ptr())
+    ws = WORKSPACES.get(lib.idiwf_chargesharing_workspace_size(B, nx, ny, injected), dev, "charge")
+    rng = make_rng(key, stream, first_image)
+    nat.check(lib.idiwf_chargesharing(
+        ctypes.c_void_p(counts.data_ptr()), _ELEM_CODE[counts.dtype], B, nx, ny, float(s), float(ns),
+        ctypes.byref(rng), pos_ptr,
+        ctypes.c_void_p(scales.data_ptr()) if scales is not None else None, npos,
+        ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(), _stream(dev)))
+    if check:
+        _value_check(dev, "charge")
+    return out

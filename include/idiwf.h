@@ -61,9 +61,12 @@ typedef int32_t idiwf_status;
 #define IDIWF_OUT_I64 2  /* float64 intensity |E|^2 */
 #define IDIWF_OUT_I32 3  /* float32 intensity */
 
-/* amplitude / real-array element types */
+/* element types of amplitude, probability and count arrays */
 #define IDIWF_F64 0
 #define IDIWF_F32 1
+#define IDIWF_I32 2
+#define IDIWF_U32 3
+#define IDIWF_I64 4
 
 typedef struct idiwf_geom {
     int32_t nx, ny;   /* detector pixels: Ndet[0] (rows), Ndet[1] (columns) */
@@ -204,6 +207,94 @@ idiwf_status idiwf_time_order(const idiwf_geom *geom, const double *atoms, const
                               int64_t n, double c, int32_t ix, int32_t iy, int32_t *order,
                               double *sorted_keys, void *workspace, size_t workspace_bytes,
                               cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* detector: photon sampling and charge sharing                              */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Counter-based random stream: Philox4x64-10 (Salmon, Moraes, Dror, Shaw,
+ * "Parallel random numbers: as easy as 1, 2, 3", SC 2011) with the counter
+ * convention of numpy.random.Philox: a stream with counter (0, c1, c2, c3)
+ * yields the blocks of counters (1, c1, c2, c3), (2, c1, c2, c3), ..., four
+ * 64-bit words each, and a uniform double is (word >> 11) * 2^-53.  So
+ * numpy.random.Generator(numpy.random.Philox(counter=[0, c1, c2, c3],
+ * key=key)).random() reproduces a stream bit for bit.  `stream` is counter
+ * word 3: calls that should draw independent numbers use distinct values.
+ */
+typedef struct idiwf_rng {
+    uint64_t key[2];
+    uint64_t stream;
+    uint64_t first_image; /* image b of a call draws as image first_image + b, so a
+                             batch split over several calls draws the same numbers */
+} idiwf_rng;
+
+/* Bytes of workspace idiwf_photons needs. */
+size_t idiwf_photons_workspace_size(int32_t n_images, int64_t npix);
+
+/*
+ * Poisson photon counts on the device:
+ *     out[b, p] ~ Poisson(probs[b, p] * (n_photons / sum_p probs[b, p]))
+ * for every image b of `probs` ((n_images, npix), DEVICE, probs_dtype
+ * IDIWF_F64 or IDIWF_F32; the rate is formed in FP64).  out_dtype: IDIWF_F64,
+ * IDIWF_F32, IDIWF_I32, IDIWF_U32 or IDIWF_I64 (the reference's `dtype`).
+ *
+ * Replaces idi/simulation/common.py:11-23 randomphotons, which calls
+ * numpy's / cupy's Generator.poisson on the host or device array.  The
+ * per-image sum is a fixed-order FP64 reduction (deterministic; within a few
+ * ulps of numpy's pairwise sum).  Pixel p of image b draws from its own
+ * stream, counter (0, p, rng->first_image + b, rng->stream), so results do
+ * not depend on the launch shape or on how a batch is split into calls.  Sampler: inversion by sequential search for rates below 10,
+ * otherwise the transformed rejection with squeeze PTRS (W. Hoermann, "The
+ * transformed rejection method for generating Poisson random variables",
+ * Insurance: Mathematics and Economics 12, 1993).  A negative or NaN
+ * probability or an all-zero image records an invalid-value error in the
+ * workspace (idiwf_workspace_error) and yields zero counts for the pixel.
+ * n_photons must be finite and >= 0 (the reference returns `probs`
+ * unchanged for infinite n_photons; the host side handles that case).
+ */
+idiwf_status idiwf_photons(const void *probs, int32_t probs_dtype, int32_t n_images, int64_t npix,
+                           double n_photons, const idiwf_rng *rng, void *out, int32_t out_dtype,
+                           void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/* Bytes of workspace idiwf_chargesharing needs (`injected`: nonzero when
+ * `positions` will be given). */
+size_t idiwf_chargesharing_workspace_size(int32_t n_images, int32_t nx, int32_t ny, int32_t injected);
+
+/*
+ * Charge sharing between neighbouring pixels (idi/simulation/common.py:26-67):
+ * every photon counted in pixel (ix, iy) of `counts` ((n_images, nx, ny),
+ * DEVICE, counts_dtype IDIWF_F64/F32/I32/U32/I64, truncated toward zero as
+ * numpy's astype(int)) lands at offset mu = (mu_x, mu_y) in [-0.5, 0.5)^2
+ * from the pixel centre and deposits into pixel (ix + dr, iy + dc),
+ * |dr|, |dc| <= w = ceil(2 s), the charge
+ *     1/4 [erf(c + a_x) + erf(c - a_x)] [erf(c + a_y) + erf(c - a_y)],
+ *     a_x = (mu_x - dc) / (sqrt(2) s),  a_y = (mu_y - dr) / (sqrt(2) s),
+ *     c = 1 / (2 sqrt(2) s),
+ * times its scale (1 when ns == 0); charge leaving the detector is lost.
+ * The pairing of mu_x with the column offset follows the reference's
+ * deposit loop (common.py:63-67).  For s <= 0 the result is
+ * counts * scale per pixel (counts itself when ns == 0), as in common.py:35-39.
+ * out: DEVICE (n_images, nx, ny) float64.  Each output pixel gathers its
+ * neighbours' photons in the reference's photon order, so every pixel sums
+ * in the same order as the reference's scatter loop (deterministic).
+ *
+ * Random draws, generated mode (positions == NULL): photon i of pixel p of
+ * image b uses the first block of the stream with counter
+ * (i, p, (rng->first_image + b) | 2^63, rng->stream): words 0 and 1 give mu_x, mu_y (uniform
+ * - 0.5), words 2 and 3 a Box-Muller normal z; scale = 1 + ns z.  For
+ * s <= 0, pixel p uses counter (0, p, (rng->first_image + b) | 2^62,
+ * rng->stream) the same way.
+ * Injected mode: `positions` (n_positions, 2) float64 mu of every photon and
+ * `scales` (n_positions) float64 factors or NULL, in the reference's photon
+ * order (image, then row-major pixel, then photon within the pixel); for
+ * s <= 0, `scales` holds one factor per pixel.  A photon total different
+ * from n_positions records an invalid-value error in the workspace.
+ */
+idiwf_status idiwf_chargesharing(const void *counts, int32_t counts_dtype, int32_t n_images, int32_t nx,
+                                 int32_t ny, double s, double ns, const idiwf_rng *rng,
+                                 const double *positions, const double *scales, int64_t n_positions,
+                                 double *out, void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
 /* tuning, diagnostics                                                       */

@@ -46,8 +46,8 @@ class OrcGeom(ctypes.Structure):
 
 
 def build(force: bool = False) -> str:
-    src = os.path.join(_HERE, "wavefield_oracle.c")
-    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+    srcs = [os.path.join(_HERE, f) for f in ("wavefield_oracle.c", "detector_oracle.c")]
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < max(map(os.path.getmtime, srcs)):
         subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
     return _LIB_PATH
 
@@ -75,6 +75,18 @@ def lib():
         L.orc_time_keys.argtypes = [P(OrcGeom), ctypes.c_int, vp, vp, ctypes.c_int64, d,
                                     ctypes.c_int, ctypes.c_int, vp, vp, vp]
         L.orc_time_keys.restype = None
+        u64 = ctypes.c_uint64
+        L.orc_philox4x64.argtypes = [vp, vp, vp]
+        L.orc_philox4x64.restype = None
+        L.orc_uniforms.argtypes = [u64, u64, u64, u64, u64, ctypes.c_int64, vp]
+        L.orc_uniforms.restype = None
+        L.orc_image_sum.argtypes = [vp, ctypes.c_int64]
+        L.orc_image_sum.restype = d
+        L.orc_photons.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, d, u64, u64, u64, u64, vp, vp]
+        L.orc_photons.restype = None
+        L.orc_chargesharing.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, d, d, u64, u64, u64,
+                                        u64, vp, vp, vp]
+        L.orc_chargesharing.restype = None
         _lib = L
     return _lib
 
@@ -206,3 +218,60 @@ def intensity_metrics(I, I_ref, floor=1e-3):
         "masked_fraction": float(mask.mean()),
         "floor": floor,
     }
+
+
+# ---------------------------------------------------------------------------
+# detector stage (detector_oracle.c)
+# ---------------------------------------------------------------------------
+def philox4x64(counter, key) -> np.ndarray:
+    """One Philox4x64-10 block: four uint64 words for a 4-word counter and 2-word key."""
+    c = _c(np.asarray(counter, dtype=np.uint64), np.uint64)
+    k = _c(np.asarray(key, dtype=np.uint64), np.uint64)
+    out = np.empty(4, np.uint64)
+    lib().orc_philox4x64(c.ctypes.data, k.ctypes.data, out.ctypes.data)
+    return out
+
+
+def uniforms(c1, c2, c3, key, n) -> np.ndarray:
+    """First n uniform doubles of the stream with counter (0, c1, c2, c3)."""
+    out = np.empty(int(n), np.float64)
+    lib().orc_uniforms(int(c1), int(c2), int(c3), int(key[0]), int(key[1]), int(n), out.ctypes.data)
+    return out
+
+
+def image_sum(img) -> float:
+    """Sum of one image in the device's fixed reduction tree."""
+    a = _c(np.ravel(img))
+    return float(lib().orc_image_sum(a.ctypes.data, a.size))
+
+
+def photons(probs, n_photons, key, stream=0, return_rates=False, first_image=0):
+    """Poisson counts (float64) of ``probs`` (..., nx, ny) restating common.py:11-23
+    with the device's per-pixel streams; optionally also the rates."""
+    p = _c(probs)
+    shape = p.shape
+    npix = shape[-1] * shape[-2]
+    B = int(p.size // npix)
+    counts = np.empty(p.size, np.float64)
+    rates = np.empty(p.size, np.float64) if return_rates else None
+    lib().orc_photons(p.ctypes.data, B, npix, float(n_photons), int(key[0]), int(key[1]), int(stream),
+                      int(first_image), counts.ctypes.data, rates.ctypes.data if rates is not None else None)
+    counts = counts.reshape(shape)
+    return (counts, rates.reshape(shape)) if return_rates else counts
+
+
+def chargesharing(counts, s, ns=0.0, key=(0, 0), stream=0, positions=None, scales=None, first_image=0) -> np.ndarray:
+    """Charge sharing of integer counts (..., nx, ny), restating the scatter loop of
+    common.py:49-67; photon offsets injected (``positions``, ``scales``) or drawn
+    from the device's streams."""
+    c = _c(np.asarray(counts).astype(np.int64), np.int64)
+    shape = c.shape
+    nx, ny = shape[-2], shape[-1]
+    B = int(c.size // (nx * ny))
+    out = np.empty(c.size, np.float64)
+    pos = _c(positions) if positions is not None else None
+    sc = _c(scales) if scales is not None else None
+    lib().orc_chargesharing(c.ctypes.data, B, nx, ny, float(s), float(ns), int(key[0]), int(key[1]), int(stream),
+                            int(first_image), pos.ctypes.data if pos is not None else None, sc.ctypes.data if sc is not None else None,
+                            out.ctypes.data)
+    return out.reshape(shape)

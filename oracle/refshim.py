@@ -101,7 +101,7 @@ _cache = {}
 
 
 def load():
-    """Return a namespace with the reference modules ``cpu``, ``time``, ``simobj``, ``util``."""
+    """Return a namespace with the reference modules ``cpu``, ``time``, ``simobj``, ``common``, ``util``."""
     if _cache:
         return types.SimpleNamespace(**_cache)
     if not available():
@@ -118,7 +118,8 @@ def load():
     cpu = _load("simulation.cpu", os.path.join(idi_dir, "simulation", "cpu.py"))
     tim = _load("simulation.time", os.path.join(idi_dir, "simulation", "time.py"))
     simobj = _load("simulation.simobj", os.path.join(idi_dir, "simulation", "simobj.py"))
-    _cache.update(cpu=cpu, time=tim, simobj=simobj, util=util)
+    common = _load("simulation.common", os.path.join(idi_dir, "simulation", "common.py"))
+    _cache.update(cpu=cpu, time=tim, simobj=simobj, util=util, common=common)
     return types.SimpleNamespace(**_cache)
 
 

@@ -3,7 +3,8 @@
     python tests/golden/make_golden.py
 
 Runs the reference's own CPU implementations -- ``idi/simulation/cpu.py``
-``simulate`` and ``idi/simulation/time.py`` ``simulate`` -- unmodified, through
+``simulate``, ``idi/simulation/time.py`` ``simulate`` and
+``idi/simulation/common.py`` ``randomphotons`` / ``chargesharing`` -- unmodified, through
 ``oracle/refshim.py``, on seeded inputs (numpy Philox), and stores inputs and
 outputs.  For the time path it also records, per pixel, the arrival-time keys
 the reference computes and the order its ``_psort`` puts them in, by wrapping
@@ -109,12 +110,94 @@ def make_time(ref):
     return out
 
 
+class _RateSpy:
+    """Stands in for the Generator handed to the reference's ``randomphotons``:
+    records the Poisson rates it is asked for and returns zeros."""
+
+    def __init__(self):
+        self.rates = []
+
+    def poisson(self, lam):
+        self.rates.append(np.array(lam, copy=True))
+        return np.zeros(np.shape(lam))
+
+
+PHOTON_CASES = [
+    # name, image shape, n_photons (low rates: inversion; high rates: PTRS)
+    ("photons_low", (2, 24, 20), 300.0),
+    ("photons_high", (2, 24, 20), 2.0e5),
+]
+
+CHARGE_CASES = [
+    # name, image shape, mean count, s, ns
+    ("cs_w2", (16, 12), 0.7, 0.6, 0.0),
+    ("cs_w1_noise", (16, 12), 1.5, 0.3, 0.1),
+    ("cs_w3_edges", (9, 7), 2.0, 1.3, 0.0),
+    ("cs_noshare_noise", (10, 8), 3.0, 0.0, 0.2),
+]
+
+
+def make_detector(ref):
+    """Rates of ``common.randomphotons`` (recorded through a stand-in rng) and
+    ``common.chargesharing`` outputs together with the random draws the
+    reference made: its photon offsets come from numba's generator
+    (``common.py:50``), seeded here through a jitted ``np.random.seed`` and read
+    back by a jitted function drawing the same sequence; the s <= 0 branch
+    draws from numpy's global generator (``common.py:39``)."""
+    import numba
+
+    @numba.njit
+    def nb_seed(seed):
+        np.random.seed(seed)
+
+    @numba.njit(fastmath=True)
+    def nb_draws(n, ns):
+        mu = np.random.rand(n, 2) - 0.5
+        scale = np.ones(n)
+        if ns > 0:
+            scale = 1 + np.random.randn(n) * ns
+        return mu, scale
+
+    out = {}
+    for i, (name, shape, nph) in enumerate(PHOTON_CASES):
+        rng = np.random.Generator(np.random.Philox(4000 + i))
+        probs = rng.gamma(0.5, 1.0, shape) * rng.uniform(0.5, 1.5, shape[:1] + (1, 1))
+        spy = _RateSpy()
+        ref.common.randomphotons(probs, nph, rng=spy)
+        out[f"{name}__probs"] = probs
+        out[f"{name}__n_photons"] = np.array(nph)
+        out[f"{name}__rates"] = spy.rates[0]
+    for i, (name, shape, mean, s, ns) in enumerate(CHARGE_CASES):
+        rng = np.random.Generator(np.random.Philox(5000 + i))
+        img = rng.poisson(mean, shape)
+        img[0, 0] += 2  # photons in the corner: charge leaves the detector
+        seed = 6000 + i
+        if s > 0:
+            nb_seed(seed)
+            res = ref.common.chargesharing(img, s, ns)
+            nb_seed(seed)
+            mu, scale = nb_draws(int(img.sum()), ns)
+        else:
+            np.random.seed(seed)
+            res = ref.common.chargesharing(img, s, ns)
+            np.random.seed(seed)
+            mu = np.zeros((0, 2))
+            scale = 1 + ns * np.random.randn(*img.shape)
+        out[f"{name}__counts"] = img
+        out[f"{name}__meta"] = np.array([s, ns])
+        out[f"{name}__positions"] = mu
+        out[f"{name}__scales"] = scale
+        out[f"{name}__out"] = res
+    return out
+
+
 def main():
     if not refshim.available():
         raise SystemExit("reference tree not available")
     ref = refshim.load()
     np.savez_compressed(os.path.join(HERE, "forward_ref.npz"), **make_forward(ref))
     np.savez_compressed(os.path.join(HERE, "time_ref.npz"), **make_time(ref))
+    np.savez_compressed(os.path.join(HERE, "detector_ref.npz"), **make_detector(ref))
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 
