@@ -231,7 +231,7 @@ def main():
                     help="small: 8 images on a 512x512 detector (profiling-sized capture of the same kernel)")
     ap.add_argument("--no-tune", action="store_true", help="use the default kernel shape instead of autotuning")
     ap.add_argument("--config", default=None, help='kernel shape as JSON, e.g. {"threads":256,"pixels_per_thread":4}')
-    ap.add_argument("--leg", default="main", choices=["main", "fwd_bwd", "time", "batched"],
+    ap.add_argument("--leg", default="main", choices=["main", "fwd_bwd", "time", "batched", "detector"],
                     help="run one secondary leg alone (for profiling) instead of the headline measurement")
     args = ap.parse_args()
     global N_IMG, NDET
@@ -413,6 +413,7 @@ def extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, 
     res["fwd_bwd"] = fwd_bwd_leg(torch, dev, _core, nat, timed)
     res["batched_uneven"] = batched_leg(torch, dev, _core, nat)
     res["time_path"] = time_leg(torch, dev, _core, nat, args)
+    res["detector"] = detector_leg(torch, dev, _core, nat, args, cuda=cuda, simobj=simobj, pos=pos, ph=ph, k=k)
     return res
 
 
@@ -479,6 +480,8 @@ def single_leg(args):
         out = fwd_bwd_leg(torch, dev, _core, nat, timed_fn(torch))
     elif args.leg == "time":
         out = time_leg(torch, dev, _core, nat, args)
+    elif args.leg == "detector":
+        out = detector_leg(torch, dev, _core, nat, args)
     else:
         out = batched_leg(torch, dev, _core, nat)
     print(json.dumps({"leg": args.leg, **out}), flush=True)
@@ -568,6 +571,73 @@ def time_leg(torch, dev, _core, nat, args):
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": rows * 256 * n / dt, "unit": "pairs/s", "cores": os.cpu_count(),
                                "kind": "port", "sample": f"{rows} rows x 256 px x {n} emitters of image 0"}
+    return out
+
+
+def hbm_peak():
+    """Measured HBM copy bandwidth (GB/s) and where it came from."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json copy bandwidth)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback (earlier measurement on this GPU type)"
+
+
+def detector_leg(torch, dev, _core, nat, args, cuda=None, simobj=None, pos=None, ph=None, k=None):
+    """Detector stage at the headline output size: 32 images x 1024 x 1024
+    float64 intensities (268 MB, larger than L2), exponentially distributed
+    like speckle.  Poisson photons with 1e5 and 1e9 expected photons per image
+    (rates ~0.1: inversion; ~1000: PTRS) into uint32 counts; charge sharing
+    (s = 0.5 px, w = 1, generated draws) of the 1e5-photon counts into float64.
+    HBM roofline: photons move 20 B per pixel (two reads of the intensity and
+    the count write), charge sharing 12 B (count read, float64 write)."""
+    nimg, nd = N_IMG, NDET
+    npix = nimg * nd * nd
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(5)
+    I = -torch.log1p(-torch.rand((nimg, nd, nd), dtype=torch.float64, device=dev, generator=gen))
+    cnt = torch.empty((nimg, nd, nd), dtype=torch.uint32, device=dev)
+    shared = torch.empty((nimg, nd, nd), dtype=torch.float64, device=dev)
+    peak, peak_src = hbm_peak()
+    timed = timed_fn(torch)
+    out = {"workload": f"{nimg} images x {nd}x{nd} float64 intensities (exponential), uint32 counts",
+           "hbm_peak_gbs": peak, "peak_source": peak_src}
+    for label, nph in (("photons_1e5", 1e5), ("photons_1e9", 1e9)):
+        ms = timed(lambda: _core.photons(I, nph, (1, 2), 0, dtype=torch.uint32, out=cnt), reps=5)
+        gbs = 20.0 * npix / (ms * 1e-3) / 1e9
+        out[label] = {"ms": ms, "pixels_per_s": npix / (ms * 1e-3), "achieved_gbs": gbs, "frac": gbs / peak,
+                      "bytes_per_pixel": 20, "launches": 2}
+    _core.workspace_error(dev, "photons")
+    _core.photons(I, 1e5, (1, 2), 0, dtype=torch.uint32, out=cnt)
+    photons_per_image = float(cnt.to(torch.float64).sum().item()) / nimg
+    ms = timed(lambda: _core.chargesharing(cnt, 0.5, 0.0, (3, 4), 0, out=shared), reps=5)
+    gbs = 12.0 * npix / (ms * 1e-3) / 1e9
+    out["chargesharing_s0.5"] = {"ms": ms, "pixels_per_s": npix / (ms * 1e-3), "achieved_gbs": gbs,
+                                 "frac": gbs / peak, "bytes_per_pixel": 12, "photons_per_image": photons_per_image}
+    _core.workspace_error(dev, "charge")
+    del I, shared
+    if cuda is not None:
+        # end to end through the public API: host emitters in, host uint32 counts out
+        obj = simobj.fixed(E_EV, pos, phases=ph)
+        cuda.simulate_photons(2, obj, NDET, PIXEL, DETZ, 1e5, k, settings=SETTINGS, verbose=False, rng=1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cuda.simulate_photons(N_IMG, obj, NDET, PIXEL, DETZ, 1e5, k, settings=SETTINGS, verbose=False, rng=1)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out["e2e_simulate_photons"] = {
+            "value": N_IMG * N_EMIT * NDET * NDET / dt, "unit": "pairs/s", "s": dt,
+            "h2d_bytes_per_step": N_IMG * N_EMIT * 32, "d2h_bytes_per_step": N_IMG * NDET * NDET * 4,
+            "call": "simulate_photons(32, simobject, 1024, 50, 2e5, 1e5, k, settings='nf split')"}
+    if not args.no_cpu_baseline:
+        # the reference's randomphotons on the host is numpy's Generator.poisson
+        # of p * (N / sum p) (common.py:17): timed on 2 images of the same size
+        h = np.random.default_rng(5).exponential(1.0, (2, nd, nd))
+        t0 = time.perf_counter()
+        np.random.default_rng(1).poisson(h * (1e5 / h.sum(axis=(-2, -1), keepdims=True)))
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": h.size / dt, "unit": "pixels/s", "cores": 1, "kind": "port",
+                               "sample": f"numpy Generator.poisson of 2 x {nd}x{nd} rates ~0.1 (common.py:17)"}
     return out
 
 

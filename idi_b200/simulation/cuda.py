@@ -24,7 +24,7 @@ import torch
 from .. import _native as nat
 from . import _core
 
-__all__ = ["simulate", "simulate_gen"]
+__all__ = ["simulate", "simulate_gen", "simulate_photons"]
 
 # output bytes per launch in simulate(): bounds device memory for large Nimg
 _MAX_OUT_BYTES = 1 << 30
@@ -202,18 +202,36 @@ def simulate(
                 print("Interrupted")
             return result[:done]
 
-    result = np.empty((Nimg, Ndet[0], Ndet[1]), np.complex128)
+    dtype = torch.complex64 if out_kind == nat.OUT_C64 else torch.complex128
+    return _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, dtype, amplitudes, verbose,
+                      np.complex128)
+
+
+def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, out_dtype, amplitudes, verbose,
+               result_dtype, post=None):
+    """Chunked device pipeline with host output: chunk i's device-to-host copy
+    (pinned staging, second stream) overlaps chunk i+1's emitter upload and
+    kernels.  ``post(field_or_intensity, first_image, slot)`` runs further device
+    work on a chunk and returns the tensor to copy back (default: the forward
+    output).  Ctrl-C returns the images finished so far."""
+    result = None
     compute = torch.cuda.current_stream(dev)
     copy = torch.cuda.Stream(dev)
-    dtype = torch.complex64 if out_kind == nat.OUT_C64 else torch.complex128
     stagers = [_Stager(N, chunk, dev, ("sim_in", dev.index, i)) for i in range(2)]
-    d_out = [torch.empty((chunk, Ndet[0], Ndet[1]), dtype=dtype, device=dev) for _ in range(2)]
-    h_raw = [_pinned(("sim_out", dev.index, i), chunk * per_img) for i in range(2)]
-    h_out = [h[: chunk * per_img].view(dtype).view(chunk, Ndet[0], Ndet[1]) for h in h_raw]
+    d_out = [torch.empty((chunk, Ndet[0], Ndet[1]), dtype=out_dtype, device=dev) for _ in range(2)]
+    h_out = [None, None]
     ev_done = [torch.cuda.Event(), torch.cuda.Event()]
     ev_copied = [torch.cuda.Event(), torch.cuda.Event()]
     ev_h2d = [None, None]
     pending = None  # (slot, start, count) of the chunk whose copy is in flight
+    done = 0
+
+    def _collect(ps, pstart, pn):
+        ev_copied[ps].synchronize()
+        result[pstart:pstart + pn] = h_out[ps][:pn].numpy()
+        if verbose:
+            print(pstart + pn, end=". ", flush=True)
+
     try:
         i = 0
         while done < Nimg:
@@ -226,33 +244,122 @@ def simulate(
             ev_h2d[slot].record(compute)
             amps = _upload_amps(_amplitude_rows(amplitudes, nb, N, done), dev)
             offsets = np.arange(nb + 1, dtype=np.int64) * N
-            compute.wait_event(ev_copied[slot])  # device output buffer copied out
+            compute.wait_event(ev_copied[slot])  # device buffers of this slot copied out
             _core.forward(d_atoms, offsets, geom, precision, out_kind, amplitudes=amps, out=d_out[slot][:nb])
+            src = d_out[slot][:nb] if post is None else post(d_out[slot][:nb], done, slot)
+            if h_out[slot] is None:
+                per = src[0].numel() * src.element_size()
+                raw = _pinned(("sim_out", dev.index, slot), chunk * per)
+                h_out[slot] = raw[: chunk * per].view(src.dtype).view((chunk,) + tuple(src.shape[1:]))
+            if result is None:
+                result = np.empty((Nimg,) + tuple(src.shape[1:]), result_dtype)
             ev_done[slot].record(compute)
             copy.wait_event(ev_done[slot])
             with torch.cuda.stream(copy):
-                h_out[slot][:nb].copy_(d_out[slot][:nb], non_blocking=True)
+                h_out[slot][:nb].copy_(src, non_blocking=True)
             ev_copied[slot].record(copy)
             if pending is not None:
-                ps, pstart, pn = pending
-                ev_copied[ps].synchronize()
-                result[pstart:pstart + pn] = h_out[ps][:pn].numpy()
-                if verbose:
-                    print(pstart + pn, end=". ", flush=True)
+                _collect(*pending)
             pending = (slot, done, nb)
             done += nb
             i += 1
-        ps, pstart, pn = pending
-        ev_copied[ps].synchronize()
-        result[pstart:pstart + pn] = h_out[ps][:pn].numpy()
-        if verbose:
-            print(pstart + pn, end=". ", flush=True)
+        _collect(*pending)
         return result
     except KeyboardInterrupt:
         if verbose:
             print("Interrupted")
         torch.cuda.synchronize(dev)
+        if result is None:
+            return np.empty((0, Ndet[0], Ndet[1]), result_dtype)
         return result[: pending[1] if pending else 0]
+
+
+def simulate_photons(
+    Nimg,
+    simobject,
+    Ndet,
+    pixelsize,
+    detz,
+    Nphotons,
+    k=None,
+    settings="double",
+    verbose=True,
+    detangles=(0, 0),
+    detoffset=(0, 0),
+    returngpu=False,
+    *args,
+    dtype=np.uint32,
+    rng=None,
+    chargesharing=None,
+    amplitudes=None,
+    device=None,
+    **kwargs,
+):
+    """``Nimg`` photon-count images from one device pipeline: direct sum,
+    ``|E|^2``, Poisson photons with ``Nphotons`` expected per image
+    (:func:`idi_b200.simulation.common.randomphotons`) and, with
+    ``chargesharing=(s, ns)``, charge sharing.  The intensities never leave the
+    GPU; only the counts are copied back.
+
+    Replaces the reference's two-step ``randomphotons(np.abs(simulate(...))**2,
+    Nphotons)`` (``scripts/idi_simrecon.py:38-45``).  Arguments as
+    :func:`simulate`; ``dtype`` is the count type (float64 with charge
+    sharing); ``rng`` as :func:`~idi_b200.simulation.common.randomphotons`.
+    Image i draws from the same streams however the images are chunked.
+    """
+    from . import common
+
+    Ndet, geom, precision, out_kind = _setup(simobject, Ndet, pixelsize, detz, k, settings, detangles, detoffset)
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    N = int(simobject.N)
+    Nimg = int(Nimg)
+    npix = Ndet[0] * Ndet[1]
+    key, stream = common._key_stream(rng)
+    tdt, nd = common._count_dtype(dtype)
+    if chargesharing is not None:
+        cs_s, cs_ns = (tuple(chargesharing) + (0.0,))[:2]
+        final = torch.float64
+    else:
+        final = tdt
+    cap = int(max(1, _MAX_OUT_BYTES // max(npix * 16, 1)))
+    nchunks = 4 if (npix * 8 * Nimg >= (64 << 20) and Nimg >= 4) else 1
+    chunk = int(max(1, min(cap, -(-Nimg // nchunks))))
+    counts = [None, None]
+    shared = [None, None]
+
+    def post(intensity, first, slot):
+        nb = intensity.shape[0]
+        if counts[slot] is None:
+            counts[slot] = torch.empty((chunk, Ndet[0], Ndet[1]), dtype=tdt, device=dev)
+        c = _core.photons(intensity, Nphotons, key, stream, dtype=tdt, out=counts[slot][:nb], first_image=first)
+        if chargesharing is None:
+            return c
+        if shared[slot] is None:
+            shared[slot] = torch.empty((chunk, Ndet[0], Ndet[1]), dtype=torch.float64, device=dev)
+        return _core.chargesharing(c, cs_s, cs_ns, key, stream, out=shared[slot][:nb], first_image=first)
+
+    if returngpu:
+        result = torch.empty((Nimg, Ndet[0], Ndet[1]), dtype=final, device=dev)
+        stager = _Stager(N, chunk, dev)
+        d_int = torch.empty((chunk, Ndet[0], Ndet[1]), dtype=torch.float64, device=dev)
+        done = 0
+        while done < Nimg:
+            nb = min(chunk, Nimg - done)
+            d_atoms = stager.fill(simobject, nb)
+            amps = _upload_amps(_amplitude_rows(amplitudes, nb, N, done), dev)
+            offsets = np.arange(nb + 1, dtype=np.int64) * N
+            _core.forward(d_atoms, offsets, geom, precision, nat.OUT_I64, amplitudes=amps, out=d_int[:nb])
+            result[done:done + nb] = post(d_int[:nb], done, 0)
+            done += nb
+        _core.workspace_error(dev, "photons")
+        return result
+    res_np = torch.empty(0, dtype=final).numpy().dtype
+    out = _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, nat.OUT_I64, torch.float64, amplitudes,
+                     verbose, res_np, post=post)
+    _core.workspace_error(dev, "photons")
+    if nd is not None and chargesharing is None and out.dtype != nd:
+        out = out.astype(nd)
+    return out
 
 
 def simulate_batch(

@@ -169,3 +169,32 @@ def test_chargesharing_position_count_mismatch_raises():
         common.chargesharing(-c, 0.5, 0, rng=3)
     ok = common.chargesharing(c, 0.5, 0, positions=np.zeros((16, 2)))
     assert ok.sum() > 0
+
+
+def test_simulate_photons_pipeline_matches_two_step():
+    """simulate_photons == randomphotons(|simulate|^2) on the same streams, for
+    host output (chunked, pipelined) and device output."""
+    from idi_b200.simulation import cuda as sim
+    from tests.helpers import rng, sphere
+    from idi_b200.simulation.simobj import fixed
+
+    g = rng(31)
+    n, nimg = 300, 9
+    pos = sphere(g, n, 0.01)
+    phases = g.uniform(0, 2 * np.pi, (nimg, n))
+    mk = lambda: fixed(6400.0, pos, phases)  # noqa: E731
+    E = sim.simulate(nimg, mk(), 48, 75.0, 1e5, settings="double", verbose=False)
+    I = np.abs(E) ** 2
+    want = oracle.photons(I, 5e3, (123, 0), 0)
+    got = sim.simulate_photons(nimg, mk(), 48, 75.0, 1e5, 5e3, settings="double", verbose=False, rng=123)
+    assert got.dtype == np.uint32 and got.shape == (nimg, 48, 48)
+    # |E|^2 of the device (re^2 + im^2) and numpy's |E|**2 may differ in the
+    # last ulp, which can move a draw across a boundary: allow a few pixels
+    assert (got.astype(np.float64) != want).mean() < 1e-3
+    gpu = sim.simulate_photons(nimg, mk(), 48, 75.0, 1e5, 5e3, settings="double", returngpu=True, rng=123,
+                               dtype=np.float64)
+    np.testing.assert_array_equal(gpu.cpu().numpy(), got.astype(np.float64))
+    cs = sim.simulate_photons(nimg, mk(), 48, 75.0, 1e5, 5e3, settings="double", verbose=False, rng=123,
+                              chargesharing=(0.5, 0.0))
+    ref_cs = oracle.chargesharing(got.astype(np.int64), 0.5, 0.0, key=(123, 0), stream=0)
+    np.testing.assert_allclose(cs, ref_cs, rtol=1e-12, atol=1e-14)
