@@ -231,7 +231,7 @@ def main():
                     help="small: 8 images on a 512x512 detector (profiling-sized capture of the same kernel)")
     ap.add_argument("--no-tune", action="store_true", help="use the default kernel shape instead of autotuning")
     ap.add_argument("--config", default=None, help='kernel shape as JSON, e.g. {"threads":256,"pixels_per_thread":4}')
-    ap.add_argument("--leg", default="main", choices=["main", "fwd_bwd", "time", "batched", "detector"],
+    ap.add_argument("--leg", default="main", choices=["main", "fwd_bwd", "time", "batched", "detector", "emitters"],
                     help="run one secondary leg alone (for profiling) instead of the headline measurement")
     args = ap.parse_args()
     global N_IMG, NDET
@@ -414,6 +414,7 @@ def extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, 
     res["batched_uneven"] = batched_leg(torch, dev, _core, nat)
     res["time_path"] = time_leg(torch, dev, _core, nat, args)
     res["detector"] = detector_leg(torch, dev, _core, nat, args, cuda=cuda, simobj=simobj, pos=pos, ph=ph, k=k)
+    res["emitters"] = emitters_leg(torch, dev, _core, nat, args)
     return res
 
 
@@ -482,6 +483,8 @@ def single_leg(args):
         out = time_leg(torch, dev, _core, nat, args)
     elif args.leg == "detector":
         out = detector_leg(torch, dev, _core, nat, args)
+    elif args.leg == "emitters":
+        out = emitters_leg(torch, dev, _core, nat, args)
     else:
         out = batched_leg(torch, dev, _core, nat)
     print(json.dumps({"leg": args.leg, **out}), flush=True)
@@ -638,6 +641,47 @@ def detector_leg(torch, dev, _core, nat, args, cuda=None, simobj=None, pos=None,
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": h.size / dt, "unit": "pixels/s", "cores": 1, "kind": "port",
                                "sample": f"numpy Generator.poisson of 2 x {nd}x{nd} rates ~0.1 (common.py:17)"}
+    return out
+
+
+def emitters_leg(torch, dev, _core, nat, args):
+    """Emitter sources drawn on the device.  Crystal: the fcc lattice of the
+    headline workload (a = 0.36 nm, 34^3 cells = 157,216 sites filling 12 nm),
+    50,000 sites per image without replacement, random phases, 32 images,
+    with and without a random orientation per image.  Sphere: 2,000 emitters
+    in 10 nm, 8 images (the small CPU-runnable configuration)."""
+    import warnings
+
+    from idi_b200.simulation import simobj
+
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        c = simobj.fcc(E_EV, N_EMIT, 3.6e-4, repeats=[34, 34, 34], seed=1)
+    sites = torch.from_numpy(c._allpos.astype(np.float64)).to(dev)
+    timed = timed_fn(torch)
+    out = {"workload": "fcc 157,216 sites -> 50,000 per image x 32 images; sphere 2,000 x 8 images"}
+    for label, orient in (("crystal_fixed", nat.ORIENT_FIXED), ("crystal_random_orientation", nat.ORIENT_RANDOM)):
+        desc = _core.emitters_desc(nat.EMIT_SITES, sites=sites, orientation=orient)
+        buf = torch.empty((N_IMG * N_EMIT, 4), dtype=torch.float64, device=dev)
+        ms = timed(lambda: _core.emitters(desc, N_IMG, N_EMIT, (1, 2), 0, 0, dev, out=buf), reps=5)
+        out[label] = {"ms": ms, "emitters_per_s": N_IMG * N_EMIT / (ms * 1e-3),
+                      "sites_per_s": N_IMG * sites.shape[0] / (ms * 1e-3), "launches": 3}
+    desc = _core.emitters_desc(nat.EMIT_SPHERE, r=0.01)
+    ms = timed(lambda: _core.emitters(desc, 8, 2000, (1, 2), 0, 0, dev), reps=5)
+    out["sphere"] = {"ms": ms, "emitters_per_s": 8 * 2000 / (ms * 1e-3), "launches": 1}
+    if not args.no_cpu_baseline:
+        # the reference's host draw per image (simobj.py:446-487 and 50-60):
+        # numpy choice without replacement of 50,000 of the 157,216 sites
+        # and uniform phases, timed on 4 images
+        rng = np.random.default_rng(1)
+        allpos = c._allpos
+        t0 = time.perf_counter()
+        for _ in range(4):
+            idx = rng.choice(len(allpos), N_EMIT, replace=False)
+            np.concatenate([allpos[idx], rng.uniform(0, 2 * np.pi, (N_EMIT, 1))], 1)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 4 * N_EMIT / dt, "unit": "emitters/s", "cores": 1, "kind": "port",
+                               "sample": "numpy choice(157216, 50000, replace=False) + phases, 4 images"}
     return out
 
 

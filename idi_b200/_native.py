@@ -44,6 +44,15 @@ I32 = 2
 U32 = 3
 I64 = 4
 
+EMIT_SPHERE = 0
+EMIT_GNORM = 1
+EMIT_FOIL = 2
+EMIT_SITES = 3
+EMIT_FIXED = 4
+ORIENT_FIXED = 0
+ORIENT_RANDOM = 1
+ORIENT_AXIS = 2
+
 # every symbol include/idiwf.h declares
 EXPORTED = (
     "idiwf_forward_workspace_size",
@@ -60,6 +69,8 @@ EXPORTED = (
     "idiwf_photons",
     "idiwf_chargesharing_workspace_size",
     "idiwf_chargesharing",
+    "idiwf_emitters_workspace_size",
+    "idiwf_emitters",
     "idiwf_tune",
     "idiwf_workspace_error",
     "idiwf_microbench",
@@ -119,6 +130,24 @@ class Rng(ctypes.Structure):
     ]
 
 
+class EmittersDesc(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32),
+        ("random_phase", ctypes.c_int32),
+        ("orientation", ctypes.c_int32),
+        ("weighted", ctypes.c_int32),
+        ("r", ctypes.c_double),
+        ("fwhm", ctypes.c_double * 3),
+        ("rho", ctypes.c_double * 3),
+        ("depth", ctypes.c_double),
+        ("attenuation", ctypes.c_double),
+        ("rot", ctypes.c_double * 9),
+        ("axis", ctypes.c_double * 3),
+        ("sites", ctypes.c_void_p),
+        ("n_sites", ctypes.c_int64),
+    ]
+
+
 _lib = None
 
 
@@ -170,6 +199,10 @@ def load():
                                       ctypes.c_double, ctypes.c_double, P(Rng), vp, vp, ctypes.c_int64, vp, vp,
                                       ctypes.c_size_t, vp]
     L.idiwf_chargesharing.restype = st
+    L.idiwf_emitters_workspace_size.argtypes = [P(EmittersDesc), ctypes.c_int32, ctypes.c_int64]
+    L.idiwf_emitters_workspace_size.restype = ctypes.c_size_t
+    L.idiwf_emitters.argtypes = [P(EmittersDesc), ctypes.c_int32, ctypes.c_int64, P(Rng), vp, vp, ctypes.c_size_t, vp]
+    L.idiwf_emitters.restype = st
     L.idiwf_tune.argtypes = [P(Geom), P(Batch), ctypes.c_int32, ctypes.c_int32, vp, vp, ctypes.c_size_t, vp,
                              P(Config)]
     L.idiwf_tune.restype = st

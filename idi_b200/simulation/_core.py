@@ -29,6 +29,7 @@ __all__ = [
     "workspace_error",
     "photons",
     "chargesharing",
+    "emitters",
 ]
 
 
@@ -475,4 +476,63 @@ def chargesharing(counts: torch.Tensor, s: float, ns: float = 0.0, key=(0, 0), s
         ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(), _stream(dev)))
     if check:
         _value_check(dev, "charge")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# emitter sources
+# ---------------------------------------------------------------------------
+def _vec3(x, pad):
+    """A scalar repeated on three axes, or up to three per-axis values padded with ``pad``."""
+    a = np.atleast_1d(np.asarray(x, np.float64)).ravel()
+    if a.size == 1:
+        return np.repeat(a, 3)
+    return np.concatenate([a[:3], np.full(max(0, 3 - a.size), pad)])
+
+
+def emitters_desc(kind, random_phase=True, r=0.0, fwhm=(0.0, 0.0, 0.0), rho=(2.0, 2.0, 2.0), depth=0.0,
+                  attenuation=float("inf"), rot=None, orientation=0, axis=(0.0, 0.0, 1.0), weighted=False,
+                  sites: Optional[torch.Tensor] = None) -> nat.EmittersDesc:
+    d = nat.EmittersDesc()
+    d.kind = int(kind)
+    d.random_phase = int(bool(random_phase))
+    d.orientation = int(orientation)
+    d.weighted = int(bool(weighted))
+    d.r = float(r)
+    f = _vec3(fwhm, 1.0)
+    g = _vec3(rho, 2.0)
+    for a in range(3):
+        d.fwhm[a] = float(f[a])
+        d.rho[a] = float(g[a])
+        d.axis[a] = float(axis[a])
+    d.depth = float(depth)
+    d.attenuation = float(attenuation)
+    M = np.eye(3) if rot is None else np.asarray(rot, np.float64).reshape(3, 3)
+    for i, v in enumerate(M.ravel()):
+        d.rot[i] = float(v)
+    if sites is not None:
+        _require_cuda(sites, "sites", torch.float64)
+        d.sites = ctypes.c_void_p(sites.data_ptr())
+        d.n_sites = int(sites.shape[0])
+    return d
+
+
+def emitters(desc: nat.EmittersDesc, n_images: int, n: int, key, stream: int = 0, first_image: int = 0,
+             device=None, out: Optional[torch.Tensor] = None, check: bool = False,
+             keep: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """(n_images * n, 4) float64 emitter rows [x, y, z, phase] drawn on the
+    device.  ``keep`` holds a tensor that ``desc`` points into alive for the call."""
+    lib = nat.load()
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    if out is None:
+        out = torch.empty((n_images * n, 4), dtype=torch.float64, device=dev)
+    elif out.shape != (n_images * n, 4) or out.dtype != torch.float64 or not out.is_contiguous():
+        raise ValueError("out must be a contiguous (n_images * n, 4) float64 tensor")
+    ws = WORKSPACES.get(lib.idiwf_emitters_workspace_size(ctypes.byref(desc), n_images, n), dev, "emitters")
+    rng = make_rng(key, stream, first_image)
+    nat.check(lib.idiwf_emitters(ctypes.byref(desc), int(n_images), int(n), ctypes.byref(rng),
+                                 ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                                 _stream(dev)))
+    if check:
+        _value_check(dev, "emitters")
     return out

@@ -66,20 +66,32 @@ def _pinned(key, nbytes):
 
 
 class _Stager:
-    """Pinned host staging of emitter blocks and their upload.  With a `key`,
-    the pinned buffer comes from a cache reused across calls."""
+    """Pinned host staging of emitter blocks and their upload (sources whose
+    ``ondevice`` is set draw on the GPU instead).  With a `key`, the pinned
+    buffer comes from a cache reused across calls."""
 
     def __init__(self, N, max_imgs, device, key=None):
         self.N = N
         self.device = device
-        if key is None:
-            self.host = torch.empty((max_imgs * N, 4), dtype=torch.float64, pin_memory=True)
+        self.max_imgs = max_imgs
+        self.key = key
+        self.host = None
+
+    def _alloc(self):
+        N, m = self.N, self.max_imgs
+        if self.key is None:
+            self.host = torch.empty((m * N, 4), dtype=torch.float64, pin_memory=True)
         else:
-            raw = _pinned(key, max_imgs * N * 32)
-            self.host = raw[: max_imgs * N * 32].view(torch.float64).view(max_imgs * N, 4)
+            raw = _pinned(self.key, m * N * 32)
+            self.host = raw[: m * N * 32].view(torch.float64).view(m * N, 4)
         self.hnp = self.host.numpy()
 
     def fill(self, simobject, n_img):
+        if getattr(simobject, "ondevice", False):
+            # the source draws straight into device memory (idiwf_emitters)
+            return simobject.device_batch(n_img, self.device)
+        if self.host is None:
+            self._alloc()
         N = self.N
         for i in range(n_img):
             pos, ph = simobject.get2()

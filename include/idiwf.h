@@ -297,6 +297,75 @@ idiwf_status idiwf_chargesharing(const void *counts, int32_t counts_dtype, int32
                                  double *out, void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* emitter sources on the device                                             */
+/* ------------------------------------------------------------------------ */
+
+/* emitter families (the reference's simulation objects, idi/simulation/simobj.py) */
+#define IDIWF_EMIT_SPHERE 0 /* uniform in a ball of radius r: rndSphere (idi/util/random.py:39-51), simobj.py:119-130 */
+#define IDIWF_EMIT_GNORM 1  /* generalised normal volume: gnorm / gauss (simobj.py:154-184,
+                               rndgennorm idi/util/random.py:6-26) */
+#define IDIWF_EMIT_FOIL 2   /* foil: in-plane generalised normal, depth uniform or truncated
+                               exponential (simobj.py:703-760, rndtruncexp idi/util/random.py:142-151) */
+#define IDIWF_EMIT_SITES 3  /* subsample of lattice sites without replacement, optionally
+                               weighted and randomly oriented: crystal.updatePos (simobj.py:446-487) */
+#define IDIWF_EMIT_FIXED 4  /* the same positions in every image (rndPos = False), new phases */
+
+/* SITES orientation per image */
+#define IDIWF_ORIENT_FIXED 0   /* positions = rot @ site */
+#define IDIWF_ORIENT_RANDOM 1  /* uniformly random rotation A per image (idi/util/random.py:130-139):
+                                  positions = A @ rot @ site */
+#define IDIWF_ORIENT_AXIS 2    /* random angle about `axis` (idi/util/__init__.py:338-345) */
+
+typedef struct idiwf_emitters_desc {
+    int32_t kind;         /* IDIWF_EMIT_* */
+    int32_t random_phase; /* nonzero: phase ~ U[0, 2 pi) per emitter and image (rndPhase); zero: 0 */
+    int32_t orientation;  /* SITES: IDIWF_ORIENT_* */
+    int32_t weighted;     /* SITES: weight site i by exp(-sum_a |x_a|^rho_a ln2 (2/fwhm_a)^rho_a)
+                             of its rotated position (the crystal's fwhm envelope) */
+    double r;             /* SPHERE: radius */
+    double fwhm[3];       /* GNORM: per axis; FOIL: [0], [1] in plane; SITES: envelope */
+    double rho[3];        /* shape (2 = Gaussian) of the same */
+    double depth;         /* FOIL: path through the foil, thickness / rot[8] */
+    double attenuation;   /* FOIL: attenuation length; not finite or <= 0: uniform depth */
+    double rot[9];        /* GNORM, FOIL, SITES, FIXED: row-major rotation applied to positions */
+    double axis[3];       /* SITES with IDIWF_ORIENT_AXIS */
+    const double *sites;  /* SITES, FIXED: DEVICE (n_sites, 3) float64 */
+    int64_t n_sites;      /* SITES: lattice sites; FIXED: must equal n */
+} idiwf_emitters_desc;
+
+size_t idiwf_emitters_workspace_size(const idiwf_emitters_desc *desc, int32_t n_images, int64_t n);
+
+/*
+ * Emitters of n_images images, n each, generated on the device into `atoms`
+ * (DEVICE, (n_images * n, 4) float64 [x, y, z, phase], the forward's input
+ * layout), replacing the host simobject.get2() draws that feed
+ * idi/simulation/cuda.py:89,115.  Emitter j of image b draws from the stream
+ * with counter (0, j, (rng->first_image + b) | 2^61, rng->stream): so a batch
+ * split into several calls (first_image) draws the same emitters.  The
+ * numbers differ from the reference's numpy draws; the distributions are the
+ * reference's.
+ *   SPHERE: t = 2u0 - 1, p = 2 pi u1, radius r cbrt(u2), phase 2 pi u3.
+ *   GNORM:  rho == 2 on every axis: x_a = N(0,1) fwhm_a / 2.355 (Box-Muller);
+ *           otherwise x_a = +-fwhm_a/2 (G_a / ln 2)^(1/rho_a), G_a ~
+ *           Gamma(1/rho_a) (G. Marsaglia, W. Tsang, ACM TOMS 26, 2000).  Then rot.
+ *   FOIL:   in plane as GNORM with fwhm / 2.35 (the reference's constant for
+ *           foils), mapped by rot's first two columns; z += depth draw:
+ *           -lam log1p(u expm1(-depth/lam)) or u depth.
+ *   SITES:  per image and round (n > n_sites takes ceil(n / n_sites) rounds of
+ *           at most n_sites distinct sites, as the reference's repeated
+ *           choice), the smallest keys -log(1-u_i)/w_i (weighted; u_i
+ *           otherwise) -- the successive weighted sampling without replacement
+ *           of numpy's choice(replace=False, p=w/sum w), by the exponential-key
+ *           method of P. Efraimidis, P. Spirakis (Inf. Proc. Letters 97, 2006)
+ *           -- selected by an exact radix select (ties by site index) and
+ *           written in site order.  Fewer positive weights than needed records
+ *           an invalid-value error.
+ *   FIXED:  sites[j] every image.
+ */
+idiwf_status idiwf_emitters(const idiwf_emitters_desc *desc, int32_t n_images, int64_t n, const idiwf_rng *rng,
+                            double *atoms, void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* tuning, diagnostics                                                       */
 /* ------------------------------------------------------------------------ */
 

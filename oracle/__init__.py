@@ -46,7 +46,8 @@ class OrcGeom(ctypes.Structure):
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(_HERE, f) for f in ("wavefield_oracle.c", "detector_oracle.c")]
+    srcs = [os.path.join(_HERE, f) for f in ("wavefield_oracle.c", "detector_oracle.c", "emitters_oracle.c",
+                                              "philox_oracle.h")]
     if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < max(map(os.path.getmtime, srcs)):
         subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
     return _LIB_PATH
@@ -87,6 +88,16 @@ def lib():
         L.orc_chargesharing.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, d, d, u64, u64, u64,
                                         u64, vp, vp, vp]
         L.orc_chargesharing.restype = None
+        L.orc_emit.argtypes = [ctypes.c_int, ctypes.c_int32, ctypes.c_int64, d, vp, vp, d, d, vp, ctypes.c_int,
+                               u64, u64, u64, u64, vp]
+        L.orc_emit.restype = None
+        L.orc_site_rotation.argtypes = [ctypes.c_int, vp, vp, u64, u64, u64, u64, vp]
+        L.orc_site_rotation.restype = None
+        L.orc_emit_sites.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int64, ctypes.c_int, vp, vp,
+                                     ctypes.c_int, vp, vp, ctypes.c_int, u64, u64, u64, u64, vp, vp]
+        L.orc_emit_sites.restype = None
+        L.orc_site_weights.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp]
+        L.orc_site_weights.restype = None
         _lib = L
     return _lib
 
@@ -275,3 +286,61 @@ def chargesharing(counts, s, ns=0.0, key=(0, 0), stream=0, positions=None, scale
                             int(first_image), pos.ctypes.data if pos is not None else None, sc.ctypes.data if sc is not None else None,
                             out.ctypes.data)
     return out.reshape(shape)
+
+
+# ---------------------------------------------------------------------------
+# emitter sources (emitters_oracle.c)
+# ---------------------------------------------------------------------------
+EMIT_KINDS = {"sphere": 0, "gnorm": 1, "foil": 2}
+
+
+def _v3(x, pad):
+    a = np.atleast_1d(np.asarray(x, np.float64)).ravel()
+    if a.size == 1:
+        a = np.repeat(a, 3)
+    return _c(np.concatenate([a[:3], np.full(max(0, 3 - a.size), pad)]))
+
+
+def emit(kind, n_images, n, key, stream=0, first_image=0, r=0.0, fwhm=1.0, rho=2.0, depth=0.0,
+         attenuation=np.inf, rot=None, random_phase=True) -> np.ndarray:
+    """(n_images * n, 4) rows of the sphere / gnorm / foil sources."""
+    out = np.empty((int(n_images) * int(n), 4))
+    f, g = _v3(fwhm, 1.0), _v3(rho, 2.0)
+    M = _c(np.eye(3) if rot is None else np.asarray(rot, np.float64).reshape(3, 3))
+    lib().orc_emit(EMIT_KINDS[kind], int(n_images), int(n), float(r), f.ctypes.data, g.ctypes.data, float(depth),
+                   float(attenuation), M.ctypes.data, int(bool(random_phase)), int(key[0]), int(key[1]), int(stream),
+                   int(first_image), out.ctypes.data)
+    return out
+
+
+def site_rotation(orientation, key, stream=0, image=0, axis=(0, 0, 1), rot=None) -> np.ndarray:
+    M = np.empty(9)
+    ax = _c(np.asarray(axis, np.float64))
+    R = _c(np.eye(3) if rot is None else np.asarray(rot, np.float64).reshape(3, 3))
+    lib().orc_site_rotation(int(orientation), ax.ctypes.data, R.ctypes.data, int(key[0]), int(key[1]), int(stream),
+                            int(image), M.ctypes.data)
+    return M.reshape(3, 3)
+
+
+def emit_sites(sites, n_images, n, key, stream=0, first_image=0, weighted=False, fwhm=1.0, rho=2.0, orientation=0,
+               axis=(0, 0, 1), rot=None, random_phase=True):
+    """(rows (n_images * n, 4), selected site index per row) of the lattice-site subsample."""
+    s = _c(sites)
+    out = np.empty((int(n_images) * int(n), 4))
+    sel = np.empty(int(n_images) * int(n), np.int64)
+    f, g = _v3(fwhm, 1.0), _v3(rho, 2.0)
+    ax = _c(np.asarray(axis, np.float64))
+    R = _c(np.eye(3) if rot is None else np.asarray(rot, np.float64).reshape(3, 3))
+    lib().orc_emit_sites(s.ctypes.data, s.shape[0], int(n_images), int(n), int(bool(weighted)), f.ctypes.data,
+                         g.ctypes.data, int(orientation), ax.ctypes.data, R.ctypes.data, int(bool(random_phase)),
+                         int(key[0]), int(key[1]), int(stream), int(first_image), out.ctypes.data, sel.ctypes.data)
+    return out, sel
+
+
+def site_weights(sites, fwhm, rho=2.0, rot=None) -> np.ndarray:
+    s = _c(sites)
+    w = np.empty(s.shape[0])
+    f, g = _v3(fwhm, 1.0), _v3(rho, 2.0)
+    R = _c(np.eye(3) if rot is None else np.asarray(rot, np.float64).reshape(3, 3))
+    lib().orc_site_weights(s.ctypes.data, s.shape[0], R.ctypes.data, f.ctypes.data, g.ctypes.data, w.ctypes.data)
+    return w

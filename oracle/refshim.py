@@ -50,6 +50,7 @@ _NE_FUNCS = {
     "abs": np.abs,
     "real": np.real,
     "imag": np.imag,
+    "sum": np.sum,  # numexpr's reduction sum(expr, axis=...)
 }
 
 

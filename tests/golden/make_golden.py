@@ -4,7 +4,8 @@
 
 Runs the reference's own CPU implementations -- ``idi/simulation/cpu.py``
 ``simulate``, ``idi/simulation/time.py`` ``simulate`` and
-``idi/simulation/common.py`` ``randomphotons`` / ``chargesharing`` -- unmodified, through
+``idi/simulation/common.py`` ``randomphotons`` / ``chargesharing`` and the
+simulation objects of ``idi/simulation/simobj.py`` -- unmodified, through
 ``oracle/refshim.py``, on seeded inputs (numpy Philox), and stores inputs and
 outputs.  For the time path it also records, per pixel, the arrival-time keys
 the reference computes and the order its ``_psort`` puts them in, by wrapping
@@ -191,6 +192,62 @@ def make_detector(ref):
     return out
 
 
+LATTICE_CASES = [
+    # name, class, args, kwargs
+    ("sc", "sc", (8000.0, 500, 3.6e-4), dict(repeats=[5, 6, 7])),
+    ("fcc", "fcc", (8000.0, 3000, 3.6e-4), dict(repeats=[6, 5, 4])),
+    ("hcp", "hcp", (8000.0, 800, 3.2e-4), dict(repeats=[5, 5, 6])),
+    ("cuso4", "cuso4", (700, 8000.0), dict(repeats=[4, 3, 5])),
+    ("fcc_rot_fwhm", "fcc", (8000.0, 3000, 3.6e-4), dict(rotangles=(0.1, 0.2, 0.3), fwhm=0.002)),
+]
+
+FOIL_CASES = [
+    dict(E=8000.0, excitation=1e6, thickness=0.01, fwhm=0.1),
+    dict(E=8000.0, excitation=3e5, thickness=0.02, fwhm=(0.1, 0.2), attenuationlength=0.01, rho=(2, 4),
+         rotangles=(0.3, 0, 0)),
+    dict(E=6400.0, excitation=2e5, thickness=0.005, fwhm=0.3, attenuationlength=0.002, rho=3),
+]
+
+
+def make_emitters(ref):
+    """Lattices (bit-exact targets), foil emitter counts, the crystal's fwhm
+    weights, and samples of the reference's own generators (sphere, gnorm,
+    rndgennorm, foil; numpy draws) plus per-site inclusion counts of its
+    weighted choice without replacement, for distribution tests."""
+    sim = ref.simobj
+    out = {}
+    for name, cls, args, kw in LATTICE_CASES:
+        obj = getattr(sim, cls)(*args, **kw)
+        out[f"lattice_{name}__sites"] = obj._allpos
+    obj = sim.fcc(8000.0, 3000, 3.6e-4, rotangles=(0.1, 0.2, 0.3), fwhm=0.002)
+    obj.updatePos()
+    out["crystal_weights__p"] = obj._p
+    out["foil__N"] = np.array([sim.foil(**kw).N for kw in FOIL_CASES])
+    n = 8000
+    s = sim.sphere(6400.0, n, 0.01)
+    s.rng = np.random.default_rng(7000)
+    out["sample_sphere"] = s.get2()[0]
+    g = sim.gnorm(6400.0, n, np.array([0.01, 0.02, 0.03]), 2)
+    g.rng = np.random.default_rng(7001)
+    out["sample_gnorm2"] = g.get2()[0]
+    out["sample_gennorm4"] = ref.util.rndgennorm(0, 0.01, 4, (n, 3), np.random.default_rng(7002))
+    f = sim.foil(8000.0, 1e6, 0.01, (0.1, 0.2), attenuationlength=0.005, rotangles=(0.2, 0, 0))
+    f.rng = np.random.default_rng(7003)
+    f._N = n
+    out["sample_foil"] = f.get2()[0]
+    # weighted choice without replacement: 3000 draws of 40 of 216 sc sites
+    c = sim.sc(8000.0, 40, 1e-3, repeats=[6, 6, 6], fwhm=0.003)
+    c.rng = np.random.default_rng(7004)
+    counts = np.zeros(len(c._allpos), np.int64)
+    for _ in range(3000):
+        c.updatePos()
+        idx = np.flatnonzero((c._allpos[:, None, :] == c._pos[None, :, :]).all(-1).any(1))
+        counts[idx] += 1
+    out["choice_sc__sites"] = c._allpos
+    out["choice_sc__counts"] = counts
+    return out
+
+
 def main():
     if not refshim.available():
         raise SystemExit("reference tree not available")
@@ -198,6 +255,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "forward_ref.npz"), **make_forward(ref))
     np.savez_compressed(os.path.join(HERE, "time_ref.npz"), **make_time(ref))
     np.savez_compressed(os.path.join(HERE, "detector_ref.npz"), **make_detector(ref))
+    np.savez_compressed(os.path.join(HERE, "emitters_ref.npz"), **make_emitters(ref))
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 
