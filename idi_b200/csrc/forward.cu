@@ -32,6 +32,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -829,6 +830,28 @@ static idiwf_status ensure_smem(void *fn, size_t bytes) {
     return IDIWF_OK;
 }
 
+// CTAs of `fn` that fit on one SM at this shape (cached per device).  The
+// persistent grid never exceeds SMs x this: a CTA that only starts after the
+// queue has drained would do no work and report a zero busy time.
+static int resident_ctas(void *fn, int threads, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<void *, int, int, size_t>, int> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    const auto key = std::make_tuple(fn, dev, threads, smem);
+    auto it = done.find(key);
+    if (it != done.end()) return it->second;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        occ = 1;
+    }
+    occ = std::max(occ, 1);
+    done[key] = occ;
+    return occ;
+}
+
 // Launch the forward for images [i0, i1) of the batch (records of the whole
 // batch are laid out by `rec_base`).
 static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, int precision,
@@ -888,7 +911,8 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
     const size_t smem = 2 * (size_t)s.te * (precision == IDIWF_SPLIT ? kSplitRecBytes : kDoubleRecBytes);
     idiwf_status st = ensure_smem(fn, smem);
     if (st != IDIWF_OK) return st;
-    const int grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * s.ctas_per_sm), kMaxCtas);
+    const int per_sm = std::min(s.ctas_per_sm, resident_ctas(fn, s.threads, smem));
+    const int grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * per_sm), kMaxCtas);
     if (precision == IDIWF_SPLIT) {
         SplitRecs rec = split_recs(ws, nrec);
         double2 *partials = ksplit > 1 ? reinterpret_cast<double2 *>(static_cast<char *>(ws) + kWsDataOffset +
@@ -1023,6 +1047,11 @@ extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *ba
     LaunchShape best_s = default_shape(precision);
     for (const LaunchShape &s : cands) {
         if (forward_ws_bytes(geom, batch, precision, s) > workspace_bytes) continue;
+        {  // more CTAs per SM than fit would only repeat a smaller candidate
+            void *fn = kernel_for(precision, s.ppt, geom->flags, false);
+            const size_t smem = 2 * (size_t)s.te * (precision == IDIWF_SPLIT ? kSplitRecBytes : kDoubleRecBytes);
+            if (ensure_smem(fn, smem) == IDIWF_OK && s.ctas_per_sm > resident_ctas(fn, s.threads, smem)) continue;
+        }
         st = forward_impl(geom, batch, precision, out_kind, out, workspace, workspace_bytes, s, stream);
         if (st != IDIWF_OK) break;
         float ms_best = 1e30f;
