@@ -231,7 +231,8 @@ def main():
                     help="small: 8 images on a 512x512 detector (profiling-sized capture of the same kernel)")
     ap.add_argument("--no-tune", action="store_true", help="use the default kernel shape instead of autotuning")
     ap.add_argument("--config", default=None, help='kernel shape as JSON, e.g. {"threads":256,"pixels_per_thread":4}')
-    ap.add_argument("--leg", default="main", choices=["main", "fwd_bwd", "time", "batched", "detector", "emitters"],
+    ap.add_argument("--leg", default="main",
+                    choices=["main", "fwd_bwd", "time", "batched", "detector", "emitters", "qcorr"],
                     help="run one secondary leg alone (for profiling) instead of the headline measurement")
     args = ap.parse_args()
     global N_IMG, NDET
@@ -415,6 +416,7 @@ def extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, 
     res["time_path"] = time_leg(torch, dev, _core, nat, args)
     res["detector"] = detector_leg(torch, dev, _core, nat, args, cuda=cuda, simobj=simobj, pos=pos, ph=ph, k=k)
     res["emitters"] = emitters_leg(torch, dev, _core, nat, args)
+    res["qcorr"] = qcorr_leg(torch, dev, args)
     return res
 
 
@@ -485,6 +487,8 @@ def single_leg(args):
         out = detector_leg(torch, dev, _core, nat, args)
     elif args.leg == "emitters":
         out = emitters_leg(torch, dev, _core, nat, args)
+    elif args.leg == "qcorr":
+        out = qcorr_leg(torch, dev, args)
     else:
         out = batched_leg(torch, dev, _core, nat)
     print(json.dumps({"leg": args.leg, **out}), flush=True)
@@ -682,6 +686,51 @@ def emitters_leg(torch, dev, _core, nat, args):
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": 4 * N_EMIT / dt, "unit": "emitters/s", "cores": 1, "kind": "port",
                                "sample": "numpy choice(157216, 50000, replace=False) + phases, 4 images"}
+    return out
+
+
+def qcorr_pairs(nr, nc, row_offsets, col_offsets):
+    """Pixel pairs the correlators visit: rows r, r + dr (dr in
+    [0, row_offsets)), columns c, c + dc (|dc| <= col_offsets)."""
+    rows = sum(max(0, nr - dr) for dr in range(row_offsets))
+    cols = sum(max(0, nc - abs(dc)) for dc in range(-col_offsets, col_offsets + 1))
+    return rows * cols
+
+
+def qcorr_leg(torch, dev, args):
+    """Direct q-space correlation of speckle images (exponential intensities):
+    radial, 512 x 512 at z = 2000 px, 256 bins, 4 images; 3d, 512 x 512 at
+    z = 2000 px, maxq 128, 2 images.  One unit = one pixel pair."""
+    from idi_b200.reconstruction import _geometry, cucor, cucorrad
+
+    g = np.random.default_rng(3)
+    out = {"workload": "radial: 4 x 512x512, z 2000 px, 256 bins; 3d: 2 x 512x512, z 2000 px, maxq 128"}
+    imgs = torch.from_numpy(g.exponential(1.0, (4, 512, 512)).astype(np.float32)).to(dev)
+    timed = timed_fn(torch)
+    with cucorrad.corrfunction((512, 512), 2000.0, 256, return_gpu=True) as f:
+        ms = timed(lambda: f(imgs), reps=3)
+    pairs = 4 * qcorr_pairs(512, 512, 256, 256)
+    out["radial"] = {"ms": ms, "pairs_per_s": pairs / (ms * 1e-3), "pairs": pairs}
+    with cucor.corrfunction((512, 512), 2000.0, 128) as f3:
+        ms3 = timed(lambda: f3(imgs[:2]), reps=2)
+    pairs3 = 2 * qcorr_pairs(512, 512, 128, 127)
+    out["3d"] = {"ms": ms3, "pairs_per_s": pairs3 / (ms3 * 1e-3), "pairs": pairs3,
+                 "note": "includes the device-to-host copy of the float64 volume, as the reference's corr()"}
+    if not args.no_cpu_baseline:
+        import oracle
+
+        # the oracle's restatement of the reference kernel (one thread) on the
+        # first 2 reference rows of image 0
+        sub = imgs[0].cpu().numpy()
+        q = _geometry.q_rows((512, 512), 2000.0)
+        rows = 2
+        # pairs whose reference row is 0 or 1 need target rows up to 1 + 255
+        t0 = time.perf_counter()
+        oracle.qcorr_radial(q[: (rows + 255) * 512], sub[: rows + 255], 256)
+        dt = time.perf_counter() - t0
+        sample = qcorr_pairs(rows + 255, 512, 256, 256)
+        out["cpu_baseline"] = {"value": sample / dt, "unit": "pairs/s", "cores": 1, "kind": "port",
+                               "sample": f"radial restatement on a {rows + 255} x 512 strip of image 0"}
     return out
 
 

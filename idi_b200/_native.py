@@ -71,6 +71,9 @@ EXPORTED = (
     "idiwf_chargesharing",
     "idiwf_emitters_workspace_size",
     "idiwf_emitters",
+    "idiwf_qcorr_workspace_size",
+    "idiwf_qcorr_radial",
+    "idiwf_qcorr_3d",
     "idiwf_tune",
     "idiwf_workspace_error",
     "idiwf_microbench",
@@ -203,6 +206,15 @@ def load():
     L.idiwf_emitters_workspace_size.restype = ctypes.c_size_t
     L.idiwf_emitters.argtypes = [P(EmittersDesc), ctypes.c_int32, ctypes.c_int64, P(Rng), vp, vp, ctypes.c_size_t, vp]
     L.idiwf_emitters.restype = st
+    L.idiwf_qcorr_workspace_size.argtypes = [ctypes.c_int32, ctypes.c_int32]
+    L.idiwf_qcorr_workspace_size.restype = ctypes.c_size_t
+    L.idiwf_qcorr_radial.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, vp,
+                                     ctypes.c_size_t, vp]
+    L.idiwf_qcorr_radial.restype = st
+    L.idiwf_qcorr_3d.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                 ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float, vp, vp,
+                                 ctypes.c_size_t, vp]
+    L.idiwf_qcorr_3d.restype = st
     L.idiwf_tune.argtypes = [P(Geom), P(Batch), ctypes.c_int32, ctypes.c_int32, vp, vp, ctypes.c_size_t, vp,
                              P(Config)]
     L.idiwf_tune.restype = st

@@ -30,6 +30,8 @@ __all__ = [
     "photons",
     "chargesharing",
     "emitters",
+    "qcorr_radial",
+    "qcorr_3d",
 ]
 
 
@@ -535,4 +537,41 @@ def emitters(desc: nat.EmittersDesc, n_images: int, n: int, key, stream: int = 0
                                  _stream(dev)))
     if check:
         _value_check(dev, "emitters")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# direct q-space correlators
+# ---------------------------------------------------------------------------
+def qcorr_radial(q: torch.Tensor, images: torch.Tensor, qmax: int) -> torch.Tensor:
+    """(B, qmax) float64 radial correlation of float32 images (B, nr, nc);
+    q: (nr * nc, 4) float32 [qx, qy, qz, 0] on the same device."""
+    lib = nat.load()
+    _require_cuda(q, "q", torch.float32)
+    _require_cuda(images, "images", torch.float32)
+    B, nr, nc = images.shape
+    dev = images.device
+    out = torch.empty((B, int(qmax)), dtype=torch.float64, device=dev)
+    ws = WORKSPACES.get(lib.idiwf_qcorr_workspace_size(nr, nc), dev, "qcorr")
+    nat.check(lib.idiwf_qcorr_radial(ctypes.c_void_p(q.data_ptr()), ctypes.c_void_p(images.data_ptr()), B, nr, nc,
+                                     int(qmax), ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
+                                     ws.numel(), _stream(dev)))
+    return out
+
+
+def qcorr_3d(zd: torch.Tensor, images: torch.Tensor, qmax: int, maxdqz: int, xcenter: float, ycenter: float,
+             z: float) -> torch.Tensor:
+    """(B, 2 maxdqz, 2 qmax, 2 qmax) float64 3d correlation of float32 images
+    (B, nr, nc); zd: (nr, nc) float32 z / d on the same device."""
+    lib = nat.load()
+    _require_cuda(zd, "zd", torch.float32)
+    _require_cuda(images, "images", torch.float32)
+    B, nr, nc = images.shape
+    dev = images.device
+    out = torch.empty((B, 2 * int(maxdqz), 2 * int(qmax), 2 * int(qmax)), dtype=torch.float64, device=dev)
+    ws = WORKSPACES.get(lib.idiwf_qcorr_workspace_size(nr, nc), dev, "qcorr")
+    nat.check(lib.idiwf_qcorr_3d(ctypes.c_void_p(zd.data_ptr()), ctypes.c_void_p(images.data_ptr()), B, nr, nc,
+                                 int(qmax), int(maxdqz), float(xcenter), float(ycenter), float(z),
+                                 ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                                 _stream(dev)))
     return out

@@ -366,6 +366,54 @@ idiwf_status idiwf_emitters(const idiwf_emitters_desc *desc, int32_t n_images, i
                             double *atoms, void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* direct q-space autocorrelation of detector images                         */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Both correlators sum v(p) v(p') over pixel pairs p = (r, c), p' = (r + dr,
+ * c + dc) with 0 <= dr < qmax and |dc| <= qmax (radial) or < qmax (3d), the
+ * pair set of the reference's launch grids, and bin each pair by the
+ * difference of the pixels' q vectors.  Each thread walks one column offset
+ * along a row pair and sums the products of consecutive pairs that fall in
+ * the same bin in FP32 before adding the run to the FP64 histogram (the
+ * radial reference kernel does the same; the 3d one adds every pair to FP32
+ * bins, which agree with these sums to FP32 rounding).  Images are
+ * (n_images, nr, nc) float32, DEVICE.  Results are deterministic up to the
+ * order of FP64 additions.
+ */
+size_t idiwf_qcorr_workspace_size(int32_t nr, int32_t nc);
+
+/*
+ * Radial correlation, idi/reconstruction/cucorrad.py:10-152: bin
+ * round(|q(p) - q(p')|) (FP32, round half to even), bins 0..qmax-1 into out
+ * (n_images, qmax) float64.  q: DEVICE (nr * nc, 4) float32 rows
+ * [qx, qy, qz, unused] (the reference's float32 q = k z / d), 16-byte
+ * aligned; nc <= 4096, qmax <= 511.  As in the reference, a run is added when
+ * the bin changes, and at the end of a row pair only if the last pair's bin
+ * is below qmax (cucorrad.py:102-116).
+ */
+idiwf_status idiwf_qcorr_radial(const float *q, const float *images, int32_t n_images, int32_t nr, int32_t nc,
+                                int32_t qmax, double *out, void *workspace, size_t workspace_bytes,
+                                cudaStream_t stream);
+
+/*
+ * 3d correlation, idi/reconstruction/cucor.py:10-128: bin
+ *   (maxdqz + round(z (zd(p) - zd(p'))),
+ *    qmax + round((c' - yc) zd(p') - (c - yc) zd(p)),
+ *    qmax + round((r' - xc) zd(p') - (r - xc) zd(p)))
+ * (FP32, round half to even) into out (n_images, 2 maxdqz, 2 qmax, 2 qmax)
+ * float64, then symmetrise it about the centre as the reference's assemble
+ * step does (cucor.py:101-104, x extent of its launch): bins i and -i (mod
+ * the shape) both receive the sum of the two, a bin that is its own mirror
+ * doubles.  zd: DEVICE (nr, nc) float32 z / d; nc <= 8192, qmax <= 1024.
+ * Pairs whose bin falls outside the array are dropped (the reference's kernel
+ * writes them past the end of its array).
+ */
+idiwf_status idiwf_qcorr_3d(const float *zd, const float *images, int32_t n_images, int32_t nr, int32_t nc,
+                            int32_t qmax, int32_t maxdqz, float xcenter, float ycenter, float z, double *out,
+                            void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* tuning, diagnostics                                                       */
 /* ------------------------------------------------------------------------ */
 

@@ -47,7 +47,7 @@ class OrcGeom(ctypes.Structure):
 
 def build(force: bool = False) -> str:
     srcs = [os.path.join(_HERE, f) for f in ("wavefield_oracle.c", "detector_oracle.c", "emitters_oracle.c",
-                                              "philox_oracle.h")]
+                                              "qcorr_oracle.c", "philox_oracle.h")]
     if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < max(map(os.path.getmtime, srcs)):
         subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
     return _LIB_PATH
@@ -98,6 +98,12 @@ def lib():
         L.orc_emit_sites.restype = None
         L.orc_site_weights.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp]
         L.orc_site_weights.restype = None
+        i32 = ctypes.c_int32
+        L.orc_qcorr_radial.argtypes = [vp, vp, i32, i32, i32, i32, vp]
+        L.orc_qcorr_radial.restype = None
+        L.orc_qcorr_3d.argtypes = [vp, vp, i32, i32, i32, i32, i32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                   vp]
+        L.orc_qcorr_3d.restype = None
         _lib = L
     return _lib
 
@@ -344,3 +350,31 @@ def site_weights(sites, fwhm, rho=2.0, rot=None) -> np.ndarray:
     R = _c(np.eye(3) if rot is None else np.asarray(rot, np.float64).reshape(3, 3))
     lib().orc_site_weights(s.ctypes.data, s.shape[0], R.ctypes.data, f.ctypes.data, g.ctypes.data, w.ctypes.data)
     return w
+
+
+# ---------------------------------------------------------------------------
+# direct q-space correlators (qcorr_oracle.c)
+# ---------------------------------------------------------------------------
+def qcorr_radial(q, images, qmax) -> np.ndarray:
+    """(B, qmax) radial correlation; q (nr*nc, 4) float32, images (B, nr, nc)."""
+    qq = _c(q, np.float32)
+    im = _c(images, np.float32)
+    if im.ndim == 2:
+        im = im[None]
+    B, nr, nc = im.shape
+    out = np.empty((B, int(qmax)))
+    lib().orc_qcorr_radial(qq.ctypes.data, im.ctypes.data, B, nr, nc, int(qmax), out.ctypes.data)
+    return out
+
+
+def qcorr_3d(zd, images, qmax, maxdqz, xcenter, ycenter, z) -> np.ndarray:
+    """(B, 2 maxdqz, 2 qmax, 2 qmax) 3d correlation; zd (nr, nc) float32."""
+    zz = _c(zd, np.float32)
+    im = _c(images, np.float32)
+    if im.ndim == 2:
+        im = im[None]
+    B, nr, nc = im.shape
+    out = np.empty((B, 2 * int(maxdqz), 2 * int(qmax), 2 * int(qmax)))
+    lib().orc_qcorr_3d(zz.ctypes.data, im.ctypes.data, B, nr, nc, int(qmax), int(maxdqz), float(xcenter),
+                       float(ycenter), float(z), out.ctypes.data)
+    return out
