@@ -698,9 +698,10 @@ def qcorr_pairs(nr, nc, row_offsets, col_offsets):
 
 
 def qcorr_leg(torch, dev, args):
-    """Direct q-space correlation of speckle images (exponential intensities):
-    radial, 512 x 512 at z = 2000 px, 256 bins, 4 images; 3d, 512 x 512 at
-    z = 2000 px, maxq 128, 2 images.  One unit = one pixel pair."""
+    """Correlation of speckle images (exponential intensities): direct radial,
+    512 x 512 at z = 2000 px, 256 bins, 4 images; direct 3d, 512 x 512 at
+    z = 2000 px, maxq 128, 2 images (one unit = one pixel pair); FFT
+    autocorrelation of 8 x 1024 x 1024."""
     from idi_b200.reconstruction import _geometry, cucor, cucorrad
 
     g = np.random.default_rng(3)
@@ -716,6 +717,12 @@ def qcorr_leg(torch, dev, args):
     pairs3 = 2 * qcorr_pairs(512, 512, 128, 127)
     out["3d"] = {"ms": ms3, "pairs_per_s": pairs3 / (ms3 * 1e-3), "pairs": pairs3,
                  "note": "includes the device-to-host copy of the float64 volume, as the reference's corr()"}
+    from idi_b200.reconstruction import cusimple
+
+    stack = torch.from_numpy(g.exponential(1.0, (8, 1024, 1024))).to(dev)
+    msf = timed(lambda: cusimple.corr(stack, returngpu=True), reps=3)
+    out["fft_corr"] = {"ms": msf, "images_per_s": 8 / (msf * 1e-3),
+                       "workload": "cusimple.corr of 8 x 1024x1024 float64 (2048^2 transforms), on the device"}
     if not args.no_cpu_baseline:
         import oracle
 

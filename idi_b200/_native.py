@@ -74,6 +74,9 @@ EXPORTED = (
     "idiwf_qcorr_workspace_size",
     "idiwf_qcorr_radial",
     "idiwf_qcorr_3d",
+    "idiwf_power_spectrum",
+    "idiwf_corr_crop",
+    "idiwf_welford_update",
     "idiwf_tune",
     "idiwf_workspace_error",
     "idiwf_microbench",
@@ -215,6 +218,13 @@ def load():
                                  ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float, vp, vp,
                                  ctypes.c_size_t, vp]
     L.idiwf_qcorr_3d.restype = st
+    L.idiwf_power_spectrum.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, vp]
+    L.idiwf_power_spectrum.restype = st
+    L.idiwf_corr_crop.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, P(ctypes.c_int32),
+                                  P(ctypes.c_int32), vp, ctypes.c_int32, ctypes.c_double, vp, vp]
+    L.idiwf_corr_crop.restype = st
+    L.idiwf_welford_update.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_int64, vp]
+    L.idiwf_welford_update.restype = st
     L.idiwf_tune.argtypes = [P(Geom), P(Batch), ctypes.c_int32, ctypes.c_int32, vp, vp, ctypes.c_size_t, vp,
                              P(Config)]
     L.idiwf_tune.restype = st

@@ -1,0 +1,180 @@
+"""Drop-in for ``idi.reconstruction.cusimple``: FFT autocorrelation on the GPU
+(``idi/reconstruction/cusimple.py:6-121``).
+
+The transforms are cuFFT's (through ``torch.fft``); the power spectrum, the
+fftshift + centre crop with its normalisation and the correlator's running
+mean / variance are this library's kernels (``idiwf_power_spectrum``,
+``idiwf_corr_crop``, ``idiwf_welford_update``).  Inputs may be numpy arrays
+or CUDA tensors; results are numpy unless ``returngpu``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import functools
+
+import numpy as np
+import torch
+
+from .. import _native as nat
+from ..simulation import _core
+
+__all__ = ["corr", "correlator2d", "fastlen"]
+
+
+@functools.lru_cache(maxsize=None)
+def fastlen(x, factors=(2, 3, 5, 7, 11)):
+    """Smallest N >= x whose prime factors are all in ``factors`` (FFT-friendly length)."""
+    n = max(1, int(np.ceil(x)))
+    while True:
+        m = n
+        for f in factors:
+            while m % f == 0:
+                m //= f
+        if m == 1:
+            return n
+        n += 1
+
+
+def _device():
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _code(t):
+    if t.dtype == torch.float64 or t.dtype == torch.complex128:
+        return nat.F64
+    if t.dtype == torch.float32 or t.dtype == torch.complex64:
+        return nat.F32
+    raise ValueError(f"unsupported dtype {t.dtype}")
+
+
+def _stream(dev):
+    return ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+
+def _power_(spec):
+    nat.check(nat.load().idiwf_power_spectrum(ctypes.c_void_p(spec.data_ptr()), spec.numel(), _code(spec),
+                                              _stream(spec.device)))
+    return spec
+
+
+def _crop(full, nax, halves, norm=None, mode=0, threshold=0.0):
+    """Centre crop of the last ``nax`` axes of ``full`` (batch leading)."""
+    full = full.contiguous()
+    g = (ctypes.c_int32 * nax)(*full.shape[-nax:])
+    n = (ctypes.c_int32 * nax)(*halves)
+    lead = full.shape[:-nax]
+    batch = int(np.prod(lead)) if lead else 1
+    out = torch.empty(tuple(lead) + tuple(2 * h for h in halves), dtype=full.dtype, device=full.device)
+    if norm is not None:
+        norm = norm.to(full.dtype).contiguous()
+    nat.check(nat.load().idiwf_corr_crop(
+        ctypes.c_void_p(full.data_ptr()), _code(full), batch, nax, g, n,
+        ctypes.c_void_p(norm.data_ptr()) if norm is not None else None, int(mode), float(threshold),
+        ctypes.c_void_p(out.data_ptr()), _stream(full.device)))
+    return out
+
+
+def _autocorr(x, nax, fftshape):
+    """Autocorrelation along the last ``nax`` axes, uncropped: irfftn(|rfftn(x, s)|^2)
+    with the inverse's default sizes, as the reference's calls."""
+    dims = tuple(range(-nax, 0))
+    spec = torch.fft.rfftn(x, s=fftshape, dim=dims)
+    _power_(spec)
+    return torch.fft.irfftn(spec, dim=dims)
+
+
+def corr(input, axes=(-1, -2), norm=False, returngpu=False, **kwargs):
+    """Autocorrelation of ``input`` along ``axes`` (default the last two),
+    output 2n per correlated axis with zero shift at index n.  ``norm``
+    divides by the mean over the other axes (over everything when there are
+    none) and by the pair count, with NaN where fewer than 0.9 pairs overlap."""
+    x = input if isinstance(input, torch.Tensor) else torch.from_numpy(np.asarray(input))
+    x = x.to(_device())
+    if not x.is_floating_point():
+        x = x.to(torch.float64)
+    axes = sorted([x.ndim + a if a < 0 else a for a in axes])
+    others = [i for i in range(x.ndim) if i not in axes]
+    sizes = [x.shape[a] for a in axes]
+    fftshape = [fastlen(2 * s) for s in sizes]
+    if norm:
+        x = x * (1 / x.mean(dim=others if others else None, keepdim=bool(others)))
+    moved = torch.movedim(x, axes, list(range(x.ndim - len(axes), x.ndim))).contiguous()
+    full = _autocorr(moved, len(axes), fftshape)
+    pairs = None
+    if norm:
+        ones = torch.ones(sizes, dtype=x.dtype, device=x.device)
+        pairs = _crop(_autocorr(ones, len(axes), fftshape), len(axes), sizes)
+    ret = _crop(full, len(axes), sizes, norm=pairs, mode=0, threshold=0.9)
+    ret = torch.movedim(ret, list(range(x.ndim - len(axes), x.ndim)), axes)
+    if returngpu:
+        return ret
+    return ret.cpu().numpy()
+
+
+class correlator2d:
+    """Running 2D autocorrelation divided by the mask autocorrelation
+    (``idi/reconstruction/cusimple.py:40-121``), FP32 like the reference:
+    ``add(image, mask=None)`` accumulates, ``mean`` / ``std`` / ``n`` report."""
+
+    def __init__(self, mask=None, norm=True) -> None:
+        self._fftshape = None
+        self._dev = _device()
+        if mask is not None:
+            m = torch.as_tensor(np.asarray(mask) if not isinstance(mask, torch.Tensor) else mask)
+            self._mask = m.to(self._dev, torch.float32)
+            self._maskcorr = self._corr(self._mask)
+        else:
+            self._mask = None
+            self._maskcorr = None
+        self._mean = None
+        self._nvar = None
+        self._n = 0
+        self._norm = norm
+
+    def _corr(self, x):
+        if self._fftshape is None:
+            self._fftshape = [fastlen(2 * s) for s in x.shape[-2:]]
+        return _crop(_autocorr(x, 2, self._fftshape), 2, list(x.shape[-2:]))
+
+    def add(self, input, mask=None) -> None:
+        if np.ndim(input) != 2:
+            raise ValueError("input must be 2D.")
+        x = input if isinstance(input, torch.Tensor) else torch.from_numpy(np.asarray(input))
+        x = x.to(self._dev, torch.float32).clone()
+        if self._norm:
+            x /= x.mean()
+        if mask is not None:
+            m = torch.as_tensor(np.asarray(mask) if not isinstance(mask, torch.Tensor) else mask)
+            m = m.to(self._dev, torch.float32)
+            x *= m
+            maskcorr = self._corr(m)
+        elif self._mask is not None:
+            x *= self._mask
+            maskcorr = self._maskcorr
+        elif self._maskcorr is not None:
+            maskcorr = self._maskcorr
+        else:
+            maskcorr = self._corr(torch.ones_like(x))
+            self._maskcorr = maskcorr
+        c = _crop(_autocorr(x, 2, self._fftshape or [fastlen(2 * s) for s in x.shape]), 2, list(x.shape),
+                  norm=maskcorr, mode=1, threshold=0.5)
+        if self._mean is None:
+            self._mean = torch.empty_like(c)
+            self._nvar = torch.empty_like(c)
+        self._n += 1
+        nat.check(nat.load().idiwf_welford_update(ctypes.c_void_p(c.data_ptr()), ctypes.c_void_p(self._mean.data_ptr()),
+                                                  ctypes.c_void_p(self._nvar.data_ptr()), c.numel(), self._n,
+                                                  _stream(self._dev)))
+
+    @property
+    def mean(self) -> np.ndarray:
+        return self._mean.cpu().numpy()
+
+    @property
+    def n(self) -> int:
+        return self._n
+
+    @property
+    def std(self) -> np.ndarray:
+        return torch.sqrt(self._nvar / self._n).cpu().numpy()

@@ -414,6 +414,39 @@ idiwf_status idiwf_qcorr_3d(const float *zd, const float *images, int32_t n_imag
                             void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* FFT autocorrelation helpers (the transforms are the caller's, e.g. cuFFT)  */
+/* ------------------------------------------------------------------------ */
+
+/* In place |X|^2 of n complex values (dtype IDIWF_F64: complex128, IDIWF_F32:
+ * complex64): re <- re^2 + im^2, im <- 0.  The `ret = abs(ret) ** 2` of
+ * idi/reconstruction/cusimple.py:20 and :70. */
+idiwf_status idiwf_power_spectrum(void *spectrum, int64_t n, int32_t dtype, cudaStream_t stream);
+
+/*
+ * Centre crop of an inverse-transformed autocorrelation, fused with its
+ * normalisation: for every batch entry b and index i (up to 3 trailing axes),
+ *     y = full[b, (i_k - n_k) mod g_k ...]      (fftshift, then the
+ *                                                 [F/2 - n, F/2 + n) slice)
+ * full: (batch, g...) of dtype, out: (batch, 2n...) of dtype.  With `norm`
+ * ((2n...) of dtype): mode 0 gives y / norm, NaN where norm < threshold
+ * (cusimple.py:23-34); mode 1 gives y / norm where norm > threshold, else 0
+ * (the correlator's division, cusimple.py:38).  Without norm, y.
+ * Replaces the fftshift / slice / divide steps of cusimple.py:22-34,72-95.
+ */
+idiwf_status idiwf_corr_crop(const void *full, int32_t dtype, int64_t batch, int32_t ndim, const int32_t *g,
+                             const int32_t *n, const void *norm, int32_t mode, double threshold, void *out,
+                             cudaStream_t stream);
+
+/*
+ * The running mean / variance update of idi/reconstruction/cusimple.py:97-105
+ * (Welford), FP32 like the reference: with count the number of samples after
+ * adding x, count == 1 sets mean = x, nvar = 0; otherwise
+ * delta = x - mean, mean += delta / count, nvar += delta (x - mean).
+ */
+idiwf_status idiwf_welford_update(const float *x, float *mean, float *nvar, int64_t n, int64_t count,
+                                  cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* tuning, diagnostics                                                       */
 /* ------------------------------------------------------------------------ */
 

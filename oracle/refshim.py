@@ -124,6 +124,22 @@ def load():
     return types.SimpleNamespace(**_cache)
 
 
+def load_module(relname: str):
+    """One more module of the reference package, e.g. ``reconstruction.cpusimple``
+    (after :func:`load`; a subpackage is registered as an empty package, so its
+    ``__init__`` with GPU imports does not run)."""
+    load()
+    idi_dir = os.path.join(REF_ROOT, "idi")
+    parts = relname.split(".")
+    for i in range(1, len(parts)):
+        pkg = f"{_PKG}." + ".".join(parts[:i])
+        if pkg not in sys.modules:
+            m = types.ModuleType(pkg)
+            m.__path__ = [os.path.join(idi_dir, *parts[:i])]
+            sys.modules[pkg] = m
+    return _load(relname, os.path.join(idi_dir, *parts[:-1], parts[-1] + ".py"))
+
+
 class InjectedObject:
     """Duck-typed simobject (``.N``, ``.k``, ``.E``, ``.get()``, ``.get2()``) over fixed arrays.
 

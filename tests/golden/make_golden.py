@@ -4,8 +4,9 @@
 
 Runs the reference's own CPU implementations -- ``idi/simulation/cpu.py``
 ``simulate``, ``idi/simulation/time.py`` ``simulate`` and
-``idi/simulation/common.py`` ``randomphotons`` / ``chargesharing`` and the
-simulation objects of ``idi/simulation/simobj.py`` -- unmodified, through
+``idi/simulation/common.py`` ``randomphotons`` / ``chargesharing``, the
+simulation objects of ``idi/simulation/simobj.py`` and
+``idi/reconstruction/cpusimple.py`` -- unmodified, through
 ``oracle/refshim.py``, on seeded inputs (numpy Philox), and stores inputs and
 outputs.  For the time path it also records, per pixel, the arrival-time keys
 the reference computes and the order its ``_psort`` puts them in, by wrapping
@@ -224,6 +225,12 @@ def make_emitters(ref):
     out["crystal_weights__p"] = obj._p
     out["foil__N"] = np.array([sim.foil(**kw).N for kw in FOIL_CASES])
     n = 8000
+    # sphere.updatePos and foil.updatePos call rndSphere / rndtruncexp
+    # without a generator (fresh OS entropy each run); wrapped here to pass a
+    # seeded one so the fixture is reproducible
+    orig_sphere, orig_texp = sim._rndSphere, sim._rndtruncexp
+    sim._rndSphere = lambda r, N: ref.util.rndSphere(r, N, rng=np.random.default_rng(7005))
+    sim._rndtruncexp = lambda lam, b, N: ref.util.rndtruncexp(lam, b, N, rng=np.random.default_rng(7006))
     s = sim.sphere(6400.0, n, 0.01)
     s.rng = np.random.default_rng(7000)
     out["sample_sphere"] = s.get2()[0]
@@ -235,6 +242,7 @@ def make_emitters(ref):
     f.rng = np.random.default_rng(7003)
     f._N = n
     out["sample_foil"] = f.get2()[0]
+    sim._rndSphere, sim._rndtruncexp = orig_sphere, orig_texp
     # weighted choice without replacement: 3000 draws of 40 of 216 sc sites
     c = sim.sc(8000.0, 40, 1e-3, repeats=[6, 6, 6], fwhm=0.003)
     c.rng = np.random.default_rng(7004)
@@ -248,6 +256,42 @@ def make_emitters(ref):
     return out
 
 
+def make_fftcorr(ref):
+    """``idi/reconstruction/cpusimple.py`` (the numpy twin of the cupy
+    ``cusimple``, which needs cupy): ``corr`` on the reference test's inputs
+    and on seeded stacks, and ``correlator2d`` with and without masks."""
+    simple = refshim.load_module("reconstruction.cpusimple")
+    out = {}
+    t1 = np.arange(32 * 16).reshape(32, 16).astype(float)
+    out["corr_arange__in"] = t1
+    out["corr_arange__out"] = simple.corr(t1)
+    t2 = np.arange(15 * 33).reshape(15, 33).astype(float)
+    out["corr_arange_norm__in"] = t2
+    out["corr_arange_norm__out"] = simple.corr(t2, norm=True)
+    g = np.random.Generator(np.random.Philox(9000))
+    st = g.exponential(1.0, (3, 20, 24))
+    out["corr_stack__in"] = st
+    out["corr_stack__out"] = simple.corr(st)
+    # cusimple turns the axes positive before picking the mean's axes
+    # (cusimple.py:13,17); cpusimple compares the negative defaults and would
+    # average over everything, so pass them positive to get cusimple's result
+    out["corr_stack_norm__out"] = simple.corr(st, axes=(1, 2), norm=True)
+    line = g.exponential(1.0, (4, 30))
+    out["corr_line__in"] = line
+    out["corr_line__out"] = simple.corr(line, axes=(-1,))
+    imgs = g.exponential(1.0, (3, 20, 24)).astype(np.float32)
+    mask = (g.uniform(0, 1, (20, 24)) > 0.2).astype(np.float32)
+    out["c2d__images"] = imgs
+    out["c2d__mask"] = mask
+    for name, kw, per_add in (("plain", {}, None), ("mask", {"mask": mask}, None), ("addmask", {}, mask)):
+        c = simple.correlator2d(**kw)
+        for im in imgs:
+            c.add(im, mask=per_add) if per_add is not None else c.add(im)
+        out[f"c2d_{name}__mean"] = c.mean
+        out[f"c2d_{name}__std"] = c.std
+    return out
+
+
 def main():
     if not refshim.available():
         raise SystemExit("reference tree not available")
@@ -256,6 +300,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "time_ref.npz"), **make_time(ref))
     np.savez_compressed(os.path.join(HERE, "detector_ref.npz"), **make_detector(ref))
     np.savez_compressed(os.path.join(HERE, "emitters_ref.npz"), **make_emitters(ref))
+    np.savez_compressed(os.path.join(HERE, "fftcorr_ref.npz"), **make_fftcorr(ref))
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 

@@ -1,0 +1,69 @@
+"""FFT autocorrelation on the device (cuFFT transforms, this library's power
+spectrum / crop / running-statistics kernels) against the reference's numpy
+twin ``idi/reconstruction/cpusimple.py`` (fixtures) and the reference's own
+checks against scipy (``tests/test_recon.py:106-121``)."""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from idi_b200.reconstruction import cusimple
+from tests.conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return np.load(os.path.join(GOLDEN, "fftcorr_ref.npz"))
+
+
+def test_corr_known_answers():
+    import scipy.signal as ss
+
+    t = np.arange(32 * 16).reshape(32, 16).astype(float)
+    c = cusimple.corr(t)
+    np.testing.assert_allclose(c[1:, 1:], ss.correlate(t, t, "full", "fft"), atol=1e-7)
+    t = np.arange(15 * 33).reshape(15, 33).astype(float)
+    c = cusimple.corr(t, norm=True)
+    gc = ss.correlate(t / t.mean(), t / t.mean(), "full", "fft")
+    gn = ss.correlate(np.ones_like(t), np.ones_like(t), "full", "fft")
+    g = gc / gn
+    g[gn < 0.9] = np.nan
+    np.testing.assert_allclose(c[1:, 1:], g, atol=1e-7)
+
+
+@pytest.mark.parametrize("name,kw", [("corr_arange", {}), ("corr_arange_norm", {"norm": True})])
+def test_corr_reference(golden, name, kw):
+    out = cusimple.corr(golden[f"{name}__in"], **kw)
+    ref = golden[f"{name}__out"]
+    np.testing.assert_allclose(out, ref, rtol=1e-10, atol=1e-9 * np.nanmax(np.abs(ref)))
+
+
+def test_corr_stack_and_line(golden):
+    st = golden["corr_stack__in"]
+    for key, kw in (("corr_stack__out", {}), ("corr_stack_norm__out", {"norm": True})):
+        ref = golden[key]
+        np.testing.assert_allclose(cusimple.corr(st, **kw), ref, rtol=1e-10, atol=1e-10 * np.nanmax(np.abs(ref)))
+    ref = golden["corr_line__out"]
+    np.testing.assert_allclose(cusimple.corr(golden["corr_line__in"], axes=(-1,)), ref, rtol=1e-10,
+                               atol=1e-10 * np.abs(ref).max())
+    g = cusimple.corr(torch.from_numpy(st).cuda(), returngpu=True)
+    assert g.is_cuda and g.shape == (3, 40, 48)
+
+
+@pytest.mark.parametrize("name", ["plain", "mask", "addmask"])
+def test_correlator2d_reference(golden, name):
+    imgs, mask = golden["c2d__images"], golden["c2d__mask"]
+    c = cusimple.correlator2d(mask=mask) if name == "mask" else cusimple.correlator2d()
+    for im in imgs:
+        if name == "addmask":
+            c.add(im, mask=mask)
+        else:
+            c.add(im)
+    assert c.n == len(imgs)
+    for attr in ("mean", "std"):
+        ref = golden[f"c2d_{name}__{attr}"]
+        np.testing.assert_allclose(getattr(c, attr), ref, rtol=2e-4, atol=2e-4 * np.abs(ref).max())
