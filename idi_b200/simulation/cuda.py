@@ -24,7 +24,7 @@ import torch
 from .. import _native as nat
 from . import _core
 
-__all__ = ["simulate", "simulate_gen", "simulate_photons"]
+__all__ = ["simulate", "simulate_gen", "simulate_photons", "simulate_to_npz"]
 
 # output bytes per launch in simulate(): bounds device memory for large Nimg
 _MAX_OUT_BYTES = 1 << 30
@@ -220,12 +220,15 @@ def simulate(
 
 
 def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, out_dtype, amplitudes, verbose,
-               result_dtype, post=None):
+               result_dtype, post=None, sink=None):
     """Chunked device pipeline with host output: chunk i's device-to-host copy
     (pinned staging, second stream) overlaps chunk i+1's emitter upload and
     kernels.  ``post(field_or_intensity, first_image, slot)`` runs further device
     work on a chunk and returns the tensor to copy back (default: the forward
-    output).  Ctrl-C returns the images finished so far."""
+    output).  With ``sink(first_image, array)`` every chunk goes to the sink
+    (which must consume it before returning) instead of into one result array,
+    and the images finished are counted instead.  Ctrl-C returns the images
+    finished so far."""
     result = None
     compute = torch.cuda.current_stream(dev)
     copy = torch.cuda.Stream(dev)
@@ -238,9 +241,15 @@ def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, 
     pending = None  # (slot, start, count) of the chunk whose copy is in flight
     done = 0
 
+    finished = [0]
+
     def _collect(ps, pstart, pn):
         ev_copied[ps].synchronize()
-        result[pstart:pstart + pn] = h_out[ps][:pn].numpy()
+        if sink is not None:
+            sink(pstart, h_out[ps][:pn].numpy())
+        else:
+            result[pstart:pstart + pn] = h_out[ps][:pn].numpy()
+        finished[0] = pstart + pn
         if verbose:
             print(pstart + pn, end=". ", flush=True)
 
@@ -263,7 +272,7 @@ def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, 
                 per = src[0].numel() * src.element_size()
                 raw = _pinned(("sim_out", dev.index, slot), chunk * per)
                 h_out[slot] = raw[: chunk * per].view(src.dtype).view((chunk,) + tuple(src.shape[1:]))
-            if result is None:
+            if result is None and sink is None:
                 result = np.empty((Nimg,) + tuple(src.shape[1:]), result_dtype)
             ev_done[slot].record(compute)
             copy.wait_event(ev_done[slot])
@@ -276,14 +285,63 @@ def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, 
             done += nb
             i += 1
         _collect(*pending)
-        return result
+        return finished[0] if sink is not None else result
     except KeyboardInterrupt:
         if verbose:
             print("Interrupted")
         torch.cuda.synchronize(dev)
+        if sink is not None:
+            return finished[0]
         if result is None:
             return np.empty((0, Ndet[0], Ndet[1]), result_dtype)
         return result[: pending[1] if pending else 0]
+
+
+def simulate_to_npz(
+    outfile,
+    Nimg,
+    simobject,
+    Ndet,
+    pixelsize,
+    detz,
+    k=None,
+    settings="double",
+    verbose=True,
+    detangles=(0, 0),
+    detoffset=(0, 0),
+    *args,
+    extra=None,
+    compress=True,
+    amplitudes=None,
+    device=None,
+    **kwargs,
+):
+    """``Nimg`` intensity images |E|^2 written to ``outfile`` as the ``.npz``
+    of ``scripts/idi_sim.py:86-88``: array ``result`` (Nimg, Nx, Ny) float64,
+    plus the arrays of ``extra`` (e.g. the run's settings).  The intensities
+    are formed on the device (8 bytes per pixel cross PCIe instead of 16) and
+    streamed into the archive chunk by chunk, so host memory holds two chunks,
+    not the run.  Arguments as :func:`simulate`.  Returns the number of
+    images written (fewer after Ctrl-C, in which case the file is incomplete
+    and raises on close)."""
+    from .output import NpzStream
+
+    Ndet, geom, precision, _ = _setup(simobject, Ndet, pixelsize, detz, k, settings, detangles, detoffset)
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    N = int(simobject.N)
+    Nimg = int(Nimg)
+    per_img = Ndet[0] * Ndet[1] * 8
+    cap = int(max(1, _MAX_OUT_BYTES // max(per_img, 1)))
+    nchunks = 4 if (per_img * Nimg >= (64 << 20) and Nimg >= 4) else 1
+    chunk = int(max(1, min(cap, -(-Nimg // nchunks))))
+    with NpzStream(outfile, compress=compress) as npz:
+        member = npz.array("result", (Nimg, Ndet[0], Ndet[1]), np.float64)
+        done = _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, nat.OUT_I64, torch.float64,
+                          amplitudes, verbose, np.float64, sink=lambda first, a: member.write(a))
+        npz.close_array()
+        for name, value in (extra or {}).items():
+            npz.add(name, value)
+    return done
 
 
 def simulate_photons(
