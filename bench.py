@@ -572,6 +572,15 @@ def time_leg(torch, dev, _core, nat, args):
     pairs = nimg * n * 256 * 256
     out = {"workload": "20k emitters, 10 nm sphere, 5 fs FWHM emission, tau 2 fs, 256x256 @ 75 um, 0.1 m, 4 images",
            "ms": ms, "pairs_per_s": pairs / (ms * 1e-3)}
+    # above the on-chip table: 200,000 emitters, 64x64 detector, one image
+    nl = 200000
+    posl = sphere_points(g, nl, 0.01)
+    atl = torch.from_numpy(np.concatenate([posl, g.uniform(0, 2 * np.pi, (nl, 1))], 1)).to(dev)
+    tl = torch.from_numpy(g.normal(0, 5.0 / 2.35, nl)).to(dev)
+    geoml = _core.make_geom(64, 75.0, 1e5, k_of(6400.0))
+    msl = timed_fn(torch)(lambda: _core.time_forward(atl, tl, geoml, 0.3, 2.0), reps=2)
+    out["large_n"] = {"workload": "200k emitters, 64x64, one image (workspace-resident sort)", "ms": msl,
+                      "pairs_per_s": nl * 64 * 64 / (msl * 1e-3)}
     if not args.no_cpu_baseline:
         # CPU: the oracle's C restatement of time.py on a row-block sample of image 0
         rows = 2

@@ -439,6 +439,315 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Large emitter counts (n > kTimeMaxN): the same algorithm with the per-pixel
+// arrays in a global workspace slice per CTA -- keys (FP64, by emitter),
+// two int32 permutations -- and the bucket counters (uint32, up to
+// kLargeBuckets) in shared memory.  Fallback for an overfull bucket: a
+// stable LSD radix sort over the whole array in tiles.
+// ---------------------------------------------------------------------------
+constexpr int kLargeBuckets = 16384;
+constexpr int kLargeMaxBucket = 256;
+constexpr size_t kLargeSmem = (size_t)kLargeBuckets * 4;  // also holds the radix counters
+
+__host__ __device__ __forceinline__ int large_buckets(int64_t n) {
+    int nb = kTimeThreads;
+    while (nb < kLargeBuckets && (int64_t)nb * 4 < n) nb <<= 1;
+    return nb;
+}
+
+__host__ __device__ __forceinline__ size_t large_slice_bytes(int64_t n) {
+    return ((size_t)n * 16 + 255) & ~(size_t)255;
+}
+
+__device__ __forceinline__ uint32_t bucket_of_n(double t, double kmin, double scale, int nb) {
+    const int b = __double2int_rz(__dmul_rn(__dsub_rn(t, kmin), scale));
+    return (uint32_t)min(max(b, 0), nb - 1);
+}
+
+__device__ bool bucket_sort_large(const double *keys, int *perm, uint32_t *cnt, int n, int nb, double kmin,
+                                  double kmax, double *scratch, int *s_flag) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (!(kmax > kmin)) {
+        for (int m = tid; m < n; m += kTimeThreads) perm[m] = m;
+        __syncthreads();
+        return true;
+    }
+    const double scale = (double)nb / (kmax - kmin);
+    const int per = nb / kTimeThreads;
+    for (int b = tid; b < nb; b += kTimeThreads) cnt[b] = 0u;
+    if (tid == 0) *s_flag = 0;
+    __syncthreads();
+    for (int j = tid; j < n; j += kTimeThreads) atomicAdd(&cnt[bucket_of_n(keys[j], kmin, scale, nb)], 1u);
+    __syncthreads();
+    uint32_t sum = 0, big = 0;
+    for (int i = 0; i < per; ++i) {
+        const uint32_t c = cnt[tid * per + i];
+        sum += c;
+        big |= c > kLargeMaxBucket;
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    uint32_t *wsum = reinterpret_cast<uint32_t *>(scratch);
+    if (lane == 31) wsum[warp] = incl;
+    if (big) *s_flag = 1;
+    __syncthreads();
+    uint32_t run = incl - sum;
+    for (int w = 0; w < warp; ++w) run += wsum[w];
+    __syncthreads();
+    for (int i = 0; i < per; ++i) {
+        const uint32_t c = cnt[tid * per + i];
+        cnt[tid * per + i] = run;
+        run += c;
+    }
+    __syncthreads();
+    if (*s_flag) return false;
+    // scatter: afterwards cnt[b] is the end of bucket b
+    for (int j = tid; j < n; j += kTimeThreads) {
+        const uint32_t pos = atomicAdd(&cnt[bucket_of_n(keys[j], kmin, scale, nb)], 1u);
+        perm[pos] = j;
+    }
+    __syncthreads();
+    for (int i = 0; i < per; ++i) {
+        const int b = tid * per + i;
+        const int start = b == 0 ? 0 : (int)cnt[b - 1];
+        const int end = (int)cnt[b];
+        for (int m = start + 1; m < end; ++m) {
+            const int v = perm[m];
+            const double kv = keys[v];
+            int q = m - 1;
+            while (q >= start) {
+                const int u = perm[q];
+                const double ku = keys[u];
+                if (ku < kv || (ku == kv && u < v)) break;
+                perm[q + 1] = u;
+                --q;
+            }
+            perm[q + 1] = v;
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
+// Stable LSD radix sort (8 passes of 8 bits) of emitter indices by the
+// order-preserving image of their keys.  Items go through in tiles of
+// kTimeThreads * kLargeIPT; inside a tile warp w takes the items
+// [w S, (w+1) S), lane-interleaved, so ranks follow item order; digit bases
+// carry over from tile to tile.  Result in a (the input order is built here).
+constexpr int kLargeIPT = 16;
+
+__device__ void radix_sort_large(const double *keys, int *a, int *b, int n, uint32_t *H, uint32_t *base) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int S = 32 * kLargeIPT, T = kTimeThreads * kLargeIPT;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    for (int m = tid; m < n; m += kTimeThreads) a[m] = m;
+    __syncthreads();
+    for (int pass = 0; pass < 8; ++pass) {
+        const int shift = pass * 8;
+        // global digit histogram -> exclusive bases
+        for (int k = tid; k < 256; k += kTimeThreads) base[k] = 0;
+        __syncthreads();
+        for (int m = tid; m < n; m += kTimeThreads)
+            atomicAdd(&base[(uint32_t)(sortable(keys[a[m]]) >> shift) & 255u], 1u);
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t v[8], sum = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                v[k] = base[lane * 8 + k];
+                sum += v[k];
+            }
+            uint32_t incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            uint32_t run = incl - sum;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                base[lane * 8 + k] = run;
+                run += v[k];
+            }
+        }
+        __syncthreads();
+        for (int t0 = 0; t0 < n; t0 += T) {
+            uint32_t *Hw = H + warp * 256;
+            for (int k = lane; k < 256; k += 32) Hw[k] = 0;
+            __syncwarp();
+            // per-warp digit counts of this tile
+            for (int i = 0; i < kLargeIPT; ++i) {
+                const int m = t0 + warp * S + i * 32 + lane;
+                const uint32_t dg = m < n ? (uint32_t)(sortable(keys[a[m]]) >> shift) & 255u : 256u;
+                const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+                if (dg < 256u && (peers & lt_mask) == 0) Hw[dg] += __popc(peers);
+                __syncwarp();
+            }
+            __syncthreads();
+            // warp offsets inside the tile, and the tile's totals added to the bases
+            if (tid < 256) {
+                uint32_t run = base[tid];
+                for (int w = 0; w < kTimeWarps; ++w) {
+                    const uint32_t h = H[w * 256 + tid];
+                    H[w * 256 + tid] = run;
+                    run += h;
+                }
+                base[tid] = run;
+            }
+            __syncthreads();
+            for (int i = 0; i < kLargeIPT; ++i) {
+                const int m = t0 + warp * S + i * 32 + lane;
+                const int e = m < n ? a[m] : 0;
+                const uint32_t dg = m < n ? (uint32_t)(sortable(keys[e]) >> shift) & 255u : 256u;
+                const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+                const uint32_t b0 = dg < 256u ? Hw[dg] : 0u;
+                const uint32_t rank = b0 + __popc(peers & lt_mask);
+                __syncwarp();
+                if (dg < 256u && (peers & lt_mask) == 0) Hw[dg] = b0 + __popc(peers);
+                __syncwarp();
+                if (m < n) b[rank] = e;
+            }
+            __syncthreads();
+        }
+        int *t = a;
+        a = b;
+        b = t;
+    }
+    // 8 passes: the sorted order is back in the first array
+}
+
+template <bool NF, bool SCALE>
+__global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
+    const GeomParams g, const double *__restrict__ atoms, const double *__restrict__ times, int n, double c,
+    double tau, double *__restrict__ out, WsHeader *__restrict__ hdr, int order_pixel, int *__restrict__ order_out,
+    double *__restrict__ keys_out, unsigned char *__restrict__ slices) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t *cnt = reinterpret_cast<uint32_t *>(smem);
+    uint32_t *H = cnt;                       // radix fallback: per-warp counters
+    uint32_t *base = cnt + kTimeWarps * 256;  // and digit bases
+    __shared__ double scratch[128];
+    __shared__ int s_pix, s_flag;
+    unsigned char *slice = slices + (size_t)blockIdx.x * large_slice_bytes(n);
+    double *keys = reinterpret_cast<double *>(slice);
+    int *perm = reinterpret_cast<int *>(slice + (size_t)n * 8);
+    int *perm2 = perm + n;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int npix = g.nx * g.ny;
+    const int nb = large_buckets(n);
+    const int per = (n + kTimeThreads - 1) / kTimeThreads;
+    int iter = 0;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0)
+            s_pix = order_pixel >= 0 ? (iter == 0 ? order_pixel : npix) : (int)atomicAdd(&hdr->work_counter, 1u);
+        __syncthreads();
+        ++iter;
+        const int p = s_pix;
+        if (p >= npix) break;
+        const int ix = p / g.ny, iy = p - ix * g.ny;
+        double dx, dy, dz;
+        pixel_time(g, ix, iy, dx, dy, dz);
+        const double dn = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+        const double q0 = __ddiv_rn(dx, dn), q1 = __ddiv_rn(dy, dn), q2 = __dsub_rn(__ddiv_rn(dz, dn), 1.0);
+        const double inv_tau = 1.0 / tau;
+        double kmin = __longlong_as_double(0x7FF0000000000000ll), kmax = -kmin;
+        for (int j = tid; j < n; j += kTimeThreads) {
+            const double4 a = reinterpret_cast<const double4 *>(atoms)[j];
+            double t, s, dist;
+            arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, t, s, dist);
+            kmin = fmin(kmin, t);
+            kmax = fmax(kmax, t);
+            keys[j] = t;
+        }
+        block_minmax(kmin, kmax, scratch + 96);
+        __syncthreads();
+        const int *sorted = perm;
+        if (!bucket_sort_large(keys, perm, cnt, n, nb, kmin, kmax, scratch, &s_flag)) {
+            radix_sort_large(keys, perm, perm2, n, H, base);
+            sorted = perm;
+        }
+        if (p == order_pixel) {
+            for (int m = tid; m < n; m += kTimeThreads) {
+                order_out[m] = sorted[m];
+                keys_out[m] = keys[sorted[m]];
+            }
+        }
+        const int m0 = tid * per;
+        double Dm = 1.0, Br = 0.0, Bi = 0.0;
+        double S1 = 0.0, S2r = 0.0, S2i = 0.0, S3 = 0.0;
+        for (int i = 0; i < per; ++i) {
+            const int m = m0 + i;
+            if (m >= n) break;
+            const int j = sorted[m];
+            const double tj = keys[j];
+            const double4 a = reinterpret_cast<const double4 *>(atoms)[j];
+            double s, dist, re, im;
+            path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
+            amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
+            const double dec = m == 0 ? 0.0 : exp(-__dsub_rn(tj, keys[sorted[m - 1]]) * inv_tau);
+            Dm *= dec;
+            Br = fma(dec, Br, re);
+            Bi = fma(dec, Bi, im);
+            const double w = m < n - 1 ? (-tau / 2) * expm1(-2 * __dsub_rn(keys[sorted[m + 1]], tj) * inv_tau)
+                                       : tau / 2;
+            const double wD = w * Dm;
+            S1 = fma(wD, Dm, S1);
+            S2r = fma(wD, Br, S2r);
+            S2i = fma(wD, Bi, S2i);
+            S3 = fma(w, fma(Br, Br, Bi * Bi), S3);
+        }
+        Affine incl = {Dm, Br, Bi};
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            Affine y;
+            y.d = __shfl_up_sync(0xffffffffu, incl.d, o);
+            y.br = __shfl_up_sync(0xffffffffu, incl.br, o);
+            y.bi = __shfl_up_sync(0xffffffffu, incl.bi, o);
+            if (lane >= o) incl = compose(y, incl);
+        }
+        __syncthreads();
+        if (lane == 31) {
+            scratch[warp * 3 + 0] = incl.d;
+            scratch[warp * 3 + 1] = incl.br;
+            scratch[warp * 3 + 2] = incl.bi;
+        }
+        __syncthreads();
+        Affine wpre = {1.0, 0.0, 0.0};
+        for (int w = 0; w < warp; ++w) {
+            const Affine y = {scratch[w * 3 + 0], scratch[w * 3 + 1], scratch[w * 3 + 2]};
+            wpre = compose(wpre, y);
+        }
+        Affine excl;
+        excl.d = __shfl_up_sync(0xffffffffu, incl.d, 1);
+        excl.br = __shfl_up_sync(0xffffffffu, incl.br, 1);
+        excl.bi = __shfl_up_sync(0xffffffffu, incl.bi, 1);
+        if (lane == 0) excl = Affine{1.0, 0.0, 0.0};
+        excl = compose(wpre, excl);
+        const double Xr = excl.br, Xi = excl.bi;
+        double part = fma(fma(Xr, Xr, Xi * Xi), S1, fma(2.0, fma(Xr, S2r, Xi * S2i), S3));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+        __syncthreads();
+        if (lane == 0) scratch[64 + warp] = part;
+        __syncthreads();
+        if (tid == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < kTimeWarps; ++w) tot += scratch[64 + w];
+            out[order_pixel >= 0 ? 0 : p] = tot;
+        }
+    }
+}
+
+template <bool NF, bool SCALE>
+static void *time_kernel_large_ptr() {
+    return (void *)time_kernel_large<NF, SCALE>;
+}
+
 template <bool NF, bool SCALE>
 static void *time_kernel_ptr() {
     return (void *)time_kernel<NF, SCALE>;
@@ -453,23 +762,56 @@ static idiwf_status time_validate(const idiwf_geom *geom, const double *atoms, c
     if (geom->flags & IDIWF_SECONDORDER)
         return set_error(IDIWF_ERR_UNSUPPORTED, "secondorder is not defined for the time path");
     if (n < 1) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "the time path needs at least one emitter");
-    if (n > kTimeMaxN) return set_error(IDIWF_ERR_UNSUPPORTED, "too many emitters for the on-chip sort");
+    if (n > ((int64_t)1 << 28)) return set_error(IDIWF_ERR_UNSUPPORTED, "at most 2^28 emitters");
     if (!atoms || !times) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "atoms/times are NULL");
     if (reinterpret_cast<uintptr_t>(atoms) & 31) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "atoms must be 32-byte aligned");
     if (!(c > 0) || !(tau > 0)) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "c and tau must be positive");
     return IDIWF_OK;
 }
 
+// CTAs of the large-n kernel on this device (each owns one workspace slice)
+static int large_ctas(int npix) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int occ = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, time_kernel_large<false, false>, kTimeThreads,
+                                                      kLargeSmem) != cudaSuccess) {
+        cudaGetLastError();
+        occ = 1;
+    }
+    return std::max(1, std::min(npix, sms * std::max(occ, 1)));
+}
+
+static size_t time_ws_bytes(const idiwf_geom *geom, int64_t n, int order_pixel) {
+    if (n <= kTimeMaxN) return kWsDataOffset;
+    const int ctas = order_pixel >= 0 ? 1 : large_ctas(geom->nx * geom->ny);
+    return kWsDataOffset + (size_t)ctas * large_slice_bytes(n);
+}
+
 static idiwf_status time_launch(const idiwf_geom *geom, const double *atoms, const double *times, int64_t n,
                                 double c, double tau, double *out, void *workspace, size_t workspace_bytes,
                                 int order_pixel, int *order_out, double *keys_out, cudaStream_t stream) {
-    if (!workspace || workspace_bytes < kWsDataOffset)
+    if (!workspace || workspace_bytes < time_ws_bytes(geom, n, order_pixel))
         return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_time_workspace_size()");
     if (reinterpret_cast<uintptr_t>(workspace) & 255)
         return set_error(IDIWF_ERR_WORKSPACE, "workspace must be 256-byte aligned");
     WsHeader *hdr = static_cast<WsHeader *>(workspace);
     const GeomParams g = make_geom(geom);
     const bool nf = geom->flags & IDIWF_NF, sc = geom->flags & IDIWF_SCALE;
+    if (n > kTimeMaxN) {
+        void *fl = nf ? (sc ? time_kernel_large_ptr<true, true>() : time_kernel_large_ptr<true, false>())
+                      : (sc ? time_kernel_large_ptr<false, true>() : time_kernel_large_ptr<false, false>());
+        IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLargeSmem));
+        IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 2 * sizeof(uint32_t), stream));
+        const int grid = order_pixel >= 0 ? 1 : large_ctas(geom->nx * geom->ny);
+        int ni = (int)n;
+        unsigned char *slices = static_cast<unsigned char *>(workspace) + kWsDataOffset;
+        void *args[] = {(void *)&g, &atoms, &times, &ni, &c, &tau, &out, &hdr, &order_pixel, &order_out, &keys_out,
+                        &slices};
+        IDIWF_CUDA_CHECK(cudaLaunchKernel(fl, dim3(grid), dim3(kTimeThreads), args, kLargeSmem, stream));
+        return IDIWF_OK;
+    }
     void *fn = nf ? (sc ? time_kernel_ptr<true, true>() : time_kernel_ptr<true, false>())
                   : (sc ? time_kernel_ptr<false, true>() : time_kernel_ptr<false, false>());
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTimeSmem));
@@ -492,9 +834,8 @@ using namespace idiwf;
 extern "C" int64_t idiwf_time_max_emitters(void) { return kTimeMaxN; }
 
 extern "C" size_t idiwf_time_workspace_size(const idiwf_geom *geom, int64_t n) {
-    (void)geom;
-    (void)n;
-    return kWsDataOffset;
+    if (!geom || geom->nx <= 0 || geom->ny <= 0) return kWsDataOffset;
+    return time_ws_bytes(geom, n, -1);
 }
 
 extern "C" idiwf_status idiwf_time_forward(const idiwf_geom *geom, const double *atoms, const double *times,
@@ -515,8 +856,6 @@ extern "C" idiwf_status idiwf_time_order(const idiwf_geom *geom, const double *a
     if (!order || !sorted_keys) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "order/sorted_keys are NULL");
     if (ix < 0 || iy < 0 || ix >= geom->nx || iy >= geom->ny)
         return set_error(IDIWF_ERR_INVALID_ARGUMENT, "pixel outside the detector");
-    if (!workspace || workspace_bytes < kWsDataOffset)
-        return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_time_workspace_size()");
     // the intensity of the pixel goes to a scratch slot of the workspace header
     double *scratch = reinterpret_cast<double *>(&static_cast<WsHeader *>(workspace)->pad[0]);
     return time_launch(geom, atoms, times, n, c, 1.0, scratch, workspace, workspace_bytes, ix * geom->ny + iy, order,

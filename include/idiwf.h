@@ -179,9 +179,13 @@ idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch *batch,
 /* time-dependent path                                                       */
 /* ------------------------------------------------------------------------ */
 
-/* Largest emitter count the on-chip per-pixel sort handles. */
+/* Largest emitter count the on-chip per-pixel sort handles.  Above it (up to
+ * 2^28 emitters) a kernel with the per-pixel keys and permutations in the
+ * workspace runs instead, and the workspace grows with n. */
 int64_t idiwf_time_max_emitters(void);
 
+/* Workspace for n emitters on this detector (for n above
+ * idiwf_time_max_emitters(): 16 n bytes per resident CTA on the current device). */
 size_t idiwf_time_workspace_size(const idiwf_geom *geom, int64_t n);
 
 /*

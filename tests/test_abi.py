@@ -111,7 +111,10 @@ def test_time_path_validation(lib):
     at = ctypes.c_void_p(4096)
     n_max = lib.idiwf_time_max_emitters()
     assert n_max >= 20000
-    assert lib.idiwf_time_forward(ctypes.byref(g), at, at, n_max + 1, 0.3, 2.0, ws, ws, 1 << 20, None) == nat.ERR_UNSUPPORTED
+    # above the on-chip table the global-memory kernel needs a workspace that grows with n
+    assert lib.idiwf_time_workspace_size(ctypes.byref(g), n_max + 1) > 1 << 20
+    assert lib.idiwf_time_forward(ctypes.byref(g), at, at, n_max + 1, 0.3, 2.0, ws, ws, 1 << 20, None) == nat.ERR_WORKSPACE
+    assert lib.idiwf_time_forward(ctypes.byref(g), at, at, (1 << 28) + 1, 0.3, 2.0, ws, ws, 1 << 20, None) == nat.ERR_UNSUPPORTED
     assert lib.idiwf_time_forward(ctypes.byref(g), at, at, 0, 0.3, 2.0, ws, ws, 1 << 20, None) == nat.ERR_INVALID_ARGUMENT
     assert lib.idiwf_time_forward(ctypes.byref(g), at, at, 10, -1.0, 2.0, ws, ws, 1 << 20, None) == nat.ERR_INVALID_ARGUMENT
     g.offset[0] = 1.0

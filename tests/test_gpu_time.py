@@ -125,3 +125,29 @@ def test_time_sort_fallback_and_degenerate_keys():
     one = at[:1]
     img = _core.time_forward(_gpu(one), _gpu(np.zeros(1)), geom, 0.3, 2.0).cpu().numpy()
     assert np.allclose(img, oracle.time_image(og, 0, one, np.zeros(1), 0.3, 2.0), rtol=1e-12)
+
+
+@pytest.mark.parametrize("n,settings,outlier", [(30000, "", False), (70000, "nf scale", False),
+                                                (25000, "nf", True)])
+def test_time_large_emitter_counts(n, settings, outlier):
+    """Emitter counts above the on-chip table (the global-memory kernel):
+    intensities against the oracle and the sorted order bit for bit; with
+    one far outlying emission time every other key falls in one bucket and
+    the radix fallback sorts them."""
+    assert n > _core.time_max_emitters()
+    g0 = rng(n)
+    at = atoms(sphere(g0, n, 0.01), g0.uniform(0, 2 * np.pi, n))
+    times = g0.normal(0, 5.0 / 2.35, n)
+    if outlier:
+        times[n // 3] = 1e6
+    flags, _, _ = _core.parse_settings(settings)
+    geom = _core.make_geom([4, 3], 75.0, 1e5, K64, (0.02, 0.0), (0, 0), flags)
+    og = oracle.geometry([4, 3], 75.0, 1e5, K64, (0.02, 0.0))
+    of = oracle.flags_from_settings(settings)
+    img = _core.time_forward(_gpu(at), _gpu(times), geom, 0.3, 2.0).cpu().numpy()
+    ref = oracle.time_image(og, of, at, times, 0.3, 2.0)
+    assert np.max(np.abs(img - ref) / np.abs(ref)) < 1e-9
+    for ix, iy in ((0, 0), (3, 2)):
+        order, keys = _core.time_order(_gpu(at), _gpu(times), geom, 0.3, ix, iy)
+        np.testing.assert_array_equal(order.cpu().numpy(), oracle.time_order(og, of, at, times, 0.3, ix, iy))
+        assert np.all(np.diff(keys.cpu().numpy()) >= 0)
