@@ -625,7 +625,8 @@ template <bool NF, bool SCALE>
 __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
     const GeomParams g, const double *__restrict__ atoms, const double *__restrict__ times, int n, double c,
     double tau, double *__restrict__ out, WsHeader *__restrict__ hdr, int order_pixel, int *__restrict__ order_out,
-    double *__restrict__ keys_out, unsigned char *__restrict__ slices) {
+    double *__restrict__ keys_out, unsigned char *__restrict__ slices, int n_slices) {
+    if ((int)blockIdx.x >= n_slices) return;  // one workspace slice per CTA
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t *cnt = reinterpret_cast<uint32_t *>(smem);
     uint32_t *H = cnt;                       // radix fallback: per-warp counters
@@ -769,29 +770,38 @@ static idiwf_status time_validate(const idiwf_geom *geom, const double *atoms, c
     return IDIWF_OK;
 }
 
-// CTAs of the large-n kernel on this device (each owns one workspace slice)
-static int large_ctas(int npix) {
-    int dev = 0, sms = 148;
+static void *large_fn(const idiwf_geom *geom) {
+    const bool nf = geom->flags & IDIWF_NF, sc = geom->flags & IDIWF_SCALE;
+    return nf ? (sc ? time_kernel_large_ptr<true, true>() : time_kernel_large_ptr<true, false>())
+              : (sc ? time_kernel_large_ptr<false, true>() : time_kernel_large_ptr<false, false>());
+}
+
+// CTAs of the large-n kernel on this device, each owning one workspace
+// slice.  The shared-memory attribute is set before the occupancy query, so
+// the workspace size and the launch see the same count.
+static int large_ctas(const idiwf_geom *geom, int order_pixel) {
+    if (order_pixel >= 0) return 1;
+    void *fn = large_fn(geom);
+    int dev = 0, sms = 148, occ = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int occ = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, time_kernel_large<false, false>, kTimeThreads,
-                                                      kLargeSmem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLargeSmem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kTimeThreads, kLargeSmem) != cudaSuccess) {
         cudaGetLastError();
         occ = 1;
     }
-    return std::max(1, std::min(npix, sms * std::max(occ, 1)));
+    return std::max(1, std::min(geom->nx * geom->ny, sms * std::max(occ, 1)));
 }
 
 static size_t time_ws_bytes(const idiwf_geom *geom, int64_t n, int order_pixel) {
     if (n <= kTimeMaxN) return kWsDataOffset;
-    const int ctas = order_pixel >= 0 ? 1 : large_ctas(geom->nx * geom->ny);
-    return kWsDataOffset + (size_t)ctas * large_slice_bytes(n);
+    return kWsDataOffset + (size_t)large_ctas(geom, order_pixel) * large_slice_bytes(n);
 }
 
 static idiwf_status time_launch(const idiwf_geom *geom, const double *atoms, const double *times, int64_t n,
                                 double c, double tau, double *out, void *workspace, size_t workspace_bytes,
                                 int order_pixel, int *order_out, double *keys_out, cudaStream_t stream) {
+    const int slices_fit = n > kTimeMaxN ? large_ctas(geom, order_pixel) : 0;
     if (!workspace || workspace_bytes < time_ws_bytes(geom, n, order_pixel))
         return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_time_workspace_size()");
     if (reinterpret_cast<uintptr_t>(workspace) & 255)
@@ -800,15 +810,18 @@ static idiwf_status time_launch(const idiwf_geom *geom, const double *atoms, con
     const GeomParams g = make_geom(geom);
     const bool nf = geom->flags & IDIWF_NF, sc = geom->flags & IDIWF_SCALE;
     if (n > kTimeMaxN) {
-        void *fl = nf ? (sc ? time_kernel_large_ptr<true, true>() : time_kernel_large_ptr<true, false>())
-                      : (sc ? time_kernel_large_ptr<false, true>() : time_kernel_large_ptr<false, false>());
+        void *fl = large_fn(geom);
         IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLargeSmem));
         IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 2 * sizeof(uint32_t), stream));
-        const int grid = order_pixel >= 0 ? 1 : large_ctas(geom->nx * geom->ny);
+        // slices the workspace holds (the caller may pass more than the minimum)
+        const size_t avail = (workspace_bytes - kWsDataOffset) / large_slice_bytes(n);
+        int n_slices = (int)std::min<size_t>(avail, (size_t)1 << 20);
+        const int grid = std::min(slices_fit, n_slices);
+        n_slices = grid;
         int ni = (int)n;
         unsigned char *slices = static_cast<unsigned char *>(workspace) + kWsDataOffset;
         void *args[] = {(void *)&g, &atoms, &times, &ni, &c, &tau, &out, &hdr, &order_pixel, &order_out, &keys_out,
-                        &slices};
+                        &slices, &n_slices};
         IDIWF_CUDA_CHECK(cudaLaunchKernel(fl, dim3(grid), dim3(kTimeThreads), args, kLargeSmem, stream));
         return IDIWF_OK;
     }

@@ -151,3 +151,16 @@ def test_time_large_emitter_counts(n, settings, outlier):
         order, keys = _core.time_order(_gpu(at), _gpu(times), geom, 0.3, ix, iy)
         np.testing.assert_array_equal(order.cpu().numpy(), oracle.time_order(og, of, at, times, 0.3, ix, iy))
         assert np.all(np.diff(keys.cpu().numpy()) >= 0)
+
+
+def test_time_large_emitter_counts_many_pixels():
+    """More pixels than SMs: the workspace-resident kernel's grid is as large
+    as the slices the workspace holds (one per resident CTA)."""
+    n = 21000
+    g0 = rng(909)
+    at = atoms(sphere(g0, n, 0.01), g0.uniform(0, 2 * np.pi, n))
+    times = g0.normal(0, 5.0 / 2.35, n)
+    geom = _core.make_geom([20, 20], 75.0, 1e5, K64)
+    img = _core.time_forward(_gpu(at), _gpu(times), geom, 0.3, 2.0).cpu().numpy()
+    ref = oracle.time_image(oracle.geometry([20, 20], 75.0, 1e5, K64), 0, at, times, 0.3, 2.0)
+    assert np.max(np.abs(img - ref) / np.abs(ref)) < 1e-9
