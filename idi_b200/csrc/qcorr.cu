@@ -12,8 +12,10 @@
 //  * qcorr_radial_kernel — CTA = (reference row, group of kRowsPerCta target
 //    rows, image).  The reference row and each target row are staged in
 //    shared memory as float4 {qx, qy, qz, v}: one broadcast LDS.128 and one
-//    conflict-free LDS.128 per pair.  Bins go to an FP64 shared-memory
-//    histogram, added to the output once per CTA.
+//    conflict-free LDS.128 per pair.  The bin round(sqrt(d2)) is re-derived
+//    only when d2 leaves the current bin's interval (a table of the exact
+//    d2 thresholds), since it rarely changes along a row.  Bins go to an FP64
+//    shared-memory histogram, added to the output once per CTA.
 //  * qcorr_3d_kernel — the same walk over float2 {zd, v} rows; runs go to the
 //    FP64 output with global atomics (the 3d histogram does not fit on chip);
 //    bins outside the array are dropped.
@@ -38,11 +40,33 @@ __global__ void __launch_bounds__(1024) qcorr_radial_kernel(const float4 *__rest
     float4 *sref = reinterpret_cast<float4 *>(qsm);
     float4 *stgt = sref + nc;
     double *hist = reinterpret_cast<double *>(stgt + nc);
+    float *bound = reinterpret_cast<float *>(hist + qmax + 1);  // qmax + 3 entries
     const int refr = blockIdx.x;
     const int img = blockIdx.z;
     const float *v = images + (int64_t)img * nr * nc;
     const int tid = threadIdx.x;
     for (int i = tid; i <= qmax; i += blockDim.x) hist[i] = 0.0;
+    // bound[k]: smallest float d2 >= 0 with rint(sqrt(d2)) >= k, k = 0..qmax+1,
+    // by bisection over the (monotone) float bit patterns with the very
+    // operations of the bin below; bound[qmax+2] = +inf.  Bins above qmax are
+    // one class (the reference only tests dq <= qmax and dq < qmax there).
+    for (int k = tid; k <= qmax + 2; k += blockDim.x) {
+        float b;
+        if (k == 0) {
+            b = 0.0f;
+        } else if (k == qmax + 2) {
+            b = __int_as_float(0x7F800000);
+        } else {
+            uint32_t lo = 0u, hi = 0x7F800000u;  // rint(sqrt(+0)) = 0 < k <= rint(sqrt(+inf))
+            while (hi - lo > 1u) {
+                const uint32_t mid = lo + (hi - lo) / 2u;
+                if ((int)rintf(__fsqrt_rn(__uint_as_float(mid))) >= k) hi = mid;
+                else lo = mid;
+            }
+            b = __uint_as_float(hi);
+        }
+        bound[k] = b;
+    }
     for (int c = tid; c < nc; c += blockDim.x) {
         float4 a = q[(int64_t)refr * nc + c];
         a.w = v[(int64_t)refr * nc + c];
@@ -66,12 +90,19 @@ __global__ void __launch_bounds__(1024) qcorr_radial_kernel(const float4 *__rest
             float val = 0.0f;
             int dqold = tid / 2;  // the reference's initial run bin (receives an empty run)
             int dq = qmax + 1;
+            int k = 0;
+            float lo = 1.0f, hi = 0.0f;  // empty: the first pair derives its bin
             for (int refc = c0; refc < c1; ++refc) {
                 const float4 a = sref[refc];
                 const float4 b = stgt[refc + offsetc];
                 const float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y), dz = __fsub_rn(a.z, b.z);
                 const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-                dq = (int)rintf(__fsqrt_rn(d2));
+                if (!(d2 >= lo && d2 < hi)) {  // left the current bin's interval
+                    k = min((int)rintf(__fsqrt_rn(d2)), qmax + 1);
+                    lo = bound[k];
+                    hi = bound[k + 1];
+                }
+                dq = k;
                 if (dq <= qmax) {
                     if (dq != dqold) {
                         atomicAdd(&hist[dqold], (double)val);
@@ -209,7 +240,8 @@ extern "C" idiwf_status idiwf_qcorr_radial(const float *q, const float *images, 
     if (!workspace || workspace_bytes < 256) return set_error(IDIWF_ERR_WORKSPACE, "workspace too small");
     IDIWF_CUDA_CHECK(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)n_images * qmax, stream));
     const int threads = ((2 * qmax + 1) + 31) / 32 * 32;
-    const size_t smem = 2 * (size_t)nc * sizeof(float4) + (size_t)(qmax + 1) * sizeof(double);
+    const size_t smem = 2 * (size_t)nc * sizeof(float4) + (size_t)(qmax + 1) * sizeof(double) +
+                        (size_t)(qmax + 3) * sizeof(float);
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(qcorr_radial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const dim3 grid(nr, (qmax + kRowsPerCta - 1) / kRowsPerCta, n_images);
     qcorr_radial_kernel<<<grid, threads, smem, stream>>>(reinterpret_cast<const float4 *>(q), images, nr, nc, qmax,
