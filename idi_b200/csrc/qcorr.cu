@@ -90,27 +90,30 @@ __global__ void __launch_bounds__(1024) qcorr_radial_kernel(const float4 *__rest
             float val = 0.0f;
             int dqold = tid / 2;  // the reference's initial run bin (receives an empty run)
             int dq = qmax + 1;
-            int k = 0;
             float lo = 1.0f, hi = 0.0f;  // empty: the first pair derives its bin
+            // The reference, per pair: if dq <= qmax { if dq != dqold { add the
+            // run to dqold; dqold = dq; val = 0 } val += v v' }.  While the bin
+            // stays the same, dq == dqold whenever dq <= qmax, so that test
+            // only needs to run when the bin changes.
+            bool in_range = false;
+#pragma unroll 4
             for (int refc = c0; refc < c1; ++refc) {
                 const float4 a = sref[refc];
                 const float4 b = stgt[refc + offsetc];
                 const float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y), dz = __fsub_rn(a.z, b.z);
                 const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
                 if (!(d2 >= lo && d2 < hi)) {  // left the current bin's interval
-                    k = min((int)rintf(__fsqrt_rn(d2)), qmax + 1);
-                    lo = bound[k];
-                    hi = bound[k + 1];
-                }
-                dq = k;
-                if (dq <= qmax) {
-                    if (dq != dqold) {
+                    dq = min((int)rintf(__fsqrt_rn(d2)), qmax + 1);
+                    lo = bound[dq];
+                    hi = bound[dq + 1];
+                    in_range = dq <= qmax;
+                    if (in_range && dq != dqold) {
                         atomicAdd(&hist[dqold], (double)val);
                         dqold = dq;
                         val = 0.0f;
                     }
-                    val = __fadd_rn(val, __fmul_rn(a.w, b.w));
                 }
+                if (in_range) val = __fadd_rn(val, __fmul_rn(a.w, b.w));
             }
             if (dq < qmax) atomicAdd(&hist[dq], (double)val);
         }
