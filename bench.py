@@ -686,6 +686,23 @@ def emitters_leg(torch, dev, _core, nat, args):
     desc = _core.emitters_desc(nat.EMIT_SPHERE, r=0.01)
     ms = timed(lambda: _core.emitters(desc, 8, 2000, (1, 2), 0, 0, dev), reps=5)
     out["sphere"] = {"ms": ms, "emitters_per_s": 8 * 2000 / (ms * 1e-3), "launches": 1}
+    # end to end on the small configuration: simulate() of 64 images of a
+    # 2,000-emitter sphere (10 nm), 256x256 @ 75 um, 0.1 m, 6.4 keV, split,
+    # with the emitters drawn on the host (get2) and on the device
+    from idi_b200.simulation import cuda as sim
+
+    e2e = {}
+    for label, ondevice in (("host_draws", False), ("device_draws", True)):
+        obj = simobj.sphere(6400.0, 2000, 0.01, rng=np.random.default_rng(1), seed=1)
+        obj.ondevice = ondevice
+        sim.simulate(8, obj, 256, 75.0, 1e5, settings="split", verbose=False)  # warm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.simulate(64, obj, 256, 75.0, 1e5, settings="split", verbose=False)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        e2e[label] = {"s": dt, "images_per_s": 64 / dt, "pairs_per_s": 64 * 2000 * 256 * 256 / dt}
+    out["e2e_small_config"] = e2e
     if not args.no_cpu_baseline:
         # the reference's host draw per image (simobj.py:446-487 and 50-60):
         # numpy choice without replacement of 50,000 of the 157,216 sites
