@@ -9,10 +9,13 @@
 //  * cs_seg_kernel / cs_seg_scan_kernel / cs_start_kernel — exclusive scan of
 //    the photon counts (injected positions only: photon g's row in the
 //    caller's arrays).
-//  * cs_gather_kernel — one thread per output pixel sums the charge of every
-//    photon within w pixels, walking source pixels in row-major order and the
-//    photons of a pixel in order: the reference's scatter loop adds to each
-//    pixel in exactly that order.
+//  * cs_tile_kernel (w <= 4) / cs_gather_kernel — every output pixel sums the
+//    charge of every photon within w pixels, walking source pixels in
+//    row-major order and the photons of a pixel in order: the reference's
+//    scatter loop adds to each pixel in exactly that order.  The tiled kernel
+//    computes each photon's charge factors once per CTA in shared memory; the
+//    plain one (and the tiled one for crowded regions) recomputes them per
+//    target pixel.
 #include <cmath>
 
 #include "idiwf_internal.cuh"
@@ -285,6 +288,65 @@ __device__ __forceinline__ double cs_factor(double mu, int d, const CsParams &P)
     return erf(P.c + a) + erf(P.c - a);
 }
 
+// Offsets and charge scale of photon i of source pixel q (image b), from the
+// injected arrays or the photon's stream; false when an injected row is
+// missing (count mismatch).
+template <bool INJ>
+__device__ __forceinline__ bool cs_photon(const CsParams &P, const double *__restrict__ positions,
+                                          const double *__restrict__ scales, const int64_t *__restrict__ start,
+                                          int64_t gq, int64_t q, int b, int64_t i, double &mux, double &muy,
+                                          double &sc) {
+    sc = 1.0;
+    if (INJ) {
+        const int64_t g = start[gq] + i;
+        if (g >= P.n_positions) return false;
+        mux = positions[2 * g];
+        muy = positions[2 * g + 1];
+        if (P.ns > 0.0 && scales) sc = scales[g];
+    } else {
+        uint64_t w0, w1, w2, w3;
+        philox4x64((uint64_t)i + 1, (uint64_t)q, (P.img0 + (uint64_t)b) | (1ull << 63), P.stream, P.k0, P.k1, w0, w1,
+                   w2, w3);
+        mux = u01(w0) - 0.5;
+        muy = u01(w1) - 0.5;
+        if (P.ns > 0.0) sc = 1.0 + box_muller(u01(w2), u01(w3)) * P.ns;
+    }
+    return true;
+}
+
+// Charge deposited into output pixel (r, col) of image b: source pixels in
+// row-major order, photons of a pixel in order (the reference's addition
+// order for this pixel).
+template <typename T, bool INJ>
+__device__ double cs_pixel(const T *__restrict__ counts, const CsParams &P, const double *__restrict__ positions,
+                           const double *__restrict__ scales, const int64_t *__restrict__ start, int b, int r,
+                           int col, bool &bad) {
+    const int64_t npix = (int64_t)P.nx * P.ny;
+    double acc = 0.0;
+    const int r0 = max(r - P.w, 0), r1 = min(r + P.w, P.nx - 1);
+    const int c0 = max(col - P.w, 0), c1 = min(col + P.w, P.ny - 1);
+    for (int qr = r0; qr <= r1; ++qr) {
+        const int dr = r - qr;
+        for (int qc = c0; qc <= c1; ++qc) {
+            const int dc = col - qc;
+            const int64_t q = (int64_t)qr * P.ny + qc;
+            const int64_t gq = (int64_t)b * npix + q;
+            const int64_t n = photon_count(counts, gq, bad);
+            for (int64_t i = 0; i < n; ++i) {
+                double mux, muy, sc;
+                if (!cs_photon<INJ>(P, positions, scales, start, gq, q, b, i, mux, muy, sc)) {
+                    bad = true;
+                    break;
+                }
+                // k[x, y] = (1/4 f_x) f_y, deposited at (hit_x + y - w, hit_y + x - w)
+                const double kxy = (0.25 * cs_factor(mux, dc, P)) * cs_factor(muy, dr, P);
+                acc += P.ns > 0.0 ? sc * kxy : kxy;
+            }
+        }
+    }
+    return acc;
+}
+
 template <typename T, bool INJ>
 __global__ void __launch_bounds__(256) cs_gather_kernel(const T *__restrict__ counts, const CsParams P,
                                                         const double *__restrict__ positions,
@@ -298,42 +360,125 @@ __global__ void __launch_bounds__(256) cs_gather_kernel(const T *__restrict__ co
         const int b = (int)(o / npix);
         const int64_t po = o - (int64_t)b * npix;
         const int r = (int)(po / P.ny), col = (int)(po - (int64_t)r * P.ny);
-        double acc = 0.0;
-        const int r0 = max(r - P.w, 0), r1 = min(r + P.w, P.nx - 1);
-        const int c0 = max(col - P.w, 0), c1 = min(col + P.w, P.ny - 1);
-        for (int qr = r0; qr <= r1; ++qr) {
-            const int dr = r - qr;
-            for (int qc = c0; qc <= c1; ++qc) {
-                const int dc = col - qc;
-                const int64_t q = (int64_t)qr * P.ny + qc;
-                const int64_t gq = (int64_t)b * npix + q;
-                const int64_t n = photon_count(counts, gq, bad);
-                for (int64_t i = 0; i < n; ++i) {
-                    double mux, muy, sc = 1.0;
-                    if (INJ) {
-                        const int64_t g = start[gq] + i;
-                        if (g >= P.n_positions) {
-                            bad = true;
-                            break;
-                        }
-                        mux = positions[2 * g];
-                        muy = positions[2 * g + 1];
-                        if (P.ns > 0.0 && scales) sc = scales[g];
-                    } else {
-                        uint64_t w0, w1, w2, w3;
-                        philox4x64((uint64_t)i + 1, (uint64_t)q, (P.img0 + (uint64_t)b) | (1ull << 63), P.stream,
-                                   P.k0, P.k1, w0, w1, w2, w3);
-                        mux = u01(w0) - 0.5;
-                        muy = u01(w1) - 0.5;
-                        if (P.ns > 0.0) sc = 1.0 + box_muller(u01(w2), u01(w3)) * P.ns;
-                    }
-                    // k[x, y] = (1/4 f_x) f_y, deposited at (hit_x + y - w, hit_y + x - w)
-                    const double kxy = (0.25 * cs_factor(mux, dc, P)) * cs_factor(muy, dr, P);
-                    acc += P.ns > 0.0 ? sc * kxy : kxy;
+        out[o] = cs_pixel<T, INJ>(counts, P, positions, scales, start, b, r, col, bad);
+    }
+    if (bad) record_error(err, kErrValue);
+}
+
+// Tiled gather: a CTA owns a kCsTR x kCsTC tile of output pixels.  It stages
+// the counts of the tile and its w-pixel halo, numbers the region's photons
+// (exclusive scan), computes each photon's 2 (2w + 1) charge factors once,
+// and every output pixel then sums over its neighbours' photons from those
+// factors -- the same products in the same order as cs_pixel.  A region with
+// more photons than the shared memory holds takes cs_pixel.
+constexpr int kCsTR = 8, kCsTC = 32, kCsMaxW = 4;
+constexpr size_t kCsFactorBytes = 64 * 1024;
+
+template <typename T, bool INJ>
+__global__ void __launch_bounds__(256) cs_tile_kernel(const T *__restrict__ counts, const CsParams P,
+                                                      const double *__restrict__ positions,
+                                                      const double *__restrict__ scales,
+                                                      const int64_t *__restrict__ start, double *__restrict__ out,
+                                                      uint32_t *__restrict__ err, int cap) {
+    extern __shared__ __align__(16) double csm[];
+    __shared__ int wsum[8];
+    __shared__ int s_total;
+    const int w = P.w, KW = 2 * w + 1;
+    const int RH = kCsTR + 2 * w, RW = kCsTC + 2 * w, RN = RH * RW;
+    double *fx = csm;
+    double *fy = fx + (size_t)cap * KW;
+    double *scl = fy + (size_t)cap * KW;
+    double *mu = scl + cap;  // (mu_x, mu_y) per photon
+    int *rc = reinterpret_cast<int *>(mu + 2 * (size_t)cap);
+    int *rs = rc + RN;
+    const int64_t npix = (int64_t)P.nx * P.ny;
+    const int b = blockIdx.z;
+    const int r0 = blockIdx.y * kCsTR, c0 = blockIdx.x * kCsTC;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    bool bad = false;
+    for (int ri = tid; ri < RN; ri += blockDim.x) {
+        const int gr = r0 - w + ri / RW, gc = c0 - w + ri % RW;
+        int n = 0;
+        if (gr >= 0 && gr < P.nx && gc >= 0 && gc < P.ny)
+            n = (int)min(photon_count(counts, (int64_t)b * npix + (int64_t)gr * P.ny + gc, bad), (int64_t)1 << 24);
+        rc[ri] = n;
+    }
+    __syncthreads();
+    // exclusive scan of the region's counts (RN <= 16 x 40 < 3 per thread)
+    const int E = (RN + blockDim.x - 1) / blockDim.x;
+    const int e0 = tid * E, e1 = min(e0 + E, RN);
+    int sum = 0;
+    for (int e = e0; e < e1; ++e) sum = min(sum + rc[e], 1 << 28);
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl = min(incl + y, 1 << 28);
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int run = incl - sum;
+    for (int v = 0; v < warp; ++v) run = min(run + wsum[v], 1 << 28);
+    for (int e = e0; e < e1; ++e) {
+        rs[e] = run;
+        run = min(run + rc[e], 1 << 28);
+    }
+    if (tid == blockDim.x - 1) s_total = run;
+    __syncthreads();
+    const int r = r0 + tid / kCsTC, col = c0 + tid % kCsTC;
+    const bool inside = r < P.nx && col < P.ny;
+    if (s_total > cap) {  // uniform across the CTA
+        if (inside) out[(int64_t)b * npix + (int64_t)r * P.ny + col] =
+            cs_pixel<T, INJ>(counts, P, positions, scales, start, b, r, col, bad);
+    } else {
+        // the photons' offsets and scales, then their factors, one (photon,
+        // factor) item per thread so the erf work spreads over the CTA
+        for (int ri = tid; ri < RN; ri += blockDim.x) {
+            const int n = rc[ri];
+            if (n == 0) continue;
+            const int gr = r0 - w + ri / RW, gc = c0 - w + ri % RW;
+            const int64_t q = (int64_t)gr * P.ny + gc, gq = (int64_t)b * npix + q;
+            for (int i = 0; i < n; ++i) {
+                const int slot = rs[ri] + i;
+                double mux = 0.0, muy = 0.0, sc = 1.0;
+                if (!cs_photon<INJ>(P, positions, scales, start, gq, q, b, i, mux, muy, sc)) {
+                    bad = true;
+                    sc = 0.0;
                 }
+                mu[2 * slot] = mux;
+                mu[2 * slot + 1] = muy;
+                scl[slot] = sc;
             }
         }
-        out[o] = acc;
+        __syncthreads();
+        const int items = s_total * 2 * KW;
+        for (int it = tid; it < items; it += blockDim.x) {
+            const int slot = it / (2 * KW), f = it - slot * 2 * KW;
+            if (f < KW)
+                fx[(size_t)slot * KW + f] = cs_factor(mu[2 * slot], f - w, P);
+            else
+                fy[(size_t)slot * KW + f - KW] = cs_factor(mu[2 * slot + 1], f - KW - w, P);
+        }
+        __syncthreads();
+        if (inside) {
+            double acc = 0.0;
+            const int qr0 = max(r - w, 0), qr1 = min(r + w, P.nx - 1);
+            const int qc0 = max(col - w, 0), qc1 = min(col + w, P.ny - 1);
+            for (int qr = qr0; qr <= qr1; ++qr) {
+                const int dr = r - qr;
+                for (int qc = qc0; qc <= qc1; ++qc) {
+                    const int dc = col - qc;
+                    const int ri = (qr - (r0 - w)) * RW + (qc - (c0 - w));
+                    const int n = rc[ri], base = rs[ri];
+                    for (int i = 0; i < n; ++i) {
+                        const int sl = base + i;
+                        const double kxy = (0.25 * fx[(size_t)sl * KW + dc + w]) * fy[(size_t)sl * KW + dr + w];
+                        acc += P.ns > 0.0 ? scl[sl] * kxy : kxy;
+                    }
+                }
+            }
+            out[(int64_t)b * npix + (int64_t)r * P.ny + col] = acc;
+        }
     }
     if (bad) record_error(err, kErrValue);
 }
@@ -410,6 +555,27 @@ static idiwf_status photons_out(int32_t out_dtype, const void *probs, int32_t n_
     }
 }
 
+template <typename T, bool INJ>
+static idiwf_status launch_cs_gather(const T *counts, const CsParams &P, const double *positions,
+                                     const double *scales, const int64_t *start, double *out, WsHeader *hdr,
+                                     int blocks, cudaStream_t stream) {
+    if (P.w <= kCsMaxW && P.n_images <= 65535) {
+        const int KW = 2 * P.w + 1;
+        const int RN = (kCsTR + 2 * P.w) * (kCsTC + 2 * P.w);
+        const int cap = (int)(kCsFactorBytes / ((2 * (size_t)KW + 3) * sizeof(double)));
+        const size_t smem = (size_t)cap * (2 * KW + 3) * sizeof(double) + 2 * (size_t)RN * sizeof(int);
+        IDIWF_CUDA_CHECK(cudaFuncSetAttribute(cs_tile_kernel<T, INJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+        const dim3 grid((P.ny + kCsTC - 1) / kCsTC, (P.nx + kCsTR - 1) / kCsTR, P.n_images);
+        cs_tile_kernel<T, INJ><<<grid, kCsTR * kCsTC, smem, stream>>>(counts, P, positions, scales, start, out,
+                                                                       &hdr->error, cap);
+    } else {
+        cs_gather_kernel<T, INJ><<<blocks, 256, 0, stream>>>(counts, P, positions, scales, start, out, &hdr->error);
+    }
+    IDIWF_CUDA_CHECK(cudaGetLastError());
+    return IDIWF_OK;
+}
+
 static size_t cs_ws_bytes(int32_t n_images, int32_t nx, int32_t ny, int32_t injected) {
     const int64_t n = (int64_t)n_images * nx * ny;
     const int64_t nseg = (n + kScanSeg - 1) / kScanSeg;
@@ -454,12 +620,9 @@ static idiwf_status launch_cs(const void *counts_v, int32_t n_images, int32_t nx
         cs_seg_kernel<T><<<(unsigned)nseg, kScanThreads, 0, stream>>>(counts, n, seg, &hdr->error);
         cs_seg_scan_kernel<<<1, kScanThreads, 0, stream>>>(seg, nseg, n_positions, &hdr->error);
         cs_start_kernel<T><<<(unsigned)nseg, kScanThreads, 0, stream>>>(counts, n, seg, start);
-        cs_gather_kernel<T, true><<<blocks, 256, 0, stream>>>(counts, P, positions, scales, start, out, &hdr->error);
-    } else {
-        cs_gather_kernel<T, false><<<blocks, 256, 0, stream>>>(counts, P, nullptr, nullptr, nullptr, out, &hdr->error);
+        return launch_cs_gather<T, true>(counts, P, positions, scales, start, out, hdr, blocks, stream);
     }
-    IDIWF_CUDA_CHECK(cudaGetLastError());
-    return IDIWF_OK;
+    return launch_cs_gather<T, false>(counts, P, nullptr, nullptr, nullptr, out, hdr, blocks, stream);
 }
 
 }  // namespace idiwf

@@ -198,3 +198,16 @@ def test_simulate_photons_pipeline_matches_two_step():
                               chargesharing=(0.5, 0.0))
     ref_cs = oracle.chargesharing(got.astype(np.int64), 0.5, 0.0, key=(123, 0), stream=0)
     np.testing.assert_allclose(cs, ref_cs, rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("s,mean,ns", [(2.6, 0.4, 0.0), (0.5, 40.0, 0.0), (0.5, 40.0, 0.1)])
+def test_chargesharing_wide_and_crowded_vs_oracle(s, mean, ns):
+    """w = ceil(2 s) above the tiled kernel's 4, and images so crowded that a
+    tile's region holds more photons than its shared memory: both take the
+    per-pixel gather, which must agree with the tiled one's order and sums."""
+    g = np.random.default_rng(int(s * 10 + mean))
+    counts = g.poisson(mean, (2, 37, 45)).astype(np.int64)
+    key = (12, 34)
+    gpu = _core.chargesharing(_dev(counts), s, ns, key, 3, check=True).cpu().numpy()
+    orc = oracle.chargesharing(counts, s, ns, key=key, stream=3)
+    np.testing.assert_allclose(gpu, orc, rtol=1e-12, atol=1e-12)
