@@ -45,19 +45,19 @@ namespace idiwf {
 // record layouts
 // ---------------------------------------------------------------------------
 // split:  r64 double4 {x, y, z, Psi}              (32 B)  Psi = magic + 1/4 + psi/2pi mod 1
-//         rA  float4  {x, x, y, y}                (16 B)  duplicated for f32x2
-//         rB  float4  {z, z, -w, -w}              (16 B)  w = |r|^2 (nf) or x^2+y^2
-//         rC  float2  {a, a}                      ( 8 B)
+//         rA  float4  {x, y, z, -w}               (16 B)  w = |r|^2 (nf) or x^2+y^2
+//         rC  float   a                           ( 4 B)
+//         (the kernel pairs each value with itself for the f32x2 operations;
+//         storing the pairs would cost a fifth shared-memory load per emitter)
 // double: r64 double4 {x, y, z, psi}, ra double a
-constexpr int kSplitRecBytes = 72;
+constexpr int kSplitRecBytes = 52;
 constexpr int kDoubleRecBytes = 40;
 constexpr int kFold = 64;  // emitters per FP32 partial before the Kahan fold
 
 struct SplitRecs {
     double4 *r64;
     float4 *rA;
-    float4 *rB;
-    float2 *rC;
+    float *rC;
 };
 struct DoubleRecs {
     double4 *r64;
@@ -71,13 +71,11 @@ static inline SplitRecs split_recs(void *ws, int64_t nrec) {
     base += align256(nrec * 32);
     r.rA = reinterpret_cast<float4 *>(base);
     base += align256(nrec * 16);
-    r.rB = reinterpret_cast<float4 *>(base);
-    base += align256(nrec * 16);
-    r.rC = reinterpret_cast<float2 *>(base);
+    r.rC = reinterpret_cast<float *>(base);
     return r;
 }
 static inline size_t split_recs_bytes(int64_t nrec) {
-    return align256(nrec * 32) + 2 * align256(nrec * 16) + align256(nrec * 8);
+    return align256(nrec * 32) + align256(nrec * 16) + align256(nrec * 4);
 }
 static inline DoubleRecs double_recs(void *ws, int64_t nrec) {
     char *base = static_cast<char *>(ws) + kWsDataOffset;
@@ -123,14 +121,12 @@ __global__ void prep_split_kernel(const __grid_constant__ BatchParams bp, const 
             // w is stored negated: the kernel forms s^2 - w and subtracts h times it
             const float fx = (float)a.x, fy = (float)a.y, fz = (float)a.z, fw = (float)(-w);
             rec.r64[r] = make_double4(a.x, a.y, a.z, psi);
-            rec.rA[r] = make_float4(fx, fx, fy, fy);
-            rec.rB[r] = make_float4(fz, fz, fw, fw);
-            rec.rC[r] = make_float2(amp, amp);
+            rec.rA[r] = make_float4(fx, fy, fz, fw);
+            rec.rC[r] = amp;
         } else {
             rec.r64[r] = make_double4(0, 0, 0, 0);
             rec.rA[r] = make_float4(0, 0, 0, 0);
-            rec.rB[r] = make_float4(0, 0, 0, 0);
-            rec.rC[r] = make_float2(0, 0);
+            rec.rC[r] = 0.0f;
         }
     }
 }
@@ -322,8 +318,7 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
                 mbar_arrive_expect_tx(&bar[slot], stage_bytes);
                 bulk_g2s(st, rec.r64 + r0, TE * 32, &bar[slot]);
                 bulk_g2s(st + TE * 32, rec.rA + r0, TE * 16, &bar[slot]);
-                bulk_g2s(st + TE * 48, rec.rB + r0, TE * 16, &bar[slot]);
-                bulk_g2s(st + TE * 64, rec.rC + r0, TE * 8, &bar[slot]);
+                bulk_g2s(st + TE * 48, rec.rC + r0, TE * 4, &bar[slot]);
                 ++issued;
             }
         }
@@ -336,8 +331,7 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
             const unsigned char *st = smem + slot * stage_bytes;
             const double4 *s64 = reinterpret_cast<const double4 *>(st);
             const float4 *sA = reinterpret_cast<const float4 *>(st + TE * 32);
-            const float4 *sB = reinterpret_cast<const float4 *>(st + TE * 48);
-            const float2 *sC = reinterpret_cast<const float2 *>(st + TE * 64);
+            const float *sC = reinterpret_cast<const float *>(st + TE * 48);
 
             for (int jb = 0; jb < TE; jb += kFold) {
                 float2 are[PH], aim[PH];
@@ -347,8 +341,8 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
                 for (int j = jb; j < jb + kFold; ++j) {
                     const double4 r = s64[j];
                     const float4 A = sA[j];
-                    const float4 B = sB[j];
-                    const float2 a2 = sC[j];
+                    const float a1 = sC[j];
+                    const float2 a2 = f2(a1, a1);
 #pragma unroll
                     for (int q = 0; q < PH; ++q) {
                         uint32_t lo[2];
@@ -371,15 +365,15 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
                         float2 arg = __ffma2_rn(u, PI2, NEG_15PI2);
                         float2 amp = a2;
                         if (NF) {
-                            float2 s = __fmul2_rn(dhx[q], f2(A.x, A.y));
-                            s = __ffma2_rn(dhy[q], f2(A.z, A.w), s);
-                            s = __ffma2_rn(dhz[q], f2(B.x, B.y), s);
+                            float2 s = __fmul2_rn(dhx[q], f2(A.x, A.x));
+                            s = __ffma2_rn(dhy[q], f2(A.y, A.y), s);
+                            s = __ffma2_rn(dhz[q], f2(A.z, A.z), s);
                             // -h (s^2 - |r|^2) = h (|r|^2 - s^2)
-                            const float2 w2 = __ffma2_rn(s, s, f2(B.z, B.w));
+                            const float2 w2 = __ffma2_rn(s, s, f2(A.w, A.w));
                             arg = __ffma2_rn(hh[q], w2, arg);
                             if (SCALE) amp = __fmul2_rn(a2, __ffma2_rn(s, iD2[q], iD[q]));
                         } else if (SECOND) {
-                            arg = __ffma2_rn(hh[q], f2(B.z, B.w), arg);  // (-h)(-(x^2+y^2))
+                            arg = __ffma2_rn(hh[q], f2(A.w, A.w), arg);  // (-h)(-(x^2+y^2))
                         }
                         amp.x = __uint_as_float(__float_as_uint(amp.x) ^ (lo[0] & 0x80000000u));
                         amp.y = __uint_as_float(__float_as_uint(amp.y) ^ (lo[1] & 0x80000000u));
@@ -422,8 +416,7 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
                 mbar_arrive_expect_tx(&bar[slot2], stage_bytes);
                 bulk_g2s(st2, rec.r64 + r0, TE * 32, &bar[slot2]);
                 bulk_g2s(st2 + TE * 32, rec.rA + r0, TE * 16, &bar[slot2]);
-                bulk_g2s(st2 + TE * 48, rec.rB + r0, TE * 16, &bar[slot2]);
-                bulk_g2s(st2 + TE * 64, rec.rC + r0, TE * 8, &bar[slot2]);
+                bulk_g2s(st2 + TE * 48, rec.rC + r0, TE * 4, &bar[slot2]);
                 ++issued;
             }
         }
@@ -1164,7 +1157,7 @@ extern "C" idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiw
     if (kWsDataOffset + split_recs_bytes(nrec) > (size_t)IDIWF_NOALLOC_SCRATCH_BYTES)
         return set_error(IDIWF_ERR_UNSUPPORTED,
                          "idiwf_forward_noalloc: batch needs more than the 16 MiB static scratch "
-                         "(at most 232448 emitters in total after padding every image to a multiple of 256); "
+                         "(at most 321792 emitters in total after padding every image to a multiple of 256); "
                          "use idiwf_forward with a caller workspace");
     // images by descending emitter count (stable insertion sort, no heap)
     for (int i = 0; i < bp.n_images; ++i) {

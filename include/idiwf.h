@@ -138,8 +138,8 @@ idiwf_status idiwf_forward_cta_times(const void *workspace, uint64_t *host_ns, i
  * GPU which loads this library holds until the process exits.
  *
  * Limits: at most 512 images per call, and the emitters of all images, each
- * image padded to a multiple of 256, must fit the scratch at 72 bytes each:
- * 232,448 emitters in total.  Larger batches are rejected with
+ * image padded to a multiple of 256, must fit the scratch at 52 bytes each:
+ * 321,792 emitters in total.  Larger batches are rejected with
  * IDIWF_ERR_UNSUPPORTED before anything is enqueued.
  *
  * The first call on a device looks up the array's device address (with that

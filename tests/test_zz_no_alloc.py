@@ -83,7 +83,7 @@ def test_noalloc_intensity_output_and_size_limit():
     torch.cuda.synchronize()
     assert torch.allclose(I, ref, rtol=1e-6, atol=0)
     # beyond the static scratch: rejected on the host with a clear message
-    big = torch.zeros((240000, 4), dtype=torch.float64, device="cuda")
-    st, _ = _noalloc(lib, geom, big, [0, 240000])
+    big = torch.zeros((330000, 4), dtype=torch.float64, device="cuda")
+    st, _ = _noalloc(lib, geom, big, [0, 330000])
     assert st == nat.ERR_UNSUPPORTED
     assert b"16 MiB" in lib.idiwf_last_error_string()
