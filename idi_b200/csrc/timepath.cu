@@ -32,10 +32,12 @@ constexpr int kTimeThreads = 512;
 constexpr int kTimeWarps = kTimeThreads / 32;
 constexpr int kTimeIPT = 40;                                 // items per thread
 constexpr int kTimeMaxN = kTimeThreads * kTimeIPT;           // 20480
+constexpr int kCoarse = 1024;                                 // coarse bins of the bucket map
 constexpr size_t kTimeSmem = (size_t)kTimeMaxN * 8           // key table
                              + (size_t)kTimeMaxN * 2         // permutation
                              + (size_t)kTimeWarps * 256 * 4  // per-warp digit counters
-                             + 256 * 4 + 1024;               // digit bases + scan scratch
+                             + 256 * 4 + 1024                // digit bases + scan scratch
+                             + (kCoarse + 4) * 4;            // first fine bucket per coarse bin
 
 __device__ __forceinline__ uint64_t sortable(double v) {
     const uint64_t b = (uint64_t)__double_as_longlong(v);
@@ -128,26 +130,40 @@ __device__ __forceinline__ void block_minmax(double &lo, double &hi, double *sm)
 }
 
 // Exact sort of emitter indices by key, by buckets.  The bucket of a key is
-// floor((t - kmin) * NB / (kmax - kmin)), a non-decreasing function of t in
-// IEEE arithmetic, so bucket order is key order; each bucket is then
-// insertion-sorted by (key, emitter index).  Returns false (perm undefined)
-// when a bucket holds more than kMaxBucket keys; the caller then runs the
-// radix sort.  cnt: kBuckets/2 words of packed 16-bit counters.
+// a non-decreasing function of the key in IEEE arithmetic, so bucket order is
+// key order; each bucket is then insertion-sorted by (key, emitter index).
+// The map has two levels so that buckets hold about the same number of keys
+// whatever the keys' distribution (arrival times are near-Gaussian, and a
+// linear map crowds the middle buckets, whose insertion sort then holds the
+// whole CTA at the next barrier): u = (t - kmin) kCoarse / (kmax - kmin) picks
+// coarse bin c = floor(u); coarse bin c owns the fine buckets [B_c, B_c+1),
+// B_c = c + floor(P_c (kBuckets - kCoarse) / n) with P_c the keys below bin c
+// (at least one bucket per coarse bin), and the key goes to fine bucket
+// B_c + floor((u - c) (B_c+1 - B_c)), clamped into the bin's range.  Every step
+// is monotone in t.  Returns false (perm undefined) when a bucket holds more
+// than kMaxBucket keys; the caller then runs the radix sort.  cnt: kBuckets/2
+// words of packed 16-bit counters; coarse: kCoarse + 1 words.
 constexpr int kBuckets = 8192;
 constexpr int kMaxBucket = 128;
 constexpr int kBucketsPerThread = kBuckets / kTimeThreads;  // 16
+constexpr int kCoarsePerThread = kCoarse / kTimeThreads;    // 2
 
-__device__ __forceinline__ uint32_t bucket_of(double t, double kmin, double scale) {
-    const int b = __double2int_rz(__dmul_rn(__dsub_rn(t, kmin), scale));
-    return (uint32_t)min(max(b, 0), kBuckets - 1);
+__device__ __forceinline__ int coarse_of(double u) { return min(max(__double2int_rz(u), 0), kCoarse - 1); }
+
+__device__ __forceinline__ uint32_t fine_bucket(double t, double kmin, double scale, const uint32_t *coarse) {
+    const double u = __dmul_rn(__dsub_rn(t, kmin), scale);
+    const int c = coarse_of(u);
+    const uint32_t b0 = coarse[c], nb = coarse[c + 1] - b0;
+    const int f = __double2int_rz(__dmul_rn(__dsub_rn(u, (double)c), (double)nb));
+    return b0 + (uint32_t)min(max(f, 0), (int)nb - 1);
 }
 __device__ __forceinline__ uint32_t cnt_get(const uint32_t *cnt, uint32_t b) {
     const uint32_t w = cnt[b >> 1];
     return (b & 1) ? (w >> 16) : (w & 0xFFFFu);
 }
 
-__device__ bool bucket_sort(const double *keytab, uint16_t *perm, uint32_t *cnt, int n, double kmin, double kmax,
-                            double *scratch, int *s_flag) {
+__device__ bool bucket_sort(const double *keytab, uint16_t *perm, uint32_t *cnt, uint32_t *coarse, int n,
+                            double kmin, double kmax, double *scratch, int *s_flag) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (!(kmax > kmin)) {
         // all keys equal (or one key): stable order is emitter order
@@ -155,12 +171,45 @@ __device__ bool bucket_sort(const double *keytab, uint16_t *perm, uint32_t *cnt,
         __syncthreads();
         return true;
     }
-    const double scale = (double)kBuckets / (kmax - kmin);
+    const double scale = (double)kCoarse / (kmax - kmin);
     for (int w = tid; w < kBuckets / 2; w += kTimeThreads) cnt[w] = 0u;
+    for (int c = tid; c <= kCoarse; c += kTimeThreads) coarse[c] = 0u;
     if (tid == 0) *s_flag = 0;
     __syncthreads();
+    for (int j = tid; j < n; j += kTimeThreads)
+        atomicAdd(&coarse[coarse_of(__dmul_rn(__dsub_rn(keytab[j], kmin), scale))], 1u);
+    __syncthreads();
+    uint32_t *wsum = reinterpret_cast<uint32_t *>(scratch);  // 16 words
+    {
+        // B_c from the exclusive prefix of the coarse counts; thread t owns bins [2t, 2t+2)
+        uint32_t cc[kCoarsePerThread], sum = 0;
+#pragma unroll
+        for (int i = 0; i < kCoarsePerThread; ++i) {
+            cc[i] = coarse[tid * kCoarsePerThread + i];
+            sum += cc[i];
+        }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t pre = incl - sum;
+        for (int w = 0; w < warp; ++w) pre += wsum[w];
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kCoarsePerThread; ++i) {
+            const int c = tid * kCoarsePerThread + i;
+            coarse[c] = (uint32_t)c + (uint32_t)(((uint64_t)pre * (kBuckets - kCoarse)) / (uint64_t)n);
+            pre += cc[i];
+        }
+        if (tid == kTimeThreads - 1) coarse[kCoarse] = kBuckets;
+    }
+    __syncthreads();
     for (int j = tid; j < n; j += kTimeThreads) {
-        const uint32_t b = bucket_of(keytab[j], kmin, scale);
+        const uint32_t b = fine_bucket(keytab[j], kmin, scale, coarse);
         atomicAdd(&cnt[b >> 1], (b & 1) ? 0x10000u : 1u);
     }
     __syncthreads();
@@ -178,7 +227,6 @@ __device__ bool bucket_sort(const double *keytab, uint16_t *perm, uint32_t *cnt,
         const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += y;
     }
-    uint32_t *wsum = reinterpret_cast<uint32_t *>(scratch);  // 16 words
     if (lane == 31) wsum[warp] = incl;
     __syncthreads();
     uint32_t run = incl - sum;
@@ -195,7 +243,7 @@ __device__ bool bucket_sort(const double *keytab, uint16_t *perm, uint32_t *cnt,
     if (*s_flag) return false;  // uniform: every thread read the same flag after the barrier
     // scatter: afterwards cnt holds the end (= next start) of every bucket
     for (int j = tid; j < n; j += kTimeThreads) {
-        const uint32_t b = bucket_of(keytab[j], kmin, scale);
+        const uint32_t b = fine_bucket(keytab[j], kmin, scale, coarse);
         const uint32_t old = atomicAdd(&cnt[b >> 1], (b & 1) ? 0x10000u : 1u);
         perm[(b & 1) ? (old >> 16) : (old & 0xFFFFu)] = (uint16_t)j;
     }
@@ -309,6 +357,7 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
     uint32_t *H = reinterpret_cast<uint32_t *>(smem + (size_t)kTimeMaxN * 10);
     uint32_t *base = H + kTimeWarps * 256;
     double *scratch = reinterpret_cast<double *>(base + 256);  // 128 doubles
+    uint32_t *coarse = reinterpret_cast<uint32_t *>(scratch + 128);
     __shared__ int s_pix, s_flag;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -349,7 +398,7 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
             keytab[j] = t;
         }
         block_minmax(kmin, kmax, scratch + 96);
-        if (!bucket_sort(keytab, perm, reinterpret_cast<uint32_t *>(H), n, kmin, kmax, scratch, &s_flag)) {
+        if (!bucket_sort(keytab, perm, reinterpret_cast<uint32_t *>(H), coarse, n, kmin, kmax, scratch, &s_flag)) {
             radix_sort(keytab, perm, H, base);
         }
         // perm[m] = emitter at sorted position m (positions >= n hold padding)
