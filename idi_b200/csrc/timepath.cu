@@ -497,10 +497,11 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
 // ---------------------------------------------------------------------------
 constexpr int kLargeBuckets = 16384;
 constexpr int kLargeMaxBucket = 256;
-constexpr size_t kLargeSmem = (size_t)kLargeBuckets * 4;  // also holds the radix counters
+constexpr size_t kLargeSmem = (size_t)kLargeBuckets * 4  // also holds the radix counters
+                              + (kCoarse + 4) * 4;      // first fine bucket per coarse bin
 
 __host__ __device__ __forceinline__ int large_buckets(int64_t n) {
-    int nb = kTimeThreads;
+    int nb = 8 * kCoarse;  // n > 20480 here: at least 8192 buckets, a multiple of the threads
     while (nb < kLargeBuckets && (int64_t)nb * 4 < n) nb <<= 1;
     return nb;
 }
@@ -509,25 +510,57 @@ __host__ __device__ __forceinline__ size_t large_slice_bytes(int64_t n) {
     return ((size_t)n * 16 + 255) & ~(size_t)255;
 }
 
-__device__ __forceinline__ uint32_t bucket_of_n(double t, double kmin, double scale, int nb) {
-    const int b = __double2int_rz(__dmul_rn(__dsub_rn(t, kmin), scale));
-    return (uint32_t)min(max(b, 0), nb - 1);
+// The two-level map of bucket_sort with nb fine buckets (nb >= 8192 here).
+__device__ __forceinline__ uint32_t fine_bucket_n(double t, double kmin, double scale, const uint32_t *coarse) {
+    return fine_bucket(t, kmin, scale, coarse);
 }
 
-__device__ bool bucket_sort_large(const double *keys, int *perm, uint32_t *cnt, int n, int nb, double kmin,
-                                  double kmax, double *scratch, int *s_flag) {
+__device__ bool bucket_sort_large(const double *keys, int *perm, uint32_t *cnt, uint32_t *coarse, int n, int nb,
+                                  double kmin, double kmax, double *scratch, int *s_flag) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (!(kmax > kmin)) {
         for (int m = tid; m < n; m += kTimeThreads) perm[m] = m;
         __syncthreads();
         return true;
     }
-    const double scale = (double)nb / (kmax - kmin);
+    const double scale = (double)kCoarse / (kmax - kmin);
     const int per = nb / kTimeThreads;
     for (int b = tid; b < nb; b += kTimeThreads) cnt[b] = 0u;
+    for (int c = tid; c <= kCoarse; c += kTimeThreads) coarse[c] = 0u;
     if (tid == 0) *s_flag = 0;
     __syncthreads();
-    for (int j = tid; j < n; j += kTimeThreads) atomicAdd(&cnt[bucket_of_n(keys[j], kmin, scale, nb)], 1u);
+    for (int j = tid; j < n; j += kTimeThreads)
+        atomicAdd(&coarse[coarse_of(__dmul_rn(__dsub_rn(keys[j], kmin), scale))], 1u);
+    __syncthreads();
+    uint32_t *wsum = reinterpret_cast<uint32_t *>(scratch);
+    {
+        uint32_t cc[kCoarsePerThread], csum = 0;
+#pragma unroll
+        for (int i = 0; i < kCoarsePerThread; ++i) {
+            cc[i] = coarse[tid * kCoarsePerThread + i];
+            csum += cc[i];
+        }
+        uint32_t cincl = csum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, cincl, o);
+            if (lane >= o) cincl += y;
+        }
+        if (lane == 31) wsum[warp] = cincl;
+        __syncthreads();
+        uint32_t pre = cincl - csum;
+        for (int w = 0; w < warp; ++w) pre += wsum[w];
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kCoarsePerThread; ++i) {
+            const int c = tid * kCoarsePerThread + i;
+            coarse[c] = (uint32_t)c + (uint32_t)(((uint64_t)pre * (uint64_t)(nb - kCoarse)) / (uint64_t)n);
+            pre += cc[i];
+        }
+        if (tid == kTimeThreads - 1) coarse[kCoarse] = (uint32_t)nb;
+    }
+    __syncthreads();
+    for (int j = tid; j < n; j += kTimeThreads) atomicAdd(&cnt[fine_bucket_n(keys[j], kmin, scale, coarse)], 1u);
     __syncthreads();
     uint32_t sum = 0, big = 0;
     for (int i = 0; i < per; ++i) {
@@ -541,7 +574,6 @@ __device__ bool bucket_sort_large(const double *keys, int *perm, uint32_t *cnt, 
         const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += y;
     }
-    uint32_t *wsum = reinterpret_cast<uint32_t *>(scratch);
     if (lane == 31) wsum[warp] = incl;
     if (big) *s_flag = 1;
     __syncthreads();
@@ -557,7 +589,7 @@ __device__ bool bucket_sort_large(const double *keys, int *perm, uint32_t *cnt, 
     if (*s_flag) return false;
     // scatter: afterwards cnt[b] is the end of bucket b
     for (int j = tid; j < n; j += kTimeThreads) {
-        const uint32_t pos = atomicAdd(&cnt[bucket_of_n(keys[j], kmin, scale, nb)], 1u);
+        const uint32_t pos = atomicAdd(&cnt[fine_bucket_n(keys[j], kmin, scale, coarse)], 1u);
         perm[pos] = j;
     }
     __syncthreads();
@@ -680,6 +712,7 @@ __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
     uint32_t *cnt = reinterpret_cast<uint32_t *>(smem);
     uint32_t *H = cnt;                       // radix fallback: per-warp counters
     uint32_t *base = cnt + kTimeWarps * 256;  // and digit bases
+    uint32_t *coarse = cnt + kLargeBuckets;
     __shared__ double scratch[128];
     __shared__ int s_pix, s_flag;
     unsigned char *slice = slices + (size_t)blockIdx.x * large_slice_bytes(n);
@@ -717,7 +750,7 @@ __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
         block_minmax(kmin, kmax, scratch + 96);
         __syncthreads();
         const int *sorted = perm;
-        if (!bucket_sort_large(keys, perm, cnt, n, nb, kmin, kmax, scratch, &s_flag)) {
+        if (!bucket_sort_large(keys, perm, cnt, coarse, n, nb, kmin, kmax, scratch, &s_flag)) {
             radix_sort_large(keys, perm, perm2, n, H, base);
             sorted = perm;
         }
