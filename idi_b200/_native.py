@@ -115,6 +115,7 @@ class Config(ctypes.Structure):
         ("pixels_per_thread", ctypes.c_int32),
         ("emitters_per_tile", ctypes.c_int32),
         ("ctas_per_sm", ctypes.c_int32),
+        ("pixel_groups", ctypes.c_int32),
     ]
 
 

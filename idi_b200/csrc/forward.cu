@@ -58,6 +58,7 @@ struct SplitRecs {
     double4 *r64;
     float4 *rA;
     float *rC;
+    uint32_t *rmax2;  // per image of the launch: max |r|^2 (float bits, rounded up)
 };
 struct DoubleRecs {
     double4 *r64;
@@ -72,10 +73,12 @@ static inline SplitRecs split_recs(void *ws, int64_t nrec) {
     r.rA = reinterpret_cast<float4 *>(base);
     base += align256(nrec * 16);
     r.rC = reinterpret_cast<float *>(base);
+    base += align256(nrec * 4);
+    r.rmax2 = reinterpret_cast<uint32_t *>(base);
     return r;
 }
 static inline size_t split_recs_bytes(int64_t nrec) {
-    return align256(nrec * 32) + align256(nrec * 16) + align256(nrec * 4);
+    return align256(nrec * 32) + align256(nrec * 16) + align256(nrec * 4) + align256(kMaxImagesPerLaunch * 4);
 }
 static inline DoubleRecs double_recs(void *ws, int64_t nrec) {
     char *base = static_cast<char *>(ws) + kWsDataOffset;
@@ -98,12 +101,14 @@ __global__ void prep_split_kernel(const __grid_constant__ BatchParams bp, const 
     const int b = blockIdx.y;
     const ImageDesc d = bp.img[b];
     const int64_t nrec = (int64_t)d.ntiles * bp.te;
+    uint32_t r2max = 0;  // float bits; non-negative floats order like their bits
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nrec;
          j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t r = d.rec + j;
         if (j < d.n) {
             const int64_t s = d.src + j;
             const double4 a = reinterpret_cast<const double4 *>(atoms)[s];
+            r2max = max(r2max, __float_as_uint(__double2float_ru((a.x * a.x + a.y * a.y) + a.z * a.z)));
             double psi = a.w * kInvTwoPi;
             psi = psi - rint(psi);
             // the DFMA chain of the kernel starts from this value: the magic
@@ -129,6 +134,10 @@ __global__ void prep_split_kernel(const __grid_constant__ BatchParams bp, const 
             rec.rC[r] = 0.0f;
         }
     }
+    // |r|_max of the image for the split kernel's pixel-run bound (the caller
+    // zeroes rmax2 before the launch)
+    r2max = __reduce_max_sync(0xffffffffu, r2max);
+    if ((threadIdx.x & 31) == 0 && r2max) atomicMax(&rec.rmax2[b], r2max);
 }
 
 __global__ void prep_double_kernel(const __grid_constant__ BatchParams bp, const double *__restrict__ atoms,
@@ -226,117 +235,217 @@ __global__ void fwd_finish_kernel(const GeomParams g, const double2 *__restrict_
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
-template <int PPT, bool NF, bool SCALE, bool SECOND, bool CHUNKED>
-__global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(const __grid_constant__ BatchParams bp,
-                                                        const GeomParams g, SplitRecs rec,
-                                                        void *__restrict__ out, int out_kind,
-                                                        WsHeader *__restrict__ hdr,
-                                                        uint64_t *__restrict__ cta_ns,
-                                                        double2 *__restrict__ partials) {
-    static_assert(PPT % 2 == 0, "pixels are processed in f32x2 pairs");
-    constexpr int PH = PPT / 2;
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bar[2];
-    __shared__ int s_unit, s_abort;
+// Pixel runs of the split kernel: aligned blocks of kRun pixels along a
+// detector row share one FP64 base phase, taken at the middle of the run.
+constexpr int kRun = 4;
+// Largest phase offset (radians) that a run adds in FP32 to its base phase,
+// bounded per image by k * run_span * |r|_max.  Up to 1 rad the FP32 offset is
+// good to about 1e-7 rad and the sine/cosine arguments stay inside [-pi, pi].
+constexpr double kGroupMaxPhase = 1.0;
+// Constants of a run's base angle with the 8 low fixed-point bits, in units
+// of pi_f = FP32 pi as in the per-pixel path: C is -pi_f (1.5 + 2^-8 + 2^-24)
+// rounded to FP32 and S = pi_f 2^-8 minus C's rounding error, so that C + S
+// is exact up to the FP32 rounding of S (< 5e-10 rad).
+constexpr double kPiF = (double)3.14159274f;
+constexpr double kRunBaseCExact = -kPiF * (1.5 + 1.0 / 256.0 + 1.0 / 16777216.0);
+constexpr float kRunBaseC = (float)kRunBaseCExact;
+constexpr float kRunBaseS = (float)(kPiF / 256.0 - ((double)kRunBaseC - kRunBaseCExact));
 
+// Direction of a detector point for the split kernel: the FP64 turn
+// coefficients nq = -k (d_hat - z_hat) / 2pi (z part without cancellation),
+// d_hat and 1/|d|.
+struct PixelDir {
+    double nqx, nqy, nqz, ux, uy, uz, invD;
+};
+__device__ __forceinline__ PixelDir pixel_dir(const GeomParams &g, double fix, double fiy) {
+    double dx, dy, dz;
+    pixel_cpu_at(g, fix, fiy, dx, dy, dz);
+    const double rho2 = dx * dx + dy * dy;
+    const double D = sqrt(rho2 + dz * dz);
+    const double invD = 1.0 / D;
+    const double dzm1 = dz > 0 ? -rho2 / (D * (D + dz)) : dz * invD - 1.0;
+    PixelDir p;
+    p.ux = dx * invD;
+    p.uy = dy * invD;
+    p.uz = dz * invD;
+    p.nqx = -g.kp * p.ux;
+    p.nqy = -g.kp * p.uy;
+    p.nqz = -g.kp * dzm1;
+    p.invD = invD;
+    return p;
+}
+
+// Base point of run b of the thread whose first pixel is p0: the middle of
+// the aligned run (rows hold a whole number of runs when runs are in use).
+__device__ __forceinline__ PixelDir run_base(const GeomParams &g, int p0, int b, int npix) {
+    const int rs = min((p0 & ~(kRun - 1)) + kRun * b, npix - kRun);
+    const int ix = rs / g.ny;
+    return pixel_dir(g, (double)ix, (double)(rs - ix * g.ny) + 0.5 * (kRun - 1));
+}
+
+// One work unit (image, pixel tile[, emitter chunk]) of the split kernel.
+//
+// GROUP = false: every pixel forms its phase with its own FP64 DFMA chain.
+// GROUP = true:  one FP64 chain per run of kRun pixels forms the phase at the
+//   middle of the run (fixed point, half-turn fold as below); pixel i adds the
+//   FP32 offset D_i . r with D_i = 2 pi (nq_i - nq_base) = -k (d_hat_i -
+//   d_hat_base), exact up to FP32 rounding because |D_i . r| <= kGroupMaxPhase
+//   (checked per image by the caller).  The near-field term uses
+//   s_i = d_hat_i . r = s_base - D_i.r / k.  The half-turn sign of the base
+//   applies to the whole run.
+// Returns true when a bounded wait gave up (the unit is abandoned).
+template <int PPT, bool NF, bool SCALE, bool SECOND, bool CHUNKED, bool GROUP>
+__device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomParams &g, const SplitRecs &rec,
+                                           void *__restrict__ out, int out_kind, WsHeader *__restrict__ hdr,
+                                           double2 *__restrict__ partials, unsigned char *smem, uint64_t *bar,
+                                           int *s_abort, uint32_t &issued, uint32_t &consumed, int img,
+                                           int chunk, const ImageDesc &d, int p0, int tbeg, int tend) {
+    constexpr int PH = PPT / 2;
+    constexpr int NB = PPT >= kRun ? PPT / kRun : 1;  // runs (base phases) per thread
+    constexpr int NQ = GROUP ? NB : PPT;
     const int tid = threadIdx.x;
     const int TE = bp.te;
     const uint32_t stage_bytes = (uint32_t)TE * kSplitRecBytes;
-    const uint64_t t_start = globaltimer_ns();
-    if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        s_abort = 0;
-        mbar_fence_init();
-        if (blockIdx.x == 0) hdr->n_ctas = gridDim.x;
-    }
-    __syncthreads();
-
     const int npix = g.nx * g.ny;
-    const int tile_px = blockDim.x * PPT;
-    uint32_t issued = 0, consumed = 0;
-    bool aborted = false;
-
     const float2 PI2 = f2(3.14159274f, 3.14159274f);
     const float2 NEG_15PI2 = f2(-4.71238898f, -4.71238898f);
 
-    for (;;) {
-        __syncthreads();
-        if (tid == 0) s_unit = (int)atomicAdd(&hdr->work_counter, 1u);
-        __syncthreads();
-        const int unit = s_unit;
-        if (unit >= bp.total_units) break;
-        const int ks = CHUNKED ? bp.ksplit : 1;
-        const int chunk = unit % ks;
-        const int pu = unit / ks;
-        const int img = bp.order[pu / bp.tiles_per_image];
-        const int ptile = pu % bp.tiles_per_image;
-        const ImageDesc d = bp.img[img];
-        const int p0 = ptile * tile_px + tid * PPT;
-        // emitter tiles of this unit: the whole image, or one chunk of it
-        const int tbeg = CHUNKED ? min(chunk * d.tpc, d.ntiles) : 0;
-        const int tend = CHUNKED ? min(tbeg + d.tpc, d.ntiles) : d.ntiles;
-
-        // ---- per-pixel constants (FP64 geometry) ----
-        double nqx[PPT], nqy[PPT], nqz[PPT];
-        float2 dhx[PH], dhy[PH], dhz[PH], hh[PH], iD[PH], iD2[PH];
+    // ---- per-pixel constants (FP64 geometry) ----
+    // cx/cy/cz: d_hat of each pixel, or (GROUP) its offset coefficients D_i
+    double nqx[NQ], nqy[NQ], nqz[NQ];
+    float2 cx[PH], cy[PH], cz[PH], hh[PH], iD[PH], iD2[PH];
+    float dbx[NB], dby[NB], dbz[NB];
+    PixelDir base[NB];
+    if (GROUP) {
 #pragma unroll
-        for (int i = 0; i < PPT; ++i) {
-            const int p = min(p0 + i, npix - 1);
-            const int ix = p / g.ny, iy = p - ix * g.ny;
-            double dx, dy, dz;
-            pixel_cpu(g, ix, iy, dx, dy, dz);
-            const double rho2 = dx * dx + dy * dy;
-            const double D = sqrt(rho2 + dz * dz);
-            const double invD = 1.0 / D;
-            const double dzm1 = dz > 0 ? -rho2 / (D * (D + dz)) : dz * invD - 1.0;
-            nqx[i] = -g.kp * (dx * invD);
-            nqy[i] = -g.kp * (dy * invD);
-            nqz[i] = -g.kp * dzm1;
-            const float fh = (float)(-g.k * 0.5 * invD);  // -h, pairs with the negated w
-            const float fdx = (float)(dx * invD), fdy = (float)(dy * invD), fdz = (float)(dz * invD);
-            const float fi = (float)invD, fi2 = (float)(invD * invD);
-            if (i & 1) {
-                dhx[i / 2].y = fdx; dhy[i / 2].y = fdy; dhz[i / 2].y = fdz;
-                hh[i / 2].y = fh; iD[i / 2].y = fi; iD2[i / 2].y = fi2;
+        for (int b = 0; b < NB; ++b) {
+            base[b] = run_base(g, p0, b, npix);
+            nqx[b] = base[b].nqx;
+            nqy[b] = base[b].nqy;
+            nqz[b] = base[b].nqz;
+            dbx[b] = (float)base[b].ux;
+            dby[b] = (float)base[b].uy;
+            dbz[b] = (float)base[b].uz;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) {
+        const int p = min(p0 + i, npix - 1);
+        const int ix = p / g.ny, iy = p - ix * g.ny;
+        const PixelDir q = pixel_dir(g, (double)ix, (double)iy);
+        float fx, fy, fz;
+        if (GROUP) {
+            const PixelDir &bs = base[PPT >= kRun ? i / kRun : 0];
+            fx = (float)(kTwoPi * (q.nqx - bs.nqx));
+            fy = (float)(kTwoPi * (q.nqy - bs.nqy));
+            fz = (float)(kTwoPi * (q.nqz - bs.nqz));
+        } else {
+            nqx[i] = q.nqx;
+            nqy[i] = q.nqy;
+            nqz[i] = q.nqz;
+            fx = (float)q.ux;
+            fy = (float)q.uy;
+            fz = (float)q.uz;
+        }
+        const float fh = (float)(-g.k * 0.5 * q.invD);  // -h, pairs with the negated w
+        const float fi = (float)q.invD, fi2 = (float)(q.invD * q.invD);
+        if (i & 1) {
+            cx[i / 2].y = fx; cy[i / 2].y = fy; cz[i / 2].y = fz;
+            hh[i / 2].y = fh; iD[i / 2].y = fi; iD2[i / 2].y = fi2;
+        } else {
+            cx[i / 2].x = fx; cy[i / 2].x = fy; cz[i / 2].x = fz;
+            hh[i / 2].x = fh; iD[i / 2].x = fi; iD2[i / 2].x = fi2;
+        }
+    }
+    const float ninvk = (float)(-1.0 / g.k);
+    const float2 NEG_INVK2 = f2(ninvk, ninvk);
+
+    float sre[PPT], cre[PPT], sim[PPT], cim[PPT];
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) sre[i] = cre[i] = sim[i] = cim[i] = 0.0f;
+
+    const int nt = tend - tbeg;
+    if (tid == 0) {
+        for (int s = 0; s < 2 && s < nt; ++s) {
+            const uint32_t slot = issued & 1;
+            unsigned char *st = smem + slot * stage_bytes;
+            const int64_t r0 = d.rec + (int64_t)(tbeg + s) * TE;
+            mbar_arrive_expect_tx(&bar[slot], stage_bytes);
+            bulk_g2s(st, rec.r64 + r0, TE * 32, &bar[slot]);
+            bulk_g2s(st + TE * 32, rec.rA + r0, TE * 16, &bar[slot]);
+            bulk_g2s(st + TE * 48, rec.rC + r0, TE * 4, &bar[slot]);
+            ++issued;
+        }
+    }
+    for (int it = 0; it < nt; ++it) {
+        const uint32_t slot = consumed & 1;
+        if (!mbar_wait_bounded(&bar[slot], (consumed >> 1) & 1)) {
+            record_error(&hdr->error, kErrTimeout);
+            *s_abort = 1;
+        }
+        const unsigned char *st = smem + slot * stage_bytes;
+        const double4 *s64 = reinterpret_cast<const double4 *>(st);
+        const float4 *sA = reinterpret_cast<const float4 *>(st + TE * 32);
+        const float *sC = reinterpret_cast<const float *>(st + TE * 48);
+
+        for (int jb = 0; jb < TE; jb += kFold) {
+            float2 are[PH], aim[PH];
+#pragma unroll
+            for (int q = 0; q < PH; ++q) are[q] = aim[q] = f2(0.f, 0.f);
+            if (GROUP) {
+#pragma unroll(PPT <= 4 ? 4 : 2)
+                for (int j = jb; j < jb + kFold; ++j) {
+                    const double4 r = s64[j];
+                    const float4 A = sA[j];
+                    const float a1 = sC[j];
+                    const float2 X2 = f2(A.x, A.x), Y2 = f2(A.y, A.y), Z2 = f2(A.z, A.z);
+                    float2 XB2[NB], AS2[NB], SB2[NB];
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) {
+                        double t = __fma_rn(nqx[b], r.x, r.w);
+                        t = __fma_rn(nqy[b], r.y, t);
+                        t = __fma_rn(nqz[b], r.z, t);
+                        const uint32_t lo = (uint32_t)__double2loint(t);
+                        // base angle and half-turn sign as in the per-pixel path below,
+                        // plus the 8 fixed-point bits below the 23 kept there:
+                        // pi u + C + (1 + r 2^-23) S = pi (u - 1.5) + pi r 2^-31 - pi 2^-24
+                        // (the last term takes back the record's half-step rounding offset)
+                        float xb = __fmaf_rn(__uint_as_float(((lo >> 8) & 0x007FFFFFu) | 0x3F800000u),
+                                             PI2.x, kRunBaseC);
+                        xb = __fmaf_rn(__uint_as_float((lo & 0xFFu) | 0x3F800000u), kRunBaseS, xb);
+                        const float as = __uint_as_float(__float_as_uint(a1) ^ (lo & 0x80000000u));
+                        XB2[b] = f2(xb, xb);
+                        AS2[b] = f2(as, as);
+                        SB2[b] = f2(0.f, 0.f);
+                        if (NF) {
+                            const float sb = __fmaf_rn(dbz[b], A.z, __fmaf_rn(dby[b], A.y, __fmul_rn(dbx[b], A.x)));
+                            SB2[b] = f2(sb, sb);
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < PH; ++q) {
+                        const int b = PPT >= kRun ? q / (kRun / 2) : 0;
+                        float2 dl = __fmul2_rn(cx[q], X2);
+                        dl = __ffma2_rn(cy[q], Y2, dl);
+                        dl = __ffma2_rn(cz[q], Z2, dl);
+                        float2 amp = AS2[b];
+                        if (NF) {
+                            const float2 s = __ffma2_rn(dl, NEG_INVK2, SB2[b]);
+                            const float2 w2 = __ffma2_rn(s, s, f2(A.w, A.w));
+                            dl = __ffma2_rn(hh[q], w2, dl);
+                            if (SCALE) amp = __fmul2_rn(AS2[b], __ffma2_rn(s, iD2[q], iD[q]));
+                        } else if (SECOND) {
+                            dl = __ffma2_rn(hh[q], f2(A.w, A.w), dl);  // (-h)(-(x^2+y^2))
+                        }
+                        const float2 arg = __fadd2_rn(XB2[b], dl);
+                        float s0, c0, s1, c1;
+                        __sincosf(arg.x, &s0, &c0);
+                        __sincosf(arg.y, &s1, &c1);
+                        are[q] = __ffma2_rn(amp, f2(c0, c1), are[q]);
+                        aim[q] = __ffma2_rn(amp, f2(s0, s1), aim[q]);
+                    }
+                }
             } else {
-                dhx[i / 2].x = fdx; dhy[i / 2].x = fdy; dhz[i / 2].x = fdz;
-                hh[i / 2].x = fh; iD[i / 2].x = fi; iD2[i / 2].x = fi2;
-            }
-        }
-
-        float sre[PPT], cre[PPT], sim[PPT], cim[PPT];
-#pragma unroll
-        for (int i = 0; i < PPT; ++i) sre[i] = cre[i] = sim[i] = cim[i] = 0.0f;
-
-        const int nt = tend - tbeg;
-        if (tid == 0) {
-            for (int s = 0; s < 2 && s < nt; ++s) {
-                const uint32_t slot = issued & 1;
-                unsigned char *st = smem + slot * stage_bytes;
-                const int64_t r0 = d.rec + (int64_t)(tbeg + s) * TE;
-                mbar_arrive_expect_tx(&bar[slot], stage_bytes);
-                bulk_g2s(st, rec.r64 + r0, TE * 32, &bar[slot]);
-                bulk_g2s(st + TE * 32, rec.rA + r0, TE * 16, &bar[slot]);
-                bulk_g2s(st + TE * 48, rec.rC + r0, TE * 4, &bar[slot]);
-                ++issued;
-            }
-        }
-        for (int it = 0; it < nt; ++it) {
-            const uint32_t slot = consumed & 1;
-            if (!mbar_wait_bounded(&bar[slot], (consumed >> 1) & 1)) {
-                record_error(&hdr->error, kErrTimeout);
-                s_abort = 1;
-            }
-            const unsigned char *st = smem + slot * stage_bytes;
-            const double4 *s64 = reinterpret_cast<const double4 *>(st);
-            const float4 *sA = reinterpret_cast<const float4 *>(st + TE * 32);
-            const float *sC = reinterpret_cast<const float *>(st + TE * 48);
-
-            for (int jb = 0; jb < TE; jb += kFold) {
-                float2 are[PH], aim[PH];
-#pragma unroll
-                for (int q = 0; q < PH; ++q) are[q] = aim[q] = f2(0.f, 0.f);
 #pragma unroll(PPT <= 4 ? 4 : 2)
                 for (int j = jb; j < jb + kFold; ++j) {
                     const double4 r = s64[j];
@@ -365,9 +474,9 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
                         float2 arg = __ffma2_rn(u, PI2, NEG_15PI2);
                         float2 amp = a2;
                         if (NF) {
-                            float2 s = __fmul2_rn(dhx[q], f2(A.x, A.x));
-                            s = __ffma2_rn(dhy[q], f2(A.y, A.y), s);
-                            s = __ffma2_rn(dhz[q], f2(A.z, A.z), s);
+                            float2 s = __fmul2_rn(cx[q], f2(A.x, A.x));
+                            s = __ffma2_rn(cy[q], f2(A.y, A.y), s);
+                            s = __ffma2_rn(cz[q], f2(A.z, A.z), s);
                             // -h (s^2 - |r|^2) = h (|r|^2 - s^2)
                             const float2 w2 = __ffma2_rn(s, s, f2(A.w, A.w));
                             arg = __ffma2_rn(hh[q], w2, arg);
@@ -384,56 +493,118 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
                         aim[q] = __ffma2_rn(amp, f2(s0, s1), aim[q]);
                     }
                 }
-                // Kahan fold of the block partials
+            }
+            // Kahan fold of the block partials
 #pragma unroll
-                for (int q = 0; q < PH; ++q) {
+            for (int q = 0; q < PH; ++q) {
 #pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const int i = 2 * q + e;
-                        const float pr = e ? are[q].y : are[q].x;
-                        const float pi = e ? aim[q].y : aim[q].x;
-                        float y = pr - cre[i];
-                        float t = sre[i] + y;
-                        cre[i] = (t - sre[i]) - y;
-                        sre[i] = t;
-                        y = pi - cim[i];
-                        t = sim[i] + y;
-                        cim[i] = (t - sim[i]) - y;
-                        sim[i] = t;
-                    }
+                for (int e = 0; e < 2; ++e) {
+                    const int i = 2 * q + e;
+                    const float pr = e ? are[q].y : are[q].x;
+                    const float pi = e ? aim[q].y : aim[q].x;
+                    float y = pr - cre[i];
+                    float t = sre[i] + y;
+                    cre[i] = (t - sre[i]) - y;
+                    sre[i] = t;
+                    y = pi - cim[i];
+                    t = sim[i] + y;
+                    cim[i] = (t - sim[i]) - y;
+                    sim[i] = t;
                 }
             }
-            ++consumed;
-            __syncthreads();
-            if (s_abort) {
-                aborted = true;
-                break;
-            }
-            if (tid == 0 && it + 2 < nt) {
-                const uint32_t slot2 = issued & 1;
-                unsigned char *st2 = smem + slot2 * stage_bytes;
-                const int64_t r0 = d.rec + (int64_t)(tbeg + it + 2) * TE;
-                mbar_arrive_expect_tx(&bar[slot2], stage_bytes);
-                bulk_g2s(st2, rec.r64 + r0, TE * 32, &bar[slot2]);
-                bulk_g2s(st2 + TE * 32, rec.rA + r0, TE * 16, &bar[slot2]);
-                bulk_g2s(st2 + TE * 48, rec.rC + r0, TE * 4, &bar[slot2]);
-                ++issued;
-            }
         }
-        if (aborted) break;
+        ++consumed;
+        __syncthreads();
+        if (*s_abort) return true;
+        if (tid == 0 && it + 2 < nt) {
+            const uint32_t slot2 = issued & 1;
+            unsigned char *st2 = smem + slot2 * stage_bytes;
+            const int64_t r0 = d.rec + (int64_t)(tbeg + it + 2) * TE;
+            mbar_arrive_expect_tx(&bar[slot2], stage_bytes);
+            bulk_g2s(st2, rec.r64 + r0, TE * 32, &bar[slot2]);
+            bulk_g2s(st2 + TE * 32, rec.rA + r0, TE * 16, &bar[slot2]);
+            bulk_g2s(st2 + TE * 48, rec.rC + r0, TE * 4, &bar[slot2]);
+            ++issued;
+        }
+    }
 
-        const int64_t obase = (int64_t)img * npix;
+    const int64_t obase = (int64_t)img * npix;
 #pragma unroll
-        for (int i = 0; i < PPT; ++i) {
-            const int p = p0 + i;
-            if (p < npix) {
-                const double re = (double)sre[i] - (double)cre[i];
-                const double im = (double)sim[i] - (double)cim[i];
-                if (CHUNKED)
-                    partials[((int64_t)chunk * bp.n_images + img) * npix + p] = make_double2(re, im);
-                else
-                    finish_pixel<NF, SCALE>(g, p, re, im, out, out_kind, obase + p);
-            }
+    for (int i = 0; i < PPT; ++i) {
+        const int p = p0 + i;
+        if (p < npix) {
+            const double re = (double)sre[i] - (double)cre[i];
+            const double im = (double)sim[i] - (double)cim[i];
+            if (CHUNKED)
+                partials[((int64_t)chunk * bp.n_images + img) * npix + p] = make_double2(re, im);
+            else
+                finish_pixel<NF, SCALE>(g, p, re, im, out, out_kind, obase + p);
+        }
+    }
+    return false;
+}
+
+template <int PPT, bool NF, bool SCALE, bool SECOND, bool CHUNKED>
+__global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(const __grid_constant__ BatchParams bp,
+                                                        const GeomParams g, SplitRecs rec,
+                                                        void *__restrict__ out, int out_kind,
+                                                        WsHeader *__restrict__ hdr,
+                                                        uint64_t *__restrict__ cta_ns,
+                                                        double2 *__restrict__ partials) {
+    static_assert(PPT % 2 == 0, "pixels are processed in f32x2 pairs");
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_unit, s_abort;
+
+    const int tid = threadIdx.x;
+    const uint64_t t_start = globaltimer_ns();
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        s_abort = 0;
+        mbar_fence_init();
+        if (blockIdx.x == 0) hdr->n_ctas = gridDim.x;
+    }
+    __syncthreads();
+
+    const int tile_px = blockDim.x * PPT;
+    uint32_t issued = 0, consumed = 0;
+    bool aborted = false;
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_unit = (int)atomicAdd(&hdr->work_counter, 1u);
+        __syncthreads();
+        const int unit = s_unit;
+        if (unit >= bp.total_units) break;
+        const int ks = CHUNKED ? bp.ksplit : 1;
+        const int chunk = unit % ks;
+        const int pu = unit / ks;
+        const int img = bp.order[pu / bp.tiles_per_image];
+        const int ptile = pu % bp.tiles_per_image;
+        const ImageDesc d = bp.img[img];
+        const int p0 = ptile * tile_px + tid * PPT;
+        // emitter tiles of this unit: the whole image, or one chunk of it
+        const int tbeg = CHUNKED ? min(chunk * d.tpc, d.ntiles) : 0;
+        const int tend = CHUNKED ? min(tbeg + d.tpc, d.ntiles) : d.ntiles;
+
+        // pixel runs with a base phase for images whose offsets stay bounded
+        // (|r|_max from the prep kernel; NaN fails the test).  The choice
+        // depends on the image only, so results do not depend on the shape.
+        bool grp = false;
+        if (bp.groups) {
+            const double rmax = sqrt((double)__uint_as_float(rec.rmax2[img]));
+            grp = g.k * g.run_span * rmax <= kGroupMaxPhase;
+        }
+        const bool ab = grp ? split_unit<PPT, NF, SCALE, SECOND, CHUNKED, true>(
+                                  bp, g, rec, out, out_kind, hdr, partials, smem, bar, &s_abort, issued,
+                                  consumed, img, chunk, d, p0, tbeg, tend)
+                            : split_unit<PPT, NF, SCALE, SECOND, CHUNKED, false>(
+                                  bp, g, rec, out, out_kind, hdr, partials, smem, bar, &s_abort, issued,
+                                  consumed, img, chunk, d, p0, tbeg, tend);
+        if (ab) {
+            aborted = true;
+            break;
         }
     }
     if (aborted) {
@@ -620,6 +791,7 @@ __global__ void __launch_bounds__(256) fwd_double_kernel(const __grid_constant__
 
 struct LaunchShape {
     int threads, ppt, te, ctas_per_sm;
+    int groups = 1;  // split: pixel runs with a base phase where bounded
 };
 
 static int sm_count() {
@@ -648,6 +820,14 @@ GeomParams make_geom(const idiwf_geom *g) {
     p.offx = g->offset[0];
     p.offy = g->offset[1];
     for (int i = 0; i < 9; ++i) p.rot[i] = g->has_rot ? g->rot[i] : (i % 4 == 0 ? 1.0 : 0.0);
+    // pixel (px, py) sits at px c0 + py c1 + detz c2 (columns of rot); rows run along c1
+    const double *M = p.rot;
+    const double c0[3] = {M[0], M[3], M[6]}, c1[3] = {M[1], M[4], M[7]}, c2[3] = {M[2], M[5], M[8]};
+    const double n[3] = {c0[1] * c1[2] - c0[2] * c1[1], c0[2] * c1[0] - c0[0] * c1[2], c0[0] * c1[1] - c0[1] * c1[0]};
+    const double nn = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    const double h = nn > 0 ? std::fabs(g->detz * (c2[0] * n[0] + c2[1] * n[1] + c2[2] * n[2])) / nn : 0.0;
+    const double half = 0.5 * (kRun - 1) * std::fabs(g->pixelsize) * std::sqrt(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
+    p.run_span = h > 0 ? half / h : INFINITY;
     return p;
 }
 
@@ -718,6 +898,7 @@ static idiwf_status resolve_shape(const idiwf_geom *g, const idiwf_batch *b, int
         if (cfg->pixels_per_thread) s.ppt = cfg->pixels_per_thread;
         if (cfg->emitters_per_tile) s.te = cfg->emitters_per_tile;
         if (cfg->ctas_per_sm) s.ctas_per_sm = cfg->ctas_per_sm;
+        if (cfg->pixel_groups) s.groups = cfg->pixel_groups > 0;
     }
     if (s.threads != 64 && s.threads != 128 && s.threads != 256)
         return set_error(IDIWF_ERR_INVALID_ARGUMENT, "threads must be 64, 128 or 256");
@@ -861,6 +1042,7 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
     bp.te = s.te;
     if (precision != IDIWF_SPLIT) ksplit = 1;
     bp.ksplit = ksplit;
+    bp.groups = precision == IDIWF_SPLIT && s.groups && geom->ny % kRun == 0;
     bp.total_units = bp.n_images * bp.tiles_per_image * ksplit;
     int max_tiles = 0;
     std::vector<int> ord(bp.n_images);
@@ -884,6 +1066,8 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
                       (size_t)i0 * npix * (out_kind == IDIWF_OUT_C128 ? 16 : (out_kind == IDIWF_OUT_I32 ? 4 : 8));
 
     // prep
+    if (precision == IDIWF_SPLIT)
+        IDIWF_CUDA_CHECK(cudaMemsetAsync(split_recs(ws, nrec).rmax2, 0, sizeof(uint32_t) * bp.n_images, stream));
     if (max_tiles > 0) {
         dim3 pgrid((unsigned)std::min<int64_t>(((int64_t)max_tiles * s.te + 255) / 256, 1024), bp.n_images);
         if (precision == IDIWF_SPLIT) {
@@ -1077,6 +1261,7 @@ extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *ba
         best->pixels_per_thread = best_s.ppt;
         best->emitters_per_tile = best_s.te;
         best->ctas_per_sm = best_s.ctas_per_sm;
+        best->pixel_groups = best_s.groups ? 1 : -1;
     }
     return IDIWF_OK;
 }
@@ -1142,6 +1327,7 @@ extern "C" idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiw
     bp.tiles_per_image = (npix + tile_px - 1) / tile_px;
     bp.te = s.te;
     bp.total_units = bp.n_images * bp.tiles_per_image;
+    bp.groups = geom->ny % kRun == 0;
     int64_t nrec = 0;
     int max_tiles = 0;
     for (int i = 0; i < bp.n_images; ++i) {
@@ -1179,6 +1365,7 @@ extern "C" idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiw
     // every call starts from a zero work counter and error word; the records
     // are rewritten in full by the prep kernel
     IDIWF_CUDA_CHECK(cudaMemsetAsync(ws, 0, 2 * sizeof(uint32_t), stream));
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(rec.rmax2, 0, sizeof(uint32_t) * bp.n_images, stream));
     if (max_tiles > 0) {
         const int w_mode = (geom->flags & IDIWF_NF) ? 1 : ((geom->flags & IDIWF_SECONDORDER) ? 2 : 0);
         const double max_abs = kMaxTurns / (3.0 * 2.0 * geom->k * kInvTwoPi);

@@ -60,6 +60,10 @@ struct GeomParams {
     double pixelsize, detz, k, kp;  // kp = k / 2pi
     double offx, offy;
     double rot[9];
+    // largest |d_hat_i - d_hat_base| between a pixel of a run of 4 along a row
+    // and the run's middle: half the run's length over the detector plane's
+    // distance from the origin (the angle a segment subtends bounds the chord)
+    double run_span;
 };
 
 struct ImageDesc {
@@ -77,7 +81,7 @@ struct BatchParams {
     int32_t te;               // emitters per tile
     int32_t total_units;      // n_images * tiles_per_image * ksplit
     int32_t ksplit;           // emitter chunks per (image, pixel tile); 0 or 1 = none
-    int32_t pad;
+    int32_t groups;           // split forward: phase per pixel run + FP32 offsets where bounded
     ImageDesc img[kMaxImagesPerLaunch];
     uint16_t order[kMaxImagesPerLaunch];  // images by descending emitter count
 };
@@ -155,10 +159,12 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 
 // Detector pixel position, idi/simulation/cpu.py:76-80 rounding sequence
 // (float nx/2, separate multiply and add, numba's contracted mat-vec).
-__device__ __forceinline__ void pixel_cpu(const GeomParams &g, int ix, int iy, double &x,
-                                          double &y, double &z) {
-    const double px = __dadd_rn(__dmul_rn(__dsub_rn((double)ix, g.nx * 0.5), g.pixelsize), g.offx);
-    const double py = __dadd_rn(__dmul_rn(__dsub_rn((double)iy, g.ny * 0.5), g.pixelsize), g.offy);
+// (fractional indices give points between pixel centres, e.g. the centre of a
+// run of pixels)
+__device__ __forceinline__ void pixel_cpu_at(const GeomParams &g, double fix, double fiy, double &x,
+                                             double &y, double &z) {
+    const double px = __dadd_rn(__dmul_rn(__dsub_rn(fix, g.nx * 0.5), g.pixelsize), g.offx);
+    const double py = __dadd_rn(__dmul_rn(__dsub_rn(fiy, g.ny * 0.5), g.pixelsize), g.offy);
     const double pz = g.detz;
     if (g.has_rot) {
         const double *M = g.rot;
@@ -170,6 +176,10 @@ __device__ __forceinline__ void pixel_cpu(const GeomParams &g, int ix, int iy, d
         y = py;
         z = pz;
     }
+}
+__device__ __forceinline__ void pixel_cpu(const GeomParams &g, int ix, int iy, double &x,
+                                          double &y, double &z) {
+    pixel_cpu_at(g, (double)ix, (double)iy, x, y, z);
 }
 
 // Detector pixel position, idi/simulation/time.py:77-81 (meshgrid, dets @ M.T

@@ -195,6 +195,7 @@ def _config(config) -> Optional[nat.Config]:
     c.pixels_per_thread = int(config.get("pixels_per_thread", 0))
     c.emitters_per_tile = int(config.get("emitters_per_tile", 0))
     c.ctas_per_sm = int(config.get("ctas_per_sm", 0))
+    c.pixel_groups = int(config.get("pixel_groups", 0))
     return c
 
 
@@ -264,7 +265,8 @@ def tune(atoms, offsets, geom, precision=nat.SPLIT, out_kind=nat.OUT_I32, amplit
                              ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
                              _stream(atoms.device), ctypes.byref(best)))
     return {"threads": best.threads, "pixels_per_thread": best.pixels_per_thread,
-            "emitters_per_tile": best.emitters_per_tile, "ctas_per_sm": best.ctas_per_sm}
+            "emitters_per_tile": best.emitters_per_tile, "ctas_per_sm": best.ctas_per_sm,
+            "pixel_groups": best.pixel_groups}
 
 
 def cta_times(device=None, role="main") -> np.ndarray:

@@ -85,6 +85,9 @@ typedef struct idiwf_config {
     int32_t pixels_per_thread;  /* split forward: 4 or 8; double forward: 2 */
     int32_t emitters_per_tile;  /* emitters staged per shared-memory tile: 64..512 */
     int32_t ctas_per_sm;        /* persistent grid = SMs * ctas_per_sm */
+    int32_t pixel_groups;       /* split forward: 0 or 1 = one FP64 phase per run of pixels plus
+                                   FP32 offsets wherever the offsets stay below 1 rad (checked per
+                                   work unit on the device), -1 = an FP64 phase for every pixel */
 } idiwf_config;
 
 /* Batch of images with uneven emitter counts.  Image b owns emitter rows

@@ -68,7 +68,7 @@ def test_workspace_size_validates(lib):
     assert lib.idiwf_forward_workspace_size(ctypes.byref(_geom()), ctypes.byref(bad), nat.SPLIT, None) == 0
     # workspace grows with padded emitters
     b2, _keep3 = _batch([0, 100000])
-    assert lib.idiwf_forward_workspace_size(ctypes.byref(_geom()), ctypes.byref(b2), nat.SPLIT, None) > 100000 * 72
+    assert lib.idiwf_forward_workspace_size(ctypes.byref(_geom()), ctypes.byref(b2), nat.SPLIT, None) > 100000 * 52
 
 
 def _fwd(lib, g, b, precision=nat.SPLIT, out_kind=nat.OUT_C128, out=4096, ws=4096, ws_bytes=1 << 20, cfg=None):

@@ -93,7 +93,7 @@ def test_batched_uneven_and_edge_sizes(precision):
     imgs = [atoms(sphere(g0, c, 0.01), g0.uniform(0, 2 * np.pi, c)) for c in counts]
     at = np.concatenate(imgs)
     off = np.concatenate([[0], np.cumsum(counts)])
-    for ndet in ([13, 7], [1, 1], [5, 129]):
+    for ndet in ([13, 7], [1, 1], [5, 129], [9, 12]):
         geom = _core.make_geom(ndet, 75.0, 1e5, K64, flags=nat.NF)
         og = oracle.geometry(ndet, 75.0, 1e5, K64)
         E = _run(at, off, geom, precision)
@@ -138,6 +138,60 @@ def test_kernel_shapes_agree():
     for cfg in ({"threads": 256, "pixels_per_thread": 1, "emitters_per_tile": 64},
                 {"threads": 64, "pixels_per_thread": 4, "emitters_per_tile": 32}):
         assert np.array_equal(_run(at, [0, n], geom, nat.DOUBLE, config=cfg), dbase), cfg
+
+
+@pytest.mark.parametrize("settings", ["", "nf", "nf scale", "scale", "secondorder"])
+def test_pixel_runs_vs_per_pixel_and_oracle(settings):
+    """Split forward with one FP64 base phase per run of 4 pixels plus FP32
+    offsets (the default wherever the image's bound holds) and with an FP64
+    phase per pixel: both against the oracle.  Rotated, offset detector whose
+    rows are a multiple of 4 pixels long; amplitudes."""
+    g0 = rng(17)
+    n = 3000
+    pos = sphere(g0, n, 0.02)  # k * 1.5 px * 75 um / 0.1 m * 0.02 um = 0.73 rad: runs in use
+    ph = g0.uniform(0, 2 * np.pi, n)
+    amp = g0.uniform(0.5, 1.5, n).astype(np.float32)
+    flags, _, _ = _core.parse_settings(settings)
+    geom = _core.make_geom([36, 44], 75.0, 1e5, K64, (0.02, -0.03), (40.0, 10.0), flags)
+    ref = oracle.wavefield(oracle.geometry([36, 44], 75.0, 1e5, K64, (0.02, -0.03), (40.0, 10.0)),
+                           oracle.flags_from_settings(settings), atoms(pos, ph), amp.astype(np.float64))
+    E_run = _run(atoms(pos, ph), [0, n], geom, nat.SPLIT, amps=amp, config={"pixel_groups": 1})[0]
+    E_pix = _run(atoms(pos, ph), [0, n], geom, nat.SPLIT, amps=amp, config={"pixel_groups": -1})[0]
+    assert not np.array_equal(E_run, E_pix)  # the run path was taken
+    for E in (E_run, E_pix):
+        assert rel_field_err(E, ref) < SPLIT_FIELD
+        m = oracle.intensity_metrics(np.abs(E) ** 2, np.abs(ref) ** 2)
+        assert m["max_rel_masked"] < SPLIT_REL_MASKED, m
+
+
+def test_pixel_runs_fall_back_beyond_their_bound():
+    """An object too large for the runs' 1 rad offset bound (and rows that are
+    not a multiple of 4 long) takes the per-pixel path: identical results."""
+    g0 = rng(18)
+    n = 1200
+    at = atoms(sphere(g0, n, 0.05), g0.uniform(0, 2 * np.pi, n))  # bound 1.8 rad
+    geom = _core.make_geom([24, 32], 75.0, 1e5, K64, flags=nat.NF)
+    assert np.array_equal(_run(at, [0, n], geom, nat.SPLIT, config={"pixel_groups": 1}),
+                          _run(at, [0, n], geom, nat.SPLIT, config={"pixel_groups": -1}))
+    at = atoms(sphere(g0, n, 0.01), g0.uniform(0, 2 * np.pi, n))
+    geom = _core.make_geom([24, 30], 75.0, 1e5, K64, flags=nat.NF)
+    assert np.array_equal(_run(at, [0, n], geom, nat.SPLIT, config={"pixel_groups": 1}),
+                          _run(at, [0, n], geom, nat.SPLIT, config={"pixel_groups": -1}))
+
+
+def test_pixel_runs_shapes_agree():
+    """With pixel runs the sums are still the same for every kernel shape: a
+    run's base phase is fixed by the detector, not by the thread layout."""
+    g0 = rng(9)
+    n = 2100
+    at = atoms(sphere(g0, n, 0.012), g0.uniform(0, 2 * np.pi, n))
+    geom = _core.make_geom([37, 28], 75.0, 1e5, K64, flags=nat.NF)
+    base = _run(at, [0, n], geom, nat.SPLIT)
+    assert not np.array_equal(base, _run(at, [0, n], geom, nat.SPLIT, config={"pixel_groups": -1}))
+    for cfg in ({"threads": 128, "pixels_per_thread": 4, "emitters_per_tile": 128},
+                {"threads": 256, "pixels_per_thread": 2, "emitters_per_tile": 512, "ctas_per_sm": 2},
+                {"threads": 64, "pixels_per_thread": 8, "emitters_per_tile": 64}):
+        assert np.array_equal(_run(at, [0, n], geom, nat.SPLIT, config=cfg), base), cfg
 
 
 def test_split_accuracy_against_accurate_fp64():

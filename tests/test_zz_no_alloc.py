@@ -81,7 +81,13 @@ def test_noalloc_intensity_output_and_size_limit():
     assert st == nat.OK
     ref = _core.forward(at, [0, n], geom, nat.SPLIT, nat.OUT_I64)
     torch.cuda.synchronize()
-    assert torch.allclose(I, ref, rtol=1e-6, atol=0)
+    # The regular entry point splits this small detector's work over emitter
+    # chunks and adds the chunk sums in FP64; the allocation-free one sums in
+    # one pass.  The field tolerance above, |dE| <= SPLIT_FIELD * E_rms, bounds
+    # the intensity difference by 2 |E| |dE|.
+    I, ref = I.cpu().numpy(), ref.cpu().numpy()
+    bound = 2 * SPLIT_FIELD * np.sqrt(ref) * np.sqrt(ref.mean())
+    assert np.all(np.abs(I - ref) <= bound), float(np.max(np.abs(I - ref) / bound))
     # beyond the static scratch: rejected on the host with a clear message
     big = torch.zeros((330000, 4), dtype=torch.float64, device="cuda")
     st, _ = _noalloc(lib, geom, big, [0, 330000])
