@@ -51,12 +51,25 @@ constexpr int kBwdMaxPE = 8;                     // largest emitters-per-thread 
 // Values are duplicated in pairs because f32x2 instructions process two
 // emitters of a thread against the same pixel.
 constexpr int kPixRecBytes = 32 + 80 + 16;
+// pixel runs (kRun pixels share one FP64 base phase), in addition:
+//   PD   float4 x2  {Dx,Dx,Dy,Dy} {Dz,Dz,-h,-h}   D = 2 pi (nq_p - nq_base)   32 B per pixel
+//   RB64 double4    {-q'x, -q'y, -q'z, 0} at the run's middle                 32 B per run
+//   RBF  float4 x2  {dbx,dbx,dby,dby} {dbz,dbz,0,0}  d_hat at the run's middle 32 B per run
+// Stage layouts (bytes): per-pixel path P64 | PF | PG; run path PF | PD | PG | RB64 | RBF.
+constexpr uint32_t kStagePixels = kBwdTP * kPixRecBytes;
+constexpr uint32_t kOffRunPF = 0;
+constexpr uint32_t kOffRunPD = kBwdTP * 80;
+constexpr uint32_t kOffRunPG = kOffRunPD + kBwdTP * 32;
+constexpr uint32_t kOffRunB64 = kOffRunPG + kBwdTP * 16;
+constexpr uint32_t kOffRunBF = kOffRunB64 + kBwdTP / kRun * 32;
+constexpr uint32_t kStageRuns = kOffRunBF + kBwdTP / kRun * 32;
+static_assert(kBwdTP % kRun == 0 && kBwdChunk % kRun == 0, "tiles hold whole runs");
 
 struct BwdLayout {
     int npix_pad;          // pixels rounded up to the chunk size
     int n_chunks;
     int64_t nrec;          // emitter records (images padded to the emitter block)
-    size_t off_p64, off_pf, off_pg, off_erec64, off_erecf, off_part, total;
+    size_t off_p64, off_pf, off_pg, off_pd, off_rb64, off_rbf, off_rmax, off_erec64, off_erecf, off_part, total;
 };
 
 static BwdLayout bwd_layout(const idiwf_geom *g, const idiwf_batch *b) {
@@ -75,6 +88,10 @@ static BwdLayout bwd_layout(const idiwf_geom *g, const idiwf_batch *b) {
     L.off_p64 = o; o += align256((size_t)L.npix_pad * 32);
     L.off_pf = o;  o += align256((size_t)L.npix_pad * 80);
     L.off_pg = o;  o += align256((size_t)L.npix_pad * 16 * b->n_images);
+    L.off_pd = o;  o += align256((size_t)L.npix_pad * 32);
+    L.off_rb64 = o; o += align256((size_t)L.npix_pad / kRun * 32);
+    L.off_rbf = o; o += align256((size_t)L.npix_pad / kRun * 32);
+    L.off_rmax = o; o += align256((size_t)kMaxImagesPerLaunch * 4);
     L.off_erec64 = o; o += align256((size_t)L.nrec * 32);
     L.off_erecf = o;  o += align256((size_t)L.nrec * 16);
     L.off_part = o;   o += align256((size_t)L.n_chunks * L.nrec * kBwdNAcc * 4);
@@ -88,8 +105,19 @@ struct BwdImage {
 };
 struct BwdParams {
     int32_t n_images, n_chunks, npix, npix_pad, total_units, eb;
+    int32_t runs, pad;  // runs: pixel runs allowed (rows hold whole runs)
     BwdImage img[kMaxImagesPerLaunch];
     int32_t unit_img[kMaxImagesPerLaunch];   // images by descending emitter count
+};
+
+struct BwdRecs {
+    const double4 *e64;
+    const float4 *ef;
+    const double4 *p64;
+    const float4 *pf, *pg, *pd;
+    const double4 *rb64;
+    const float4 *rbf;
+    const uint32_t *rmax2;  // per image: max |r|^2 (float bits, rounded up)
 };
 
 __device__ __forceinline__ double nf_constant_turns(const GeomParams &g, double dx, double dy, double dz) {
@@ -101,8 +129,9 @@ __device__ __forceinline__ double nf_constant_turns(const GeomParams &g, double 
 }
 
 // ---- pixel prep: geometry (image independent) ------------------------------
-__global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad, double4 *__restrict__ p64,
-                                      float4 *__restrict__ pf) {
+__global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad, int runs,
+                                      double4 *__restrict__ p64, float4 *__restrict__ pf, float4 *__restrict__ pd,
+                                      double4 *__restrict__ rb64, float4 *__restrict__ rbf) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix_pad; p += gridDim.x * blockDim.x) {
         const int pc = min(p, npix - 1);
         const int ix = pc / g.ny, iy = pc - ix * g.ny;
@@ -124,6 +153,24 @@ __global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad
         r[2] = make_float4(qx, qx, qy, qy);
         r[3] = make_float4(qz, qz, kap, kap);
         r[4] = make_float4(fi, fi, fi2, fi2);
+        if (runs) {
+            // the run's middle (rows hold whole runs), and this pixel's offset coefficients
+            const int rs = min(p / kRun * kRun, npix - kRun);
+            const int rix = rs / g.ny;
+            const PixelDir b = pixel_dir(g, (double)rix, (double)(rs - rix * g.ny) + 0.5 * (kRun - 1));
+            const PixelDir q = pixel_dir(g, (double)ix, (double)iy);
+            const float Dx = (float)(kTwoPi * (q.nqx - b.nqx)), Dy = (float)(kTwoPi * (q.nqy - b.nqy)),
+                        Dz = (float)(kTwoPi * (q.nqz - b.nqz));
+            pd[(size_t)p * 2] = make_float4(Dx, Dx, Dy, Dy);
+            pd[(size_t)p * 2 + 1] = make_float4(Dz, Dz, fh, fh);
+            if (p % kRun == 0) {
+                const int run = p / kRun;
+                rb64[run] = make_double4(b.nqx, b.nqy, b.nqz, 0.0);
+                const float ux = (float)b.ux, uy = (float)b.uy, uz = (float)b.uz;
+                rbf[(size_t)run * 2] = make_float4(ux, ux, uy, uy);
+                rbf[(size_t)run * 2 + 1] = make_float4(uz, uz, 0.f, 0.f);
+            }
+        }
     }
 }
 
@@ -163,14 +210,17 @@ __global__ void bwd_pixel_g_kernel(const GeomParams g, const double2 *__restrict
 
 // ---- emitter prep: records padded per image to the emitter block ------------
 __global__ void bwd_emitter_prep_kernel(const __grid_constant__ BwdParams bp, const double *__restrict__ atoms,
-                                        double4 *__restrict__ e64, float4 *__restrict__ ef, int w_mode) {
+                                        double4 *__restrict__ e64, float4 *__restrict__ ef, int w_mode,
+                                        uint32_t *__restrict__ rmax2) {
     const int b = blockIdx.y;
     const BwdImage d = bp.img[b];
     const int64_t nrec = (int64_t)d.nblocks * bp.eb;
+    uint32_t r2max = 0;  // float bits; non-negative floats order like their bits
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nrec; j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t r = d.rec + j;
         if (j < d.n) {
             const double4 a = reinterpret_cast<const double4 *>(atoms)[d.src + j];
+            r2max = max(r2max, __float_as_uint(__double2float_ru((a.x * a.x + a.y * a.y) + a.z * a.z)));
             double psi = a.w * kInvTwoPi;
             psi = psi - rint(psi);
             // magic binade + 1/2 turn (angle = 2pi (u - 1.5)) + 2^-24 turn rounding bias
@@ -184,6 +234,9 @@ __global__ void bwd_emitter_prep_kernel(const __grid_constant__ BwdParams bp, co
             ef[r] = make_float4(0, 0, 0, 0);
         }
     }
+    // |r|_max of the image for the pixel-run bound (zeroed by the caller)
+    r2max = __reduce_max_sync(0xffffffffu, r2max);
+    if ((threadIdx.x & 31) == 0 && r2max) atomicMax(&rmax2[b], r2max);
 }
 
 __device__ __forceinline__ float2 g2(float a, float b) { return make_float2(a, b); }
@@ -198,97 +251,170 @@ __device__ __forceinline__ float2 g2(float a, float b) { return make_float2(a, b
 // -q + kappa P r with P = I - dhat dhat^T ~ diag(1, 1, 0); the neglected part
 // is of relative size theta (the pixel angle) times the correction, which is
 // itself r / (|d| theta) of the main term: below 1e-7 of the gradient.
-template <bool NF, bool SCALE, bool SECOND, int PE>
-__global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
-    const __grid_constant__ BwdParams bp, const double4 *__restrict__ e64, const float4 *__restrict__ ef,
-    const double4 *__restrict__ p64, const float4 *__restrict__ pf, const float4 *__restrict__ pg,
-    float *__restrict__ part, int64_t nrec, WsHeader *__restrict__ hdr) {
+// One work unit (image, emitter block, pixel chunk).  RUNS = false: every
+// emitter-pixel pair forms its phase with its own FP64 DFMA chain.  RUNS =
+// true: one chain per emitter and run of kRun pixels at the run's middle, and
+// the FP32 offset D_p . r per pixel (D_p = 2 pi (nq_p - nq_base); bounded per
+// image by the caller), with s_p = d_hat_p . r = s_base - D_p.r / k for the
+// near-field term.  Returns true when a bounded wait gave up.
+template <bool NF, bool SCALE, bool SECOND, int PE, bool RUNS>
+__device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, float *__restrict__ part,
+                                         int64_t nrec, WsHeader *__restrict__ hdr, unsigned char *smem,
+                                         uint64_t *bar, int *s_abort, uint32_t &issued, uint32_t &consumed,
+                                         int img, int ib, int chunk, float ninvk) {
     constexpr int PH = PE / 2;
-    constexpr uint32_t kStage = kBwdTP * kPixRecBytes;
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bar[2];
-    __shared__ int s_unit, s_abort;
+    constexpr uint32_t kStage = RUNS ? kStageRuns : kStagePixels;
     const int tid = threadIdx.x;
-    if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        s_abort = 0;
-        mbar_fence_init();
-    }
-    __syncthreads();
-    uint32_t issued = 0, consumed = 0;
-    bool aborted = false;
     const float2 TWO_PI2 = g2(6.28318548f, 6.28318548f);
     const float2 NEG_3PI2 = g2(-9.42477796f, -9.42477796f);
+    const float2 NEG_INVK2 = g2(ninvk, ninvk);
     const int eb = kBwdThreads * PE;
+    const BwdImage d = bp.img[img];
+    const int64_t rec0 = d.rec + (int64_t)ib * eb + tid * PE;
 
-    for (;;) {
-        __syncthreads();
-        if (tid == 0) s_unit = (int)atomicAdd(&hdr->work_counter, 1u);
-        __syncthreads();
-        const int unit = s_unit;
-        if (unit >= bp.total_units) break;
-        const int chunk = unit % bp.n_chunks;
-        int ib = unit / bp.n_chunks;
-        int img = 0;
-        for (int k = 0; k < bp.n_images; ++k) {
-            const int b = bp.unit_img[k];
-            if (ib < bp.img[b].nblocks) { img = b; break; }
-            ib -= bp.img[b].nblocks;
-        }
-        const BwdImage d = bp.img[img];
-        const int64_t rec0 = d.rec + (int64_t)ib * eb + tid * PE;
+    double ex[PE], ey[PE], ez[PE], epsi[PE];
+    float2 fx[PH], fy[PH], fz[PH], fw[PH];
+#pragma unroll
+    for (int e = 0; e < PE; ++e) {
+        const double4 r = R.e64[rec0 + e];
+        ex[e] = r.x; ey[e] = r.y; ez[e] = r.z; epsi[e] = r.w;
+        const float4 f = R.ef[rec0 + e];
+        if (e & 1) { fx[e / 2].y = f.x; fy[e / 2].y = f.y; fz[e / 2].y = f.z; fw[e / 2].y = f.w; }
+        else       { fx[e / 2].x = f.x; fy[e / 2].x = f.y; fz[e / 2].x = f.z; fw[e / 2].x = f.w; }
+    }
+    float2 ac[kBwdNAcc][PH];
+#pragma unroll
+    for (int a = 0; a < kBwdNAcc; ++a)
+#pragma unroll
+        for (int q = 0; q < PH; ++q) ac[a][q] = g2(0.f, 0.f);
 
-        double ex[PE], ey[PE], ez[PE], epsi[PE];
-        float2 fx[PH], fy[PH], fz[PH], fw[PH];
-#pragma unroll
-        for (int e = 0; e < PE; ++e) {
-            const double4 r = e64[rec0 + e];
-            ex[e] = r.x; ey[e] = r.y; ez[e] = r.z; epsi[e] = r.w;
-            const float4 f = ef[rec0 + e];
-            if (e & 1) { fx[e / 2].y = f.x; fy[e / 2].y = f.y; fz[e / 2].y = f.z; fw[e / 2].y = f.w; }
-            else       { fx[e / 2].x = f.x; fy[e / 2].x = f.y; fz[e / 2].x = f.z; fw[e / 2].x = f.w; }
+    const int p_begin = chunk * kBwdChunk;
+    constexpr int nt = kBwdChunk / kBwdTP;
+    auto issue = [&](int t) {
+        const uint32_t slot = issued & 1;
+        unsigned char *st = smem + slot * kStage;
+        const int p0 = p_begin + t * kBwdTP;
+        mbar_arrive_expect_tx(&bar[slot], kStage);
+        if (RUNS) {
+            bulk_g2s(st + kOffRunPF, R.pf + (size_t)p0 * 5, kBwdTP * 80, &bar[slot]);
+            bulk_g2s(st + kOffRunPD, R.pd + (size_t)p0 * 2, kBwdTP * 32, &bar[slot]);
+            bulk_g2s(st + kOffRunPG, R.pg + (size_t)img * bp.npix_pad + p0, kBwdTP * 16, &bar[slot]);
+            bulk_g2s(st + kOffRunB64, R.rb64 + p0 / kRun, kBwdTP / kRun * 32, &bar[slot]);
+            bulk_g2s(st + kOffRunBF, R.rbf + (size_t)(p0 / kRun) * 2, kBwdTP / kRun * 32, &bar[slot]);
+        } else {
+            bulk_g2s(st, R.p64 + p0, kBwdTP * 32, &bar[slot]);
+            bulk_g2s(st + kBwdTP * 32, R.pf + (size_t)p0 * 5, kBwdTP * 80, &bar[slot]);
+            bulk_g2s(st + kBwdTP * 112, R.pg + (size_t)img * bp.npix_pad + p0, kBwdTP * 16, &bar[slot]);
         }
-        float2 ac[kBwdNAcc][PH];
-#pragma unroll
-        for (int a = 0; a < kBwdNAcc; ++a)
-#pragma unroll
-            for (int q = 0; q < PH; ++q) ac[a][q] = g2(0.f, 0.f);
-
-        const int p_begin = chunk * kBwdChunk;
-        constexpr int nt = kBwdChunk / kBwdTP;
-        auto issue = [&](int t) {
-            const uint32_t slot = issued & 1;
-            unsigned char *st = smem + slot * kStage;
-            const int p0 = p_begin + t * kBwdTP;
-            mbar_arrive_expect_tx(&bar[slot], kStage);
-            bulk_g2s(st, p64 + p0, kBwdTP * 32, &bar[slot]);
-            bulk_g2s(st + kBwdTP * 32, pf + (size_t)p0 * 5, kBwdTP * 80, &bar[slot]);
-            bulk_g2s(st + kBwdTP * 112, pg + (size_t)img * bp.npix_pad + p0, kBwdTP * 16, &bar[slot]);
-            ++issued;
-        };
-        if (tid == 0) {
-            issue(0);
-            issue(1);
+        ++issued;
+    };
+    if (tid == 0) {
+        issue(0);
+        issue(1);
+    }
+    for (int it = 0; it < nt; ++it) {
+        const uint32_t slot = consumed & 1;
+        if (!mbar_wait_bounded(&bar[slot], (consumed >> 1) & 1)) {
+            record_error(&hdr->error, kErrTimeout);
+            *s_abort = 1;
         }
-        for (int it = 0; it < nt; ++it) {
-            const uint32_t slot = consumed & 1;
-            if (!mbar_wait_bounded(&bar[slot], (consumed >> 1) & 1)) {
-                record_error(&hdr->error, kErrTimeout);
-                s_abort = 1;
+        const unsigned char *st = smem + slot * kStage;
+        // one emitter pair q against pixel j: the sincos, z and the accumulators
+        auto accumulate = [&](int q, float2 arg, float2 s, const float4 &F2, const float4 &F3, const float4 &GG,
+                              const float4 *sf, int j) {
+            float s0, c0, s1, c1;
+            __sincosf(arg.x, &s0, &c0);
+            __sincosf(arg.y, &s1, &c1);
+            const float2 cc = g2(c0, c1), ss = g2(s0, s1);
+            // z = G' e^{i phi'}: Im z = Gr s + Gi c, Re z = Gr c - Gi s
+            float2 zi = __fmul2_rn(g2(GG.x, GG.y), ss);
+            zi = __ffma2_rn(g2(GG.z, GG.w), cc, zi);
+            if (SCALE) {
+                const float4 F4 = sf[5 * j + 4];  // iD iD iD2 iD2
+                const float2 w = NF ? __ffma2_rn(s, g2(F4.z, F4.w), g2(F4.x, F4.y)) : g2(F4.x, F4.y);
+                float2 zr = __fmul2_rn(g2(GG.x, GG.y), cc);
+                zr = __ffma2_rn(g2(-GG.z, -GG.w), ss, zr);
+                zi = __fmul2_rn(zi, w);
+                ac[0][q] = __ffma2_rn(zr, w, ac[0][q]);
+            } else {
+                ac[0][q] = __ffma2_rn(g2(GG.x, GG.y), cc, ac[0][q]);
+                ac[0][q] = __ffma2_rn(g2(-GG.z, -GG.w), ss, ac[0][q]);
             }
-            const unsigned char *st = smem + slot * kStage;
+            ac[1][q] = __fadd2_rn(ac[1][q], zi);
+            ac[2][q] = __ffma2_rn(zi, g2(F2.x, F2.y), ac[2][q]);
+            ac[3][q] = __ffma2_rn(zi, g2(F2.z, F2.w), ac[3][q]);
+            ac[4][q] = __ffma2_rn(zi, g2(F3.x, F3.y), ac[4][q]);
+            if (NF || SECOND) ac[5][q] = __ffma2_rn(zi, g2(F3.z, F3.w), ac[5][q]);
+        };
+        if (RUNS) {
+            const float4 *sf = reinterpret_cast<const float4 *>(st + kOffRunPF);
+            const float4 *sd = reinterpret_cast<const float4 *>(st + kOffRunPD);
+            const float4 *sg = reinterpret_cast<const float4 *>(st + kOffRunPG);
+            const double4 *sb64 = reinterpret_cast<const double4 *>(st + kOffRunB64);
+            const float4 *sbf = reinterpret_cast<const float4 *>(st + kOffRunBF);
+#pragma unroll 1
+            for (int rr = 0; rr < kBwdTP / kRun; ++rr) {
+                const double4 B = sb64[rr];
+                float2 XB2[PH], SB2[PH];
+#pragma unroll
+                for (int q = 0; q < PH; ++q) {
+                    uint32_t lo[2];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int i = 2 * q + e;
+                        double t = __fma_rn(B.x, ex[i], epsi[i]);
+                        t = __fma_rn(B.y, ey[i], t);
+                        t = __fma_rn(B.z, ez[i], t);
+                        lo[e] = (uint32_t)__double2loint(t);
+                    }
+                    const float2 u = g2(__uint_as_float((lo[0] >> 9) | 0x3F800000u),
+                                        __uint_as_float((lo[1] >> 9) | 0x3F800000u));
+                    XB2[q] = __ffma2_rn(u, TWO_PI2, NEG_3PI2);
+                    SB2[q] = g2(0.f, 0.f);
+                    if (NF) {
+                        const float4 B0 = sbf[2 * rr], B1 = sbf[2 * rr + 1];  // dbx dbx dby dby | dbz dbz
+                        float2 sb = __fmul2_rn(g2(B0.x, B0.y), fx[q]);
+                        sb = __ffma2_rn(g2(B0.z, B0.w), fy[q], sb);
+                        SB2[q] = __ffma2_rn(g2(B1.x, B1.y), fz[q], sb);
+                    }
+                }
+#pragma unroll 2
+                for (int jj = 0; jj < kRun; ++jj) {
+                    const int j = rr * kRun + jj;
+                    const float4 D0 = sd[2 * j + 0];  // Dx Dx Dy Dy
+                    const float4 D1 = sd[2 * j + 1];  // Dz Dz -h -h
+                    const float4 F2 = sf[5 * j + 2];  // qx qx qy qy
+                    const float4 F3 = sf[5 * j + 3];  // qz qz kap kap
+                    const float4 GG = sg[j];          // G'r G'r G'i G'i
+#pragma unroll
+                    for (int q = 0; q < PH; ++q) {
+                        float2 dl = __fmul2_rn(g2(D0.x, D0.y), fx[q]);
+                        dl = __ffma2_rn(g2(D0.z, D0.w), fy[q], dl);
+                        dl = __ffma2_rn(g2(D1.x, D1.y), fz[q], dl);
+                        float2 s = g2(0.f, 0.f);
+                        if (NF) {
+                            s = __ffma2_rn(dl, NEG_INVK2, SB2[q]);
+                            const float2 w2 = __ffma2_rn(s, s, fw[q]);  // s^2 - |r|^2
+                            dl = __ffma2_rn(g2(D1.z, D1.w), w2, dl);
+                        } else if (SECOND) {
+                            dl = __ffma2_rn(g2(D1.z, D1.w), fw[q], dl);
+                        }
+                        accumulate(q, __fadd2_rn(XB2[q], dl), s, F2, F3, GG, sf, j);
+                    }
+                }
+            }
+        } else {
             const double4 *s64 = reinterpret_cast<const double4 *>(st);
             const float4 *sf = reinterpret_cast<const float4 *>(st + kBwdTP * 32);
             const float4 *sg = reinterpret_cast<const float4 *>(st + kBwdTP * 112);
 #pragma unroll 2
             for (int j = 0; j < kBwdTP; ++j) {
                 const double4 P = s64[j];
-                const float4 F0 = sf[5 * j + 0];   // dx dx dy dy
-                const float4 F1 = sf[5 * j + 1];   // dz dz h h
-                const float4 F2 = sf[5 * j + 2];   // qx qx qy qy
-                const float4 F3 = sf[5 * j + 3];   // qz qz kap kap
-                const float4 GG = sg[j];           // G'r G'r G'i G'i
+                const float4 F0 = sf[5 * j + 0];  // dx dx dy dy
+                const float4 F1 = sf[5 * j + 1];  // dz dz h h
+                const float4 F2 = sf[5 * j + 2];  // qx qx qy qy
+                const float4 F3 = sf[5 * j + 3];  // qz qz kap kap
+                const float4 GG = sg[j];          // G'r G'r G'i G'i
 #pragma unroll
                 for (int q = 0; q < PH; ++q) {
                     uint32_t lo[2];
@@ -313,49 +439,73 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(
                     } else if (SECOND) {
                         arg = __ffma2_rn(g2(F1.z, F1.w), fw[q], arg);
                     }
-                    float s0, c0, s1, c1;
-                    __sincosf(arg.x, &s0, &c0);
-                    __sincosf(arg.y, &s1, &c1);
-                    const float2 cc = g2(c0, c1), ss = g2(s0, s1);
-                    // z = G' e^{i phi'}: Im z = Gr s + Gi c, Re z = Gr c - Gi s
-                    float2 zi = __fmul2_rn(g2(GG.x, GG.y), ss);
-                    zi = __ffma2_rn(g2(GG.z, GG.w), cc, zi);
-                    if (SCALE) {
-                        const float4 F4 = sf[5 * j + 4];  // iD iD iD2 iD2
-                        const float2 w = NF ? __ffma2_rn(s, g2(F4.z, F4.w), g2(F4.x, F4.y)) : g2(F4.x, F4.y);
-                        float2 zr = __fmul2_rn(g2(GG.x, GG.y), cc);
-                        zr = __ffma2_rn(g2(-GG.z, -GG.w), ss, zr);
-                        zi = __fmul2_rn(zi, w);
-                        ac[0][q] = __ffma2_rn(zr, w, ac[0][q]);
-                    } else {
-                        ac[0][q] = __ffma2_rn(g2(GG.x, GG.y), cc, ac[0][q]);
-                        ac[0][q] = __ffma2_rn(g2(-GG.z, -GG.w), ss, ac[0][q]);
-                    }
-                    ac[1][q] = __fadd2_rn(ac[1][q], zi);
-                    ac[2][q] = __ffma2_rn(zi, g2(F2.x, F2.y), ac[2][q]);
-                    ac[3][q] = __ffma2_rn(zi, g2(F2.z, F2.w), ac[3][q]);
-                    ac[4][q] = __ffma2_rn(zi, g2(F3.x, F3.y), ac[4][q]);
-                    if (NF || SECOND) ac[5][q] = __ffma2_rn(zi, g2(F3.z, F3.w), ac[5][q]);
+                    accumulate(q, arg, s, F2, F3, GG, sf, j);
                 }
             }
-            ++consumed;
-            __syncthreads();
-            if (s_abort) {
-                aborted = true;
-                break;
-            }
-            if (tid == 0 && it + 2 < nt) issue(it + 2);
         }
-        if (aborted) break;
-        // partials: part[chunk][rec][acc]
-        float *dst = part + ((size_t)chunk * nrec + rec0) * kBwdNAcc;
+        ++consumed;
+        __syncthreads();
+        if (*s_abort) return true;
+        if (tid == 0 && it + 2 < nt) issue(it + 2);
+    }
+    // partials: part[chunk][rec][acc]
+    float *dst = part + ((size_t)chunk * nrec + rec0) * kBwdNAcc;
 #pragma unroll
-        for (int q = 0; q < PH; ++q)
+    for (int q = 0; q < PH; ++q)
 #pragma unroll
-            for (int a = 0; a < kBwdNAcc; ++a) {
-                dst[(2 * q) * kBwdNAcc + a] = ac[a][q].x;
-                dst[(2 * q + 1) * kBwdNAcc + a] = ac[a][q].y;
-            }
+        for (int a = 0; a < kBwdNAcc; ++a) {
+            dst[(2 * q) * kBwdNAcc + a] = ac[a][q].x;
+            dst[(2 * q + 1) * kBwdNAcc + a] = ac[a][q].y;
+        }
+    return false;
+}
+
+template <bool NF, bool SCALE, bool SECOND, int PE>
+__global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(const __grid_constant__ BwdParams bp,
+                                                                const BwdRecs R, float *__restrict__ part,
+                                                                int64_t nrec, WsHeader *__restrict__ hdr,
+                                                                GeomParams g) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_unit, s_abort;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        s_abort = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+    uint32_t issued = 0, consumed = 0;
+    bool aborted = false;
+    const float ninvk = (float)(-1.0 / g.k);
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_unit = (int)atomicAdd(&hdr->work_counter, 1u);
+        __syncthreads();
+        const int unit = s_unit;
+        if (unit >= bp.total_units) break;
+        const int chunk = unit % bp.n_chunks;
+        int ib = unit / bp.n_chunks;
+        int img = 0;
+        for (int k = 0; k < bp.n_images; ++k) {
+            const int b = bp.unit_img[k];
+            if (ib < bp.img[b].nblocks) { img = b; break; }
+            ib -= bp.img[b].nblocks;
+        }
+        // pixel runs for images whose offsets stay bounded (|r|_max from the
+        // emitter prep; NaN fails the test); the choice depends on the image only
+        bool runs = false;
+        if (bp.runs) runs = g.k * g.run_span * sqrt((double)__uint_as_float(R.rmax2[img])) <= kGroupMaxPhase;
+        const bool ab = runs ? bwd_unit<NF, SCALE, SECOND, PE, true>(bp, R, part, nrec, hdr, smem, bar, &s_abort,
+                                                                     issued, consumed, img, ib, chunk, ninvk)
+                             : bwd_unit<NF, SCALE, SECOND, PE, false>(bp, R, part, nrec, hdr, smem, bar, &s_abort,
+                                                                      issued, consumed, img, ib, chunk, ninvk);
+        if (ab) {
+            aborted = true;
+            break;
+        }
     }
     if (aborted && tid == 0)
         while (consumed < issued) {
@@ -457,6 +607,10 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
     double4 *e64 = reinterpret_cast<double4 *>(ws + L.off_erec64);
     float4 *ef = reinterpret_cast<float4 *>(ws + L.off_erecf);
     float *part = reinterpret_cast<float *>(ws + L.off_part);
+    float4 *pd = reinterpret_cast<float4 *>(ws + L.off_pd);
+    double4 *rb64 = reinterpret_cast<double4 *>(ws + L.off_rb64);
+    float4 *rbf = reinterpret_cast<float4 *>(ws + L.off_rbf);
+    uint32_t *rmax2 = reinterpret_cast<uint32_t *>(ws + L.off_rmax);
 
     const GeomParams g = make_geom(geom);
     const int npix = geom->nx * geom->ny;
@@ -473,6 +627,8 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
     bp.npix = npix;
     bp.npix_pad = L.npix_pad;
     bp.eb = eb;
+    // pixel runs unless switched off (pixel_groups = -1) or rows do not hold whole runs
+    bp.runs = !(cfg && cfg->pixel_groups < 0) && geom->ny % kRun == 0;
     int64_t rec = 0;
     int total_blocks = 0, max_blocks = 0;
     std::vector<int> ord(batch->n_images);
@@ -492,7 +648,8 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
     bp.total_units = total_blocks * L.n_chunks;
 
     const int pthreads = 256;
-    bwd_pixel_geom_kernel<<<(L.npix_pad + pthreads - 1) / pthreads, pthreads, 0, stream>>>(g, npix, L.npix_pad, p64, pf);
+    bwd_pixel_geom_kernel<<<(L.npix_pad + pthreads - 1) / pthreads, pthreads, 0, stream>>>(
+        g, npix, L.npix_pad, bp.runs, p64, pf, pd, rb64, rbf);
     IDIWF_CUDA_CHECK(cudaGetLastError());
     {
         const int64_t tot = (int64_t)L.npix_pad * batch->n_images;
@@ -510,12 +667,13 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
     {
         const int w_mode = nf ? 1 : (so ? 2 : 0);
         dim3 grid((unsigned)std::max(1, (max_blocks * eb + 255) / 256), batch->n_images);
-        bwd_emitter_prep_kernel<<<grid, 256, 0, stream>>>(bp, batch->atoms, e64, ef, w_mode);
+        IDIWF_CUDA_CHECK(cudaMemsetAsync(rmax2, 0, sizeof(uint32_t) * batch->n_images, stream));
+        bwd_emitter_prep_kernel<<<grid, 256, 0, stream>>>(bp, batch->atoms, e64, ef, w_mode, rmax2);
         IDIWF_CUDA_CHECK(cudaGetLastError());
     }
     IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 2 * sizeof(uint32_t), stream));  // counter + error word
     void *fn = pe == 8 ? bwd_kernel_for<8>(nf, sc, so) : bwd_kernel_for<4>(nf, sc, so);
-    const size_t smem = 2 * (size_t)kBwdTP * kPixRecBytes;
+    const size_t smem = 2 * (size_t)std::max(kStagePixels, kStageRuns);
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev = 0, sms = 148, occ = 1;
     cudaGetDevice(&dev);
@@ -523,7 +681,8 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
     IDIWF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBwdThreads, smem));
     const int grid = (int)std::min<int64_t>(bp.total_units, (int64_t)sms * std::max(occ, 1));
     int64_t nrec = L.nrec;
-    void *args[] = {&bp, &e64, &ef, &p64, &pf, &pg, &part, &nrec, &hdr};
+    BwdRecs R{e64, ef, p64, pf, pg, pd, rb64, rbf, rmax2};
+    void *args[] = {&bp, &R, &part, &nrec, &hdr, (void *)&g};
     IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(kBwdThreads), args, smem, stream));
     {
         dim3 rgrid((unsigned)std::max<int64_t>(1, (max_blocks * eb + 255) / 256), batch->n_images);

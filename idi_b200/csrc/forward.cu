@@ -235,13 +235,6 @@ __global__ void fwd_finish_kernel(const GeomParams g, const double2 *__restrict_
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
-// Pixel runs of the split kernel: aligned blocks of kRun pixels along a
-// detector row share one FP64 base phase, taken at the middle of the run.
-constexpr int kRun = 4;
-// Largest phase offset (radians) that a run adds in FP32 to its base phase,
-// bounded per image by k * run_span * |r|_max.  Up to 1 rad the FP32 offset is
-// good to about 1e-7 rad and the sine/cosine arguments stay inside [-pi, pi].
-constexpr double kGroupMaxPhase = 1.0;
 // Constants of a run's base angle with the 8 low fixed-point bits, in units
 // of pi_f = FP32 pi as in the per-pixel path: C is -pi_f (1.5 + 2^-8 + 2^-24)
 // rounded to FP32 and S = pi_f 2^-8 minus C's rounding error, so that C + S
@@ -250,30 +243,6 @@ constexpr double kPiF = (double)3.14159274f;
 constexpr double kRunBaseCExact = -kPiF * (1.5 + 1.0 / 256.0 + 1.0 / 16777216.0);
 constexpr float kRunBaseC = (float)kRunBaseCExact;
 constexpr float kRunBaseS = (float)(kPiF / 256.0 - ((double)kRunBaseC - kRunBaseCExact));
-
-// Direction of a detector point for the split kernel: the FP64 turn
-// coefficients nq = -k (d_hat - z_hat) / 2pi (z part without cancellation),
-// d_hat and 1/|d|.
-struct PixelDir {
-    double nqx, nqy, nqz, ux, uy, uz, invD;
-};
-__device__ __forceinline__ PixelDir pixel_dir(const GeomParams &g, double fix, double fiy) {
-    double dx, dy, dz;
-    pixel_cpu_at(g, fix, fiy, dx, dy, dz);
-    const double rho2 = dx * dx + dy * dy;
-    const double D = sqrt(rho2 + dz * dz);
-    const double invD = 1.0 / D;
-    const double dzm1 = dz > 0 ? -rho2 / (D * (D + dz)) : dz * invD - 1.0;
-    PixelDir p;
-    p.ux = dx * invD;
-    p.uy = dy * invD;
-    p.uz = dz * invD;
-    p.nqx = -g.kp * p.ux;
-    p.nqy = -g.kp * p.uy;
-    p.nqz = -g.kp * dzm1;
-    p.invD = invD;
-    return p;
-}
 
 // Base point of run b of the thread whose first pixel is p0: the middle of
 // the aligned run (rows hold a whole number of runs when runs are in use).

@@ -55,6 +55,15 @@ inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 // Maximum images per launch (descriptors travel as kernel parameters).
 constexpr int kMaxImagesPerLaunch = 512;
 
+// Pixel runs of the split kernels: aligned blocks of kRun pixels along a
+// detector row share one FP64 base phase, taken at the middle of the run.
+constexpr int kRun = 4;
+// Largest phase offset (radians) that a run adds in FP32 to its base phase,
+// bounded per image by k * run_span * |r|_max.  Up to 1 rad the FP32 offset is
+// good to about 1e-7 rad and the sine/cosine arguments stay within 1 rad of
+// the base angle's range.
+constexpr double kGroupMaxPhase = 1.0;
+
 struct GeomParams {
     int32_t nx, ny, flags, has_rot;
     double pixelsize, detz, k, kp;  // kp = k / 2pi
@@ -180,6 +189,30 @@ __device__ __forceinline__ void pixel_cpu_at(const GeomParams &g, double fix, do
 __device__ __forceinline__ void pixel_cpu(const GeomParams &g, int ix, int iy, double &x,
                                           double &y, double &z) {
     pixel_cpu_at(g, (double)ix, (double)iy, x, y, z);
+}
+
+// Direction of a detector point for the split kernels: the FP64 turn
+// coefficients nq = -k (d_hat - z_hat) / 2pi (z part without cancellation),
+// d_hat and 1/|d|.
+struct PixelDir {
+    double nqx, nqy, nqz, ux, uy, uz, invD;
+};
+__device__ __forceinline__ PixelDir pixel_dir(const GeomParams &g, double fix, double fiy) {
+    double dx, dy, dz;
+    pixel_cpu_at(g, fix, fiy, dx, dy, dz);
+    const double rho2 = dx * dx + dy * dy;
+    const double D = sqrt(rho2 + dz * dz);
+    const double invD = 1.0 / D;
+    const double dzm1 = dz > 0 ? -rho2 / (D * (D + dz)) : dz * invD - 1.0;
+    PixelDir p;
+    p.ux = dx * invD;
+    p.uy = dy * invD;
+    p.uz = dz * invD;
+    p.nqx = -g.kp * p.ux;
+    p.nqy = -g.kp * p.uy;
+    p.nqz = -g.kp * dzm1;
+    p.invD = invD;
+    return p;
 }
 
 // Detector pixel position, idi/simulation/time.py:77-81 (meshgrid, dets @ M.T

@@ -296,8 +296,11 @@ def backward(
     grad_intensity: torch.Tensor,
     amplitudes: Optional[torch.Tensor] = None,
     want_amp: bool = True,
+    config=None,
 ):
-    """Adjoint of I = |E|^2: returns (grad_atoms (N,4) [dx,dy,dz,dphase], grad_amp (N) or None)."""
+    """Adjoint of I = |E|^2: returns (grad_atoms (N,4) [dx,dy,dz,dphase], grad_amp (N) or None).
+    ``config``: ``pixels_per_thread`` = emitters per thread (4 or 8), ``pixel_groups`` = -1 for an
+    FP64 phase per pair instead of per run of 4 pixels."""
     lib = nat.load()
     _require_cuda(atoms, "atoms", torch.float64)
     _require_cuda(field, "field", torch.complex128)
@@ -311,14 +314,16 @@ def backward(
     dev = atoms.device
     grad_atoms = torch.empty((atoms.shape[0], 4), dtype=torch.float64, device=dev)
     grad_amp = torch.empty((atoms.shape[0],), dtype=torch.float64, device=dev) if want_amp else None
-    nbytes = lib.idiwf_backward_workspace_size(ctypes.byref(geom), ctypes.byref(batch), None)
+    cfg = _config(config)
+    cfg_p = ctypes.byref(cfg) if cfg is not None else None
+    nbytes = lib.idiwf_backward_workspace_size(ctypes.byref(geom), ctypes.byref(batch), cfg_p)
     if nbytes == 0:
         nat.check(nat.ERR_INVALID_ARGUMENT)
     ws = WORKSPACES.get(nbytes, dev, "backward")
     nat.check(lib.idiwf_backward(ctypes.byref(geom), ctypes.byref(batch), ctypes.c_void_p(field.data_ptr()),
                                  ctypes.c_void_p(grad_intensity.data_ptr()), ctypes.c_void_p(grad_atoms.data_ptr()),
                                  ctypes.c_void_p(grad_amp.data_ptr()) if grad_amp is not None else None,
-                                 ctypes.c_void_p(ws.data_ptr()), ws.numel(), None, _stream(dev)))
+                                 ctypes.c_void_p(ws.data_ptr()), ws.numel(), cfg_p, _stream(dev)))
     return grad_atoms, grad_amp
 
 

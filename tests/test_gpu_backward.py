@@ -51,6 +51,40 @@ def test_adjoint_matches_oracle(settings):
     assert _norm_err(gamp, gamp_o) < 1e-4
 
 
+@pytest.mark.parametrize("settings", ["nf", "", "secondorder", "nf scale"])
+def test_adjoint_pixel_runs_vs_per_pair_and_oracle(settings):
+    """The adjoint with one FP64 base phase per emitter and run of 4 pixels
+    (the default where the image's bound holds: here 0.78 rad) and with an
+    FP64 phase per pair, both against the oracle adjoint."""
+    g0 = rng(43)
+    n = 700
+    pos = sphere(g0, n, 0.008)
+    ph = g0.uniform(0, 2 * np.pi, n)
+    amp = g0.uniform(0.5, 1.5, n)
+    ndet, ps, dz, ang, off = [48, 40], 200.0, 1e5, (0.03, 0.01), (500.0, -300.0)
+    flags, _, _ = _core.parse_settings(settings)
+    geom = _core.make_geom(ndet, ps, dz, K64, ang, off, flags)
+    og = oracle.geometry(ndet, ps, dz, K64, ang, off)
+    of = oracle.flags_from_settings(settings)
+    target = np.abs(oracle.wavefield(og, of, atoms(pos + g0.normal(0, 5e-5, pos.shape), ph), amp)) ** 2
+    at = atoms(pos, ph)
+    E = _core.forward(_gpu(at), [0, n], geom, nat.SPLIT, nat.OUT_C128, amplitudes=_gpu(amp))
+    I = (E.real ** 2 + E.imag ** 2)
+    gI = (2 * (I - _gpu(target)[None])).contiguous()
+    E_o = oracle.wavefield(og, of, at, amp)
+    _, gpos_o, gpsi_o, gamp_o = oracle.adjoint(og, of, at, amp, E_o, target)
+    res = []
+    for cfg in ({"pixel_groups": 1}, {"pixel_groups": -1}):
+        ga, gamp = _core.backward(_gpu(at), [0, n], geom, E, gI, amplitudes=_gpu(amp), config=cfg)
+        torch.cuda.synchronize()
+        ga, gamp = ga.cpu().numpy(), gamp.cpu().numpy()
+        assert _norm_err(ga[:, :3], gpos_o) < 1e-4, cfg
+        assert _norm_err(ga[:, 3], gpsi_o) < 1e-4, cfg
+        assert _norm_err(gamp, gamp_o) < 1e-4, cfg
+        res.append(ga)
+    assert not np.array_equal(res[0], res[1])  # the run path was taken
+
+
 def _torch_intensity_nf(pos, phase, det, k):
     """Plain torch FP64 near-field intensity (the expression of cpu.py:44-55)."""
     d = det[:, None, :] - pos[None, :, :]
