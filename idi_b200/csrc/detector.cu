@@ -3,9 +3,11 @@
 // idi/simulation/common.py:26-67).
 //
 //  * photon_sum_kernel / photon_sample_kernel — per-image FP64 sum of the
-//    probabilities in a fixed reduction tree, then one Poisson draw per pixel
-//    from the pixel's own Philox4x64-10 stream.  HBM-bound: 2 reads of the
-//    probabilities and one write of the counts per pixel.
+//    probabilities in a fixed reduction tree, then one Poisson draw per pixel:
+//    below rate 10 by inversion of a uniform from the Philox4x64-10 block of
+//    the pixel's quad (4 pixels per block), above it by PTRS from the pixel's
+//    own stream.  2 reads of the probabilities and one write of the counts per
+//    pixel.
 //  * cs_seg_kernel / cs_seg_scan_kernel / cs_start_kernel — exclusive scan of
 //    the photon counts (injected positions only: photon g's row in the
 //    caller's arrays).
@@ -29,23 +31,34 @@ namespace idiwf {
 constexpr double kPtrsMinRate = 10.0;
 constexpr int kMaxRejections = 1000;  // acceptance is above 0.88 per trial
 
-// Returns -1 when the rejection loop ran out (never in practice).
-__device__ double poisson_draw(double lam, PhiloxStream &st) {
-    if (!(lam > 0.0)) return 0.0;
-    if (lam < kPtrsMinRate) {
-        // inversion: smallest k with F(k) >= u, F accumulated term by term
-        const double u = st.uniform();
-        double p = exp(-lam), F = p;
-        double k = 0.0;
-        while (u > F) {
-            k += 1.0;
-            p = p * lam / k;
-            const double Fn = F + p;
-            if (Fn == F) break;  // the tail no longer changes F: u is in the last ulp
-            F = Fn;
-        }
-        return k;
+// Counter word 0 of the blocks that hold the inversion uniforms of pixel
+// quads: block (kQuadCounter, p / 4, image, stream) gives pixel p its uniform
+// in word p % 4.  Per-pixel streams count word 0 up from 1 and never reach it.
+constexpr uint64_t kQuadCounter = 0x8000000000000000ull;
+
+// Inversion for 0 < lam < kPtrsMinRate: smallest k with F(k) >= u, F
+// accumulated term by term in FP64.  k = 0 (u <= exp(-lam)) is settled by an
+// FP32 exponential when u is clear of exp(-lam) by a relative 2^-16, far
+// above its error (< 2e-6 for |lam| < 10); otherwise the FP64 comparison
+// decides, so the result is that of the FP64 loop alone.
+__device__ __forceinline__ double poisson_invert(double lam, double u) {
+    const double e32 = (double)__expf(-(float)lam);
+    if (u < e32 * (1.0 - 0x1p-16)) return 0.0;
+    double p = exp(-lam), F = p;
+    double k = 0.0;
+    while (u > F) {
+        k += 1.0;
+        p = p * lam / k;
+        const double Fn = F + p;
+        if (Fn == F) break;  // the tail no longer changes F: u is in the last ulp
+        F = Fn;
     }
+    return k;
+}
+
+// lam >= kPtrsMinRate, from the pixel's own stream.
+// Returns -1 when the rejection loop ran out (never in practice).
+__device__ double poisson_ptrs(double lam, PhiloxStream &st) {
     // PTRS, Hoermann (1993): transformed rejection with squeeze
     const double slam = sqrt(lam), loglam = log(lam);
     const double b = 0.931 + 2.53 * slam;
@@ -119,7 +132,14 @@ __global__ void __launch_bounds__(kSumThreads) photon_sum_kernel(const T *__rest
     if (threadIdx.x == 0) partials[(int64_t)b * nblk + blockIdx.x] = v[0];
 }
 
-template <typename TI, typename TO>
+// Pixel p below rate kPtrsMinRate inverts word p % 4 of the Philox block
+// (kQuadCounter, p / 4, image, stream); a pixel at a higher rate draws its
+// PTRS trials from its own stream (p, image, stream).  QUAD: one thread per
+// quad of 4 consecutive pixels, so one block serves four inversions (images
+// of low mean rate); otherwise one thread per pixel, and the rare inversion
+// pixel computes its quad's block itself (high mean rate: the PTRS loops then
+// spread over all threads).  Both give the same counts.
+template <typename TI, typename TO, bool QUAD>
 __global__ void __launch_bounds__(kSumThreads) photon_sample_kernel(const TI *__restrict__ probs, int64_t npix,
                                                                     int nblk, const double *__restrict__ partials,
                                                                     double n_photons, uint64_t k0, uint64_t k1,
@@ -134,21 +154,77 @@ __global__ void __launch_bounds__(kSumThreads) photon_sample_kernel(const TI *__
     const double scale = n_photons / total;
     const TI *img = probs + (int64_t)b * npix;
     TO *o = out + (int64_t)b * npix;
+    const uint64_t ib = img0 + (uint64_t)b;
     bool bad = false;
-    for (int64_t p = (int64_t)blockIdx.x * kSumThreads + threadIdx.x; p < npix; p += (int64_t)gridDim.x * kSumThreads) {
-        const double lam = load_real(img, p) * scale;
-        double k = 0.0;
-        if (lam >= 0.0 && lam < 0x1p62) {
-            PhiloxStream st((uint64_t)p, img0 + (uint64_t)b, stream, k0, k1);
-            k = poisson_draw(lam, st);
-            if (k < 0.0) {
+    if (!QUAD) {
+        for (int64_t p = (int64_t)blockIdx.x * kSumThreads + threadIdx.x; p < npix;
+             p += (int64_t)gridDim.x * kSumThreads) {
+            const double l = load_real(img, p) * scale;
+            double k = 0.0;
+            if (l > 0.0 && l < kPtrsMinRate) {
+                uint64_t w0, w1, w2, w3;
+                philox4x64(kQuadCounter, (uint64_t)(p >> 2), ib, stream, k0, k1, w0, w1, w2, w3);
+                const int i = (int)(p & 3);
+                k = poisson_invert(l, u01(i == 0 ? w0 : (i == 1 ? w1 : (i == 2 ? w2 : w3))));
+            } else if (l >= kPtrsMinRate && l < 0x1p62) {
+                PhiloxStream st((uint64_t)p, ib, stream, k0, k1);
+                k = poisson_ptrs(l, st);
+                if (k < 0.0) {
+                    bad = true;
+                    k = 0.0;
+                }
+            } else if (!(l == 0.0)) {
                 bad = true;
-                k = 0.0;
             }
-        } else if (!(lam == 0.0)) {
-            bad = true;
+            store_count(o, p, k);
         }
-        store_count(o, p, k);
+        if (bad) record_error(err, kErrValue);
+        return;
+    }
+    const int64_t nquad = (npix + 3) / 4;
+    for (int64_t q = (int64_t)blockIdx.x * kSumThreads + threadIdx.x; q < nquad; q += (int64_t)gridDim.x * kSumThreads) {
+        const int64_t p0 = 4 * q;
+        const int np = (int)(npix - p0 < 4 ? npix - p0 : 4);
+        double lam[4];
+        bool need = false;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            lam[i] = i < np ? load_real(img, p0 + i) * scale : 0.0;
+            need |= lam[i] > 0.0 && lam[i] < kPtrsMinRate;
+        }
+        uint64_t w[4] = {0, 0, 0, 0};
+        if (need) philox4x64(kQuadCounter, (uint64_t)q, ib, stream, k0, k1, w[0], w[1], w[2], w[3]);
+        double k[4];
+        bool ptrs = false;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const double l = lam[i];
+            k[i] = 0.0;
+            if (l > 0.0 && l < kPtrsMinRate) k[i] = poisson_invert(l, u01(w[i]));
+            ptrs |= l >= kPtrsMinRate && l < 0x1p62;
+            bad |= i < np && !(l >= 0.0 && l < 0x1p62);
+        }
+        if (ptrs) {
+            // one copy of the rejection loop (its log/lgamma calls are long)
+#pragma unroll 1
+            for (int i = 0; i < np; ++i) {
+                const double l = i == 0 ? lam[0] : (i == 1 ? lam[1] : (i == 2 ? lam[2] : lam[3]));
+                if (!(l >= kPtrsMinRate && l < 0x1p62)) continue;
+                PhiloxStream st((uint64_t)(p0 + i), ib, stream, k0, k1);
+                double kk = poisson_ptrs(l, st);
+                if (kk < 0.0) {
+                    bad = true;
+                    kk = 0.0;
+                }
+                if (i == 0) k[0] = kk;
+                else if (i == 1) k[1] = kk;
+                else if (i == 2) k[2] = kk;
+                else k[3] = kk;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (i < np) store_count(o, p0 + i, k[i]);
     }
     if (bad) record_error(err, kErrValue);
 }
@@ -533,11 +609,15 @@ static idiwf_status launch_photons(const void *probs, int32_t n_images, int64_t 
     photon_sum_kernel<TI><<<dim3(nblk, n_images), kSumThreads, 0, stream>>>(static_cast<const TI *>(probs), npix,
                                                                             nblk, partials, &hdr->error);
     IDIWF_CUDA_CHECK(cudaGetLastError());
-    const int64_t want = (npix + kSumThreads - 1) / kSumThreads;
+    // mean rate below 1: one thread per pixel quad (one Philox block per four
+    // inversions); above: one thread per pixel (the PTRS loops dominate)
+    const bool quad = n_photons < (double)npix;
+    const int64_t want = ((quad ? (npix + 3) / 4 : npix) + kSumThreads - 1) / kSumThreads;
     const int gx = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)8 * dev_sms() / std::max(1, n_images) + 1));
-    photon_sample_kernel<TI, TO><<<dim3(gx, n_images), kSumThreads, 0, stream>>>(
-        static_cast<const TI *>(probs), npix, nblk, partials, n_photons, rng->key[0], rng->key[1], rng->stream,
-        rng->first_image, static_cast<TO *>(out), &hdr->error);
+    auto fn = quad ? photon_sample_kernel<TI, TO, true> : photon_sample_kernel<TI, TO, false>;
+    fn<<<dim3(gx, n_images), kSumThreads, 0, stream>>>(static_cast<const TI *>(probs), npix, nblk, partials, n_photons,
+                                                       rng->key[0], rng->key[1], rng->stream, rng->first_image,
+                                                       static_cast<TO *>(out), &hdr->error);
     IDIWF_CUDA_CHECK(cudaGetLastError());
     return IDIWF_OK;
 }

@@ -10,8 +10,9 @@
  *    numpy.random.Philox's raw output by the CPU tests.
  *  - orc_photons: per-image sum in the same fixed reduction tree as the
  *    device kernel, rate = p * (n / sum) as common.py:17, and one Poisson
- *    draw per pixel from the pixel's stream (inversion below rate 10, PTRS of
- *    W. Hoermann 1993 above).
+ *    draw per pixel: below rate 10 inversion of word p % 4 of the Philox
+ *    block (2^63, p / 4, image, stream); above it PTRS (W. Hoermann 1993)
+ *    from the pixel's stream (p, image, stream).
  *  - orc_chargesharing: the reference's scatter loop (common.py:49-67) --
  *    per photon, in the reference's photon order, the (2w+1)^2 kernel
  *    k[x, y] = (1/4 f_x[x]) f_y[y] added at (hit_x + y - w, hit_y + x - w) --
@@ -35,20 +36,21 @@ void orc_uniforms(uint64_t c1, uint64_t c2, uint64_t c3, uint64_t k0, uint64_t k
     for (int64_t i = 0; i < n; ++i) out[i] = stream_uniform(&s);
 }
 
-static double poisson_draw(double lam, stream_t *st) {
-    if (!(lam > 0.0)) return 0.0;
-    if (lam < 10.0) {
-        const double u = stream_uniform(st);
-        double p = exp(-lam), F = p, k = 0.0;
-        while (u > F) {
-            k += 1.0;
-            p = p * lam / k;
-            const double Fn = F + p;
-            if (Fn == F) break;
-            F = Fn;
-        }
-        return k;
+/* Inversion for 0 < lam < 10 with the uniform u of the pixel's quad block. */
+static double poisson_invert(double lam, double u) {
+    double p = exp(-lam), F = p, k = 0.0;
+    while (u > F) {
+        k += 1.0;
+        p = p * lam / k;
+        const double Fn = F + p;
+        if (Fn == F) break;
+        F = Fn;
     }
+    return k;
+}
+
+/* PTRS (Hoermann 1993) for lam >= 10 from the pixel's own stream. */
+static double poisson_ptrs(double lam, stream_t *st) {
     const double slam = sqrt(lam), loglam = log(lam);
     const double b = 0.931 + 2.53 * slam;
     const double a = -0.059 + 0.02483 * b;
@@ -106,9 +108,20 @@ void orc_photons(const double *probs, int32_t n_images, int64_t npix, double n_p
         for (int64_t p = 0; p < npix; ++p) {
             const double lam = img[p] * scale;
             if (rates) rates[(int64_t)b * npix + p] = lam;
-            stream_t st;
-            stream_init(&st, (uint64_t)p, first_image + (uint64_t)b, stream, k0, k1);
-            counts[(int64_t)b * npix + p] = (lam >= 0.0 && lam < 0x1p62) ? poisson_draw(lam, &st) : 0.0;
+            double k = 0.0;
+            if (lam > 0.0 && lam < 10.0) {
+                /* block (2^63, p / 4, image, stream), word p % 4 */
+                const uint64_t ctr[4] = {0x8000000000000000ull, (uint64_t)p / 4, first_image + (uint64_t)b, stream};
+                const uint64_t key[2] = {k0, k1};
+                uint64_t w[4];
+                philox4x64(ctr, key, w);
+                k = poisson_invert(lam, u01(w[p % 4]));
+            } else if (lam >= 10.0 && lam < 0x1p62) {
+                stream_t st;
+                stream_init(&st, (uint64_t)p, first_image + (uint64_t)b, stream, k0, k1);
+                k = poisson_ptrs(lam, &st);
+            }
+            counts[(int64_t)b * npix + p] = k;
         }
     }
 }

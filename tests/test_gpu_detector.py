@@ -48,6 +48,22 @@ def test_photons_large_batch_bit_exact_and_chunk_invariant():
     np.testing.assert_array_equal(whole, again)
 
 
+def test_photons_quad_and_pixel_threads_vs_oracle():
+    """A mean rate below 1 takes the kernel with one thread per pixel quad,
+    above 1 the one with one thread per pixel; both against the oracle on
+    images mixing inversion and PTRS pixels, with pixel counts that are not
+    multiples of 4."""
+    g = np.random.default_rng(12)
+    probs = g.exponential(1.0, (3, 101, 67))
+    probs[:, ::13, ::7] *= 400.0  # hot pixels: rates above 10 at either mean
+    key = (5, 6)
+    for n in (0.4 * probs[0].size, 30.0 * probs[0].size):
+        gpu = _core.photons(_dev(probs), n, key, 2).cpu().numpy()
+        orc, rates = oracle.photons(probs, n, key, 2, return_rates=True)
+        assert (rates < 10).any() and (rates >= 10).any()
+        np.testing.assert_array_equal(gpu, orc)
+
+
 @pytest.mark.parametrize("dtype", [torch.float32, torch.int32, torch.int64] +
                          ([torch.uint32] if hasattr(torch, "uint32") else []))
 def test_photons_out_dtypes(dtype):
