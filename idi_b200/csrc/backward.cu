@@ -497,7 +497,10 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(const __grid_con
         // pixel runs for images whose offsets stay bounded (|r|_max from the
         // emitter prep; NaN fails the test); the choice depends on the image only
         bool runs = false;
-        if (bp.runs) runs = g.k * g.run_span * sqrt((double)__uint_as_float(R.rmax2[img])) <= kGroupMaxPhase;
+        if (bp.runs) {  // compared squared: no square-root call in the persistent loop
+            const double ks = g.k * g.run_span;
+            runs = ks * ks * (double)__uint_as_float(R.rmax2[img]) <= kGroupMaxPhase * kGroupMaxPhase;
+        }
         const bool ab = runs ? bwd_unit<NF, SCALE, SECOND, PE, true>(bp, R, part, nrec, hdr, smem, bar, &s_abort,
                                                                      issued, consumed, img, ib, chunk, ninvk)
                              : bwd_unit<NF, SCALE, SECOND, PE, false>(bp, R, part, nrec, hdr, smem, bar, &s_abort,

@@ -268,7 +268,8 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
                                            void *__restrict__ out, int out_kind, WsHeader *__restrict__ hdr,
                                            double2 *__restrict__ partials, unsigned char *smem, uint64_t *bar,
                                            int *s_abort, uint32_t &issued, uint32_t &consumed, int img,
-                                           int chunk, const ImageDesc &d, int p0, int tbeg, int tend) {
+                                           int chunk, const ImageDesc &d, int p0, int tbeg, int tend,
+                                           float *__restrict__ kahan) {
     constexpr int PH = PPT / 2;
     constexpr int NB = PPT >= kRun ? PPT / kRun : 1;  // runs (base phases) per thread
     constexpr int NQ = GROUP ? NB : PPT;
@@ -329,9 +330,20 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
     const float ninvk = (float)(-1.0 / g.k);
     const float2 NEG_INVK2 = f2(ninvk, ninvk);
 
-    float sre[PPT], cre[PPT], sim[PPT], cim[PPT];
+    // Kahan-compensated totals per pixel (sum, compensation; re, im).  The run
+    // kernel keeps them in shared memory, [4 PPT][threads] (touched once per
+    // kFold emitters), to leave its registers to the emitter loop.
+    float sre[GROUP ? 1 : PPT], cre[GROUP ? 1 : PPT], sim[GROUP ? 1 : PPT], cim[GROUP ? 1 : PPT];
+    const int nthr = blockDim.x;
 #pragma unroll
-    for (int i = 0; i < PPT; ++i) sre[i] = cre[i] = sim[i] = cim[i] = 0.0f;
+    for (int i = 0; i < PPT; ++i) {
+        if (GROUP) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) kahan[(c * PPT + i) * nthr + tid] = 0.0f;
+        } else {
+            sre[i] = cre[i] = sim[i] = cim[i] = 0.0f;
+        }
+    }
 
     const int nt = tend - tbeg;
     if (tid == 0) {
@@ -471,14 +483,28 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
                     const int i = 2 * q + e;
                     const float pr = e ? are[q].y : are[q].x;
                     const float pi = e ? aim[q].y : aim[q].x;
-                    float y = pr - cre[i];
-                    float t = sre[i] + y;
-                    cre[i] = (t - sre[i]) - y;
-                    sre[i] = t;
-                    y = pi - cim[i];
-                    t = sim[i] + y;
-                    cim[i] = (t - sim[i]) - y;
-                    sim[i] = t;
+                    if (GROUP) {
+                        float *k0 = kahan + (0 * PPT + i) * nthr + tid, *k1 = kahan + (1 * PPT + i) * nthr + tid;
+                        float *k2 = kahan + (2 * PPT + i) * nthr + tid, *k3 = kahan + (3 * PPT + i) * nthr + tid;
+                        const float s0 = *k0, c0 = *k1, s1 = *k2, c1 = *k3;
+                        float y = pr - c0;
+                        float t = s0 + y;
+                        *k1 = (t - s0) - y;
+                        *k0 = t;
+                        y = pi - c1;
+                        t = s1 + y;
+                        *k3 = (t - s1) - y;
+                        *k2 = t;
+                    } else {
+                        float y = pr - cre[i];
+                        float t = sre[i] + y;
+                        cre[i] = (t - sre[i]) - y;
+                        sre[i] = t;
+                        y = pi - cim[i];
+                        t = sim[i] + y;
+                        cim[i] = (t - sim[i]) - y;
+                        sim[i] = t;
+                    }
                 }
             }
         }
@@ -502,8 +528,14 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
     for (int i = 0; i < PPT; ++i) {
         const int p = p0 + i;
         if (p < npix) {
-            const double re = (double)sre[i] - (double)cre[i];
-            const double im = (double)sim[i] - (double)cim[i];
+            double re, im;
+            if (GROUP) {
+                re = (double)kahan[(0 * PPT + i) * nthr + tid] - (double)kahan[(1 * PPT + i) * nthr + tid];
+                im = (double)kahan[(2 * PPT + i) * nthr + tid] - (double)kahan[(3 * PPT + i) * nthr + tid];
+            } else {
+                re = (double)sre[i] - (double)cre[i];
+                im = (double)sim[i] - (double)cim[i];
+            }
             if (CHUNKED)
                 partials[((int64_t)chunk * bp.n_images + img) * npix + p] = make_double2(re, im);
             else
@@ -513,19 +545,39 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
     return false;
 }
 
-template <int PPT, bool NF, bool SCALE, bool SECOND, bool CHUNKED>
-__global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(const __grid_constant__ BatchParams bp,
-                                                        const GeomParams g, SplitRecs rec,
-                                                        void *__restrict__ out, int out_kind,
-                                                        WsHeader *__restrict__ hdr,
-                                                        uint64_t *__restrict__ cta_ns,
-                                                        double2 *__restrict__ partials) {
+// Whether image img of the launch takes the pixel-run path: runs allowed and
+// k * run_span * |r|_max <= kGroupMaxPhase (|r|_max from the prep kernel; NaN
+// fails the test).  Depends on the image only, so results do not depend on
+// the kernel shape.
+// (compared squared: a square root here would put a library call into the
+// persistent loop, which costs the run kernel 5 % of its speed)
+__device__ __forceinline__ bool image_uses_runs(const BatchParams &bp, const GeomParams &g, const SplitRecs &rec,
+                                                int img) {
+    const double ks = g.k * g.run_span;
+    return bp.groups && ks * ks * (double)__uint_as_float(rec.rmax2[img]) <= kGroupMaxPhase * kGroupMaxPhase;
+}
+
+// The split forward is two kernels launched back to back: GROUP = true takes
+// the images on the pixel-run path, GROUP = false the others, each from its
+// own work counter.  Without the per-pixel path's registers the run kernel
+// fits three 256-thread CTAs per SM (two for the per-pixel kernel).  A kernel
+// whose path no image of the launch takes returns at once.
+template <int PPT, bool NF, bool SCALE, bool SECOND, bool CHUNKED, bool GROUP>
+__global__ void __launch_bounds__(256, (PPT <= 4 ? (GROUP ? 3 : 2) : 1))
+    fwd_split_kernel(const __grid_constant__ BatchParams bp, const GeomParams g, SplitRecs rec,
+                     void *__restrict__ out, int out_kind, WsHeader *__restrict__ hdr,
+                     uint64_t *__restrict__ cta_ns, double2 *__restrict__ partials) {
     static_assert(PPT % 2 == 0, "pixels are processed in f32x2 pairs");
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int s_unit, s_abort;
 
     const int tid = threadIdx.x;
+    bool mine = false;
+    for (int i = tid; i < bp.n_images; i += blockDim.x) mine |= image_uses_runs(bp, g, rec, i) == GROUP;
+    if (!__syncthreads_or(mine)) return;
+    uint32_t *counter = GROUP ? &hdr->work_counter : &hdr->work_counter2;
+
     const uint64_t t_start = globaltimer_ns();
     if (tid == 0) {
         mbar_init(&bar[0], 1);
@@ -540,13 +592,23 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
     uint32_t issued = 0, consumed = 0;
     bool aborted = false;
 
+    const int ks = CHUNKED ? bp.ksplit : 1;
     for (;;) {
         __syncthreads();
-        if (tid == 0) s_unit = (int)atomicAdd(&hdr->work_counter, 1u);
+        if (tid == 0) {
+            // next unit of this kernel's path (units of the other kernel are
+            // skipped here, out of the CTA's control flow)
+            int u;
+            for (;;) {
+                u = (int)atomicAdd(counter, 1u);
+                if (u >= bp.total_units || image_uses_runs(bp, g, rec, bp.order[u / ks / bp.tiles_per_image]) == GROUP)
+                    break;
+            }
+            s_unit = u;
+        }
         __syncthreads();
         const int unit = s_unit;
         if (unit >= bp.total_units) break;
-        const int ks = CHUNKED ? bp.ksplit : 1;
         const int chunk = unit % ks;
         const int pu = unit / ks;
         const int img = bp.order[pu / bp.tiles_per_image];
@@ -556,22 +618,9 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? 2 : 1)) fwd_split_kernel(cons
         // emitter tiles of this unit: the whole image, or one chunk of it
         const int tbeg = CHUNKED ? min(chunk * d.tpc, d.ntiles) : 0;
         const int tend = CHUNKED ? min(tbeg + d.tpc, d.ntiles) : d.ntiles;
-
-        // pixel runs with a base phase for images whose offsets stay bounded
-        // (|r|_max from the prep kernel; NaN fails the test).  The choice
-        // depends on the image only, so results do not depend on the shape.
-        bool grp = false;
-        if (bp.groups) {
-            const double rmax = sqrt((double)__uint_as_float(rec.rmax2[img]));
-            grp = g.k * g.run_span * rmax <= kGroupMaxPhase;
-        }
-        const bool ab = grp ? split_unit<PPT, NF, SCALE, SECOND, CHUNKED, true>(
-                                  bp, g, rec, out, out_kind, hdr, partials, smem, bar, &s_abort, issued,
-                                  consumed, img, chunk, d, p0, tbeg, tend)
-                            : split_unit<PPT, NF, SCALE, SECOND, CHUNKED, false>(
-                                  bp, g, rec, out, out_kind, hdr, partials, smem, bar, &s_abort, issued,
-                                  consumed, img, chunk, d, p0, tbeg, tend);
-        if (ab) {
+        if (split_unit<PPT, NF, SCALE, SECOND, CHUNKED, GROUP>(
+                bp, g, rec, out, out_kind, hdr, partials, smem, bar, &s_abort, issued, consumed, img, chunk, d, p0,
+                tbeg, tend, reinterpret_cast<float *>(smem + 2 * (size_t)bp.te * kSplitRecBytes))) {
             aborted = true;
             break;
         }
@@ -924,19 +973,29 @@ static size_t forward_ws_bytes(const idiwf_geom *g, const idiwf_batch *b, int pr
     return kWsDataOffset + split_recs_bytes(nrec) + partials_bytes(g, b, choose_ksplit(g, b));
 }
 
-// kernel table ---------------------------------------------------------------
-template <int PPT, bool CH>
-static void *split_kernel_for2(int flags) {
-    const bool nf = flags & IDIWF_NF, sc = flags & IDIWF_SCALE, so = flags & IDIWF_SECONDORDER;
-    if (nf) return sc ? (void *)fwd_split_kernel<PPT, true, true, false, CH>
-                      : (void *)fwd_split_kernel<PPT, true, false, false, CH>;
-    if (so) return sc ? (void *)fwd_split_kernel<PPT, false, true, true, CH>
-                      : (void *)fwd_split_kernel<PPT, false, false, true, CH>;
-    return sc ? (void *)fwd_split_kernel<PPT, false, true, false, CH> : (void *)fwd_split_kernel<PPT, false, false, false, CH>;
+// Dynamic shared memory of a forward kernel: two stages of emitter records,
+// plus for the pixel-run kernel the Kahan totals (4 floats per pixel of the CTA).
+static size_t fwd_smem(int precision, const LaunchShape &s, bool group) {
+    if (precision != IDIWF_SPLIT) return 2 * (size_t)s.te * kDoubleRecBytes;
+    return 2 * (size_t)s.te * kSplitRecBytes + (group ? (size_t)16 * s.ppt * s.threads : 0);
 }
+
+// kernel table ---------------------------------------------------------------
+template <int PPT, bool CH, bool GR>
+static void *split_kernel_for3(int flags) {
+    const bool nf = flags & IDIWF_NF, sc = flags & IDIWF_SCALE, so = flags & IDIWF_SECONDORDER;
+    if (nf) return sc ? (void *)fwd_split_kernel<PPT, true, true, false, CH, GR>
+                      : (void *)fwd_split_kernel<PPT, true, false, false, CH, GR>;
+    if (so) return sc ? (void *)fwd_split_kernel<PPT, false, true, true, CH, GR>
+                      : (void *)fwd_split_kernel<PPT, false, false, true, CH, GR>;
+    return sc ? (void *)fwd_split_kernel<PPT, false, true, false, CH, GR>
+              : (void *)fwd_split_kernel<PPT, false, false, false, CH, GR>;
+}
+// group: the pixel-run kernel (true) or the per-pixel kernel (false)
 template <int PPT>
-static void *split_kernel_for(int flags, bool chunked = false) {
-    return chunked ? split_kernel_for2<PPT, true>(flags) : split_kernel_for2<PPT, false>(flags);
+static void *split_kernel_for(int flags, bool chunked, bool group) {
+    if (chunked) return group ? split_kernel_for3<PPT, true, true>(flags) : split_kernel_for3<PPT, true, false>(flags);
+    return group ? split_kernel_for3<PPT, false, true>(flags) : split_kernel_for3<PPT, false, false>(flags);
 }
 template <int PPT>
 static void *double_kernel_for(int flags) {
@@ -948,11 +1007,11 @@ static void *double_kernel_for(int flags) {
     if (so) return sc ? (void *)fwd_double_kernel<PPT, false, true, true> : (void *)fwd_double_kernel<PPT, false, false, true>;
     return sc ? (void *)fwd_double_kernel<PPT, false, true, false> : (void *)fwd_double_kernel<PPT, false, false, false>;
 }
-static void *kernel_for(int precision, int ppt, int flags, bool chunked) {
+static void *kernel_for(int precision, int ppt, int flags, bool chunked, bool group = true) {
     if (precision == IDIWF_SPLIT) {
-        if (ppt == 2) return split_kernel_for<2>(flags, chunked);
-        if (ppt == 4) return split_kernel_for<4>(flags, chunked);
-        return split_kernel_for<8>(flags, chunked);
+        if (ppt == 2) return split_kernel_for<2>(flags, chunked, group);
+        if (ppt == 4) return split_kernel_for<4>(flags, chunked, group);
+        return split_kernel_for<8>(flags, chunked, group);
     }
     if (ppt == 1) return double_kernel_for<1>(flags);
     if (ppt == 2) return double_kernel_for<2>(flags);
@@ -1053,19 +1112,31 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
     }
     IDIWF_CUDA_CHECK(cudaMemsetAsync(&hdr->work_counter, 0, sizeof(uint32_t), stream));
 
-    void *fn = kernel_for(precision, s.ppt, geom->flags, ksplit > 1);
-    const size_t smem = 2 * (size_t)s.te * (precision == IDIWF_SPLIT ? kSplitRecBytes : kDoubleRecBytes);
-    idiwf_status st = ensure_smem(fn, smem);
-    if (st != IDIWF_OK) return st;
-    const int per_sm = std::min(s.ctas_per_sm, resident_ctas(fn, s.threads, smem));
-    const int grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * per_sm), kMaxCtas);
+    auto grid_for = [&](void *fn, size_t smem, int &grid) -> idiwf_status {
+        idiwf_status st = ensure_smem(fn, smem);
+        if (st != IDIWF_OK) return st;
+        const int per_sm = std::min(s.ctas_per_sm, resident_ctas(fn, s.threads, smem));
+        grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * per_sm), kMaxCtas);
+        return IDIWF_OK;
+    };
     if (precision == IDIWF_SPLIT) {
         SplitRecs rec = split_recs(ws, nrec);
         double2 *partials = ksplit > 1 ? reinterpret_cast<double2 *>(static_cast<char *>(ws) + kWsDataOffset +
                                                                      split_recs_bytes(nrec))
                                        : nullptr;
         void *args[] = {&bp, (void *)&g, &rec, &out_chunk, &out_kind, &hdr, &cta_ns, &partials};
-        IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
+        // the pixel-run kernel, then the per-pixel kernel for the images beyond
+        // the runs' bound (each returns at once when it has no image)
+        IDIWF_CUDA_CHECK(cudaMemsetAsync(&hdr->work_counter2, 0, sizeof(uint32_t), stream));
+        for (const bool group : {true, false}) {
+            if (group && !bp.groups) continue;
+            void *fn = kernel_for(precision, s.ppt, geom->flags, ksplit > 1, group);
+            const size_t smem = fwd_smem(precision, s, group);
+            int grid = 0;
+            idiwf_status st = grid_for(fn, smem, grid);
+            if (st != IDIWF_OK) return st;
+            IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
+        }
         if (ksplit > 1) {
             const int64_t total = (int64_t)bp.n_images * npix;
             const int blocks = (int)std::min<int64_t>((total + 255) / 256, 8 * (int64_t)sm_count());
@@ -1084,6 +1155,11 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
     } else {
         DoubleRecs rec = double_recs(ws, nrec);
         void *args[] = {&bp, (void *)&g, &rec, &out_chunk, &out_kind, &hdr, &cta_ns};
+        void *fn = kernel_for(precision, s.ppt, geom->flags, false);
+        const size_t smem = fwd_smem(precision, s, false);
+        int grid = 0;
+        idiwf_status st = grid_for(fn, smem, grid);
+        if (st != IDIWF_OK) return st;
         IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
     }
     return IDIWF_OK;
@@ -1195,7 +1271,7 @@ extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *ba
         if (forward_ws_bytes(geom, batch, precision, s) > workspace_bytes) continue;
         {  // more CTAs per SM than fit would only repeat a smaller candidate
             void *fn = kernel_for(precision, s.ppt, geom->flags, false);
-            const size_t smem = 2 * (size_t)s.te * (precision == IDIWF_SPLIT ? kSplitRecBytes : kDoubleRecBytes);
+            const size_t smem = fwd_smem(precision, s, true);
             if (ensure_smem(fn, smem) == IDIWF_OK && s.ctas_per_sm > resident_ctas(fn, s.threads, smem)) continue;
         }
         st = forward_impl(geom, batch, precision, out_kind, out, workspace, workspace_bytes, s, stream);
@@ -1333,7 +1409,7 @@ extern "C" idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiw
 
     // every call starts from a zero work counter and error word; the records
     // are rewritten in full by the prep kernel
-    IDIWF_CUDA_CHECK(cudaMemsetAsync(ws, 0, 2 * sizeof(uint32_t), stream));
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(ws, 0, 4 * sizeof(uint32_t), stream));  // both work counters, error word
     IDIWF_CUDA_CHECK(cudaMemsetAsync(rec.rmax2, 0, sizeof(uint32_t) * bp.n_images, stream));
     if (max_tiles > 0) {
         const int w_mode = (geom->flags & IDIWF_NF) ? 1 : ((geom->flags & IDIWF_SECONDORDER) ? 2 : 0);
@@ -1343,13 +1419,17 @@ extern "C" idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiw
                                                      max_abs, rec, &hdr->error);
         IDIWF_CUDA_CHECK(cudaGetLastError());
     }
-    void *fn = split_kernel_for<4>(geom->flags);
-    const size_t smem = 2 * (size_t)s.te * kSplitRecBytes;
-    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * s.ctas_per_sm),
                                             kMaxCtas);
     double2 *no_partials = nullptr;  // bp.ksplit == 0: the kernel writes the outputs itself
     void *args[] = {&bp, (void *)&g, &rec, &out, &out_kind, &hdr, &cta_ns, &no_partials};
-    IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
+    // the pixel-run kernel, then the per-pixel kernel (each returns at once without images)
+    for (const bool group : {true, false}) {
+        if (group && !bp.groups) continue;
+        void *fn = split_kernel_for<4>(geom->flags, false, group);
+        const size_t smem = fwd_smem(IDIWF_SPLIT, s, group);
+        IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
+    }
     return IDIWF_OK;
 }

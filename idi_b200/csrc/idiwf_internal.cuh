@@ -39,7 +39,7 @@ struct WsHeader {
     uint32_t work_counter;  // persistent-kernel work queue
     uint32_t error;         // device error word (IDIWF_ERR_* bit set)
     uint32_t n_ctas;        // CTAs of the last forward launch
-    uint32_t pad0;
+    uint32_t work_counter2; // second work queue (split forward: per-pixel kernel)
     uint64_t pad[30];
 };
 static_assert(sizeof(WsHeader) == 256, "workspace header is 256 bytes");
