@@ -899,7 +899,7 @@ static int n_bucket(const idiwf_batch *b) {
 }
 
 static LaunchShape default_shape(int precision) {
-    if (precision == IDIWF_SPLIT) return LaunchShape{256, 8, 256, 1};
+    if (precision == IDIWF_SPLIT) return LaunchShape{256, 4, 512, 3};
     return LaunchShape{128, 2, 128, 2};
 }
 
@@ -1248,13 +1248,19 @@ extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *ba
         return set_error(IDIWF_ERR_INVALID_ARGUMENT, "precision must be IDIWF_SPLIT or IDIWF_DOUBLE");
     std::vector<LaunchShape> cands;
     if (precision == IDIWF_SPLIT) {
+        // CTAs per SM: as many as fit.  The persistent queue balances any grid,
+        // and a small tuning batch would favour fewer CTAs only through its
+        // own last-wave tail.
         for (int th : {128, 256})
             for (int ppt : {2, 4, 8})
-                for (int te : {256, 512})
-                    for (int c : {1, 2, 3, 4}) {
-                        if (ppt == 8 && c > 2) continue;
-                        cands.push_back(LaunchShape{th, ppt, te, c});
-                    }
+                for (int te : {256, 512}) {
+                    LaunchShape c{th, ppt, te, 1};
+                    void *fn = kernel_for(precision, ppt, geom->flags, false);
+                    const size_t smem = fwd_smem(precision, c, true);
+                    if (ensure_smem(fn, smem) != IDIWF_OK) continue;
+                    c.ctas_per_sm = std::min(8, resident_ctas(fn, th, smem));
+                    cands.push_back(c);
+                }
     } else {
         for (int th : {128, 256})
             for (int ppt : {1, 2})
