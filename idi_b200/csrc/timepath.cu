@@ -506,8 +506,15 @@ __host__ __device__ __forceinline__ int large_buckets(int64_t n) {
     return nb;
 }
 
+// A CTA's slice: keys (8 B per emitter), the sorted records (16 B) and two
+// index arrays for the radix fallback (4 B each).
+struct SortRec {
+    double key;
+    int idx;
+    int pad;
+};
 __host__ __device__ __forceinline__ size_t large_slice_bytes(int64_t n) {
-    return ((size_t)n * 16 + 255) & ~(size_t)255;
+    return ((size_t)n * 32 + 255) & ~(size_t)255;
 }
 
 // The two-level map of bucket_sort with nb fine buckets (nb >= 8192 here).
@@ -515,11 +522,14 @@ __device__ __forceinline__ uint32_t fine_bucket_n(double t, double kmin, double 
     return fine_bucket(t, kmin, scale, coarse);
 }
 
-__device__ bool bucket_sort_large(const double *keys, int *perm, uint32_t *cnt, uint32_t *coarse, int n, int nb,
+// Sorted (key, emitter) records in rec: the scatter moves each record to its
+// bucket and the insertion sort works on the bucket's contiguous records, so
+// no pass gathers keys through a permutation.
+__device__ bool bucket_sort_large(const double *keys, SortRec *rec, uint32_t *cnt, uint32_t *coarse, int n, int nb,
                                   double kmin, double kmax, double *scratch, int *s_flag) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (!(kmax > kmin)) {
-        for (int m = tid; m < n; m += kTimeThreads) perm[m] = m;
+        for (int m = tid; m < n; m += kTimeThreads) rec[m] = SortRec{keys[m], m, 0};
         __syncthreads();
         return true;
     }
@@ -589,8 +599,9 @@ __device__ bool bucket_sort_large(const double *keys, int *perm, uint32_t *cnt, 
     if (*s_flag) return false;
     // scatter: afterwards cnt[b] is the end of bucket b
     for (int j = tid; j < n; j += kTimeThreads) {
-        const uint32_t pos = atomicAdd(&cnt[fine_bucket_n(keys[j], kmin, scale, coarse)], 1u);
-        perm[pos] = j;
+        const double kj = keys[j];
+        const uint32_t pos = atomicAdd(&cnt[fine_bucket_n(kj, kmin, scale, coarse)], 1u);
+        rec[pos] = SortRec{kj, j, 0};
     }
     __syncthreads();
     for (int i = 0; i < per; ++i) {
@@ -598,17 +609,15 @@ __device__ bool bucket_sort_large(const double *keys, int *perm, uint32_t *cnt, 
         const int start = b == 0 ? 0 : (int)cnt[b - 1];
         const int end = (int)cnt[b];
         for (int m = start + 1; m < end; ++m) {
-            const int v = perm[m];
-            const double kv = keys[v];
+            const SortRec v = rec[m];
             int q = m - 1;
             while (q >= start) {
-                const int u = perm[q];
-                const double ku = keys[u];
-                if (ku < kv || (ku == kv && u < v)) break;
-                perm[q + 1] = u;
+                const SortRec u = rec[q];
+                if (u.key < v.key || (u.key == v.key && u.idx < v.idx)) break;
+                rec[q + 1] = u;
                 --q;
             }
-            perm[q + 1] = v;
+            rec[q + 1] = v;
         }
     }
     __syncthreads();
@@ -717,7 +726,8 @@ __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
     __shared__ int s_pix, s_flag;
     unsigned char *slice = slices + (size_t)blockIdx.x * large_slice_bytes(n);
     double *keys = reinterpret_cast<double *>(slice);
-    int *perm = reinterpret_cast<int *>(slice + (size_t)n * 8);
+    SortRec *rec = reinterpret_cast<SortRec *>(slice + (size_t)n * 8);
+    int *perm = reinterpret_cast<int *>(slice + (size_t)n * 24);
     int *perm2 = perm + n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int npix = g.nx * g.ny;
@@ -749,15 +759,15 @@ __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
         }
         block_minmax(kmin, kmax, scratch + 96);
         __syncthreads();
-        const int *sorted = perm;
-        if (!bucket_sort_large(keys, perm, cnt, coarse, n, nb, kmin, kmax, scratch, &s_flag)) {
+        if (!bucket_sort_large(keys, rec, cnt, coarse, n, nb, kmin, kmax, scratch, &s_flag)) {
             radix_sort_large(keys, perm, perm2, n, H, base);
-            sorted = perm;
+            for (int m = tid; m < n; m += kTimeThreads) rec[m] = SortRec{keys[perm[m]], perm[m], 0};
+            __syncthreads();
         }
         if (p == order_pixel) {
             for (int m = tid; m < n; m += kTimeThreads) {
-                order_out[m] = sorted[m];
-                keys_out[m] = keys[sorted[m]];
+                order_out[m] = rec[m].idx;
+                keys_out[m] = rec[m].key;
             }
         }
         const int m0 = tid * per;
@@ -766,17 +776,17 @@ __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
         for (int i = 0; i < per; ++i) {
             const int m = m0 + i;
             if (m >= n) break;
-            const int j = sorted[m];
-            const double tj = keys[j];
-            const double4 a = reinterpret_cast<const double4 *>(atoms)[j];
+            const SortRec r = rec[m];
+            const double tj = r.key;
+            const double4 a = reinterpret_cast<const double4 *>(atoms)[r.idx];
             double s, dist, re, im;
             path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
             amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
-            const double dec = m == 0 ? 0.0 : exp(-__dsub_rn(tj, keys[sorted[m - 1]]) * inv_tau);
+            const double dec = m == 0 ? 0.0 : exp(-__dsub_rn(tj, rec[m - 1].key) * inv_tau);
             Dm *= dec;
             Br = fma(dec, Br, re);
             Bi = fma(dec, Bi, im);
-            const double w = m < n - 1 ? (-tau / 2) * expm1(-2 * __dsub_rn(keys[sorted[m + 1]], tj) * inv_tau)
+            const double w = m < n - 1 ? (-tau / 2) * expm1(-2 * __dsub_rn(rec[m + 1].key, tj) * inv_tau)
                                        : tau / 2;
             const double wD = w * Dm;
             S1 = fma(wD, Dm, S1);

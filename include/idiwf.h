@@ -188,7 +188,7 @@ idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch *batch,
 int64_t idiwf_time_max_emitters(void);
 
 /* Workspace for n emitters on this detector (for n above
- * idiwf_time_max_emitters(): 16 n bytes per resident CTA on the current device). */
+ * idiwf_time_max_emitters(): 32 n bytes per resident CTA on the current device). */
 size_t idiwf_time_workspace_size(const idiwf_geom *geom, int64_t n);
 
 /*
