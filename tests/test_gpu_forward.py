@@ -179,6 +179,33 @@ def test_pixel_runs_fall_back_beyond_their_bound():
                           _run(at, [0, n], geom, nat.SPLIT, config={"pixel_groups": -1}))
 
 
+@pytest.mark.parametrize("ndet", [[40, 64], [8, 12]])
+def test_mixed_batch_runs_and_per_pixel_kernels(ndet):
+    """One batch whose images take different kernels: small objects the
+    pixel-run kernel, large ones (beyond the 1 rad bound) the per-pixel
+    kernel, each from its own work counter.  Every image against the oracle
+    and against the all-per-pixel result; the small detector also splits the
+    work over emitter chunks."""
+    g0 = rng(33)
+    radii = [0.01, 0.06, 0.015, 0.08, 0.005]  # bound 0.37, 2.2, 0.55, 2.9, 0.18 rad
+    counts = [1500, 1100, 2600, 700, 1234]
+    imgs = [atoms(sphere(g0, c, r), g0.uniform(0, 2 * np.pi, c)) for c, r in zip(counts, radii)]
+    at = np.concatenate(imgs)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    geom = _core.make_geom(ndet, 75.0, 1e5, K64, flags=nat.NF)
+    og = oracle.geometry(ndet, 75.0, 1e5, K64)
+    E = _run(at, off, geom, nat.SPLIT)
+    E_pix = _run(at, off, geom, nat.SPLIT, config={"pixel_groups": -1})
+    for b, a in enumerate(imgs):
+        ref = oracle.wavefield(og, oracle.NF, a)
+        for X in (E[b], E_pix[b]):
+            assert rel_field_err(X, ref) < SPLIT_FIELD, (ndet, b)
+        if radii[b] > 0.03:  # beyond the bound: the per-pixel kernel, bit for bit
+            assert np.array_equal(E[b], E_pix[b]), b
+        else:
+            assert not np.array_equal(E[b], E_pix[b]), b
+
+
 def test_pixel_runs_shapes_agree():
     """With pixel runs the sums are still the same for every kernel shape: a
     run's base phase is fixed by the detector, not by the thread layout."""
