@@ -91,6 +91,35 @@ __device__ __forceinline__ void path_only(double dx, double dy, double dz, doubl
     }
 }
 
+// exp(-x) and expm1(-x), x >= 0, for the scan.  The arguments are gaps
+// between neighbouring arrival times over tau, almost always far below 1: up
+// to 2^-4 a Taylor polynomial of degree 9 in Horner form (coefficients 1/k!)
+// is exact to FP64 rounding (the first omitted term is below 3e-19 of the
+// result); larger arguments use the library functions.  (Used by the on-chip
+// kernel: in the 64-register large-count kernel the inlined polynomials
+// measured slower than the library calls.)
+__device__ __forceinline__ double inv_fact(int k) {
+    constexpr double f[11] = {1.0,       1.0,        1.0 / 2,     1.0 / 6,      1.0 / 24,      1.0 / 120,
+                              1.0 / 720, 1.0 / 5040, 1.0 / 40320, 1.0 / 362880, 1.0 / 3628800};
+    return f[k];
+}
+__device__ __forceinline__ double exp_neg(double x) {
+    if (!(x <= 0.0625)) return exp(-x);
+    const double t = -x;
+    double p = inv_fact(9);
+#pragma unroll
+    for (int k = 8; k >= 0; --k) p = __fma_rn(p, t, inv_fact(k));
+    return p;
+}
+__device__ __forceinline__ double expm1_neg(double x) {
+    if (!(x <= 0.0625)) return expm1(-x);
+    const double t = -x;
+    double q = inv_fact(10);
+#pragma unroll
+    for (int k = 9; k >= 1; --k) q = __fma_rn(q, t, inv_fact(k));
+    return t * q;  // t (1 + t/2! + ... + t^9/10!)
+}
+
 template <bool NF, bool SCALE>
 __device__ __forceinline__ void amplitude(double k, double s, double psi, double dist, double &re, double &im) {
     double th;
@@ -430,12 +459,12 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
             double s, dist, re, im;
             path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
             amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
-            const double dec = m == 0 ? 0.0 : exp(-__dsub_rn(tj, keytab[perm[m - 1]]) * inv_tau);
+            const double dec = m == 0 ? 0.0 : exp_neg(__dsub_rn(tj, keytab[perm[m - 1]]) * inv_tau);
             Dm *= dec;
             Br = fma(dec, Br, re);
             Bi = fma(dec, Bi, im);
             const double w = m < n - 1
-                                 ? (-tau / 2) * expm1(-2 * __dsub_rn(keytab[perm[m + 1]], tj) * inv_tau)
+                                 ? (-tau / 2) * expm1_neg(2 * __dsub_rn(keytab[perm[m + 1]], tj) * inv_tau)
                                  : tau / 2;
             const double wD = w * Dm;
             S1 = fma(wD, Dm, S1);
