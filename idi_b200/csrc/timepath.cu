@@ -450,22 +450,37 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
         const int m0 = tid * kTimeIPT;
         double Dm = 1.0, Br = 0.0, Bi = 0.0;
         double S1 = 0.0, S2r = 0.0, S2i = 0.0, S3 = 0.0;
+        // the neighbours' keys travel in registers from one position to the
+        // next, and the next position's emitter row is loaded one step ahead
+        const double4 *atoms4 = reinterpret_cast<const double4 *>(atoms);
+        double t_prev = m0 > 0 && m0 - 1 < n ? keytab[perm[m0 - 1]] : 0.0;
+        int j_next = 0;
+        double t_next = 0.0;
+        double4 a_next = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (m0 < n) {
+            j_next = perm[m0];
+            t_next = keytab[j_next];
+            a_next = atoms4[j_next];
+        }
         for (int i = 0; i < kTimeIPT; ++i) {
             const int m = m0 + i;
             if (m >= n) break;
-            const int j = perm[m];
-            const double tj = keytab[j];
-            const double4 a = reinterpret_cast<const double4 *>(atoms)[j];
+            const double tj = t_next;
+            const double4 a = a_next;
+            if (m + 1 < n) {
+                j_next = perm[m + 1];
+                t_next = keytab[j_next];
+                if (i + 1 < kTimeIPT) a_next = atoms4[j_next];
+            }
             double s, dist, re, im;
             path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
             amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
-            const double dec = m == 0 ? 0.0 : exp_neg(__dsub_rn(tj, keytab[perm[m - 1]]) * inv_tau);
+            const double dec = m == 0 ? 0.0 : exp_neg(__dsub_rn(tj, t_prev) * inv_tau);
+            t_prev = tj;
             Dm *= dec;
             Br = fma(dec, Br, re);
             Bi = fma(dec, Bi, im);
-            const double w = m < n - 1
-                                 ? (-tau / 2) * expm1_neg(2 * __dsub_rn(keytab[perm[m + 1]], tj) * inv_tau)
-                                 : tau / 2;
+            const double w = m < n - 1 ? (-tau / 2) * expm1_neg(2 * __dsub_rn(t_next, tj) * inv_tau) : tau / 2;
             const double wD = w * Dm;
             S1 = fma(wD, Dm, S1);
             S2r = fma(wD, Br, S2r);
@@ -802,21 +817,33 @@ __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
         const int m0 = tid * per;
         double Dm = 1.0, Br = 0.0, Bi = 0.0;
         double S1 = 0.0, S2r = 0.0, S2i = 0.0, S3 = 0.0;
+        // neighbours' keys carried in registers, the next emitter row loaded one step ahead
+        const double4 *atoms4 = reinterpret_cast<const double4 *>(atoms);
+        double t_prev = m0 > 0 && m0 - 1 < n ? rec[m0 - 1].key : 0.0;
+        SortRec r_next = SortRec{0.0, 0, 0};
+        double4 a_next = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (m0 < n) {
+            r_next = rec[m0];
+            a_next = atoms4[r_next.idx];
+        }
         for (int i = 0; i < per; ++i) {
             const int m = m0 + i;
             if (m >= n) break;
-            const SortRec r = rec[m];
-            const double tj = r.key;
-            const double4 a = reinterpret_cast<const double4 *>(atoms)[r.idx];
+            const double tj = r_next.key;
+            const double4 a = a_next;
+            if (m + 1 < n) {
+                r_next = rec[m + 1];
+                if (i + 1 < per) a_next = atoms4[r_next.idx];
+            }
             double s, dist, re, im;
             path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
             amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
-            const double dec = m == 0 ? 0.0 : exp(-__dsub_rn(tj, rec[m - 1].key) * inv_tau);
+            const double dec = m == 0 ? 0.0 : exp(-__dsub_rn(tj, t_prev) * inv_tau);
+            t_prev = tj;
             Dm *= dec;
             Br = fma(dec, Br, re);
             Bi = fma(dec, Bi, im);
-            const double w = m < n - 1 ? (-tau / 2) * expm1(-2 * __dsub_rn(rec[m + 1].key, tj) * inv_tau)
-                                       : tau / 2;
+            const double w = m < n - 1 ? (-tau / 2) * expm1(-2 * __dsub_rn(r_next.key, tj) * inv_tau) : tau / 2;
             const double wD = w * Dm;
             S1 = fma(wD, Dm, S1);
             S2r = fma(wD, Br, S2r);
