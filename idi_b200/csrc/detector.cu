@@ -139,14 +139,23 @@ __global__ void __launch_bounds__(kSumThreads) photon_sum_kernel(const T *__rest
 // of low mean rate); otherwise one thread per pixel, and the rare inversion
 // pixel computes its quad's block itself (high mean rate: the PTRS loops then
 // spread over all threads).  Both give the same counts.
-template <typename TI, typename TO, bool QUAD>
+// MODE kPixels: one thread per pixel, inversion and PTRS.  kQuads: one
+// thread per quad, inversion only; a PTRS pixel is left to the kPtrs pass and
+// raises *ptrs_flag.  kPtrs: one thread per pixel, PTRS pixels only, and only
+// when *ptrs_flag is set (the quad kernel then carries no PTRS code and its
+// register count stays low).
+constexpr int kPixels = 0, kQuads = 1, kPtrs = 2;
+template <typename TI, typename TO, int MODE>
 __global__ void __launch_bounds__(kSumThreads) photon_sample_kernel(const TI *__restrict__ probs, int64_t npix,
                                                                     int nblk, const double *__restrict__ partials,
                                                                     double n_photons, uint64_t k0, uint64_t k1,
                                                                     uint64_t stream, uint64_t img0,
                                                                     TO *__restrict__ out,
-                                                                    uint32_t *__restrict__ err) {
+                                                                    uint32_t *__restrict__ err,
+                                                                    uint32_t *__restrict__ ptrs_flag) {
+    constexpr bool QUAD = MODE == kQuads;
     __shared__ double v[kSumThreads];
+    if (MODE == kPtrs && *(volatile uint32_t *)ptrs_flag == 0u) return;
     const int b = blockIdx.y;
     v[threadIdx.x] = (int)threadIdx.x < nblk ? partials[(int64_t)b * nblk + threadIdx.x] : 0.0;
     tree_sum(v);
@@ -160,8 +169,9 @@ __global__ void __launch_bounds__(kSumThreads) photon_sample_kernel(const TI *__
         for (int64_t p = (int64_t)blockIdx.x * kSumThreads + threadIdx.x; p < npix;
              p += (int64_t)gridDim.x * kSumThreads) {
             const double l = load_real(img, p) * scale;
+            if (MODE == kPtrs && !(l >= kPtrsMinRate && l < 0x1p62)) continue;
             double k = 0.0;
-            if (l > 0.0 && l < kPtrsMinRate) {
+            if (MODE == kPixels && l > 0.0 && l < kPtrsMinRate) {
                 uint64_t w0, w1, w2, w3;
                 philox4x64(kQuadCounter, (uint64_t)(p >> 2), ib, stream, k0, k1, w0, w1, w2, w3);
                 const int i = (int)(p & 3);
@@ -173,7 +183,7 @@ __global__ void __launch_bounds__(kSumThreads) photon_sample_kernel(const TI *__
                     bad = true;
                     k = 0.0;
                 }
-            } else if (!(l == 0.0)) {
+            } else if (!(l == 0.0) && MODE == kPixels) {
                 bad = true;
             }
             store_count(o, p, k);
@@ -204,24 +214,7 @@ __global__ void __launch_bounds__(kSumThreads) photon_sample_kernel(const TI *__
             ptrs |= l >= kPtrsMinRate && l < 0x1p62;
             bad |= i < np && !(l >= 0.0 && l < 0x1p62);
         }
-        if (ptrs) {
-            // one copy of the rejection loop (its log/lgamma calls are long)
-#pragma unroll 1
-            for (int i = 0; i < np; ++i) {
-                const double l = i == 0 ? lam[0] : (i == 1 ? lam[1] : (i == 2 ? lam[2] : lam[3]));
-                if (!(l >= kPtrsMinRate && l < 0x1p62)) continue;
-                PhiloxStream st((uint64_t)(p0 + i), ib, stream, k0, k1);
-                double kk = poisson_ptrs(l, st);
-                if (kk < 0.0) {
-                    bad = true;
-                    kk = 0.0;
-                }
-                if (i == 0) k[0] = kk;
-                else if (i == 1) k[1] = kk;
-                else if (i == 2) k[2] = kk;
-                else k[3] = kk;
-            }
-        }
+        if (ptrs) *(volatile uint32_t *)ptrs_flag = 1u;  // drawn by the kPtrs pass; all writers store 1
 #pragma unroll
         for (int i = 0; i < 4; ++i)
             if (i < np) store_count(o, p0 + i, k[i]);
@@ -610,16 +603,25 @@ static idiwf_status launch_photons(const void *probs, int32_t n_images, int64_t 
                                                                             nblk, partials, &hdr->error);
     IDIWF_CUDA_CHECK(cudaGetLastError());
     // mean rate below 1: one thread per pixel quad (one Philox block per four
-    // inversions); above: one thread per pixel (the PTRS loops dominate)
+    // inversions), then a PTRS pass that returns at once when no pixel needs
+    // it; above: one thread per pixel (the PTRS loops dominate)
     const bool quad = n_photons < (double)npix;
-    const int64_t want = ((quad ? (npix + 3) / 4 : npix) + kSumThreads - 1) / kSumThreads;
-    const int gx = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)8 * dev_sms() / std::max(1, n_images) + 1));
-    auto fn = quad ? photon_sample_kernel<TI, TO, true> : photon_sample_kernel<TI, TO, false>;
-    fn<<<dim3(gx, n_images), kSumThreads, 0, stream>>>(static_cast<const TI *>(probs), npix, nblk, partials, n_photons,
-                                                       rng->key[0], rng->key[1], rng->stream, rng->first_image,
-                                                       static_cast<TO *>(out), &hdr->error);
-    IDIWF_CUDA_CHECK(cudaGetLastError());
-    return IDIWF_OK;
+    uint32_t *flag = &hdr->work_counter;
+    auto launch = [&](auto fn, int64_t items) -> idiwf_status {
+        const int64_t want = (items + kSumThreads - 1) / kSumThreads;
+        const int gx =
+            (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)8 * dev_sms() / std::max(1, n_images) + 1));
+        fn<<<dim3(gx, n_images), kSumThreads, 0, stream>>>(static_cast<const TI *>(probs), npix, nblk, partials,
+                                                           n_photons, rng->key[0], rng->key[1], rng->stream,
+                                                           rng->first_image, static_cast<TO *>(out), &hdr->error, flag);
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+        return IDIWF_OK;
+    };
+    if (!quad) return launch(photon_sample_kernel<TI, TO, kPixels>, npix);
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(flag, 0, sizeof(uint32_t), stream));
+    idiwf_status st = launch(photon_sample_kernel<TI, TO, kQuads>, (npix + 3) / 4);
+    if (st != IDIWF_OK) return st;
+    return launch(photon_sample_kernel<TI, TO, kPtrs>, npix);
 }
 
 template <typename TI>
