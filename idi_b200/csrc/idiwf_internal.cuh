@@ -102,7 +102,7 @@ constexpr int kChunkEmitters = 1024;
 GeomParams make_geom(const idiwf_geom *g);
 
 // ---------------------------------------------------------------------------
-// device helpers: mbarrier + bulk async copy (TMA, no multicast)
+// device helpers: mbarrier + bulk async copy into the CTA's own shared memory
 // ---------------------------------------------------------------------------
 #if defined(__CUDACC__)
 
