@@ -72,6 +72,29 @@ def test_poisson_sampler_distribution(lam):
     assert abs(c.mean() - lam) < 5 * np.sqrt(lam / c.size)
 
 
+def test_quad_block_uniforms_match_numpy_philox():
+    """Below rate 10 pixel p inverts word p % 4 of the Philox4x64-10 block with
+    counter (2^63, p / 4, image, stream): numpy's generator, started one block
+    earlier, gives that block as its first raw output."""
+    key, stream = (0xDEADBEEF12345678, 77), 5
+    npix, lam = 32, 3.0
+    probs = np.ones((2, 4, 8))                  # two images of 32 pixels; rate exactly n / npix
+    got = oracle.photons(probs, lam * npix, key, stream).reshape(2, npix)
+    assert len(np.unique(got)) >= 4
+    for b in range(2):
+        for p in range(npix):
+            ctr = np.array([2**63 - 1, p // 4, b, stream], np.uint64)
+            w = np.random.Philox(counter=ctr, key=np.array(key, np.uint64)).random_raw(4)[p % 4]
+            u = float(int(w) >> 11) * 2.0**-53
+            k, term = 0, np.exp(-lam)
+            F = term
+            while u > F:
+                k += 1
+                term = term * lam / k
+                F += term
+            assert got[b, p] == k, (b, p)
+
+
 def test_photons_first_image_offsets_the_stream():
     g = np.random.default_rng(1)
     p = g.uniform(0.1, 1.0, (4, 9, 7))
