@@ -17,8 +17,10 @@
  *  - Every device buffer is allocated by the caller.  Scratch space is a
  *    caller-provided workspace whose size the *_workspace_size functions report;
  *    no entry point allocates device or pinned memory.
- *  - Work is enqueued on `stream` and is asynchronous: no entry point
- *    synchronises the device, so all of them can be captured in a CUDA graph.
+ *  - Work is enqueued on `stream` and is asynchronous: the compute entry points
+ *    do not synchronise, so they can be captured in a CUDA graph.  The entry
+ *    points that read results back (idiwf_tune, idiwf_forward_cta_times,
+ *    idiwf_workspace_error, idiwf_microbench) synchronise their stream.
  *  - Errors are returned as idiwf_status, never by aborting.  Asynchronous
  *    device-side failures (a bounded wait that ran out) are recorded in the
  *    workspace and reported by idiwf_workspace_error().
