@@ -59,6 +59,7 @@ EXPORTED = (
     "idiwf_forward",
     "idiwf_forward_cta_times",
     "idiwf_forward_noalloc",
+    "idiwf_forward_noalloc_error",
     "idiwf_backward_workspace_size",
     "idiwf_backward",
     "idiwf_time_max_emitters",
@@ -179,6 +180,8 @@ def load():
     L.idiwf_forward.restype = st
     L.idiwf_forward_noalloc.argtypes = [P(Geom), P(Batch), ctypes.c_int32, vp, vp]
     L.idiwf_forward_noalloc.restype = st
+    L.idiwf_forward_noalloc_error.argtypes = [vp]
+    L.idiwf_forward_noalloc_error.restype = st
     L.idiwf_forward_cta_times.argtypes = [vp, P(ctypes.c_uint64), ctypes.c_int32, P(ctypes.c_int32), vp]
     L.idiwf_forward_cta_times.restype = st
     L.idiwf_backward_workspace_size.argtypes = [P(Geom), P(Batch), P(Config)]

@@ -112,6 +112,11 @@ extern "C" idiwf_status idiwf_workspace_error(const void *workspace, cudaStream_
     if (h.error & kErrRange)
         return set_error(IDIWF_ERR_UNSUPPORTED,
                          "emitter coordinates too large for the split-precision phase range");
+    if (h.error & kErrGeometry)
+        return set_error(IDIWF_ERR_UNSUPPORTED,
+                         "near-field geometry outside the split-precision range (emitters farther than a quarter "
+                         "of the detector distance from the origin, or a path-difference remainder above 2 rad); "
+                         "use the FP64 kernel (settings 'double' or 'accurate')");
     return IDIWF_OK;
 }
 

@@ -12,9 +12,12 @@
 // k r^2/|d|^2, ~1e-10 relative), -q_p in the far field, plus kappa_p (x, y, 0)
 // for the far-field second-order term.  The near-field projector is taken
 // paraxially, P ~ diag(1, 1, 0): the kappa term is itself r / (|d| theta) of
-// the main term and the neglected part is theta times that, below 1e-7 of
-// the gradient.  The 1/r factor's own gradient (relative size
-// 1/(k |d| theta) ~ 1e-9) is not included.
+// the main term and the neglected part is theta times that, i.e. about r/|d|
+// of the gradient; images with (r/|d|)^2 > kAdjRho2, or whose phase needs the
+// forward's exact near-field remainder, take the exact adjoint instead:
+//   grad_r phi = -q_p + (k/L) ((N - s) dhat_p + r_j),  L = |d_p - r_j|,
+// with N and s as in the forward, and for "scale" grad_r (1/L) = (d_p - r_j)/L^3
+// (the paraxial path uses the gradient dhat_p/|d_p|^2 of its own 1/r factor).
 //
 // The phase is formed as in the forward split kernel (FP64 turns in a magic
 // binade -> 32-bit fixed point -> FP32 angle, MUFU sincos), with the
@@ -63,13 +66,19 @@ constexpr uint32_t kOffRunPG = kOffRunPD + kBwdTP * 32;
 constexpr uint32_t kOffRunB64 = kOffRunPG + kBwdTP * 16;
 constexpr uint32_t kOffRunBF = kOffRunB64 + kBwdTP / kRun * 32;
 constexpr uint32_t kStageRuns = kOffRunBF + kBwdTP / kRun * 32;
+// exact near-field path: the per-pixel stage plus
+//   PX   float4 {|d|, |d|, 0, 0}                                             16 B
+// and the P64 record carries the quadratic term's coefficient kp/(2|d|) in .w
+constexpr uint32_t kStageExact = kStagePixels + kBwdTP * 16;
+constexpr uint32_t kStageMax = kStageRuns > kStageExact ? (kStageRuns > kStagePixels ? kStageRuns : kStagePixels)
+                                                        : (kStageExact > kStagePixels ? kStageExact : kStagePixels);
 static_assert(kBwdTP % kRun == 0 && kBwdChunk % kRun == 0, "tiles hold whole runs");
 
 struct BwdLayout {
     int npix_pad;          // pixels rounded up to the chunk size
     int n_chunks;
     int64_t nrec;          // emitter records (images padded to the emitter block)
-    size_t off_p64, off_pf, off_pg, off_pd, off_rb64, off_rbf, off_rmax, off_erec64, off_erecf, off_part, total;
+    size_t off_p64, off_pf, off_pg, off_pd, off_rb64, off_rbf, off_px, off_rmax, off_erec64, off_erecf, off_part, total;
 };
 
 static BwdLayout bwd_layout(const idiwf_geom *g, const idiwf_batch *b) {
@@ -91,6 +100,7 @@ static BwdLayout bwd_layout(const idiwf_geom *g, const idiwf_batch *b) {
     L.off_pd = o;  o += align256((size_t)L.npix_pad * 32);
     L.off_rb64 = o; o += align256((size_t)L.npix_pad / kRun * 32);
     L.off_rbf = o; o += align256((size_t)L.npix_pad / kRun * 32);
+    L.off_px = o;  o += align256((size_t)L.npix_pad * 16);
     L.off_rmax = o; o += align256((size_t)kMaxImagesPerLaunch * 4);
     L.off_erec64 = o; o += align256((size_t)L.nrec * 32);
     L.off_erecf = o;  o += align256((size_t)L.nrec * 16);
@@ -116,7 +126,7 @@ struct BwdRecs {
     const double4 *p64;
     const float4 *pf, *pg, *pd;
     const double4 *rb64;
-    const float4 *rbf;
+    const float4 *rbf, *px;
     const uint32_t *rmax2;  // per image: max |r|^2 (float bits, rounded up)
 };
 
@@ -131,7 +141,7 @@ __device__ __forceinline__ double nf_constant_turns(const GeomParams &g, double 
 // ---- pixel prep: geometry (image independent) ------------------------------
 __global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad, int runs,
                                       double4 *__restrict__ p64, float4 *__restrict__ pf, float4 *__restrict__ pd,
-                                      double4 *__restrict__ rb64, float4 *__restrict__ rbf) {
+                                      double4 *__restrict__ rb64, float4 *__restrict__ rbf, float4 *__restrict__ px) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix_pad; p += gridDim.x * blockDim.x) {
         const int pc = min(p, npix - 1);
         const int ix = pc / g.ny, iy = pc - ix * g.ny;
@@ -141,7 +151,9 @@ __global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad
         const double D = sqrt(rho2 + dz * dz);
         const double invD = 1.0 / D;
         const double dzm1 = dz > 0 ? -rho2 / (D * (D + dz)) : dz * invD - 1.0;
-        p64[p] = make_double4(-g.kp * (dx * invD), -g.kp * (dy * invD), -g.kp * dzm1, 0.0);
+        // .w: the exact path's quadratic-term coefficient kp / (2|d|)
+        p64[p] = make_double4(-g.kp * (dx * invD), -g.kp * (dy * invD), -g.kp * dzm1, 0.5 * g.kp * invD);
+        px[p] = make_float4((float)D, (float)D, 0.f, 0.f);
         const float fdx = (float)(dx * invD), fdy = (float)(dy * invD), fdz = (float)(dz * invD);
         const float fh = (float)(-g.k * 0.5 * invD);  // -h, pairs with the negated w
         const float qx = (float)(g.k * dx * invD), qy = (float)(g.k * dy * invD), qz = (float)(g.k * dzm1);
@@ -250,20 +262,30 @@ __device__ __forceinline__ float2 g2(float a, float b) { return make_float2(a, b
 // The near-field correction uses the paraxial projector: grad phi =
 // -q + kappa P r with P = I - dhat dhat^T ~ diag(1, 1, 0); the neglected part
 // is of relative size theta (the pixel angle) times the correction, which is
-// itself r / (|d| theta) of the main term: below 1e-7 of the gradient.
-// One work unit (image, emitter block, pixel chunk).  RUNS = false: every
-// emitter-pixel pair forms its phase with its own FP64 DFMA chain.  RUNS =
-// true: one chain per emitter and run of kRun pixels at the run's middle, and
-// the FP32 offset D_p . r per pixel (D_p = 2 pi (nq_p - nq_base); bounded per
-// image by the caller), with s_p = d_hat_p . r = s_base - D_p.r / k for the
-// near-field term.  Returns true when a bounded wait gave up.
-template <bool NF, bool SCALE, bool SECOND, int PE, bool RUNS>
+// itself r / (|d| theta) of the main term, i.e. about r/|d| of the gradient
+// (bounded per image by kAdjRho2).
+// The exact path (PATH = kPathExact) keeps the same six sums with
+//   2-4  sum [w Im z q + c dhat],  c = -w Im z (k/L) (N - s) [+ Re z |d| / L^3]
+//   5    sum [w Im z k/L] [+ Re z / L^3]                    ("scale" terms in [])
+// and the final gradient a (acc[2..4] - acc[5] r) uses all of r.
+// One work unit (image, emitter block, pixel chunk).  PATH = kPathPixel: every
+// emitter-pixel pair forms its phase with its own FP64 DFMA chain.  PATH =
+// kPathRuns: one chain per emitter and run of kRun pixels at the run's middle,
+// and the FP32 offset D_p . r per pixel (D_p = 2 pi (nq_p - nq_base); bounded
+// per image by the caller), with s_p = d_hat_p . r = s_base - D_p.r / k for the
+// near-field term.  PATH = kPathExact: per pair, with the forward exact path's
+// phase (quadratic term in the FP64 chain, FP32 remainder).  Returns true when
+// a bounded wait gave up.
+template <bool NF, bool SCALE, bool SECOND, int PE, int PATH>
 __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, float *__restrict__ part,
                                          int64_t nrec, WsHeader *__restrict__ hdr, unsigned char *smem,
                                          uint64_t *bar, int *s_abort, uint32_t &issued, uint32_t &consumed,
-                                         int img, int ib, int chunk, float ninvk) {
+                                         int img, int ib, int chunk, float ninvk, const GeomParams &g) {
+    constexpr bool RUNS = PATH == kPathRuns;
+    constexpr bool EXACT = PATH == kPathExact;
+    static_assert(!EXACT || NF, "the exact path is a near-field path");
     constexpr int PH = PE / 2;
-    constexpr uint32_t kStage = RUNS ? kStageRuns : kStagePixels;
+    constexpr uint32_t kStage = RUNS ? kStageRuns : (EXACT ? kStageExact : kStagePixels);
     const int tid = threadIdx.x;
     const float2 TWO_PI2 = g2(6.28318548f, 6.28318548f);
     const float2 NEG_3PI2 = g2(-9.42477796f, -9.42477796f);
@@ -272,16 +294,18 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
     const BwdImage d = bp.img[img];
     const int64_t rec0 = d.rec + (int64_t)ib * eb + tid * PE;
 
-    double ex[PE], ey[PE], ez[PE], epsi[PE];
+    double ex[PE], ey[PE], ez[PE], epsi[PE], err[EXACT ? PE : 1];  // err: (EXACT) |r|^2 in FP64
     float2 fx[PH], fy[PH], fz[PH], fw[PH];
 #pragma unroll
     for (int e = 0; e < PE; ++e) {
         const double4 r = R.e64[rec0 + e];
         ex[e] = r.x; ey[e] = r.y; ez[e] = r.z; epsi[e] = r.w;
+        if (EXACT) err[e] = __fma_rn(r.z, r.z, __fma_rn(r.y, r.y, r.x * r.x));
         const float4 f = R.ef[rec0 + e];
         if (e & 1) { fx[e / 2].y = f.x; fy[e / 2].y = f.y; fz[e / 2].y = f.z; fw[e / 2].y = f.w; }
         else       { fx[e / 2].x = f.x; fy[e / 2].x = f.y; fz[e / 2].x = f.z; fw[e / 2].x = f.w; }
     }
+    const float kf = (float)g.k;
     float2 ac[kBwdNAcc][PH];
 #pragma unroll
     for (int a = 0; a < kBwdNAcc; ++a)
@@ -305,6 +329,7 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
             bulk_g2s(st, R.p64 + p0, kBwdTP * 32, &bar[slot]);
             bulk_g2s(st + kBwdTP * 32, R.pf + (size_t)p0 * 5, kBwdTP * 80, &bar[slot]);
             bulk_g2s(st + kBwdTP * 112, R.pg + (size_t)img * bp.npix_pad + p0, kBwdTP * 16, &bar[slot]);
+            if (EXACT) bulk_g2s(st + kStagePixels, R.px + p0, kBwdTP * 16, &bar[slot]);
         }
         ++issued;
     };
@@ -336,6 +361,14 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
                 zr = __ffma2_rn(g2(-GG.z, -GG.w), ss, zr);
                 zi = __fmul2_rn(zi, w);
                 ac[0][q] = __ffma2_rn(zr, w, ac[0][q]);
+                if (NF) {
+                    // Re z grad w, grad w = dhat / |d|^2 (the gradient of w itself)
+                    const float4 F0 = sf[5 * j + 0], F1 = sf[5 * j + 1];  // dx dx dy dy | dz dz
+                    const float2 c = __fmul2_rn(zr, g2(F4.z, F4.w));
+                    ac[2][q] = __ffma2_rn(c, g2(F0.x, F0.y), ac[2][q]);
+                    ac[3][q] = __ffma2_rn(c, g2(F0.z, F0.w), ac[3][q]);
+                    ac[4][q] = __ffma2_rn(c, g2(F1.x, F1.y), ac[4][q]);
+                }
             } else {
                 ac[0][q] = __ffma2_rn(g2(GG.x, GG.y), cc, ac[0][q]);
                 ac[0][q] = __ffma2_rn(g2(-GG.z, -GG.w), ss, ac[0][q]);
@@ -407,6 +440,7 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
             const double4 *s64 = reinterpret_cast<const double4 *>(st);
             const float4 *sf = reinterpret_cast<const float4 *>(st + kBwdTP * 32);
             const float4 *sg = reinterpret_cast<const float4 *>(st + kBwdTP * 112);
+            const float4 *spx = reinterpret_cast<const float4 *>(st + kStagePixels);
 #pragma unroll 2
             for (int j = 0; j < kBwdTP; ++j) {
                 const double4 P = s64[j];
@@ -415,6 +449,11 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
                 const float4 F2 = sf[5 * j + 2];  // qx qx qy qy
                 const float4 F3 = sf[5 * j + 3];  // qz qz kap kap
                 const float4 GG = sg[j];          // G'r G'r G'i G'i
+                float2 D2 = g2(0.f, 0.f);
+                if (EXACT) {
+                    const float4 X = spx[j];  // |d| |d|
+                    D2 = g2(X.x, X.y);
+                }
 #pragma unroll
                 for (int q = 0; q < PH; ++q) {
                     uint32_t lo[2];
@@ -424,6 +463,11 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
                         double t = __fma_rn(P.x, ex[i], epsi[i]);
                         t = __fma_rn(P.y, ey[i], t);
                         t = __fma_rn(P.z, ez[i], t);
+                        if (EXACT) {
+                            // s from the chain (t - Psi = kp (z - s)), quadratic term in FP64
+                            const double sd = __fma_rn(-g.ikp, t - epsi[i], ez[i]);
+                            t = __fma_rn(P.w, __fma_rn(-sd, sd, err[i]), t);
+                        }
                         lo[e] = (uint32_t)__double2loint(t);
                     }
                     const float2 u = g2(__uint_as_float((lo[0] >> 9) | 0x3F800000u),
@@ -435,6 +479,40 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
                         s = __ffma2_rn(g2(F0.z, F0.w), fy[q], s);
                         s = __ffma2_rn(g2(F1.x, F1.y), fz[q], s);
                         const float2 w2 = __ffma2_rn(s, s, fw[q]);  // s^2 - |r|^2
+                        if (EXACT) {
+                            // L^2 = |d|(|d| - 2s) + |r|^2; N = r_perp^2 / (|d| + L - s);
+                            // remainder (-h)(-N)(2s - N) as in the forward
+                            const float2 l2 = __ffma2_rn(__ffma2_rn(s, g2(-2.f, -2.f), D2), D2,
+                                                         g2(-fw[q].x, -fw[q].y));
+                            const float2 y = g2(rsqrt_approx(l2.x), rsqrt_approx(l2.y));  // 1/L
+                            const float2 den = __ffma2_rn(s, g2(-1.f, -1.f), __ffma2_rn(l2, y, D2));
+                            const float2 nN = __fmul2_rn(w2, g2(rcp_approx(den.x), rcp_approx(den.y)));
+                            arg = __ffma2_rn(__fmul2_rn(g2(F1.z, F1.w), nN), __ffma2_rn(s, g2(2.f, 2.f), nN), arg);
+                            float s0, c0, s1, c1;
+                            __sincosf(arg.x, &s0, &c0);
+                            __sincosf(arg.y, &s1, &c1);
+                            const float2 cc = g2(c0, c1), ss = g2(s0, s1);
+                            float2 zi = __ffma2_rn(g2(GG.z, GG.w), cc, __fmul2_rn(g2(GG.x, GG.y), ss));
+                            const float2 zr = __ffma2_rn(g2(-GG.z, -GG.w), ss, __fmul2_rn(g2(GG.x, GG.y), cc));
+                            if (SCALE) zi = __fmul2_rn(zi, y);                              // w Im z
+                            ac[0][q] = __ffma2_rn(zr, SCALE ? y : g2(1.f, 1.f), ac[0][q]);  // w Re z
+                            ac[1][q] = __fadd2_rn(ac[1][q], zi);
+                            const float2 kL = __fmul2_rn(g2(kf, kf), y);  // k / L
+                            const float2 zk = __fmul2_rn(zi, kL);
+                            // c = w Im z (k/L)(s - N) [+ Re z |d| / L^3]
+                            float2 c = __fmul2_rn(zk, __fadd2_rn(s, nN));
+                            float2 sk = zk;
+                            if (SCALE) {
+                                const float2 zy3 = __fmul2_rn(zr, __fmul2_rn(y, __fmul2_rn(y, y)));
+                                c = __ffma2_rn(zy3, D2, c);
+                                sk = __fadd2_rn(sk, zy3);
+                            }
+                            ac[2][q] = __ffma2_rn(c, g2(F0.x, F0.y), __ffma2_rn(zi, g2(F2.x, F2.y), ac[2][q]));
+                            ac[3][q] = __ffma2_rn(c, g2(F0.z, F0.w), __ffma2_rn(zi, g2(F2.z, F2.w), ac[3][q]));
+                            ac[4][q] = __ffma2_rn(c, g2(F1.x, F1.y), __ffma2_rn(zi, g2(F3.x, F3.y), ac[4][q]));
+                            ac[5][q] = __fadd2_rn(ac[5][q], sk);
+                            continue;
+                        }
                         arg = __ffma2_rn(g2(F1.z, F1.w), w2, arg);
                     } else if (SECOND) {
                         arg = __ffma2_rn(g2(F1.z, F1.w), fw[q], arg);
@@ -460,15 +538,31 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
     return false;
 }
 
-template <bool NF, bool SCALE, bool SECOND, int PE>
+// Two instances per geometry: EXACTK = false takes the units of images on the
+// paraxial paths (pixel runs or per pair), EXACTK = true (near field only) the
+// images that need the exact adjoint, each from its own work counter.  Every
+// CTA classifies the images once into shared memory; the paraxial kernel,
+// which every call runs, reports images outside the split kernels' range
+// (kErrGeometry, their gradients are left at zero by the reduction).
+template <bool NF, bool SCALE, bool SECOND, int PE, bool EXACTK>
 __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(const __grid_constant__ BwdParams bp,
                                                                 const BwdRecs R, float *__restrict__ part,
                                                                 int64_t nrec, WsHeader *__restrict__ hdr,
                                                                 GeomParams g) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar[2];
-    __shared__ int s_unit, s_abort;
+    __shared__ int s_unit, s_abort, s_img, s_ib;
+    __shared__ uint8_t s_path[kMaxImagesPerLaunch];
     const int tid = threadIdx.x;
+    bool mine = false;
+    for (int i = tid; i < bp.n_images; i += blockDim.x) {
+        const int path = split_path(g, R.rmax2[i], bp.runs != 0, true);
+        s_path[i] = (uint8_t)path;
+        mine |= EXACTK ? path == kPathExact : (path == kPathPixel || path == kPathRuns);
+        if (!EXACTK && path == kPathReject && blockIdx.x == 0) record_error(&hdr->error, kErrGeometry);
+    }
+    if (!__syncthreads_or(mine)) return;
+    uint32_t *counter = EXACTK ? &hdr->work_counter3 : &hdr->work_counter;
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -482,29 +576,44 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(const __grid_con
 
     for (;;) {
         __syncthreads();
-        if (tid == 0) s_unit = (int)atomicAdd(&hdr->work_counter, 1u);
+        if (tid == 0) {
+            // next unit of this kernel's images (the others' are skipped here)
+            int u, img = 0, ib = 0;
+            for (;;) {
+                u = (int)atomicAdd(counter, 1u);
+                if (u >= bp.total_units) break;
+                ib = u / bp.n_chunks;
+                for (int k = 0; k < bp.n_images; ++k) {
+                    const int b = bp.unit_img[k];
+                    if (ib < bp.img[b].nblocks) { img = b; break; }
+                    ib -= bp.img[b].nblocks;
+                }
+                const int path = s_path[img];
+                if (EXACTK ? path == kPathExact : (path == kPathPixel || path == kPathRuns)) break;
+            }
+            s_unit = u;
+            s_img = img;
+            s_ib = ib;
+        }
         __syncthreads();
         const int unit = s_unit;
         if (unit >= bp.total_units) break;
         const int chunk = unit % bp.n_chunks;
-        int ib = unit / bp.n_chunks;
-        int img = 0;
-        for (int k = 0; k < bp.n_images; ++k) {
-            const int b = bp.unit_img[k];
-            if (ib < bp.img[b].nblocks) { img = b; break; }
-            ib -= bp.img[b].nblocks;
+        const int img = s_img, ib = s_ib;
+        bool ab;
+        if (EXACTK) {
+            if constexpr (NF)
+                ab = bwd_unit<NF, SCALE, SECOND, PE, kPathExact>(bp, R, part, nrec, hdr, smem, bar, &s_abort, issued,
+                                                                 consumed, img, ib, chunk, ninvk, g);
+            else
+                ab = false;
+        } else if (s_path[img] == kPathRuns) {
+            ab = bwd_unit<NF, SCALE, SECOND, PE, kPathRuns>(bp, R, part, nrec, hdr, smem, bar, &s_abort, issued,
+                                                            consumed, img, ib, chunk, ninvk, g);
+        } else {
+            ab = bwd_unit<NF, SCALE, SECOND, PE, kPathPixel>(bp, R, part, nrec, hdr, smem, bar, &s_abort, issued,
+                                                             consumed, img, ib, chunk, ninvk, g);
         }
-        // pixel runs for images whose offsets stay bounded (|r|_max from the
-        // emitter prep; NaN fails the test); the choice depends on the image only
-        bool runs = false;
-        if (bp.runs) {  // compared squared: no square-root call in the persistent loop
-            const double ks = g.k * g.run_span;
-            runs = ks * ks * (double)__uint_as_float(R.rmax2[img]) <= kGroupMaxPhase * kGroupMaxPhase;
-        }
-        const bool ab = runs ? bwd_unit<NF, SCALE, SECOND, PE, true>(bp, R, part, nrec, hdr, smem, bar, &s_abort,
-                                                                     issued, consumed, img, ib, chunk, ninvk)
-                             : bwd_unit<NF, SCALE, SECOND, PE, false>(bp, R, part, nrec, hdr, smem, bar, &s_abort,
-                                                                      issued, consumed, img, ib, chunk, ninvk);
         if (ab) {
             aborted = true;
             break;
@@ -518,14 +627,25 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(const __grid_con
 }
 
 // ---- chunk reduction + final gradients -------------------------------------
+// Per image path as in the adjoint kernels: the exact path's correction
+// acc[5] multiplies all of r, the paraxial one (x, y, 0); images outside the
+// split range get zero gradients (the call reports kErrGeometry).
 template <bool KAPPA>
 __global__ void bwd_reduce_kernel(const __grid_constant__ BwdParams bp, const float *__restrict__ part,
                                   int64_t nrec, const double *__restrict__ atoms, const void *__restrict__ amps,
-                                  int amp_dtype, double *__restrict__ grad_atoms, double *__restrict__ grad_amp) {
+                                  int amp_dtype, double *__restrict__ grad_atoms, double *__restrict__ grad_amp,
+                                  const GeomParams g, const uint32_t *__restrict__ rmax2) {
     const int b = blockIdx.y;
     const BwdImage d = bp.img[b];
+    const int path = split_path(g, rmax2[b], bp.runs != 0, true);
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < d.n; j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t r = d.rec + j;
+        const int64_t s = d.src + j;
+        if (path == kPathReject) {
+            reinterpret_cast<double4 *>(grad_atoms)[s] = make_double4(0.0, 0.0, 0.0, 0.0);
+            if (grad_amp) grad_amp[s] = 0.0;
+            continue;
+        }
         double acc[kBwdNAcc];
 #pragma unroll
         for (int a = 0; a < kBwdNAcc; ++a) acc[a] = 0.0;
@@ -534,27 +654,28 @@ __global__ void bwd_reduce_kernel(const __grid_constant__ BwdParams bp, const fl
 #pragma unroll
             for (int a = 0; a < kBwdNAcc; ++a) acc[a] += (double)src[a];
         }
-        const int64_t s = d.src + j;
         const double4 at = reinterpret_cast<const double4 *>(atoms)[s];
         double aj = 1.0;
         if (amps) aj = amp_dtype == IDIWF_F32 ? (double)static_cast<const float *>(amps)[s]
                                              : static_cast<const double *>(amps)[s];
-        // dL/dr = -a sum w Im z grad(phi) = a (Q - K (x, y, 0))
-        double gx = acc[2], gy = acc[3];
+        // dL/dr = -a sum w Im z grad(phi) [+ a sum Re z grad w] = a (Q - K (x, y, 0 or z))
+        double gx = acc[2], gy = acc[3], gz = acc[4];
         if (KAPPA) {
             gx -= acc[5] * at.x;
             gy -= acc[5] * at.y;
+            if (path == kPathExact) gz -= acc[5] * at.z;
         }
-        reinterpret_cast<double4 *>(grad_atoms)[s] = make_double4(aj * gx, aj * gy, aj * acc[4], -aj * acc[1]);
+        reinterpret_cast<double4 *>(grad_atoms)[s] = make_double4(aj * gx, aj * gy, aj * gz, -aj * acc[1]);
         if (grad_amp) grad_amp[s] = acc[0];
     }
 }
 
-template <int PE>
+template <int PE, bool EX>
 static void *bwd_kernel_for(bool nf, bool sc, bool so) {
-    if (nf) return sc ? (void *)bwd_split_kernel<true, true, false, PE> : (void *)bwd_split_kernel<true, false, false, PE>;
-    if (so) return sc ? (void *)bwd_split_kernel<false, true, true, PE> : (void *)bwd_split_kernel<false, false, true, PE>;
-    return sc ? (void *)bwd_split_kernel<false, true, false, PE> : (void *)bwd_split_kernel<false, false, false, PE>;
+    if (nf) return sc ? (void *)bwd_split_kernel<true, true, false, PE, EX> : (void *)bwd_split_kernel<true, false, false, PE, EX>;
+    if (EX) return nullptr;  // the exact adjoint is a near-field path
+    if (so) return sc ? (void *)bwd_split_kernel<false, true, true, PE, false> : (void *)bwd_split_kernel<false, false, true, PE, false>;
+    return sc ? (void *)bwd_split_kernel<false, true, false, PE, false> : (void *)bwd_split_kernel<false, false, false, PE, false>;
 }
 
 }  // namespace idiwf
@@ -614,6 +735,7 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
     double4 *rb64 = reinterpret_cast<double4 *>(ws + L.off_rb64);
     float4 *rbf = reinterpret_cast<float4 *>(ws + L.off_rbf);
     uint32_t *rmax2 = reinterpret_cast<uint32_t *>(ws + L.off_rmax);
+    float4 *px = reinterpret_cast<float4 *>(ws + L.off_px);
 
     const GeomParams g = make_geom(geom);
     const int npix = geom->nx * geom->ny;
@@ -652,7 +774,7 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
 
     const int pthreads = 256;
     bwd_pixel_geom_kernel<<<(L.npix_pad + pthreads - 1) / pthreads, pthreads, 0, stream>>>(
-        g, npix, L.npix_pad, bp.runs, p64, pf, pd, rb64, rbf);
+        g, npix, L.npix_pad, bp.runs, p64, pf, pd, rb64, rbf, px);
     IDIWF_CUDA_CHECK(cudaGetLastError());
     {
         const int64_t tot = (int64_t)L.npix_pad * batch->n_images;
@@ -674,27 +796,35 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
         bwd_emitter_prep_kernel<<<grid, 256, 0, stream>>>(bp, batch->atoms, e64, ef, w_mode, rmax2);
         IDIWF_CUDA_CHECK(cudaGetLastError());
     }
-    IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 2 * sizeof(uint32_t), stream));  // counter + error word
-    void *fn = pe == 8 ? bwd_kernel_for<8>(nf, sc, so) : bwd_kernel_for<4>(nf, sc, so);
-    const size_t smem = 2 * (size_t)std::max(kStagePixels, kStageRuns);
-    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int dev = 0, sms = 148, occ = 1;
+    // work counters (paraxial and exact kernels) and the error word
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 5 * sizeof(uint32_t), stream));
+    int64_t nrec = L.nrec;
+    BwdRecs R{e64, ef, p64, pf, pg, pd, rb64, rbf, px, rmax2};
+    void *args[] = {&bp, &R, &part, &nrec, &hdr, (void *)&g};
+    const size_t smem = 2 * (size_t)kStageMax;
+    int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    IDIWF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBwdThreads, smem));
-    const int grid = (int)std::min<int64_t>(bp.total_units, (int64_t)sms * std::max(occ, 1));
-    int64_t nrec = L.nrec;
-    BwdRecs R{e64, ef, p64, pf, pg, pd, rb64, rbf, rmax2};
-    void *args[] = {&bp, &R, &part, &nrec, &hdr, (void *)&g};
-    IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(kBwdThreads), args, smem, stream));
+    // the paraxial kernel (every call), then in the near field the exact kernel;
+    // each returns at once when it has no image
+    for (const bool exact : {false, true}) {
+        if (exact && !nf) continue;
+        void *fn = exact ? (pe == 8 ? bwd_kernel_for<8, true>(nf, sc, so) : bwd_kernel_for<4, true>(nf, sc, so))
+                         : (pe == 8 ? bwd_kernel_for<8, false>(nf, sc, so) : bwd_kernel_for<4, false>(nf, sc, so));
+        IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int occ = 1;
+        IDIWF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBwdThreads, smem));
+        const int grid = (int)std::min<int64_t>(bp.total_units, (int64_t)sms * std::max(occ, 1));
+        IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(kBwdThreads), args, smem, stream));
+    }
     {
         dim3 rgrid((unsigned)std::max<int64_t>(1, (max_blocks * eb + 255) / 256), batch->n_images);
         if (nf || so)
             bwd_reduce_kernel<true><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
-                                                                batch->amp_dtype, grad_atoms, grad_amp);
+                                                                batch->amp_dtype, grad_atoms, grad_amp, g, rmax2);
         else
             bwd_reduce_kernel<false><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
-                                                                 batch->amp_dtype, grad_atoms, grad_amp);
+                                                                 batch->amp_dtype, grad_atoms, grad_amp, g, rmax2);
         IDIWF_CUDA_CHECK(cudaGetLastError());
     }
     return IDIWF_OK;

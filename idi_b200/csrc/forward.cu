@@ -254,22 +254,32 @@ __device__ __forceinline__ PixelDir run_base(const GeomParams &g, int p0, int b,
 
 // One work unit (image, pixel tile[, emitter chunk]) of the split kernel.
 //
-// GROUP = false: every pixel forms its phase with its own FP64 DFMA chain.
-// GROUP = true:  one FP64 chain per run of kRun pixels forms the phase at the
+// PATH = kPathPixel: every pixel forms its phase with its own FP64 DFMA chain;
+//   the near-field term h (|r|^2 - s^2), h = k / (2|d|), is added in FP32.
+// PATH = kPathRuns: one FP64 chain per run of kRun pixels forms the phase at the
 //   middle of the run (fixed point, half-turn fold as below); pixel i adds the
 //   FP32 offset D_i . r with D_i = 2 pi (nq_i - nq_base) = -k (d_hat_i -
 //   d_hat_base), exact up to FP32 rounding because |D_i . r| <= kGroupMaxPhase
 //   (checked per image by the caller).  The near-field term uses
 //   s_i = d_hat_i . r = s_base - D_i.r / k.  The half-turn sign of the base
 //   applies to the whole run.
+// PATH = kPathExact (near field only): as kPathPixel, but the quadratic term
+//   k r_perp^2 / (2|d|) joins the FP64 chain (s = d_hat . r recovered from the
+//   chain as z - (t - Psi)/kp, so r_perp^2 = |r|^2 - s^2 in FP64), and the
+//   exact remainder R = h N (2s - N), N = r_perp^2 / (|d| + |d - r| - s), is
+//   added in FP32 (|d - r| from a reciprocal square root, which also gives the
+//   "scale" factor 1/|d - r|).
 // Returns true when a bounded wait gave up (the unit is abandoned).
-template <int PPT, bool NF, bool SCALE, bool SECOND, bool CHUNKED, bool GROUP>
+template <int PPT, bool NF, bool SCALE, bool SECOND, bool CHUNKED, int PATH>
 __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomParams &g, const SplitRecs &rec,
                                            void *__restrict__ out, int out_kind, WsHeader *__restrict__ hdr,
                                            double2 *__restrict__ partials, unsigned char *smem, uint64_t *bar,
                                            int *s_abort, uint32_t &issued, uint32_t &consumed, int img,
                                            int chunk, const ImageDesc &d, int p0, int tbeg, int tend,
                                            float *__restrict__ kahan) {
+    constexpr bool GROUP = PATH == kPathRuns;
+    constexpr bool EXACT = PATH == kPathExact;
+    static_assert(!EXACT || NF, "the exact path is a near-field path");
     constexpr int PH = PPT / 2;
     constexpr int NB = PPT >= kRun ? PPT / kRun : 1;  // runs (base phases) per thread
     constexpr int NQ = GROUP ? NB : PPT;
@@ -282,8 +292,10 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
 
     // ---- per-pixel constants (FP64 geometry) ----
     // cx/cy/cz: d_hat of each pixel, or (GROUP) its offset coefficients D_i
-    double nqx[NQ], nqy[NQ], nqz[NQ];
-    float2 cx[PH], cy[PH], cz[PH], hh[PH], iD[PH], iD2[PH];
+    // (EXACT) hq: the quadratic term's FP64 coefficient kp / (2|d|) in turns,
+    // dd: |d| in FP32
+    double nqx[NQ], nqy[NQ], nqz[NQ], hq[EXACT ? PPT : 1];
+    float2 cx[PH], cy[PH], cz[PH], hh[PH], iD[PH], iD2[PH], dd[EXACT ? PH : 1];
     float dbx[NB], dby[NB], dbz[NB];
     PixelDir base[NB];
     if (GROUP) {
@@ -319,12 +331,19 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
         }
         const float fh = (float)(-g.k * 0.5 * q.invD);  // -h, pairs with the negated w
         const float fi = (float)q.invD, fi2 = (float)(q.invD * q.invD);
+        float fd = 0.f;
+        if (EXACT) {
+            hq[i] = 0.5 * g.kp * q.invD;
+            fd = (float)(1.0 / q.invD);
+        }
         if (i & 1) {
             cx[i / 2].y = fx; cy[i / 2].y = fy; cz[i / 2].y = fz;
             hh[i / 2].y = fh; iD[i / 2].y = fi; iD2[i / 2].y = fi2;
+            if (EXACT) dd[i / 2].y = fd;
         } else {
             cx[i / 2].x = fx; cy[i / 2].x = fy; cz[i / 2].x = fz;
             hh[i / 2].x = fh; iD[i / 2].x = fi; iD2[i / 2].x = fi2;
+            if (EXACT) dd[i / 2].x = fd;
         }
     }
     const float ninvk = (float)(-1.0 / g.k);
@@ -433,6 +452,8 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
                     const float4 A = sA[j];
                     const float a1 = sC[j];
                     const float2 a2 = f2(a1, a1);
+                    double rr = 0.0;  // (EXACT) |r|^2 in FP64
+                    if (EXACT) rr = __fma_rn(r.z, r.z, __fma_rn(r.y, r.y, r.x * r.x));
 #pragma unroll
                     for (int q = 0; q < PH; ++q) {
                         uint32_t lo[2];
@@ -442,6 +463,11 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
                             double t = __fma_rn(nqx[i], r.x, r.w);
                             t = __fma_rn(nqy[i], r.y, t);
                             t = __fma_rn(nqz[i], r.z, t);
+                            if (EXACT) {
+                                // t - Psi = nq . r = kp (z - s) exactly (same binade)
+                                const double sd = __fma_rn(-g.ikp, t - r.w, r.z);
+                                t = __fma_rn(hq[i], __fma_rn(-sd, sd, rr), t);
+                            }
                             lo[e] = (uint32_t)__double2loint(t);
                         }
                         // phase = n*pi + x, x = pi*(u - 1.5) in [-pi/2, pi/2): u from
@@ -458,10 +484,22 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
                             float2 s = __fmul2_rn(cx[q], f2(A.x, A.x));
                             s = __ffma2_rn(cy[q], f2(A.y, A.y), s);
                             s = __ffma2_rn(cz[q], f2(A.z, A.z), s);
-                            // -h (s^2 - |r|^2) = h (|r|^2 - s^2)
-                            const float2 w2 = __ffma2_rn(s, s, f2(A.w, A.w));
-                            arg = __ffma2_rn(hh[q], w2, arg);
-                            if (SCALE) amp = __fmul2_rn(a2, __ffma2_rn(s, iD2[q], iD[q]));
+                            const float2 w2 = __ffma2_rn(s, s, f2(A.w, A.w));  // s^2 - |r|^2
+                            if (EXACT) {
+                                // L^2 = |d|(|d| - 2s) + |r|^2, N = r_perp^2 / (|d| + L - s),
+                                // R = h N (2s - N) = (-h)(-N)(2s - N)
+                                const float2 l2 = __ffma2_rn(__ffma2_rn(s, f2(-2.f, -2.f), dd[q]), dd[q],
+                                                             f2(-A.w, -A.w));
+                                const float2 y = f2(rsqrt_approx(l2.x), rsqrt_approx(l2.y));
+                                const float2 den = __ffma2_rn(s, f2(-1.f, -1.f), __ffma2_rn(l2, y, dd[q]));
+                                const float2 nN = __fmul2_rn(w2, f2(rcp_approx(den.x), rcp_approx(den.y)));
+                                arg = __ffma2_rn(__fmul2_rn(hh[q], nN), __ffma2_rn(s, f2(2.f, 2.f), nN), arg);
+                                if (SCALE) amp = __fmul2_rn(a2, y);
+                            } else {
+                                // -h (s^2 - |r|^2) = h (|r|^2 - s^2)
+                                arg = __ffma2_rn(hh[q], w2, arg);
+                                if (SCALE) amp = __fmul2_rn(a2, __ffma2_rn(s, iD2[q], iD[q]));
+                            }
                         } else if (SECOND) {
                             arg = __ffma2_rn(hh[q], f2(A.w, A.w), arg);  // (-h)(-(x^2+y^2))
                         }
@@ -545,25 +583,18 @@ __device__ __forceinline__ bool split_unit(const BatchParams &bp, const GeomPara
     return false;
 }
 
-// Whether image img of the launch takes the pixel-run path: runs allowed and
-// k * run_span * |r|_max <= kGroupMaxPhase (|r|_max from the prep kernel; NaN
-// fails the test).  Depends on the image only, so results do not depend on
-// the kernel shape.
-// (compared squared: a square root here would put a library call into the
-// persistent loop, which costs the run kernel 5 % of its speed)
-__device__ __forceinline__ bool image_uses_runs(const BatchParams &bp, const GeomParams &g, const SplitRecs &rec,
-                                                int img) {
-    const double ks = g.k * g.run_span;
-    return bp.groups && ks * ks * (double)__uint_as_float(rec.rmax2[img]) <= kGroupMaxPhase * kGroupMaxPhase;
-}
-
-// The split forward is two kernels launched back to back: GROUP = true takes
-// the images on the pixel-run path, GROUP = false the others, each from its
-// own work counter.  Without the per-pixel path's registers the run kernel
-// fits three 256-thread CTAs per SM (two for the per-pixel kernel).  A kernel
-// whose path no image of the launch takes returns at once.
-template <int PPT, bool NF, bool SCALE, bool SECOND, bool CHUNKED, bool GROUP>
-__global__ void __launch_bounds__(256, (PPT <= 4 ? (GROUP ? 3 : 2) : 1))
+// The split forward is up to three kernels launched back to back, one per
+// path (split_path: pixel runs, per-pixel FP64 phase, exact near field), each
+// taking the units of its own images from its own work counter.  Without the
+// per-pixel path's registers the run kernel fits three 256-thread CTAs per SM
+// (two for the others).  A kernel whose path no image of the launch takes
+// returns at once.  The per-pixel kernel, which every launch runs, reports
+// images outside the split kernels' range (kErrGeometry); no kernel takes them.
+// Every CTA classifies the images once, into shared memory: a square root or
+// the classifier's arithmetic in the persistent loop costs the run kernel
+// several percent of its speed.
+template <int PPT, bool NF, bool SCALE, bool SECOND, bool CHUNKED, int PATH>
+__global__ void __launch_bounds__(256, (PPT <= 4 ? (PATH == kPathRuns ? 3 : 2) : 1))
     fwd_split_kernel(const __grid_constant__ BatchParams bp, const GeomParams g, SplitRecs rec,
                      void *__restrict__ out, int out_kind, WsHeader *__restrict__ hdr,
                      uint64_t *__restrict__ cta_ns, double2 *__restrict__ partials) {
@@ -571,12 +602,19 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? (GROUP ? 3 : 2) : 1))
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int s_unit, s_abort;
+    __shared__ uint8_t s_path[kMaxImagesPerLaunch];
 
     const int tid = threadIdx.x;
     bool mine = false;
-    for (int i = tid; i < bp.n_images; i += blockDim.x) mine |= image_uses_runs(bp, g, rec, i) == GROUP;
+    for (int i = tid; i < bp.n_images; i += blockDim.x) {
+        const int path = split_path(g, rec.rmax2[i], bp.groups != 0, false);
+        s_path[i] = (uint8_t)path;
+        mine |= path == PATH;
+        if (PATH == kPathPixel && path == kPathReject && blockIdx.x == 0) record_error(&hdr->error, kErrGeometry);
+    }
     if (!__syncthreads_or(mine)) return;
-    uint32_t *counter = GROUP ? &hdr->work_counter : &hdr->work_counter2;
+    uint32_t *counter = PATH == kPathRuns ? &hdr->work_counter
+                                          : (PATH == kPathPixel ? &hdr->work_counter2 : &hdr->work_counter3);
 
     const uint64_t t_start = globaltimer_ns();
     if (tid == 0) {
@@ -601,8 +639,7 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? (GROUP ? 3 : 2) : 1))
             int u;
             for (;;) {
                 u = (int)atomicAdd(counter, 1u);
-                if (u >= bp.total_units || image_uses_runs(bp, g, rec, bp.order[u / ks / bp.tiles_per_image]) == GROUP)
-                    break;
+                if (u >= bp.total_units || s_path[bp.order[u / ks / bp.tiles_per_image]] == PATH) break;
             }
             s_unit = u;
         }
@@ -618,7 +655,7 @@ __global__ void __launch_bounds__(256, (PPT <= 4 ? (GROUP ? 3 : 2) : 1))
         // emitter tiles of this unit: the whole image, or one chunk of it
         const int tbeg = CHUNKED ? min(chunk * d.tpc, d.ntiles) : 0;
         const int tend = CHUNKED ? min(tbeg + d.tpc, d.ntiles) : d.ntiles;
-        if (split_unit<PPT, NF, SCALE, SECOND, CHUNKED, GROUP>(
+        if (split_unit<PPT, NF, SCALE, SECOND, CHUNKED, PATH>(
                 bp, g, rec, out, out_kind, hdr, partials, smem, bar, &s_abort, issued, consumed, img, chunk, d, p0,
                 tbeg, tend, reinterpret_cast<float *>(smem + 2 * (size_t)bp.te * kSplitRecBytes))) {
             aborted = true;
@@ -835,6 +872,7 @@ GeomParams make_geom(const idiwf_geom *g) {
     p.detz = g->detz;
     p.k = g->k;
     p.kp = g->k * kInvTwoPi;
+    p.ikp = kTwoPi / g->k;
     p.offx = g->offset[0];
     p.offy = g->offset[1];
     for (int i = 0; i < 9; ++i) p.rot[i] = g->has_rot ? g->rot[i] : (i % 4 == 0 ? 1.0 : 0.0);
@@ -846,6 +884,10 @@ GeomParams make_geom(const idiwf_geom *g) {
     const double h = nn > 0 ? std::fabs(g->detz * (c2[0] * n[0] + c2[1] * n[1] + c2[2] * n[2])) / nn : 0.0;
     const double half = 0.5 * (kRun - 1) * std::fabs(g->pixelsize) * std::sqrt(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
     p.run_span = h > 0 ? half / h : INFINITY;
+    p.dmin = h;
+    p.inv_dmin2 = h > 0 ? 1.0 / (h * h) : INFINITY;
+    const double c3 = h > 0 ? kNfBoundC * g->k / (h * h) : INFINITY;
+    p.nf_c3 = c3 * c3;
     return p;
 }
 
@@ -975,27 +1017,35 @@ static size_t forward_ws_bytes(const idiwf_geom *g, const idiwf_batch *b, int pr
 
 // Dynamic shared memory of a forward kernel: two stages of emitter records,
 // plus for the pixel-run kernel the Kahan totals (4 floats per pixel of the CTA).
-static size_t fwd_smem(int precision, const LaunchShape &s, bool group) {
+static size_t fwd_smem(int precision, const LaunchShape &s, int path) {
     if (precision != IDIWF_SPLIT) return 2 * (size_t)s.te * kDoubleRecBytes;
-    return 2 * (size_t)s.te * kSplitRecBytes + (group ? (size_t)16 * s.ppt * s.threads : 0);
+    return 2 * (size_t)s.te * kSplitRecBytes + (path == kPathRuns ? (size_t)16 * s.ppt * s.threads : 0);
 }
 
 // kernel table ---------------------------------------------------------------
-template <int PPT, bool CH, bool GR>
+template <int PPT, bool CH, int PATH>
 static void *split_kernel_for3(int flags) {
     const bool nf = flags & IDIWF_NF, sc = flags & IDIWF_SCALE, so = flags & IDIWF_SECONDORDER;
-    if (nf) return sc ? (void *)fwd_split_kernel<PPT, true, true, false, CH, GR>
-                      : (void *)fwd_split_kernel<PPT, true, false, false, CH, GR>;
-    if (so) return sc ? (void *)fwd_split_kernel<PPT, false, true, true, CH, GR>
-                      : (void *)fwd_split_kernel<PPT, false, false, true, CH, GR>;
-    return sc ? (void *)fwd_split_kernel<PPT, false, true, false, CH, GR>
-              : (void *)fwd_split_kernel<PPT, false, false, false, CH, GR>;
+    if (nf) return sc ? (void *)fwd_split_kernel<PPT, true, true, false, CH, PATH>
+                      : (void *)fwd_split_kernel<PPT, true, false, false, CH, PATH>;
+    if (PATH == kPathExact) return nullptr;  // near field only
+    constexpr int P = PATH == kPathExact ? kPathPixel : PATH;
+    if (so) return sc ? (void *)fwd_split_kernel<PPT, false, true, true, CH, P>
+                      : (void *)fwd_split_kernel<PPT, false, false, true, CH, P>;
+    return sc ? (void *)fwd_split_kernel<PPT, false, true, false, CH, P>
+              : (void *)fwd_split_kernel<PPT, false, false, false, CH, P>;
 }
-// group: the pixel-run kernel (true) or the per-pixel kernel (false)
+// path: kPathRuns, kPathPixel or kPathExact (nullptr for the exact path
+// without "nf")
+template <int PPT, bool CH>
+static void *split_kernel_for2(int flags, int path) {
+    if (path == kPathRuns) return split_kernel_for3<PPT, CH, kPathRuns>(flags);
+    if (path == kPathExact) return split_kernel_for3<PPT, CH, kPathExact>(flags);
+    return split_kernel_for3<PPT, CH, kPathPixel>(flags);
+}
 template <int PPT>
-static void *split_kernel_for(int flags, bool chunked, bool group) {
-    if (chunked) return group ? split_kernel_for3<PPT, true, true>(flags) : split_kernel_for3<PPT, true, false>(flags);
-    return group ? split_kernel_for3<PPT, false, true>(flags) : split_kernel_for3<PPT, false, false>(flags);
+static void *split_kernel_for(int flags, bool chunked, int path) {
+    return chunked ? split_kernel_for2<PPT, true>(flags, path) : split_kernel_for2<PPT, false>(flags, path);
 }
 template <int PPT>
 static void *double_kernel_for(int flags) {
@@ -1007,11 +1057,11 @@ static void *double_kernel_for(int flags) {
     if (so) return sc ? (void *)fwd_double_kernel<PPT, false, true, true> : (void *)fwd_double_kernel<PPT, false, false, true>;
     return sc ? (void *)fwd_double_kernel<PPT, false, true, false> : (void *)fwd_double_kernel<PPT, false, false, false>;
 }
-static void *kernel_for(int precision, int ppt, int flags, bool chunked, bool group = true) {
+static void *kernel_for(int precision, int ppt, int flags, bool chunked, int path = kPathRuns) {
     if (precision == IDIWF_SPLIT) {
-        if (ppt == 2) return split_kernel_for<2>(flags, chunked, group);
-        if (ppt == 4) return split_kernel_for<4>(flags, chunked, group);
-        return split_kernel_for<8>(flags, chunked, group);
+        if (ppt == 2) return split_kernel_for<2>(flags, chunked, path);
+        if (ppt == 4) return split_kernel_for<4>(flags, chunked, path);
+        return split_kernel_for<8>(flags, chunked, path);
     }
     if (ppt == 1) return double_kernel_for<1>(flags);
     if (ppt == 2) return double_kernel_for<2>(flags);
@@ -1125,13 +1175,15 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
                                                                      split_recs_bytes(nrec))
                                        : nullptr;
         void *args[] = {&bp, (void *)&g, &rec, &out_chunk, &out_kind, &hdr, &cta_ns, &partials};
-        // the pixel-run kernel, then the per-pixel kernel for the images beyond
-        // the runs' bound (each returns at once when it has no image)
-        IDIWF_CUDA_CHECK(cudaMemsetAsync(&hdr->work_counter2, 0, sizeof(uint32_t), stream));
-        for (const bool group : {true, false}) {
-            if (group && !bp.groups) continue;
-            void *fn = kernel_for(precision, s.ppt, geom->flags, ksplit > 1, group);
-            const size_t smem = fwd_smem(precision, s, group);
+        // the pixel-run kernel, the per-pixel kernel for the images beyond the
+        // runs' bound, and in the near field the exact kernel (each returns at
+        // once when it has no image)
+        IDIWF_CUDA_CHECK(cudaMemsetAsync(&hdr->work_counter2, 0, 2 * sizeof(uint32_t), stream));  // + work_counter3
+        for (const int path : {kPathRuns, kPathPixel, kPathExact}) {
+            if (path == kPathRuns && !bp.groups) continue;
+            if (path == kPathExact && !(geom->flags & IDIWF_NF)) continue;
+            void *fn = kernel_for(precision, s.ppt, geom->flags, ksplit > 1, path);
+            const size_t smem = fwd_smem(precision, s, path);
             int grid = 0;
             idiwf_status st = grid_for(fn, smem, grid);
             if (st != IDIWF_OK) return st;
@@ -1156,7 +1208,7 @@ static idiwf_status launch_chunk(const idiwf_geom *geom, const idiwf_batch *b, i
         DoubleRecs rec = double_recs(ws, nrec);
         void *args[] = {&bp, (void *)&g, &rec, &out_chunk, &out_kind, &hdr, &cta_ns};
         void *fn = kernel_for(precision, s.ppt, geom->flags, false);
-        const size_t smem = fwd_smem(precision, s, false);
+        const size_t smem = fwd_smem(precision, s, kPathPixel);
         int grid = 0;
         idiwf_status st = grid_for(fn, smem, grid);
         if (st != IDIWF_OK) return st;
@@ -1256,7 +1308,7 @@ extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *ba
                 for (int te : {256, 512}) {
                     LaunchShape c{th, ppt, te, 1};
                     void *fn = kernel_for(precision, ppt, geom->flags, false);
-                    const size_t smem = fwd_smem(precision, c, true);
+                    const size_t smem = fwd_smem(precision, c, kPathRuns);
                     if (ensure_smem(fn, smem) != IDIWF_OK) continue;
                     c.ctas_per_sm = std::min(8, resident_ctas(fn, th, smem));
                     cands.push_back(c);
@@ -1277,7 +1329,7 @@ extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *ba
         if (forward_ws_bytes(geom, batch, precision, s) > workspace_bytes) continue;
         {  // more CTAs per SM than fit would only repeat a smaller candidate
             void *fn = kernel_for(precision, s.ppt, geom->flags, false);
-            const size_t smem = fwd_smem(precision, s, true);
+            const size_t smem = fwd_smem(precision, s, kPathRuns);
             if (ensure_smem(fn, smem) == IDIWF_OK && s.ctas_per_sm > resident_ctas(fn, s.threads, smem)) continue;
         }
         st = forward_impl(geom, batch, precision, out_kind, out, workspace, workspace_bytes, s, stream);
@@ -1323,10 +1375,13 @@ extern "C" idiwf_status idiwf_tune(const idiwf_geom *geom, const idiwf_batch *ba
 // Some hosts of this library cannot call cudaMalloc at all: code that runs
 // inside another framework's memory pool or allocator hooks, inside a stream
 // capture they do not own, or in plug-ins whose host forbids device
-// allocation.  For them this entry point keeps its scratch (work counter,
+// allocation.  For them this entry point keeps its scratch (work counters,
 // error word, per-CTA timing, emitter tile records) in one file-scope device
-// array of fixed size, so the caller passes only inputs and outputs and
-// nothing is allocated -- neither device memory nor host heap memory.
+// array of fixed size, so the caller passes only inputs and outputs and no
+// device memory is allocated.  The host side uses no heap either: the launch
+// descriptor is a static buffer, used under a mutex for the few microseconds
+// it takes to build it and enqueue the launches (kernel arguments are copied
+// at launch).
 // ---------------------------------------------------------------------------
 namespace idiwf {
 
@@ -1335,17 +1390,17 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[IDIWF_NOALLOC_S
 constexpr int kNoAllocMaxDevices = 64;
 static std::mutex g_noalloc_mu;
 static void *g_noalloc_ptr[kNoAllocMaxDevices];
+static BatchParams g_noalloc_bp;  // guarded by g_noalloc_mu
 
 // Device address of the scratch array on the current device.  The name
 // g_noalloc_scratch in host code is only a host-side stand-in, so the
 // address is looked up once per device (with that device current) and
-// cached.
-static idiwf_status noalloc_scratch(void **ptr) {
+// cached.  The caller holds g_noalloc_mu.
+static idiwf_status noalloc_scratch_locked(void **ptr) {
     int dev = 0;
     IDIWF_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices)
         return set_error(IDIWF_ERR_UNSUPPORTED, "idiwf_forward_noalloc: device ordinal out of range");
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_ptr[dev]) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -1370,7 +1425,8 @@ extern "C" idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiw
         return set_error(IDIWF_ERR_UNSUPPORTED, "idiwf_forward_noalloc: at most 512 images per call");
 
     const LaunchShape s{256, 4, 256, 2};
-    static thread_local BatchParams bp;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    BatchParams &bp = g_noalloc_bp;
     std::memset(&bp, 0, sizeof(bp));
     const int npix = geom->nx * geom->ny;
     const int tile_px = s.threads * s.ppt;
@@ -1407,15 +1463,15 @@ extern "C" idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiw
     }
 
     void *ws = nullptr;
-    if ((st = noalloc_scratch(&ws)) != IDIWF_OK) return st;
+    if ((st = noalloc_scratch_locked(&ws)) != IDIWF_OK) return st;
     WsHeader *hdr = static_cast<WsHeader *>(ws);
     uint64_t *cta_ns = reinterpret_cast<uint64_t *>(static_cast<char *>(ws) + kWsTimingOffset);
     SplitRecs rec = split_recs(ws, nrec);
     const GeomParams g = make_geom(geom);
 
-    // every call starts from a zero work counter and error word; the records
-    // are rewritten in full by the prep kernel
-    IDIWF_CUDA_CHECK(cudaMemsetAsync(ws, 0, 4 * sizeof(uint32_t), stream));  // both work counters, error word
+    // every call starts from zero work counters and a zero error word; the
+    // records are rewritten in full by the prep kernel
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(ws, 0, 6 * sizeof(uint32_t), stream));  // counters 1-3, error word, n_ctas
     IDIWF_CUDA_CHECK(cudaMemsetAsync(rec.rmax2, 0, sizeof(uint32_t) * bp.n_images, stream));
     if (max_tiles > 0) {
         const int w_mode = (geom->flags & IDIWF_NF) ? 1 : ((geom->flags & IDIWF_SECONDORDER) ? 2 : 0);
@@ -1425,17 +1481,37 @@ extern "C" idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiw
                                                      max_abs, rec, &hdr->error);
         IDIWF_CUDA_CHECK(cudaGetLastError());
     }
-    const int grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * s.ctas_per_sm),
-                                            kMaxCtas);
-    double2 *no_partials = nullptr;  // bp.ksplit == 0: the kernel writes the outputs itself
+    double2 *no_partials = nullptr;  // bp.ksplit == 0: the kernels write the outputs themselves
     void *args[] = {&bp, (void *)&g, &rec, &out, &out_kind, &hdr, &cta_ns, &no_partials};
-    // the pixel-run kernel, then the per-pixel kernel (each returns at once without images)
-    for (const bool group : {true, false}) {
-        if (group && !bp.groups) continue;
-        void *fn = split_kernel_for<4>(geom->flags, false, group);
-        const size_t smem = fwd_smem(IDIWF_SPLIT, s, group);
+    // the pixel-run, per-pixel and (near field) exact kernels, each returning
+    // at once without images; the persistent grid is clamped to the CTAs that
+    // fit at once, as in idiwf_forward
+    for (const int path : {kPathRuns, kPathPixel, kPathExact}) {
+        if (path == kPathRuns && !bp.groups) continue;
+        if (path == kPathExact && !(geom->flags & IDIWF_NF)) continue;
+        void *fn = split_kernel_for<4>(geom->flags, false, path);
+        const size_t smem = fwd_smem(IDIWF_SPLIT, s, path);
         IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int occ = 0;
+        IDIWF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, s.threads, smem));
+        const int per_sm = std::max(1, std::min(s.ctas_per_sm, occ));
+        const int grid = (int)std::min<int64_t>(std::min<int64_t>(bp.total_units, (int64_t)sm_count() * per_sm),
+                                                kMaxCtas);
         IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(s.threads), args, smem, stream));
     }
     return IDIWF_OK;
+}
+
+// Error word of the most recent idiwf_forward_noalloc call on the current
+// device, read from the static scratch into a stack variable (no allocation;
+// the read waits for `stream`).  Same bits and statuses as
+// idiwf_workspace_error.
+extern "C" idiwf_status idiwf_forward_noalloc_error(cudaStream_t stream) {
+    void *ws = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        idiwf_status st = noalloc_scratch_locked(&ws);
+        if (st != IDIWF_OK) return st;
+    }
+    return idiwf_workspace_error(ws, stream);
 }

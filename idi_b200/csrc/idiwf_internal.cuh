@@ -40,7 +40,9 @@ struct WsHeader {
     uint32_t error;         // device error word (IDIWF_ERR_* bit set)
     uint32_t n_ctas;        // CTAs of the last forward launch
     uint32_t work_counter2; // second work queue (split forward: per-pixel kernel)
-    uint64_t pad[30];
+    uint32_t work_counter3; // third work queue (split forward: exact near-field kernel)
+    uint32_t pad32;
+    uint64_t pad[29];
 };
 static_assert(sizeof(WsHeader) == 256, "workspace header is 256 bytes");
 constexpr int kMaxCtas = 4096;                       // per-CTA timing slots
@@ -49,6 +51,9 @@ constexpr size_t kWsDataOffset = 256 + 8 * kMaxCtas; // 256-aligned
 constexpr uint32_t kErrTimeout = 1u;
 constexpr uint32_t kErrRange = 2u;
 constexpr uint32_t kErrValue = 4u;  // invalid input value (negative, NaN, zero-sum, count mismatch)
+// near-field image outside the split kernels' range (emitters too far out
+// for the exact remainder to stay below kExactMaxPhase, or |r| > |d| / 4)
+constexpr uint32_t kErrGeometry = 8u;
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -64,15 +69,50 @@ constexpr int kRun = 4;
 // the base angle's range.
 constexpr double kGroupMaxPhase = 1.0;
 
+// Near field in the split kernels.  With s = d_hat . r, r_perp^2 = |r|^2 - s^2
+// and L = |d - r|, the path difference is exactly
+//   |d - r| - |d| = -s + N,   N = r_perp^2 / (|d| + L - s)
+// (no cancellation: the denominator is about 2|d|).  The split kernels use
+// N ~ r_perp^2 / (2|d|) where the dropped remainder
+//   R = N - r_perp^2/(2|d|) = r_perp^2 (2s - N) / (2|d| (|d| + L - s))
+// stays below kNfPhaseTol (radians, times k) for every emitter of the image.
+// |R| <= r^3/(3 sqrt3 D (D-r)) + r^4/(8 D (D-r)^2) for |r| <= r, |d| >= D; with
+// r <= D/4 this is at most kNfBoundC r^3 / D^2, which the classifier below
+// evaluates squared (no square root in the kernels' prologues).
+// Images above the tolerance take the exact near-field kernel: the quadratic
+// term k r_perp^2 / (2|d|) joins the FP64 turn chain and the remainder R is
+// added in FP32 from the exact expression, which needs k|R| <= kExactMaxPhase
+// so that FP32 keeps it to ~1e-7 rad; beyond that (or |r| > D/4) the image is
+// rejected (kErrGeometry).
+constexpr double kNfPhaseTol = 1e-7;
+constexpr double kExactMaxPhase = 2.0;
+constexpr double kNfBoundC = 0.3122;
+// "scale": the per-pixel path's 1/|d - r| ~ (1 + s/|d|)/|d| is off by at most
+// (r/D)^2 relative; above kNfScaleRho2 the image takes the exact kernel
+// (which forms 1/|d - r| with a reciprocal square root).
+constexpr double kNfScaleRho2 = 1e-7;
+// The adjoint's paraxial near-field gradient -q + k (x, y, 0)/|d| is off by
+// about r/D relative; above kAdjRho the image takes the exact adjoint.
+constexpr double kAdjRho2 = 1e-12;
+
+// Paths of the split kernels, chosen per image from |r|_max.
+constexpr int kPathPixel = 0;   // FP64 phase per pair, second-order near field
+constexpr int kPathRuns = 1;    // FP64 phase per run of kRun pixels + FP32 offsets
+constexpr int kPathExact = 2;   // near field with the exact remainder (per pair)
+constexpr int kPathReject = 3;  // outside the split kernels' range
+
 struct GeomParams {
     int32_t nx, ny, flags, has_rot;
-    double pixelsize, detz, k, kp;  // kp = k / 2pi
+    double pixelsize, detz, k, kp, ikp;  // kp = k / 2pi, ikp = 1 / kp
     double offx, offy;
     double rot[9];
     // largest |d_hat_i - d_hat_base| between a pixel of a run of 4 along a row
     // and the run's middle: half the run's length over the detector plane's
     // distance from the origin (the angle a segment subtends bounds the chord)
     double run_span;
+    // distance of the detector plane from the origin (a lower bound on every
+    // pixel's |d|) and the classifier's constants derived from it
+    double dmin, inv_dmin2, nf_c3;  // nf_c3 = (kNfBoundC k / dmin^2)^2
 };
 
 struct ImageDesc {
@@ -235,6 +275,39 @@ __device__ __forceinline__ void pixel_time(const GeomParams &g, int ix, int iy, 
 }
 
 __device__ __forceinline__ void record_error(uint32_t *err, uint32_t bit) { atomicOr(err, bit); }
+
+// Path of one image in the split kernels, from the image's max |r|^2 (float
+// bits, rounded up).  `runs`: pixel runs allowed in this launch; `adjoint`:
+// the backward's paraxial-gradient bound applies as well.  The choice depends
+// on the image and the geometry only, so results do not depend on the kernel
+// shape.  Squared comparisons throughout; a NaN |r|^2 fails the run test and
+// skips the near-field tests (NaN coordinates are reported by the range check).
+__device__ __forceinline__ int split_path(const GeomParams &g, uint32_t r2bits, bool runs, bool adjoint) {
+    const double r2 = (double)__uint_as_float(r2bits);
+    if ((g.flags & IDIWF_NF) && r2 > 0.0) {
+        const double rho2 = r2 * g.inv_dmin2;
+        const double t2 = g.nf_c3 * r2 * r2 * r2;  // (bound on k |R|)^2
+        if (!(rho2 <= 1.0 / 16.0 && t2 <= kExactMaxPhase * kExactMaxPhase)) return kPathReject;
+        const bool paraxial = t2 <= kNfPhaseTol * kNfPhaseTol &&
+                              (!(g.flags & IDIWF_SCALE) || rho2 <= kNfScaleRho2) && (!adjoint || rho2 <= kAdjRho2);
+        if (!paraxial) return kPathExact;
+    }
+    const double ks = g.k * g.run_span;
+    return (runs && ks * ks * r2 <= kGroupMaxPhase * kGroupMaxPhase) ? kPathRuns : kPathPixel;
+}
+
+// Reciprocal square root and reciprocal on the MUFU pipe (relative error a
+// few 2^-23; flush-to-zero, for operands of the size of detector distances).
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 
 #endif  // __CUDACC__
 

@@ -27,6 +27,7 @@ __all__ = [
     "tune",
     "microbench",
     "workspace_error",
+    "ErrorWord",
     "photons",
     "chargesharing",
     "emitters",
@@ -210,6 +211,31 @@ def _check_amplitudes(amplitudes, atoms):
     return amplitudes
 
 
+class ErrorWord:
+    """Device-side accumulator of the kernels' error words, checked later.
+
+    The library records device-side errors (emitters out of the split range, a
+    near-field image outside the split kernels' range, a bounded wait that ran
+    out) in the workspace header, and every call clears them.  Calls given an
+    ``ErrorWord`` OR their word into this 256-byte device buffer (laid out like
+    a workspace header) on their stream, without synchronising; :meth:`check`
+    reads it once (synchronises) and raises with the library's message."""
+
+    def __init__(self, device):
+        self.device = torch.device(device)
+        self.buf = torch.zeros(256, dtype=torch.uint8, device=self.device)
+        self._word = self.buf[4:8].view(torch.int32)
+
+    def collect(self, workspace: torch.Tensor):
+        self._word.bitwise_or_(workspace[4:8].view(torch.int32))
+
+    def check(self):
+        lib = nat.load()
+        st = lib.idiwf_workspace_error(ctypes.c_void_p(self.buf.data_ptr()), _stream(self.device))
+        self._word.zero_()
+        nat.check(st)
+
+
 def forward(
     atoms: torch.Tensor,
     offsets: Sequence[int],
@@ -220,9 +246,11 @@ def forward(
     out: Optional[torch.Tensor] = None,
     config=None,
     role: str = "main",
+    errors: Optional[ErrorWord] = None,
 ) -> torch.Tensor:
     """Direct sum of a batch of images: ``atoms`` (N,4) float64 on the GPU,
-    image b = rows ``offsets[b]:offsets[b+1]``.  Returns (B, nx, ny)."""
+    image b = rows ``offsets[b]:offsets[b+1]``.  Returns (B, nx, ny).
+    With ``errors``, the call's device error word is added to it."""
     lib = nat.load()
     _require_cuda(atoms, "atoms", torch.float64)
     if atoms.ndim != 2 or atoms.shape[1] != 4:
@@ -247,6 +275,8 @@ def forward(
     nat.check(lib.idiwf_forward(ctypes.byref(geom), ctypes.byref(batch), precision, out_kind,
                                 ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
                                 cfg_p, _stream(dev)))
+    if errors is not None:
+        errors.collect(ws)
     return out
 
 
@@ -280,6 +310,11 @@ def cta_times(device=None, role="main") -> np.ndarray:
     return np.frombuffer(buf, dtype=np.uint64, count=n.value).copy()
 
 
+def backward_workspace_error(device=None):
+    """Raise if the last adjoint call recorded a device-side error (synchronises)."""
+    workspace_error(device, "backward")
+
+
 def workspace_error(device=None, role="main"):
     """Raise if a kernel recorded a device-side error in the workspace (synchronises)."""
     lib = nat.load()
@@ -297,10 +332,12 @@ def backward(
     amplitudes: Optional[torch.Tensor] = None,
     want_amp: bool = True,
     config=None,
+    errors: Optional[ErrorWord] = None,
 ):
     """Adjoint of I = |E|^2: returns (grad_atoms (N,4) [dx,dy,dz,dphase], grad_amp (N) or None).
     ``config``: ``pixels_per_thread`` = emitters per thread (4 or 8), ``pixel_groups`` = -1 for an
-    FP64 phase per pair instead of per run of 4 pixels."""
+    FP64 phase per pair instead of per run of 4 pixels.  With ``errors``, the call's device
+    error word is added to it."""
     lib = nat.load()
     _require_cuda(atoms, "atoms", torch.float64)
     _require_cuda(field, "field", torch.complex128)
@@ -324,6 +361,8 @@ def backward(
                                  ctypes.c_void_p(grad_intensity.data_ptr()), ctypes.c_void_p(grad_atoms.data_ptr()),
                                  ctypes.c_void_p(grad_amp.data_ptr()) if grad_amp is not None else None,
                                  ctypes.c_void_p(ws.data_ptr()), ws.numel(), cfg_p, _stream(dev)))
+    if errors is not None:
+        errors.collect(ws)
     return grad_atoms, grad_amp
 
 

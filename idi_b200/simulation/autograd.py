@@ -6,7 +6,9 @@
     loss.backward()        # pos.grad, phase.grad, amplitudes.grad
 
 Forward and adjoint both run the split-precision kernels (FP64 phase in
-turns, FP32 sincos and sums).  ``pos`` (N,3) and ``phase`` (N,) are float64
+turns, FP32 sincos and sums).  Device-side errors of both (a near-field
+geometry outside the split range, emitters out of range) raise at the end of
+the backward pass.  ``pos`` (N,3) and ``phase`` (N,) are float64
 CUDA tensors; ``amplitudes`` (N,) float32/float64 or None.  Several images
 with uneven emitter counts can be stacked with ``offsets``.
 """
@@ -30,8 +32,10 @@ class WavefieldIntensity(torch.autograd.Function):
         atoms = torch.cat([pos.detach().to(torch.float64), phase.detach().to(torch.float64).reshape(-1, 1)], 1)
         atoms = atoms.contiguous()
         amps = None if amplitudes is None else amplitudes.detach().contiguous()
-        E = _core.forward(atoms, offsets, geom, nat.SPLIT, nat.OUT_C128, amplitudes=amps)
+        errors = _core.ErrorWord(atoms.device)
+        E = _core.forward(atoms, offsets, geom, nat.SPLIT, nat.OUT_C128, amplitudes=amps, errors=errors)
         I = E.real.square() + E.imag.square()
+        ctx.errors = errors
         ctx.geom = geom
         ctx.offsets = offsets
         ctx.has_amp = amps is not None
@@ -49,7 +53,9 @@ class WavefieldIntensity(torch.autograd.Function):
         amps = saved[2] if ctx.has_amp else None
         want_amp = bool(ctx.needs_input_grad[2])
         ga, gamp = _core.backward(atoms, ctx.offsets, ctx.geom, E, grad_I.contiguous().to(torch.float64), amps,
-                                  want_amp=want_amp)
+                                  want_amp=want_amp, errors=ctx.errors)
+        # device-side errors of the forward and the adjoint (one synchronisation per step)
+        ctx.errors.check()
         gpos = ga[:, :3] if ctx.needs_input_grad[0] else None
         gphase = ga[:, 3] if ctx.needs_input_grad[1] else None
         gamp_out = gamp.to(ctx.amp_dtype) if (want_amp and gamp is not None) else None

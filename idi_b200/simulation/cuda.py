@@ -141,6 +141,8 @@ def simulate_gen(
     batch = max(1, int(batch))
     stager = _Stager(N, batch, dev)
 
+    errors = _core.ErrorWord(dev)
+
     def _gen():
         count = 0
         while count < maximg:
@@ -148,7 +150,8 @@ def simulate_gen(
             d_atoms = stager.fill(simobject, nb)
             amps = _upload_amps(_amplitude_rows(amplitudes, nb, N, count), dev)
             offsets = np.arange(nb + 1, dtype=np.int64) * N
-            E = _core.forward(d_atoms, offsets, geom, precision, out_kind, amplitudes=amps)
+            E = _core.forward(d_atoms, offsets, geom, precision, out_kind, amplitudes=amps, errors=errors)
+            errors.check()  # device-side errors of this batch (synchronises)
             if not returngpu:
                 E = E.cpu().numpy()
             for i in range(nb):
@@ -182,6 +185,9 @@ def simulate(
     With host output, the images are processed in up to four chunks whose
     device-to-host copies (into pinned staging, on a second stream) overlap
     the next chunk's kernel.  Ctrl-C returns the images finished so far.
+    Device-side errors (split-precision emitters out of range, a near-field
+    geometry outside the split range) raise ``IdiwfError`` once all images are
+    done.
     """
     Ndet, geom, precision, out_kind = _setup(simobject, Ndet, pixelsize, detz, k, settings, detangles, detoffset)
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -198,16 +204,19 @@ def simulate(
     if returngpu:
         result = torch.empty((Nimg, Ndet[0], Ndet[1]), dtype=torch.complex128, device=dev)
         stager = _Stager(N, chunk, dev)
+        errors = _core.ErrorWord(dev)
         try:
             while done < Nimg:
                 nb = min(chunk, Nimg - done)
                 d_atoms = stager.fill(simobject, nb)
                 amps = _upload_amps(_amplitude_rows(amplitudes, nb, N, done), dev)
                 offsets = np.arange(nb + 1, dtype=np.int64) * N
-                result[done:done + nb] = _core.forward(d_atoms, offsets, geom, precision, out_kind, amplitudes=amps)
+                result[done:done + nb] = _core.forward(d_atoms, offsets, geom, precision, out_kind, amplitudes=amps,
+                                                       errors=errors)
                 done += nb
                 if verbose:
                     print(done, end=". ", flush=True)
+            errors.check()
             return result
         except KeyboardInterrupt:
             if verbose:
@@ -242,6 +251,7 @@ def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, 
     done = 0
 
     finished = [0]
+    errors = _core.ErrorWord(dev)
 
     def _collect(ps, pstart, pn):
         ev_copied[ps].synchronize()
@@ -266,7 +276,8 @@ def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, 
             amps = _upload_amps(_amplitude_rows(amplitudes, nb, N, done), dev)
             offsets = np.arange(nb + 1, dtype=np.int64) * N
             compute.wait_event(ev_copied[slot])  # device buffers of this slot copied out
-            _core.forward(d_atoms, offsets, geom, precision, out_kind, amplitudes=amps, out=d_out[slot][:nb])
+            _core.forward(d_atoms, offsets, geom, precision, out_kind, amplitudes=amps, out=d_out[slot][:nb],
+                          errors=errors)
             src = d_out[slot][:nb] if post is None else post(d_out[slot][:nb], done, slot)
             if h_out[slot] is None:
                 per = src[0].numel() * src.element_size()
@@ -285,6 +296,7 @@ def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, 
             done += nb
             i += 1
         _collect(*pending)
+        errors.check()
         return finished[0] if sink is not None else result
     except KeyboardInterrupt:
         if verbose:
@@ -412,15 +424,18 @@ def simulate_photons(
         result = torch.empty((Nimg, Ndet[0], Ndet[1]), dtype=final, device=dev)
         stager = _Stager(N, chunk, dev)
         d_int = torch.empty((chunk, Ndet[0], Ndet[1]), dtype=torch.float64, device=dev)
+        errors = _core.ErrorWord(dev)
         done = 0
         while done < Nimg:
             nb = min(chunk, Nimg - done)
             d_atoms = stager.fill(simobject, nb)
             amps = _upload_amps(_amplitude_rows(amplitudes, nb, N, done), dev)
             offsets = np.arange(nb + 1, dtype=np.int64) * N
-            _core.forward(d_atoms, offsets, geom, precision, nat.OUT_I64, amplitudes=amps, out=d_int[:nb])
+            _core.forward(d_atoms, offsets, geom, precision, nat.OUT_I64, amplitudes=amps, out=d_int[:nb],
+                          errors=errors)
             result[done:done + nb] = post(d_int[:nb], done, 0)
             done += nb
+        errors.check()
         _core.workspace_error(dev, "photons")
         return result
     res_np = torch.empty(0, dtype=final).numpy().dtype
@@ -468,4 +483,7 @@ def simulate_batch(
         kind = nat.OUT_I64
     else:
         kind = nat.OUT_C64 if c64 else nat.OUT_C128
-    return _core.forward(atoms, offsets, geom, precision, kind, amplitudes=amps, config=config)
+    errors = _core.ErrorWord(dev)
+    res = _core.forward(atoms, offsets, geom, precision, kind, amplitudes=amps, config=config, errors=errors)
+    errors.check()
+    return res

@@ -121,6 +121,15 @@ size_t idiwf_forward_workspace_size(const idiwf_geom *geom, const idiwf_batch *b
  * idi/simulation/cuda.py:88-136; IDIWF_DOUBLE follows the FP64 CPU kernel
  * idi/simulation/cpu.py:68-107.  Amplitudes (per-emitter a_j) and batching
  * have no reference counterpart.
+ *
+ * IDIWF_SPLIT in the near field (IDIWF_NF) picks a path per image from the
+ * image's largest |r| and the detector plane's distance D from the origin:
+ * the second-order path difference where the dropped remainder is below
+ * 1e-7 rad (and, with IDIWF_SCALE, (|r|/D)^2 <= 1e-7), else an exact
+ * per-pair remainder at about half the speed.  Images with |r| > D/4 or a
+ * remainder above 2 rad are not computed: the call records
+ * IDIWF_ERR_UNSUPPORTED in the workspace (idiwf_workspace_error); the FP64
+ * kernel (IDIWF_DOUBLE) has no such limit.
  */
 idiwf_status idiwf_forward(const idiwf_geom *geom, const idiwf_batch *batch, int32_t precision,
                            int32_t out_kind, void *out, void *workspace, size_t workspace_bytes,
@@ -148,16 +157,30 @@ idiwf_status idiwf_forward_cta_times(const void *workspace, uint64_t *host_ns, i
  * IDIWF_ERR_UNSUPPORTED before anything is enqueued.
  *
  * The first call on a device looks up the array's device address (with that
- * device current); make that first call before any stream capture.  All
- * calls share the one array and it keeps the last call's contents; each call
- * clears what must start at zero.  Calls whose work overlaps on the GPU
- * (other streams, other threads, other graph branches) race on the scratch:
- * serialise them.  Same semantics and results as idiwf_forward with
- * precision IDIWF_SPLIT; idiwf_workspace_error() does not apply.
+ * device current); make that first call before any stream capture.  The
+ * address is kept for the life of the process: after cudaDeviceReset the
+ * library's module is loaded again elsewhere, so a process that resets a
+ * device must not call this entry point on it afterwards.  All calls share
+ * the one array and it keeps the last call's contents; each call clears what
+ * must start at zero.  Calls whose work overlaps on the GPU (other streams,
+ * other threads, other graph branches) race on the scratch: serialise them.
+ *
+ * Same kernels and paths as idiwf_forward with precision IDIWF_SPLIT and its
+ * default shape; results agree with idiwf_forward to the split tolerance,
+ * not bit for bit, because idiwf_forward splits small detectors over
+ * emitter chunks (another summation order).  Device-side errors (emitter
+ * coordinates out of range, a near-field image outside the split range, a
+ * bounded wait that ran out) are read back with idiwf_forward_noalloc_error.
  */
 #define IDIWF_NOALLOC_SCRATCH_BYTES (16u << 20)
 idiwf_status idiwf_forward_noalloc(const idiwf_geom *geom, const idiwf_batch *batch, int32_t out_kind,
                                    void *out, cudaStream_t stream);
+
+/* Device error word of the most recent idiwf_forward_noalloc call on the
+ * current device, with the statuses of idiwf_workspace_error.  Allocates
+ * nothing (the word is copied into a stack variable) and synchronises
+ * `stream`.  No counterpart in the reference. */
+idiwf_status idiwf_forward_noalloc_error(cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
 /* adjoint                                                                   */

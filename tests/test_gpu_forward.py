@@ -256,19 +256,26 @@ def test_reference_api_shapes():
     assert isinstance(g, torch.Tensor) and g.is_cuda and tuple(g.shape) == (2, 8, 8)
 
 
-def test_simulate_matches_reference_simulate(reference):
-    """The drop-in simulate() against the reference's cpu.simulate on the same
-    injected simobject sequence (two images, near field)."""
-    from oracle import refshim
-
-    g0 = rng(31)
-    n = 600
-    pos = sphere(g0, n, 0.01)
-    ph = g0.uniform(0, 2 * np.pi, (2, n))
-    ref = reference.cpu.simulate(2, refshim.InjectedObject(E_EV, pos, ph), 20, 75.0, 1e5, K64, settings="nf")
-    ours = cuda.simulate(2, refshim.InjectedObject(E_EV, pos, ph), 20, 75.0, 1e5, K64, settings="nf double",
-                         verbose=False)
-    assert rel_field_err(ours, ref) < 1e-12
+def test_simulate_matches_reference_simulate(golden_forward):
+    """The drop-in simulate() against the reference's own cpu.simulate: every
+    fixture of forward_ref.npz was made by calling the reference's
+    cpu.simulate(2, obj, Ndet, pixelsize, detz, k, settings, detangles,
+    detoffset) on an object that hands out the stored positions and phases;
+    here cuda.simulate gets the same call with the same object sequence."""
+    names = sorted({k.split("__")[0] for k in golden_forward.files})
+    assert len(names) >= 6
+    for name in names:
+        nx, ny, ps, dz, a0, a1, o0, o1, k = golden_forward[f"{name}__meta"]
+        settings = str(golden_forward[f"{name}__settings"])
+        pos = golden_forward[f"{name}__pos"]
+        ph = golden_forward[f"{name}__phases"]
+        ref = golden_forward[f"{name}__field"]
+        for prec, tol in (("double", 1e-12), ("split", SPLIT_FIELD)):
+            obj = simobj.fixed(E_EV, pos, phases=ph)
+            ours = cuda.simulate(ph.shape[0], obj, [int(nx), int(ny)], ps, dz, k, settings=f"{settings} {prec}",
+                                 verbose=False, detangles=(a0, a1), detoffset=(o0, o1))
+            assert ours.shape == ref.shape and ours.dtype == np.complex128
+            assert rel_field_err(ours, ref) < tol, (name, prec, rel_field_err(ours, ref))
 
 
 def test_range_check_reports_error():
