@@ -183,6 +183,62 @@ def cpu_baseline(pos, ph, rows_target_s=12.0):
                       f"({pairs:.3g} pairs, {dt:.1f} s), FP64 near field, OpenMP over rows"}
 
 
+def c2_oracle_windows(out, pos, ph, k, w=64, seed=9):
+    """Split-precision intensities of the timed step (all images) against the
+    FP64 CPU oracle on a w x w window of every image, at a seeded position per
+    image.  The window's detector offset places its pixels exactly on the
+    full detector's (integer multiples of the pixel size), so both compute
+    the same points."""
+    import oracle
+
+    g = np.random.Generator(np.random.Philox(seed))
+    I_s, I_o = [], []
+    t0 = time.perf_counter()
+    for b in range(out.shape[0]):
+        ix0, iy0 = (int(v) for v in g.integers(0, NDET - w + 1, 2))
+        og = oracle.geometry([w, w], PIXEL, DETZ, k, (0, 0),
+                             ((ix0 - NDET // 2 + w // 2) * PIXEL, (iy0 - NDET // 2 + w // 2) * PIXEL))
+        at = np.ascontiguousarray(np.concatenate([pos, ph[b][:, None]], 1))
+        I_o.append(np.abs(oracle.wavefield(og, oracle.NF, at)) ** 2)
+        E = out[b, ix0:ix0 + w, iy0:iy0 + w].cpu().numpy()
+        I_s.append(np.abs(E) ** 2)
+    dt = time.perf_counter() - t0
+    st = error_stats(np.stack(I_s), np.stack(I_o))
+    st.update({"windows": f"{out.shape[0]} images x {w}x{w} px at seeded positions", "oracle_s": dt,
+               "compare": "split (the timed step's output) vs FP64 CPU oracle (reference rounding sequence)"})
+    return st
+
+
+def summarize_targets(line, t):
+    """The north-star figures in one compact object, last on the line."""
+    def r4(x):
+        return None if x is None else float(f"{x:.4g}")
+
+    out = {"c2_pairs_per_s": r4(t["c2_pairs_per_s"]), "c2_sfu_frac": r4(t["c2_sfu_frac"])}
+    fp64 = line.get("fp64", {}).get("value")
+    if fp64:
+        out["c2_split_over_fp64"] = r4(t["c2_pairs_per_s"] / fp64)
+    acc = line.get("accuracy_c2_vs_cpu_oracle")
+    if acc:
+        out["c2_err_vs_cpu_oracle"] = {"max_rel_masked": r4(acc["max_rel_masked"]),
+                                       "max_rel_to_mean": r4(acc["max_rel_to_mean"]), "pixels": acc["pixels"]}
+    if "e2e" in line:
+        out["e2e_pairs_per_s"] = r4(line["e2e"]["value"])
+    fb = line.get("fwd_bwd")
+    if fb:
+        out["c4_fwd_bwd_over_fwd"] = r4(fb["ratio"])
+    bt = line.get("batched_uneven")
+    if bt:
+        out["c3_pairs_per_s"] = r4(bt["pairs_per_s"])
+        out["c3_imbalance"] = r4(bt["load_imbalance_max_over_mean_cta_busy"])
+    tp = line.get("time_path")
+    if tp:
+        out["c5_pairs_per_s"] = r4(tp["pairs_per_s"])
+        if "roofline" in tp:
+            out["c5_frac"] = r4(tp["roofline"]["frac"])
+    return out
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -213,8 +269,51 @@ def reference_arm(args):
                                    "FP64 near field (the oracle's C restatement of idi/simulation/cpu.py)"},
         "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    gpu_point = reference_gpu_kernels(pos, ph[0], k)
+    if gpu_point is not None:
+        line["reference_gpu"] = gpu_point
     print(json.dumps(line), flush=True)
     return 0
+
+
+def reference_gpu_kernels(pos, ph0, k):
+    """The reference's own GPU kernels, wfkerneld (FP64) and wfkernelf (FP32,
+    with the near-field distance in FP64) of idi/simulation/sim.cu, compiled
+    from the reference tree for sm_100a into oracle/_ref and launched with the
+    reference's 16x16 blocks: one image of the workload, near field, timed
+    with CUDA events (best of 3 after a warm-up).  None where oracle/_ref was
+    not built or no GPU is present."""
+    import ctypes
+
+    lib = os.path.join(ROOT, "oracle", "_ref", "libref_wf.so")
+    try:
+        import torch
+
+        if not (os.path.exists(lib) and torch.cuda.is_available()):
+            return None
+        L = ctypes.CDLL(lib)
+    except (ImportError, OSError):
+        return None
+    L.ref_wf_launch.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_float] * 5 + \
+                               [ctypes.c_int] * 3 + [ctypes.c_void_p]
+    L.ref_wf_launch.restype = ctypes.c_int
+    at = np.ascontiguousarray(np.concatenate([pos, ph0[:, None]], 1))
+    res = {"workload": f"1 image: {N_EMIT} emitters x {NDET}x{NDET}, near field (sim.cu -Dusenf -Dnodist)"}
+    pairs = N_EMIT * NDET * NDET
+    for label, single in (("wfkerneld_fp64", 0), ("wfkernelf_fp32", 1)):
+        d_at = torch.from_numpy(at.astype(np.float32) if single else at).cuda()
+        out = torch.empty((NDET, NDET), dtype=torch.complex64 if single else torch.complex128, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+
+        def launch():
+            st = L.ref_wf_launch(single, out.data_ptr(), d_at.data_ptr(), 0.0, 0.0, DETZ, PIXEL, k, NDET, NDET,
+                                 N_EMIT, stream)
+            if st != 0:
+                raise RuntimeError(f"reference kernel launch failed ({st})")
+
+        ms = timed_fn(torch)(launch, reps=3)
+        res[label] = {"ms": ms, "pairs_per_s": pairs / (ms * 1e-3)}
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -344,14 +443,18 @@ def main():
                      "ops_per_pair": 2, "kernel_ms": kern_avg, "traffic": traffic,
                      "traffic_unit": "bytes per launch (ncu capture of 8 images, scaled by emitter records)"},
     }
+    targets = {"c2_pairs_per_s": value, "c2_sfu_frac": achieved_mufu / mufu}
     if not args.no_extras and rank == 0:
         line.update(extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, offsets, cfg))
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         try:
             line["cpu_baseline"] = cpu_baseline(pos, ph)
+            # C2's split error against the FP64 CPU oracle: windows of every image
+            line["accuracy_c2_vs_cpu_oracle"] = c2_oracle_windows(out, pos, ph, k)
         except Exception as e:  # the oracle library may be missing on a stripped box
             line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     if rank == 0:
+        line["targets"] = summarize_targets(line, targets)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -413,13 +516,13 @@ def extras(args, torch, dev, _core, nat, cuda, simobj, pos, ph, k, geom, atoms, 
                                 "fp64_reference_sequence": stats(Id, Ia, "FP64 reference sequence vs cancellation-free FP64")}
     del Es, Ed, Ea
 
-    res["fwd_bwd"] = fwd_bwd_leg(torch, dev, _core, nat, timed)
-    res["batched_uneven"] = batched_leg(torch, dev, _core, nat)
-    res["time_path"] = time_leg(torch, dev, _core, nat, args)
     res["detector"] = detector_leg(torch, dev, _core, nat, args, cuda=cuda, simobj=simobj, pos=pos, ph=ph, k=k)
     res["emitters"] = emitters_leg(torch, dev, _core, nat, args)
     res["qcorr"] = qcorr_leg(torch, dev, args)
     res["accuracy_per_config"] = accuracy_leg(torch, dev, _core, nat)
+    res["fwd_bwd"] = fwd_bwd_leg(torch, dev, _core, nat, timed)
+    res["batched_uneven"] = batched_leg(torch, dev, _core, nat)
+    res["time_path"] = time_leg(torch, dev, _core, nat, args)
     return res
 
 

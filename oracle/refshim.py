@@ -18,8 +18,10 @@ probes for cupy.  So the loader
   and imports ``util``, ``simulation.cpu``, ``simulation.time`` and
   ``simulation.simobj`` from it without running ``simulation/__init__.py``.
 
-The reference tree location comes from ``IDI_REFERENCE`` (default
-``/root/reference``).  :func:`available` reports whether it is present.
+The reference tree location comes from ``IDI_REFERENCE``, else the read-only
+checkout of the development container (``REF_ROOT``, the one place that names
+it; the fixture generators, the Makefile's reference target and ``build()``
+take it from here).  :func:`available` reports whether it is present.
 """
 
 from __future__ import annotations

@@ -14,7 +14,7 @@ the module's ``_integral`` (the reference calls it once per pixel block with
 the keys; the wrapper copies them before and after the in-place sort and then
 calls the original).
 
-Needs the reference tree (``IDI_REFERENCE``, default /root/reference).
+Needs the reference tree (``IDI_REFERENCE``, or ``oracle.refshim.REF_ROOT``).
 """
 
 from __future__ import annotations

@@ -16,7 +16,7 @@ one rounding each, and reports out-of-bounds writes: ``cucor`` writes bins
 past the end of its array for some geometries (a row of dqz = +maxdqz), so
 the 3d cases use geometries where every bin is inside.
 
-Needs the reference tree (``IDI_REFERENCE``, default /root/reference).
+Needs the reference tree (``IDI_REFERENCE``, or ``oracle.refshim.REF_ROOT``).
 """
 
 from __future__ import annotations
@@ -31,7 +31,11 @@ import numba  # noqa: E402
 import numpy as np  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("IDI_REFERENCE", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import refshim  # noqa: E402
+
+REF = refshim.REF_ROOT
 
 RADIAL_CASES = [
     # name, shape, z, maxq, xcenter, ycenter
