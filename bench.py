@@ -677,6 +677,25 @@ def time_leg(torch, dev, _core, nat, args):
     pairs = nimg * n * 256 * 256
     out = {"workload": "20k emitters, 10 nm sphere, 5 fs FWHM emission, tau 2 fs, 256x256 @ 75 um, 0.1 m, 4 images",
            "ms": ms, "pairs_per_s": pairs / (ms * 1e-3)}
+    # issue roofline: thread instructions per pair (ncu count of the same kernel,
+    # committed with its summary) against 4 warp instructions per clock per SM
+    try:
+        with open(os.path.join(ROOT, "profiles", "time_kernel_ff_20k_256.json")) as f:
+            ipp = float(json.load(f)["thread_instructions_per_pair"])
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                mhz, src = float(json.load(f)["sm_max_mhz"]), "MEASURED_PEAKS.json sm_max_mhz"
+        except (OSError, KeyError, ValueError):
+            mhz, src = 1965.0, "clocks.max.sm of the B200"
+        peak = 4 * 32 * sms * mhz * 1e6
+        achieved = out["pairs_per_s"] * ipp
+        out["roofline"] = {"bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9,
+                           "unit": "G thread-instructions/s", "frac": achieved / peak, "instructions_per_pair": ipp,
+                           "peak_source": f"4 warp instructions per clock per SM at {mhz:g} MHz ({src})",
+                           "instructions_source": "ncu instruction count, profiles/time_kernel_ff_20k_256.md"}
+    except (OSError, KeyError, ValueError):
+        pass
     # above the on-chip table: 200,000 emitters, 64x64 detector, one image
     nl = 200000
     posl = sphere_points(g, nl, 0.01)

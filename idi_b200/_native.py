@@ -65,6 +65,7 @@ EXPORTED = (
     "idiwf_time_max_emitters",
     "idiwf_time_workspace_size",
     "idiwf_time_forward",
+    "idiwf_time_forward_digest",
     "idiwf_time_order",
     "idiwf_photons_workspace_size",
     "idiwf_photons",
@@ -195,6 +196,9 @@ def load():
     L.idiwf_time_forward.argtypes = [P(Geom), vp, vp, ctypes.c_int64, ctypes.c_double, ctypes.c_double, vp, vp,
                                      ctypes.c_size_t, vp]
     L.idiwf_time_forward.restype = st
+    L.idiwf_time_forward_digest.argtypes = [P(Geom), vp, vp, ctypes.c_int64, ctypes.c_double, ctypes.c_double, vp,
+                                            vp, vp, ctypes.c_size_t, vp]
+    L.idiwf_time_forward_digest.restype = st
     L.idiwf_time_order.argtypes = [P(Geom), vp, vp, ctypes.c_int64, ctypes.c_double, ctypes.c_int32,
                                    ctypes.c_int32, vp, vp, vp, ctypes.c_size_t, vp]
     L.idiwf_time_order.restype = st

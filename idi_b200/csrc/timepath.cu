@@ -44,6 +44,21 @@ __device__ __forceinline__ uint64_t sortable(double v) {
     return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
 }
 
+// Order digest base: H = sum_m (j_m + 1) B^m mod 2^64 over the sorted emitter
+// indices j_m.  B = 1 mod 4, so B^d - 1 has at most 2 + log2(d) factors of 2
+// and swapping two indices (differing by less than 2^15, at positions less
+// than 2^15 apart) always changes H.
+constexpr uint64_t kDigestBase = 0x9E3779B97F4A7C15ull;
+__device__ __forceinline__ uint64_t digest_pow(int e) {
+    uint64_t r = 1, b = kDigestBase;
+    while (e) {
+        if (e & 1) r *= b;
+        b *= b;
+        e >>= 1;
+    }
+    return r;
+}
+
 struct Affine {
     double d, br, bi;
 };
@@ -56,20 +71,42 @@ __device__ __forceinline__ Affine compose(const Affine &first, const Affine &sec
     return r;
 }
 
-template <bool NF, bool SCALE>
+// Correctly rounded quotient a / c from ic = RN(1 / c): q0 = RN(a ic) is a
+// faithful quotient, r = a - c q0 is exact in one FMA, and RN(q0 + r ic) is
+// RN(a / c) (Markstein's theorem: P. Markstein, IBM J. Res. Dev. 34(1), 1990;
+// Muller et al., Handbook of Floating-Point Arithmetic, the theorem on
+// FMA-based correction of a faithful quotient).  The theorem needs normal
+// numbers away from underflow and overflow: quotients outside [2^-960, 2^1000]
+// in magnitude -- zeros, infinities and NaN included -- take the IEEE division
+// (which keeps a zero's sign and an infinity).  Bit-exact against the division
+// (the arrival keys must be the reference's bits).
+__device__ __forceinline__ double div_rn(double a, double c, double ic) {
+    const double q0 = __dmul_rn(a, ic);
+    if (!(fabs(q0) >= 0x1p-960 && fabs(q0) <= 0x1p1000)) return __ddiv_rn(a, c);
+    const double r = __fma_rn(-c, q0, a);
+    return __fma_rn(r, ic, q0);
+}
+
+// MK: divide by c with div_rn (the on-chip path) or the library division (the
+// large-count kernel, whose 64 registers the inlined correction would spill);
+// both give the correctly rounded quotient.
+// MK: divide by c with div_rn (the on-chip kernel) or the library division (the
+// large-count kernel, whose 64 registers the inlined correction would spill);
+// both give the correctly rounded quotient.
+template <bool NF, bool SCALE, bool MK = true>
 __device__ __forceinline__ void arrival(const GeomParams &g, double dx, double dy, double dz, double dn,
                                         double q0, double q1, double q2, const double4 &a, double t0,
-                                        double c, double &t, double &s_out, double &dist_out) {
+                                        double c, double ic, double &t, double &s_out, double &dist_out) {
     if (!NF) {
         const double s = __fma_rn(q2, a.z, __fma_rn(q1, a.y, __dmul_rn(q0, a.x)));
-        t = __dadd_rn(__ddiv_rn(-s, c), t0);
+        t = __dadd_rn(MK ? div_rn(-s, c, ic) : __ddiv_rn(-s, c), t0);
         s_out = s;
         dist_out = dn;
     } else {
         const double ax = __dsub_rn(dx, a.x), ay = __dsub_rn(dy, a.y), az = __dsub_rn(dz, a.z);
         const double dist = __dsqrt_rn(__fma_rn(az, az, __fma_rn(ax, ax, __dmul_rn(ay, ay))));
         const double s = __dadd_rn(__dsub_rn(dist, dn), a.z);
-        t = __dadd_rn(__ddiv_rn(s, c), t0);
+        t = __dadd_rn(MK ? div_rn(s, c, ic) : __ddiv_rn(s, c), t0);
         s_out = s;
         dist_out = dist;
     }
@@ -91,42 +128,79 @@ __device__ __forceinline__ void path_only(double dx, double dy, double dz, doubl
     }
 }
 
-// exp(-x) and expm1(-x), x >= 0, for the scan.  The arguments are gaps
-// between neighbouring arrival times over tau, almost always far below 1: up
-// to 2^-4 a Taylor polynomial of degree 9 in Horner form (coefficients 1/k!)
-// is exact to FP64 rounding (the first omitted term is below 3e-19 of the
-// result); larger arguments use the library functions.  (Used by the on-chip
-// kernel: in the 64-register large-count kernel the inlined polynomials
-// measured slower than the library calls.)
-__device__ __forceinline__ double inv_fact(int k) {
-    constexpr double f[11] = {1.0,       1.0,        1.0 / 2,     1.0 / 6,      1.0 / 24,      1.0 / 120,
-                              1.0 / 720, 1.0 / 5040, 1.0 / 40320, 1.0 / 362880, 1.0 / 3628800};
-    return f[k];
-}
-__device__ __forceinline__ double exp_neg(double x) {
-    if (!(x <= 0.0625)) return exp(-x);
-    const double t = -x;
-    double p = inv_fact(9);
-#pragma unroll
-    for (int k = 8; k >= 0; --k) p = __fma_rn(p, t, inv_fact(k));
-    return p;
-}
+// expm1(-x), x >= 0, for the scan.  The arguments are gaps between
+// neighbouring arrival times over tau, almost always far below 1: up to 2^-4
+// a Taylor polynomial of degree 10 in Horner form (coefficients 1/k!) is exact
+// to FP64 rounding (the first omitted term is below 3e-19 of the result);
+// larger arguments use the library function.  (The on-chip kernel uses it; in
+// the 64-register large-count kernel the inlined polynomial measured slower
+// than the library calls.)  The coefficient tables of this file live in
+// constant memory: an FP64 FMA takes a constant-bank operand directly, where a
+// 64-bit literal costs two moves into registers (measured: half the
+// instructions of the polynomials).
+__constant__ double kInvFact[11] = {1.0,       1.0,        1.0 / 2,     1.0 / 6,      1.0 / 24,      1.0 / 120,
+                                    1.0 / 720, 1.0 / 5040, 1.0 / 40320, 1.0 / 362880, 1.0 / 3628800};
 __device__ __forceinline__ double expm1_neg(double x) {
     if (!(x <= 0.0625)) return expm1(-x);
     const double t = -x;
-    double q = inv_fact(10);
+    double q = kInvFact[10];
 #pragma unroll
-    for (int k = 9; k >= 1; --k) q = __fma_rn(q, t, inv_fact(k));
+    for (int k = 9; k >= 1; --k) q = __fma_rn(q, t, kInvFact[k]);
     return t * q;  // t (1 + t/2! + ... + t^9/10!)
 }
 
-template <bool NF, bool SCALE>
+// sin and cos of x (FP64), for the time path's amplitudes.  Cody-Waite
+// reduction (W. J. Cody and W. Waite, Software Manual for the Elementary
+// Functions, 1980): n = rint(x 2/pi), a = (x - n P1) - n P2 with P1 + P2 = pi/2
+// to twice the precision (P1 = RN(pi/2), P2 = RN(pi/2 - P1)), |a| <= pi/4 up
+// to rounding, good to ~1e-16 rad for |x| far below 2^40; then the Taylor
+// series of sin and cos (coefficients (-1)^k / k!) to degrees 17 and 18, whose
+// first omitted terms are below 1e-19 on |a| <= pi/4, in Horner form over a^2;
+// the quadrant n mod 4 swaps and negates.  Arguments beyond 2^30 take the
+// library function.
+// Cody-Waite constants {2/pi, P1, P2} and the Taylor coefficients of sin
+// (degree 17 down to 3) and cos (degree 18 down to 2), highest first.
+__constant__ double kCW[3] = {0.63661977236758134308, 1.5707963267948966192, 6.123233995736766036e-17};
+__constant__ double kSinC[8] = {1.0 / 355687428096000.0, -1.0 / 1307674368000.0, 1.0 / 6227020800.0,
+                                -1.0 / 39916800.0,       1.0 / 362880.0,         -1.0 / 5040.0,
+                                1.0 / 120.0,             -1.0 / 6.0};
+__constant__ double kCosC[9] = {1.0 / 6402373705728000.0, -1.0 / 20922789888000.0, 1.0 / 87178291200.0,
+                                -1.0 / 479001600.0,       1.0 / 3628800.0,         -1.0 / 40320.0,
+                                1.0 / 720.0,              -1.0 / 24.0,             0.5};
+__device__ __forceinline__ void sincos_cw(double x, double &sn, double &cs) {
+    if (!(fabs(x) <= 0x1p30)) {
+        sincos(x, &sn, &cs);
+        return;
+    }
+    const double nd = rint(x * kCW[0]);
+    double a = __fma_rn(-nd, kCW[1], x);
+    a = __fma_rn(-nd, kCW[2], a);
+    const double a2 = a * a;
+    double ps = kSinC[0];
+#pragma unroll
+    for (int i = 1; i < 8; ++i) ps = __fma_rn(ps, a2, kSinC[i]);
+    const double s = __fma_rn(a * a2, ps, a);
+    double pc = kCosC[0];
+#pragma unroll
+    for (int i = 1; i < 9; ++i) pc = __fma_rn(pc, a2, kCosC[i]);
+    const double co = __fma_rn(-a2, pc, 1.0);
+    const int q = (int)(((long long)nd) & 3);
+    sn = (q & 1) ? co : s;
+    cs = (q & 1) ? s : co;
+    if (q == 1 || q == 2) cs = -cs;
+    if (q >= 2) sn = -sn;
+}
+
+// CW: sine and cosine by sincos_cw (the on-chip kernel) or the library (the
+// 64-register large-count kernel).
+template <bool NF, bool SCALE, bool CW = true>
 __device__ __forceinline__ void amplitude(double k, double s, double psi, double dist, double &re, double &im) {
     double th;
     if (!NF) th = -__dsub_rn(__dmul_rn(s, k), psi);  // time.py:94 exp(-1j*(s*k-phases))
     else th = __dadd_rn(__dmul_rn(s, k), psi);       // simtime.cu:71 phase = s*k + w
     double sn, cs;
-    sincos(th, &sn, &cs);
+    if (CW) sincos_cw(th, sn, cs);
+    else sincos(th, &sn, &cs);
     if (SCALE) {
         cs = __ddiv_rn(cs, dist);
         sn = __ddiv_rn(sn, dist);
@@ -237,9 +311,19 @@ __device__ bool bucket_sort(const double *keytab, uint16_t *perm, uint32_t *cnt,
         if (tid == kTimeThreads - 1) coarse[kCoarse] = kBuckets;
     }
     __syncthreads();
-    for (int j = tid; j < n; j += kTimeThreads) {
-        const uint32_t b = fine_bucket(keytab[j], kmin, scale, coarse);
-        atomicAdd(&cnt[b >> 1], (b & 1) ? 0x10000u : 1u);
+    // the fine bucket of each of the thread's keys, two 13-bit ids per word,
+    // kept for the scatter
+    uint32_t fb[kTimeIPT / 2];
+#pragma unroll
+    for (int i = 0; i < kTimeIPT; ++i) {
+        const int j = tid + i * kTimeThreads;
+        uint32_t b = 0;
+        if (j < n) {
+            b = fine_bucket(keytab[j], kmin, scale, coarse);
+            atomicAdd(&cnt[b >> 1], (b & 1) ? 0x10000u : 1u);
+        }
+        if (i & 1) fb[i / 2] |= b << 16;
+        else fb[i / 2] = b;
     }
     __syncthreads();
     // exclusive scan of the counters: thread t owns buckets [16t, 16t+16)
@@ -271,11 +355,16 @@ __device__ bool bucket_sort(const double *keytab, uint16_t *perm, uint32_t *cnt,
     __syncthreads();
     if (*s_flag) return false;  // uniform: every thread read the same flag after the barrier
     // scatter: afterwards cnt holds the end (= next start) of every bucket
-    for (int j = tid; j < n; j += kTimeThreads) {
-        const uint32_t b = fine_bucket(keytab[j], kmin, scale, coarse);
-        const uint32_t old = atomicAdd(&cnt[b >> 1], (b & 1) ? 0x10000u : 1u);
-        perm[(b & 1) ? (old >> 16) : (old & 0xFFFFu)] = (uint16_t)j;
+#pragma unroll
+    for (int i = 0; i < kTimeIPT; ++i) {
+        const int j = tid + i * kTimeThreads;
+        if (j < n) {
+            const uint32_t b = (i & 1) ? (fb[i / 2] >> 16) : (fb[i / 2] & 0xFFFFu);
+            const uint32_t old = atomicAdd(&cnt[b >> 1], (b & 1) ? 0x10000u : 1u);
+            perm[(b & 1) ? (old >> 16) : (old & 0xFFFFu)] = (uint16_t)j;
+        }
     }
+
     __syncthreads();
     // insertion sort inside each bucket by (key, emitter index)
     for (int i = 0; i < kBucketsPerThread; ++i) {
@@ -373,13 +462,14 @@ __device__ void radix_sort(const double *keytab, uint16_t *perm, uint32_t *H, ui
     }
 }
 
-template <bool NF, bool SCALE>
+template <bool NF, bool SCALE, bool DIGEST>
 __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams g, const double *__restrict__ atoms,
                                                                 const double *__restrict__ times, int n, double c,
                                                                 double tau, double *__restrict__ out,
                                                                 WsHeader *__restrict__ hdr, int order_pixel,
                                                                 int *__restrict__ order_out,
-                                                                double *__restrict__ keys_out) {
+                                                                double *__restrict__ keys_out,
+                                                                uint64_t *__restrict__ digest) {
     extern __shared__ __align__(16) unsigned char smem[];
     double *keytab = reinterpret_cast<double *>(smem);
     uint16_t *perm = reinterpret_cast<uint16_t *>(smem + (size_t)kTimeMaxN * 8);
@@ -387,10 +477,12 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
     uint32_t *base = H + kTimeWarps * 256;
     double *scratch = reinterpret_cast<double *>(base + 256);  // 128 doubles
     uint32_t *coarse = reinterpret_cast<uint32_t *>(scratch + 128);
+    __shared__ uint64_t s_dig[kTimeWarps];
     __shared__ int s_pix, s_flag;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int npix = g.nx * g.ny;
+    const double ic = 1.0 / c;  // correctly rounded (IEEE division)
 
     // order_pixel >= 0: process that one pixel only, record its sorted order
     // and write its intensity to out[0]
@@ -420,7 +512,7 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
             if (j < n) {
                 const double4 a = reinterpret_cast<const double4 *>(atoms)[j];
                 double s, dist;
-                arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, t, s, dist);
+                arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, ic, t, s, dist);
                 kmin = fmin(kmin, t);
                 kmax = fmax(kmax, t);
             }
@@ -446,27 +538,35 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
         // so sum_m w_m |x_m|^2 = |X|^2 S1 + 2 Re(X conj(S2)) + S3 with
         //   S1 = sum w D^2, S2 = sum w D B, S3 = sum w |B|^2
         // and w_m = -tau/2 expm1(-2 (t_{m+1} - t_m)/tau), w_{n-1} = tau/2
-        // (the interval integral of time.py:36-45).
+        // (the interval integral of time.py:36-45).  Each gap g enters twice:
+        // as the decay exp(-g/tau) = 1 + em of the later position and as the
+        // weight -tau/2 expm1(-2 g/tau) = -tau/2 em (2 + em) of the earlier one,
+        // with em = expm1(-g/tau): one polynomial per gap, no cancellation.
         const int m0 = tid * kTimeIPT;
         double Dm = 1.0, Br = 0.0, Bi = 0.0;
         double S1 = 0.0, S2r = 0.0, S2i = 0.0, S3 = 0.0;
+        uint64_t h = 0, pw = DIGEST && m0 < n ? digest_pow(m0) : 0;
         // the neighbours' keys travel in registers from one position to the
         // next, and the next position's emitter row is loaded one step ahead
         const double4 *atoms4 = reinterpret_cast<const double4 *>(atoms);
-        double t_prev = m0 > 0 && m0 - 1 < n ? keytab[perm[m0 - 1]] : 0.0;
         int j_next = 0;
-        double t_next = 0.0;
+        double t_next = 0.0, em_in = 0.0;
         double4 a_next = make_double4(0.0, 0.0, 0.0, 0.0);
         if (m0 < n) {
             j_next = perm[m0];
             t_next = keytab[j_next];
             a_next = atoms4[j_next];
+            if (m0 > 0) em_in = expm1_neg(__dsub_rn(t_next, keytab[perm[m0 - 1]]) * inv_tau);
         }
         for (int i = 0; i < kTimeIPT; ++i) {
             const int m = m0 + i;
             if (m >= n) break;
             const double tj = t_next;
             const double4 a = a_next;
+            if (DIGEST) {
+                h += (uint64_t)(j_next + 1) * pw;
+                pw *= kDigestBase;
+            }
             if (m + 1 < n) {
                 j_next = perm[m + 1];
                 t_next = keytab[j_next];
@@ -475,12 +575,15 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
             double s, dist, re, im;
             path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
             amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
-            const double dec = m == 0 ? 0.0 : exp_neg(__dsub_rn(tj, t_prev) * inv_tau);
-            t_prev = tj;
+            const double dec = m == 0 ? 0.0 : 1.0 + em_in;
             Dm *= dec;
             Br = fma(dec, Br, re);
             Bi = fma(dec, Bi, im);
-            const double w = m < n - 1 ? (-tau / 2) * expm1_neg(2 * __dsub_rn(t_next, tj) * inv_tau) : tau / 2;
+            double w = tau / 2;
+            if (m < n - 1) {
+                em_in = expm1_neg(__dsub_rn(t_next, tj) * inv_tau);
+                w = (-tau / 2) * (em_in * (2.0 + em_in));
+            }
             const double wD = w * Dm;
             S1 = fma(wD, Dm, S1);
             S2r = fma(wD, Br, S2r);
@@ -518,16 +621,27 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
         // X entering this thread's run = excl applied to x_{-1} = 0
         const double Xr = excl.br, Xi = excl.bi;
         double part = fma(fma(Xr, Xr, Xi * Xi), S1, fma(2.0, fma(Xr, S2r, Xi * S2i), S3));
-        // block sum
+        // block sum (and of the order digest)
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+        for (int o = 16; o > 0; o >>= 1) {
+            part += __shfl_down_sync(0xffffffffu, part, o);
+            if (DIGEST) h += __shfl_down_sync(0xffffffffu, h, o);
+        }
         __syncthreads();
-        if (lane == 0) scratch[64 + warp] = part;
+        if (lane == 0) {
+            scratch[64 + warp] = part;
+            if (DIGEST) s_dig[warp] = h;
+        }
         __syncthreads();
         if (tid == 0) {
             double tot = 0.0;
-            for (int w = 0; w < kTimeWarps; ++w) tot += scratch[64 + w];
+            uint64_t hh = 0;
+            for (int w = 0; w < kTimeWarps; ++w) {
+                tot += scratch[64 + w];
+                if (DIGEST) hh += s_dig[w];
+            }
             out[order_pixel >= 0 ? 0 : p] = tot;
+            if (DIGEST && order_pixel < 0) digest[p] = hh;
         }
     }
 }
@@ -755,11 +869,11 @@ __device__ void radix_sort_large(const double *keys, int *a, int *b, int n, uint
     // 8 passes: the sorted order is back in the first array
 }
 
-template <bool NF, bool SCALE>
+template <bool NF, bool SCALE, bool DIGEST>
 __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
     const GeomParams g, const double *__restrict__ atoms, const double *__restrict__ times, int n, double c,
     double tau, double *__restrict__ out, WsHeader *__restrict__ hdr, int order_pixel, int *__restrict__ order_out,
-    double *__restrict__ keys_out, unsigned char *__restrict__ slices, int n_slices) {
+    double *__restrict__ keys_out, unsigned char *__restrict__ slices, int n_slices, uint64_t *__restrict__ digest) {
     if ((int)blockIdx.x >= n_slices) return;  // one workspace slice per CTA
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t *cnt = reinterpret_cast<uint32_t *>(smem);
@@ -767,6 +881,7 @@ __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
     uint32_t *base = cnt + kTimeWarps * 256;  // and digit bases
     uint32_t *coarse = cnt + kLargeBuckets;
     __shared__ double scratch[128];
+    __shared__ uint64_t s_dig[kTimeWarps];
     __shared__ int s_pix, s_flag;
     unsigned char *slice = slices + (size_t)blockIdx.x * large_slice_bytes(n);
     double *keys = reinterpret_cast<double *>(slice);
@@ -796,7 +911,7 @@ __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
         for (int j = tid; j < n; j += kTimeThreads) {
             const double4 a = reinterpret_cast<const double4 *>(atoms)[j];
             double t, s, dist;
-            arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, t, s, dist);
+            arrival<NF, SCALE, false>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, 0.0, t, s, dist);
             kmin = fmin(kmin, t);
             kmax = fmax(kmax, t);
             keys[j] = t;
@@ -826,18 +941,23 @@ __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
             r_next = rec[m0];
             a_next = atoms4[r_next.idx];
         }
+        uint64_t h = 0, pw = DIGEST && m0 < n ? digest_pow(m0) : 0;
         for (int i = 0; i < per; ++i) {
             const int m = m0 + i;
             if (m >= n) break;
             const double tj = r_next.key;
             const double4 a = a_next;
+            if (DIGEST) {
+                h += (uint64_t)(r_next.idx + 1) * pw;
+                pw *= kDigestBase;
+            }
             if (m + 1 < n) {
                 r_next = rec[m + 1];
                 if (i + 1 < per) a_next = atoms4[r_next.idx];
             }
             double s, dist, re, im;
             path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
-            amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
+            amplitude<NF, SCALE, false>(g.k, s, a.w, dist, re, im);
             const double dec = m == 0 ? 0.0 : exp(-__dsub_rn(tj, t_prev) * inv_tau);
             t_prev = tj;
             Dm *= dec;
@@ -880,26 +1000,37 @@ __global__ void __launch_bounds__(kTimeThreads, 2) time_kernel_large(
         const double Xr = excl.br, Xi = excl.bi;
         double part = fma(fma(Xr, Xr, Xi * Xi), S1, fma(2.0, fma(Xr, S2r, Xi * S2i), S3));
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+        for (int o = 16; o > 0; o >>= 1) {
+            part += __shfl_down_sync(0xffffffffu, part, o);
+            if (DIGEST) h += __shfl_down_sync(0xffffffffu, h, o);
+        }
         __syncthreads();
-        if (lane == 0) scratch[64 + warp] = part;
+        if (lane == 0) {
+            scratch[64 + warp] = part;
+            if (DIGEST) s_dig[warp] = h;
+        }
         __syncthreads();
         if (tid == 0) {
             double tot = 0.0;
-            for (int w = 0; w < kTimeWarps; ++w) tot += scratch[64 + w];
+            uint64_t hh = 0;
+            for (int w = 0; w < kTimeWarps; ++w) {
+                tot += scratch[64 + w];
+                if (DIGEST) hh += s_dig[w];
+            }
             out[order_pixel >= 0 ? 0 : p] = tot;
+            if (DIGEST && order_pixel < 0) digest[p] = hh;
         }
     }
 }
 
 template <bool NF, bool SCALE>
-static void *time_kernel_large_ptr() {
-    return (void *)time_kernel_large<NF, SCALE>;
+static void *time_kernel_large_ptr(bool digest) {
+    return digest ? (void *)time_kernel_large<NF, SCALE, true> : (void *)time_kernel_large<NF, SCALE, false>;
 }
 
 template <bool NF, bool SCALE>
-static void *time_kernel_ptr() {
-    return (void *)time_kernel<NF, SCALE>;
+static void *time_kernel_ptr(bool digest) {
+    return digest ? (void *)time_kernel<NF, SCALE, true> : (void *)time_kernel<NF, SCALE, false>;
 }
 
 static idiwf_status time_validate(const idiwf_geom *geom, const double *atoms, const double *times, int64_t n,
@@ -918,15 +1049,16 @@ static idiwf_status time_validate(const idiwf_geom *geom, const double *atoms, c
     return IDIWF_OK;
 }
 
-static void *large_fn(const idiwf_geom *geom) {
+static void *large_fn(const idiwf_geom *geom, bool digest = false) {
     const bool nf = geom->flags & IDIWF_NF, sc = geom->flags & IDIWF_SCALE;
-    return nf ? (sc ? time_kernel_large_ptr<true, true>() : time_kernel_large_ptr<true, false>())
-              : (sc ? time_kernel_large_ptr<false, true>() : time_kernel_large_ptr<false, false>());
+    return nf ? (sc ? time_kernel_large_ptr<true, true>(digest) : time_kernel_large_ptr<true, false>(digest))
+              : (sc ? time_kernel_large_ptr<false, true>(digest) : time_kernel_large_ptr<false, false>(digest));
 }
 
 // CTAs of the large-n kernel on this device, each owning one workspace
 // slice.  The shared-memory attribute is set before the occupancy query, so
-// the workspace size and the launch see the same count.
+// the workspace size and the launch see the same count (both digest
+// instances have the same resources).
 static int large_ctas(const idiwf_geom *geom, int order_pixel) {
     if (order_pixel >= 0) return 1;
     void *fn = large_fn(geom);
@@ -946,9 +1078,11 @@ static size_t time_ws_bytes(const idiwf_geom *geom, int64_t n, int order_pixel) 
     return kWsDataOffset + (size_t)large_ctas(geom, order_pixel) * large_slice_bytes(n);
 }
 
+// digest: (nx, ny) uint64 order digests of every pixel, or NULL.
 static idiwf_status time_launch(const idiwf_geom *geom, const double *atoms, const double *times, int64_t n,
                                 double c, double tau, double *out, void *workspace, size_t workspace_bytes,
-                                int order_pixel, int *order_out, double *keys_out, cudaStream_t stream) {
+                                int order_pixel, int *order_out, double *keys_out, uint64_t *digest,
+                                cudaStream_t stream) {
     const int slices_fit = n > kTimeMaxN ? large_ctas(geom, order_pixel) : 0;
     if (!workspace || workspace_bytes < time_ws_bytes(geom, n, order_pixel))
         return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_time_workspace_size()");
@@ -958,7 +1092,7 @@ static idiwf_status time_launch(const idiwf_geom *geom, const double *atoms, con
     const GeomParams g = make_geom(geom);
     const bool nf = geom->flags & IDIWF_NF, sc = geom->flags & IDIWF_SCALE;
     if (n > kTimeMaxN) {
-        void *fl = large_fn(geom);
+        void *fl = large_fn(geom, digest != nullptr);
         IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLargeSmem));
         IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 2 * sizeof(uint32_t), stream));
         // slices the workspace holds (the caller may pass more than the minimum)
@@ -969,12 +1103,13 @@ static idiwf_status time_launch(const idiwf_geom *geom, const double *atoms, con
         int ni = (int)n;
         unsigned char *slices = static_cast<unsigned char *>(workspace) + kWsDataOffset;
         void *args[] = {(void *)&g, &atoms, &times, &ni, &c, &tau, &out, &hdr, &order_pixel, &order_out, &keys_out,
-                        &slices, &n_slices};
+                        &slices, &n_slices, &digest};
         IDIWF_CUDA_CHECK(cudaLaunchKernel(fl, dim3(grid), dim3(kTimeThreads), args, kLargeSmem, stream));
         return IDIWF_OK;
     }
-    void *fn = nf ? (sc ? time_kernel_ptr<true, true>() : time_kernel_ptr<true, false>())
-                  : (sc ? time_kernel_ptr<false, true>() : time_kernel_ptr<false, false>());
+    const bool dg = digest != nullptr;
+    void *fn = nf ? (sc ? time_kernel_ptr<true, true>(dg) : time_kernel_ptr<true, false>(dg))
+                  : (sc ? time_kernel_ptr<false, true>(dg) : time_kernel_ptr<false, false>(dg));
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTimeSmem));
     IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 2 * sizeof(uint32_t), stream));  // counter + error word
     int dev = 0, sms = 148;
@@ -983,7 +1118,8 @@ static idiwf_status time_launch(const idiwf_geom *geom, const double *atoms, con
     const int npix = geom->nx * geom->ny;
     const int grid = order_pixel >= 0 ? 1 : std::min(npix, sms);
     int ni = (int)n;
-    void *args[] = {(void *)&g, &atoms, &times, &ni, &c, &tau, &out, &hdr, &order_pixel, &order_out, &keys_out};
+    void *args[] = {(void *)&g, &atoms, &times, &ni, &c, &tau, &out, &hdr, &order_pixel, &order_out, &keys_out,
+                    &digest};
     IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(kTimeThreads), args, kTimeSmem, stream));
     return IDIWF_OK;
 }
@@ -1005,7 +1141,18 @@ extern "C" idiwf_status idiwf_time_forward(const idiwf_geom *geom, const double 
     idiwf_status st = time_validate(geom, atoms, times, n, c, tau);
     if (st != IDIWF_OK) return st;
     if (!out) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "out is NULL");
-    return time_launch(geom, atoms, times, n, c, tau, out, workspace, workspace_bytes, -1, nullptr, nullptr, stream);
+    return time_launch(geom, atoms, times, n, c, tau, out, workspace, workspace_bytes, -1, nullptr, nullptr, nullptr,
+                       stream);
+}
+
+extern "C" idiwf_status idiwf_time_forward_digest(const idiwf_geom *geom, const double *atoms, const double *times,
+                                                  int64_t n, double c, double tau, double *out, uint64_t *digest,
+                                                  void *workspace, size_t workspace_bytes, cudaStream_t stream) {
+    idiwf_status st = time_validate(geom, atoms, times, n, c, tau);
+    if (st != IDIWF_OK) return st;
+    if (!out || !digest) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "out/digest is NULL");
+    return time_launch(geom, atoms, times, n, c, tau, out, workspace, workspace_bytes, -1, nullptr, nullptr, digest,
+                       stream);
 }
 
 extern "C" idiwf_status idiwf_time_order(const idiwf_geom *geom, const double *atoms, const double *times,
@@ -1020,5 +1167,5 @@ extern "C" idiwf_status idiwf_time_order(const idiwf_geom *geom, const double *a
     // the intensity of the pixel goes to a scratch slot of the workspace header
     double *scratch = reinterpret_cast<double *>(&static_cast<WsHeader *>(workspace)->pad[0]);
     return time_launch(geom, atoms, times, n, c, 1.0, scratch, workspace, workspace_bytes, ix * geom->ny + iy, order,
-                       sorted_keys, stream);
+                       sorted_keys, nullptr, stream);
 }

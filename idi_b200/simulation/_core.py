@@ -371,8 +371,10 @@ def time_max_emitters() -> int:
 
 
 def time_forward(atoms: torch.Tensor, times: torch.Tensor, geom: nat.Geom, c: float, tau: float,
-                 out: Optional[torch.Tensor] = None) -> torch.Tensor:
-    """Time-dependent intensity (nx, ny) float64 of one image."""
+                 out: Optional[torch.Tensor] = None, digest: bool = False):
+    """Time-dependent intensity (nx, ny) float64 of one image.  With ``digest``,
+    returns (intensity, per-pixel order digests as (nx, ny) int64 holding the
+    uint64 bits)."""
     lib = nat.load()
     _require_cuda(atoms, "atoms", torch.float64)
     _require_cuda(times, "times", torch.float64)
@@ -383,6 +385,14 @@ def time_forward(atoms: torch.Tensor, times: torch.Tensor, geom: nat.Geom, c: fl
         out = torch.empty((geom.nx, geom.ny), dtype=torch.float64, device=dev)
     nbytes = lib.idiwf_time_workspace_size(ctypes.byref(geom), atoms.shape[0])
     ws = WORKSPACES.get(nbytes, dev, "time")
+    if digest:
+        dig = torch.empty((geom.nx, geom.ny), dtype=torch.int64, device=dev)
+        nat.check(lib.idiwf_time_forward_digest(ctypes.byref(geom), ctypes.c_void_p(atoms.data_ptr()),
+                                                ctypes.c_void_p(times.data_ptr()), atoms.shape[0], float(c),
+                                                float(tau), ctypes.c_void_p(out.data_ptr()),
+                                                ctypes.c_void_p(dig.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
+                                                ws.numel(), _stream(dev)))
+        return out, dig
     nat.check(lib.idiwf_time_forward(ctypes.byref(geom), ctypes.c_void_p(atoms.data_ptr()),
                                      ctypes.c_void_p(times.data_ptr()), atoms.shape[0], float(c), float(tau),
                                      ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),

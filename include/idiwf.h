@@ -230,6 +230,19 @@ idiwf_status idiwf_time_forward(const idiwf_geom *geom, const double *atoms, con
                                 size_t workspace_bytes, cudaStream_t stream);
 
 /*
+ * idiwf_time_forward plus, for every pixel, a 64-bit digest of its sorted
+ * emitter order, digest[p] = sum_m (j_m + 1) B^m mod 2^64 over the emitter
+ * indices j_m in arrival order, B = 0x9E3779B97F4A7C15 (a swap of any two
+ * emitters changes it).  digest is DEVICE (nx, ny) uint64.  Verification
+ * helper: it lets a caller compare every pixel's order with another sort of
+ * the same keys without storing n indices per pixel.  No counterpart in the
+ * reference.
+ */
+idiwf_status idiwf_time_forward_digest(const idiwf_geom *geom, const double *atoms, const double *times,
+                                       int64_t n, double c, double tau, double *out, uint64_t *digest,
+                                       void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/*
  * Sorted emitter order of one pixel, as the time path computes it
  * (order[m] = emitter of the m-th earliest arrival; sorted_keys[m] its
  * arrival time).  Verification helper for bit-exact ordering; device outputs.

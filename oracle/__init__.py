@@ -70,6 +70,8 @@ def lib():
         L.orc_adjoint.restype = d
         L.orc_time_image.argtypes = [P(OrcGeom), ctypes.c_int, vp, vp, ctypes.c_int64, d, d, vp]
         L.orc_time_image.restype = None
+        L.orc_time_image_digest.argtypes = [P(OrcGeom), ctypes.c_int, vp, vp, ctypes.c_int64, d, d, vp, vp, vp]
+        L.orc_time_image_digest.restype = None
         L.orc_time_order.argtypes = [P(OrcGeom), ctypes.c_int, vp, vp, ctypes.c_int64, d,
                                      ctypes.c_int, ctypes.c_int, vp]
         L.orc_time_order.restype = None
@@ -189,6 +191,33 @@ def time_image(g: OrcGeom, flags: int, atoms, times, c, tau) -> np.ndarray:
     lib().orc_time_image(ctypes.byref(g), int(flags), atoms.ctypes.data, times.ctypes.data,
                          atoms.shape[0], float(c), float(tau), out.ctypes.data)
     return out
+
+
+DIGEST_BASE = 0x9E3779B97F4A7C15
+
+
+def order_digest(order) -> int:
+    """sum_m (order[m] + 1) B^m mod 2^64: the per-pixel order digest of
+    ``time_image_digest`` (python, for small cases)."""
+    h, pw, mask = 0, 1, (1 << 64) - 1
+    for j in np.asarray(order, dtype=np.int64):
+        h = (h + (int(j) + 1) * pw) & mask
+        pw = (pw * DIGEST_BASE) & mask
+    return h
+
+
+def time_image_digest(g: OrcGeom, flags: int, atoms, times, c, tau):
+    """``time_image`` plus, per pixel, the digest of the sorted emitter order
+    (``order_digest``) and the number of equal neighbouring keys (ties)."""
+    atoms = _c(atoms)
+    times = _c(times)
+    out = np.empty((g.nx, g.ny), np.float64)
+    dig = np.empty((g.nx, g.ny), np.uint64)
+    ties = np.empty((g.nx, g.ny), np.int64)
+    lib().orc_time_image_digest(ctypes.byref(g), int(flags), atoms.ctypes.data, times.ctypes.data,
+                                atoms.shape[0], float(c), float(tau), out.ctypes.data, dig.ctypes.data,
+                                ties.ctypes.data)
+    return out, dig, ties
 
 
 def time_order(g: OrcGeom, flags: int, atoms, times, c, ix, iy) -> np.ndarray:

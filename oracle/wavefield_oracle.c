@@ -341,8 +341,28 @@ static double pairwise_sum(const double *a, int64_t n) {
  * Per pixel: sort by arrival (time.py:19-29), decaying scan (time.py:7-16),
  * integral (time.py:36-45).
  */
+/*
+ * Digest of one pixel's arrival order (a check on every pixel's order without
+ * storing it): H = sum_m (j_m + 1) B^m mod 2^64 over the sorted emitter
+ * indices j_m, B = 0x9E3779B97F4A7C15.  B = 1 mod 4, so B^d - 1 has at most
+ * 2 + log2(d) factors of 2 and a transposition of two indices (differing by
+ * less than 2^15 at positions less than 2^15 apart) always changes H.
+ */
+#define ORC_DIGEST_BASE 0x9E3779B97F4A7C15ull
+
+void orc_time_image_digest(const orc_geom *g, int flags, const double *atoms, const double *times,
+                           int64_t n, double c, double tau, double *out, uint64_t *digest, int64_t *ties);
+
 void orc_time_image(const orc_geom *g, int flags, const double *atoms, const double *times,
                     int64_t n, double c, double tau, double *out) {
+    orc_time_image_digest(g, flags, atoms, times, n, c, tau, out, NULL, NULL);
+}
+
+/* As orc_time_image, plus (when non-NULL) the order digest of every pixel and
+ * the number of equal neighbouring keys per pixel (0: the order is unique, so
+ * any sort -- the reference's unstable argsort included -- gives it). */
+void orc_time_image_digest(const orc_geom *g, int flags, const double *atoms, const double *times,
+                           int64_t n, double c, double tau, double *out, uint64_t *digest, int64_t *ties) {
 #pragma omp parallel
     {
         double *buf = (double *)malloc(sizeof(double) * n * 6);
@@ -367,6 +387,19 @@ void orc_time_image(const orc_geom *g, int flags, const double *atoms, const dou
                 Iprev = xi * xi + xr * xr;
             }
             out[p] = pairwise_sum(terms, n - 1) + tau / 2 * Iprev;
+            if (digest) {
+                uint64_t h = 0, pw = 1;
+                for (int64_t m = 0; m < n; m++) {
+                    h += (uint64_t)(kv[m].i + 1) * pw;
+                    pw *= ORC_DIGEST_BASE;
+                }
+                digest[p] = h;
+            }
+            if (ties) {
+                int64_t eq = 0;
+                for (int64_t m = 1; m < n; m++) eq += kv[m].t == kv[m - 1].t;
+                ties[p] = eq;
+            }
         }
         free(kv);
         free(buf);
