@@ -57,7 +57,7 @@ constexpr int kPixRecBytes = 32 + 80 + 16;
 // pixel runs (kRun pixels share one FP64 base phase), in addition:
 //   PD   float4 x2  {Dx,Dx,Dy,Dy} {Dz,Dz,-h,-h}   D = 2 pi (nq_p - nq_base)   32 B per pixel
 //   RB64 double4    {-q'x, -q'y, -q'z, 0} at the run's middle                 32 B per run
-//   RBF  float4 x2  {dbx,dbx,dby,dby} {dbz,dbz,0,0}  d_hat at the run's middle 32 B per run
+//   RBF  float4 x2  {dbx,dbx,dby,dby} {dbz,dbz,-hb,-hb}  d_hat and -k/(2|d|) at the run's middle  32 B per run
 // Stage layouts (bytes): per-pixel path P64 | PF | PG; run path PF | PD | PG | RB64 | RBF.
 constexpr uint32_t kStagePixels = kBwdTP * kPixRecBytes;
 constexpr uint32_t kOffRunPF = 0;
@@ -179,8 +179,9 @@ __global__ void bwd_pixel_geom_kernel(const GeomParams g, int npix, int npix_pad
                 const int run = p / kRun;
                 rb64[run] = make_double4(b.nqx, b.nqy, b.nqz, 0.0);
                 const float ux = (float)b.ux, uy = (float)b.uy, uz = (float)b.uz;
+                const float hb = (float)(-g.k * 0.5 * b.invD);
                 rbf[(size_t)run * 2] = make_float4(ux, ux, uy, uy);
-                rbf[(size_t)run * 2 + 1] = make_float4(uz, uz, 0.f, 0.f);
+                rbf[(size_t)run * 2 + 1] = make_float4(uz, uz, hb, hb);
             }
         }
     }
@@ -274,9 +275,12 @@ __device__ __forceinline__ float2 g2(float a, float b) { return make_float2(a, b
 // and the FP32 offset D_p . r per pixel (D_p = 2 pi (nq_p - nq_base); bounded
 // per image by the caller), with s_p = d_hat_p . r = s_base - D_p.r / k for the
 // near-field term.  PATH = kPathExact: per pair, with the forward exact path's
-// phase (quadratic term in the FP64 chain, FP32 remainder).  Returns true when
-// a bounded wait gave up.
-template <bool NF, bool SCALE, bool SECOND, int PE, int PATH>
+// phase (quadratic term in the FP64 chain, FP32 remainder).  NFB (pixel runs,
+// near field without "scale"): the second-order term h (|r|^2 - s^2) is taken
+// once per emitter and run, at the run's middle, instead of per pixel; across
+// a run it changes by at most 1.5 k r^2 run_span / |d| (bounded per image by
+// the caller).  Returns true when a bounded wait gave up.
+template <bool NF, bool SCALE, bool SECOND, int PE, int PATH, bool NFB = false>
 __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, float *__restrict__ part,
                                          int64_t nrec, WsHeader *__restrict__ hdr, unsigned char *smem,
                                          uint64_t *bar, int *s_abort, uint32_t &issued, uint32_t &consumed,
@@ -284,6 +288,7 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
     constexpr bool RUNS = PATH == kPathRuns;
     constexpr bool EXACT = PATH == kPathExact;
     static_assert(!EXACT || NF, "the exact path is a near-field path");
+    static_assert(!NFB || (RUNS && NF && !SCALE), "the run-base near-field term is a pixel-run path without scale");
     constexpr int PH = PE / 2;
     constexpr uint32_t kStage = RUNS ? kStageRuns : (EXACT ? kStageExact : kStagePixels);
     const int tid = threadIdx.x;
@@ -405,10 +410,12 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
                     XB2[q] = __ffma2_rn(u, TWO_PI2, NEG_3PI2);
                     SB2[q] = g2(0.f, 0.f);
                     if (NF) {
-                        const float4 B0 = sbf[2 * rr], B1 = sbf[2 * rr + 1];  // dbx dbx dby dby | dbz dbz
+                        const float4 B0 = sbf[2 * rr], B1 = sbf[2 * rr + 1];  // dbx dbx dby dby | dbz dbz -hb -hb
                         float2 sb = __fmul2_rn(g2(B0.x, B0.y), fx[q]);
                         sb = __ffma2_rn(g2(B0.z, B0.w), fy[q], sb);
                         SB2[q] = __ffma2_rn(g2(B1.x, B1.y), fz[q], sb);
+                        if (NFB)  // (-hb)(s_b^2 - |r|^2) once for the run's pixels
+                            XB2[q] = __ffma2_rn(g2(B1.z, B1.w), __ffma2_rn(SB2[q], SB2[q], fw[q]), XB2[q]);
                     }
                 }
 #pragma unroll 2
@@ -421,11 +428,20 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
                     const float4 GG = sg[j];          // G'r G'r G'i G'i
 #pragma unroll
                     for (int q = 0; q < PH; ++q) {
+                        if (NFB) {
+                            // the run base holds the near-field term: the offset
+                            // D_p . r goes straight onto the base angle
+                            float2 arg = __ffma2_rn(g2(D0.x, D0.y), fx[q], XB2[q]);
+                            arg = __ffma2_rn(g2(D0.z, D0.w), fy[q], arg);
+                            arg = __ffma2_rn(g2(D1.x, D1.y), fz[q], arg);
+                            accumulate(q, arg, g2(0.f, 0.f), F2, F3, GG, sf, j);
+                            continue;
+                        }
                         float2 dl = __fmul2_rn(g2(D0.x, D0.y), fx[q]);
                         dl = __ffma2_rn(g2(D0.z, D0.w), fy[q], dl);
                         dl = __ffma2_rn(g2(D1.x, D1.y), fz[q], dl);
                         float2 s = g2(0.f, 0.f);
-                        if (NF) {
+                        if (NF && !NFB) {
                             s = __ffma2_rn(dl, NEG_INVK2, SB2[q]);
                             const float2 w2 = __ffma2_rn(s, s, fw[q]);  // s^2 - |r|^2
                             dl = __ffma2_rn(g2(D1.z, D1.w), w2, dl);
@@ -552,12 +568,16 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(const __grid_con
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int s_unit, s_abort, s_img, s_ib;
-    __shared__ uint8_t s_path[kMaxImagesPerLaunch];
+    __shared__ uint8_t s_path[kMaxImagesPerLaunch], s_nfb[kMaxImagesPerLaunch];
     const int tid = threadIdx.x;
     bool mine = false;
     for (int i = tid; i < bp.n_images; i += blockDim.x) {
         const int path = split_path(g, R.rmax2[i], bp.runs != 0, true);
         s_path[i] = (uint8_t)path;
+        // run base carries the near-field term: 1.5 k r^2 run_span / D <= kNfbPhaseTol (squared)
+        const double r2 = (double)__uint_as_float(R.rmax2[i]);
+        const double e = 1.5 * g.k * g.run_span * r2;
+        s_nfb[i] = (uint8_t)(e * e * g.inv_dmin2 <= kNfbPhaseTol * kNfbPhaseTol);
         mine |= EXACTK ? path == kPathExact : (path == kPathPixel || path == kPathRuns);
         if (!EXACTK && path == kPathReject && blockIdx.x == 0) record_error(&hdr->error, kErrGeometry);
     }
@@ -608,8 +628,17 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(const __grid_con
             else
                 ab = false;
         } else if (s_path[img] == kPathRuns) {
-            ab = bwd_unit<NF, SCALE, SECOND, PE, kPathRuns>(bp, R, part, nrec, hdr, smem, bar, &s_abort, issued,
-                                                            consumed, img, ib, chunk, ninvk, g);
+            if constexpr (NF && !SCALE) {
+                if (s_nfb[img])
+                    ab = bwd_unit<NF, SCALE, SECOND, PE, kPathRuns, true>(bp, R, part, nrec, hdr, smem, bar, &s_abort,
+                                                                          issued, consumed, img, ib, chunk, ninvk, g);
+                else
+                    ab = bwd_unit<NF, SCALE, SECOND, PE, kPathRuns>(bp, R, part, nrec, hdr, smem, bar, &s_abort,
+                                                                    issued, consumed, img, ib, chunk, ninvk, g);
+            } else {
+                ab = bwd_unit<NF, SCALE, SECOND, PE, kPathRuns>(bp, R, part, nrec, hdr, smem, bar, &s_abort, issued,
+                                                                consumed, img, ib, chunk, ninvk, g);
+            }
         } else {
             ab = bwd_unit<NF, SCALE, SECOND, PE, kPathPixel>(bp, R, part, nrec, hdr, smem, bar, &s_abort, issued,
                                                              consumed, img, ib, chunk, ninvk, g);

@@ -94,6 +94,11 @@ constexpr double kNfScaleRho2 = 1e-7;
 // The adjoint's paraxial near-field gradient -q + k (x, y, 0)/|d| is off by
 // about r/D relative; above kAdjRho the image takes the exact adjoint.
 constexpr double kAdjRho2 = 1e-12;
+// The adjoint's pixel runs may take the near-field term h (|r|^2 - s^2) once
+// per run, at its middle, when its change across the run, at most
+// 1.5 k r^2 run_span / D, stays below this (radians): about the split
+// kernels' own per-pair phase rounding (1.5e-7 rad rms).
+constexpr double kNfbPhaseTol = 4e-7;
 
 // Paths of the split kernels, chosen per image from |r|_max.
 constexpr int kPathPixel = 0;   // FP64 phase per pair, second-order near field
