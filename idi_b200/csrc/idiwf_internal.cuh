@@ -39,8 +39,9 @@ struct WsHeader {
     uint32_t work_counter;  // persistent-kernel work queue
     uint32_t error;         // device error word (IDIWF_ERR_* bit set)
     uint32_t n_ctas;        // CTAs of the last forward launch
-    uint32_t work_counter2; // second work queue (split forward: per-pixel kernel)
-    uint32_t work_counter3; // third work queue (split forward: exact near-field kernel)
+    uint32_t work_counter2; // second work queue (split forward: per-pixel kernel; time path: full sorts)
+    uint32_t work_counter3; // third work queue (split forward: exact near-field kernel; time path:
+                            // warm-started sorts given up)
     uint32_t pad32;
     uint64_t pad[29];
 };

@@ -7,18 +7,32 @@
 //   x_0 = a_0,  x_m = a_m + exp(-(t_m - t_{m-1})/tau) x_{m-1}
 //   I_p = sum_{m<n-1} -tau/2 |x_m|^2 expm1(-2 (t_{m+1}-t_m)/tau) + tau/2 |x_{n-1}|^2
 //
-// One CTA (512 threads) handles one pixel at a time (persistent, atomic
-// pixel queue).  Arrival times are computed in FP64 with the exact rounding
-// sequence of the reference (np.inner as fma(q2,z,fma(q1,y,q0*x)), IEEE
-// division by c), so the keys -- and therefore the sorted order -- are bit
-// for bit those of the reference.  The keys stay in a shared-memory table
-// indexed by emitter (N <= 20480 in 160 KB) and only 16-bit emitter indices
-// move.  The sort is exact and stable: 8192 buckets by a monotone FP64 map of
-// the key (so bucket order is key order), then insertion sort inside each
-// bucket by (key, emitter index); if a bucket overflows, an on-chip LSD radix
-// sort (8 passes of 8 bits, per-warp ranking with __match_any_sync) takes
-// over.  The decaying scan is one pass: each thread keeps its run as an
-// affine map x -> D x + B plus three sums from which the run's share of the
+// One CTA (512 threads) handles one pixel at a time; CTAs take chunks of
+// consecutive pixels from an atomic queue and walk each chunk in serpentine
+// order (row by row, every other row backwards), so consecutive pixels of a
+// CTA are detector neighbours.  Arrival times are computed in FP64 with the
+// exact rounding sequence of the reference (np.inner as
+// fma(q2,z,fma(q1,y,q0*x)), IEEE division by c), so the keys -- and therefore
+// the sorted order -- are bit for bit those of the reference.
+//
+// Sorting.  Between neighbouring pixels the keys move by far less than their
+// spacing (the arrival-time spread of the emission times dominates the
+// geometric term), so the previous pixel's order is almost the new one.  The
+// kernel keeps the order in shared memory as position-ordered arrays of keys
+// (FP64) and 16-bit emitter indices, recomputes the keys in that order, and
+// repairs it with insertion sorts over windows of 40 positions, alternating
+// between two window grids offset by 20 until every window boundary is in
+// order (an exact check: each window is sorted, so the whole array is sorted
+// exactly when every boundary pair is).  After a bounded number of window
+// passes -- and for a CTA's first pixel -- the exact full sort runs: 8192
+// buckets by a monotone FP64 map of the key (so bucket order is key order),
+// insertion sort inside each bucket by (key, emitter index), and an on-chip
+// LSD radix sort (8 passes of 8 bits, per-warp ranking with __match_any_sync)
+// if a bucket overflows.  Every path sorts by (key, emitter index), so the
+// order does not depend on which one ran.
+//
+// The decaying scan is one pass: each thread keeps its run of 40 positions as
+// an affine map x -> D x + B plus three sums from which the run's share of the
 // interval integral follows once the block scan delivers the entering x.
 
 #include <algorithm>
@@ -33,11 +47,28 @@ constexpr int kTimeWarps = kTimeThreads / 32;
 constexpr int kTimeIPT = 40;                                 // items per thread
 constexpr int kTimeMaxN = kTimeThreads * kTimeIPT;           // 20480
 constexpr int kCoarse = 1024;                                 // coarse bins of the bucket map
-constexpr size_t kTimeSmem = (size_t)kTimeMaxN * 8           // key table
-                             + (size_t)kTimeMaxN * 2         // permutation
+// Slots of the position-ordered arrays: one pad slot after every 80
+// positions, so that the 40-position runs of the 16 threads of a half-warp
+// start in 16 different bank pairs (conflict-free 64-bit loads when every
+// thread walks its own run).
+constexpr int kSlotGroup = 2 * kTimeIPT;
+constexpr int kTimeSlots = kTimeMaxN + kTimeMaxN / kSlotGroup;
+__device__ __forceinline__ int slot(int m) { return m + m / kSlotGroup; }
+constexpr size_t kTimeSmem = (size_t)kTimeSlots * 8          // keys (by position; by emitter in a full sort)
+                             + (size_t)kTimeSlots * 2        // emitter index per position
                              + (size_t)kTimeWarps * 256 * 4  // per-warp digit counters
                              + 256 * 4 + 1024                // digit bases + scan scratch
                              + (kCoarse + 4) * 4;            // first fine bucket per coarse bin
+static_assert(kTimeSmem + 256 <= 232448, "time kernel shared memory above the per-block limit");
+// Window passes tried on the previous pixel's order before the full sort.
+constexpr int kWarmPasses = 8;
+// Failed warm starts in a row after which a CTA stops trying them.
+constexpr int kWarmMaxFails = 3;
+// Key of the padding positions n..kTimeMaxN-1 in a full sort: the positive NaN
+// with the largest payload, whose order-preserving image is the largest of all
+// 64-bit patterns, so the radix sort leaves the padding behind every real key
+// (NaN keys included) and positions below n always hold real emitters.
+constexpr long long kPadKeyBits = 0x7FFFFFFFFFFFFFFFll;
 
 __device__ __forceinline__ uint64_t sortable(double v) {
     const uint64_t b = (uint64_t)__double_as_longlong(v);
@@ -87,9 +118,6 @@ __device__ __forceinline__ double div_rn(double a, double c, double ic) {
     return __fma_rn(r, ic, q0);
 }
 
-// MK: divide by c with div_rn (the on-chip path) or the library division (the
-// large-count kernel, whose 64 registers the inlined correction would spill);
-// both give the correctly rounded quotient.
 // MK: divide by c with div_rn (the on-chip kernel) or the library division (the
 // large-count kernel, whose 64 registers the inlined correction would spill);
 // both give the correctly rounded quotient.
@@ -462,6 +490,82 @@ __device__ void radix_sort(const double *keytab, uint16_t *perm, uint32_t *H, ui
     }
 }
 
+// (key, emitter index) order; false both ways for an unordered (NaN) key,
+// which then never passes the boundary check and takes the full sort.
+__device__ __forceinline__ bool before(double ka, int ja, double kb, int jb) {
+    return ka < kb || (ka == kb && ja < jb);
+}
+
+// Insertion sort of positions [lo, hi) (hi - lo < kSlotGroup) of the
+// position-ordered keys K and emitter indices P by (key, emitter index).
+// The arrays come from the previous pixel's order, so the inner loop rarely
+// runs; kprev is the key at position m - 1 throughout.
+__device__ __forceinline__ void window_sort(double *K, uint16_t *P, int lo, int hi) {
+    // slots of [lo, hi): contiguous except for one pad slot at the next
+    // multiple of kSlotGroup
+    const int off = lo / kSlotGroup, cut = (off + 1) * kSlotGroup;
+    auto sl = [&](int m) { return m + off + (m >= cut ? 1 : 0); };
+    double kprev = K[sl(lo)];
+    for (int m = lo + 1; m < hi; ++m) {
+        const double kv = K[sl(m)];
+        if (kv > kprev) {
+            kprev = kv;
+            continue;
+        }
+        const int v = P[sl(m)];
+        if (kv == kprev && (int)P[sl(m - 1)] < v) continue;
+        // position m-1 is behind kv: shift the greater entries up by one
+        int q = m - 1;
+        while (q >= lo) {
+            const double ku = K[sl(q)];
+            const int u = P[sl(q)];
+            if (before(ku, u, kv, v)) break;
+            K[sl(q + 1)] = ku;
+            P[sl(q + 1)] = (uint16_t)u;
+            --q;
+        }
+        K[sl(q + 1)] = kv;
+        P[sl(q + 1)] = (uint16_t)v;
+        // position m now holds the old entry of m - 1, whose key is kprev
+    }
+}
+
+// Keys of positions [40t, 40t+40) of the thread's run, in the order P: the
+// emitter rows are gathered (the loads of eight positions in flight at a time,
+// four in the near-field and scaled kernels, whose scans need more registers).
+template <bool NF, bool SCALE>
+__device__ __forceinline__ void keys_by_position(const GeomParams &g, const double4 *__restrict__ atoms4,
+                                                 const double *__restrict__ times, int n, double dx, double dy,
+                                                 double dz, double dn, double q0, double q1, double q2, double c,
+                                                 double ic, double *K, const uint16_t *P) {
+    const int m0 = threadIdx.x * kTimeIPT;
+    if (m0 >= n) return;
+    double *Kr = K + slot(m0);  // a run never crosses a pad slot
+    const uint16_t *Pr = P + slot(m0);
+    constexpr int B = (NF || SCALE) ? 4 : 8;
+#pragma unroll 1
+    for (int b = 0; b < kTimeIPT; b += B) {
+        int jj[B];
+        double4 aa[B];
+        double tt[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) jj[u] = m0 + b + u < n ? (int)Pr[b + u] : 0;
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            aa[u] = atoms4[jj[u]];
+            tt[u] = times[jj[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            if (m0 + b + u < n) {
+                double t, s, dist;
+                arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, aa[u], tt[u], c, ic, t, s, dist);
+                Kr[b + u] = t;
+            }
+        }
+    }
+}
+
 template <bool NF, bool SCALE, bool DIGEST>
 __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams g, const double *__restrict__ atoms,
                                                                 const double *__restrict__ times, int n, double c,
@@ -469,11 +573,11 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
                                                                 WsHeader *__restrict__ hdr, int order_pixel,
                                                                 int *__restrict__ order_out,
                                                                 double *__restrict__ keys_out,
-                                                                uint64_t *__restrict__ digest) {
+                                                                uint64_t *__restrict__ digest, int chunk) {
     extern __shared__ __align__(16) unsigned char smem[];
-    double *keytab = reinterpret_cast<double *>(smem);
-    uint16_t *perm = reinterpret_cast<uint16_t *>(smem + (size_t)kTimeMaxN * 8);
-    uint32_t *H = reinterpret_cast<uint32_t *>(smem + (size_t)kTimeMaxN * 10);
+    double *K = reinterpret_cast<double *>(smem);
+    uint16_t *P = reinterpret_cast<uint16_t *>(smem + (size_t)kTimeSlots * 8);
+    uint32_t *H = reinterpret_cast<uint32_t *>(smem + (size_t)kTimeSlots * 10);
     uint32_t *base = H + kTimeWarps * 256;
     double *scratch = reinterpret_cast<double *>(base + 256);  // 128 doubles
     uint32_t *coarse = reinterpret_cast<uint32_t *>(scratch + 128);
@@ -483,165 +587,234 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int npix = g.nx * g.ny;
     const double ic = 1.0 / c;  // correctly rounded (IEEE division)
+    const double4 *atoms4 = reinterpret_cast<const double4 *>(atoms);
+    // the scan's exponents use a multiply by 1/tau (1 ulp from the reference's
+    // division, ~1e-16 relative in the decay); only the sort keys must match bit for bit
+    const double inv_tau = 1.0 / tau;
 
+    // CTA-uniform sort state: whether (K, P) hold the previous pixel's order,
+    // and whether warm starts are still tried
+    bool have = false;
+    int fails = 0;
     // order_pixel >= 0: process that one pixel only, record its sorted order
     // and write its intensity to out[0]
     int iter = 0;
     for (;;) {
         __syncthreads();
         if (tid == 0)
-            s_pix = order_pixel >= 0 ? (iter == 0 ? order_pixel : npix) : (int)atomicAdd(&hdr->work_counter, 1u);
+            s_pix = order_pixel >= 0 ? (iter == 0 ? 0 : npix) : (int)atomicAdd(&hdr->work_counter, (unsigned)chunk);
         __syncthreads();
         ++iter;
-        const int p = s_pix;
-        if (p >= npix) break;
-        const int ix = p / g.ny, iy = p - ix * g.ny;
-        double dx, dy, dz;
-        pixel_time(g, ix, iy, dx, dy, dz);
-        // time.py:89-91 (np.linalg.norm = sqrt((x*x + y*y) + z*z); q = det/d; q_z -= 1)
-        const double dn = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-        const double q0 = __ddiv_rn(dx, dn), q1 = __ddiv_rn(dy, dn), q2 = __dsub_rn(__ddiv_rn(dz, dn), 1.0);
-        // the scan's exponents use a multiply by 1/tau (1 ulp from the reference's
-        // division, ~1e-16 relative in the decay); only the sort keys must match bit for bit
-        const double inv_tau = 1.0 / tau;
+        const int c0 = s_pix;
+        if (c0 >= npix) break;
+        const int c1 = order_pixel >= 0 ? c0 + 1 : min(c0 + chunk, npix);
+        for (int pl = c0; pl < c1; ++pl) {
+            int ix, iy;
+            if (order_pixel >= 0) {
+                ix = order_pixel / g.ny;
+                iy = order_pixel - ix * g.ny;
+            } else {
+                // serpentine walk: odd rows backwards
+                ix = pl / g.ny;
+                const int r = pl - ix * g.ny;
+                iy = (ix & 1) ? g.ny - 1 - r : r;
+            }
+            const int p = ix * g.ny + iy;
+            double dx, dy, dz;
+            pixel_time(g, ix, iy, dx, dy, dz);
+            // time.py:89-91 (np.linalg.norm = sqrt((x*x + y*y) + z*z); q = det/d; q_z -= 1)
+            const double dn =
+                __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+            const double q0 = __ddiv_rn(dx, dn), q1 = __ddiv_rn(dy, dn), q2 = __dsub_rn(__ddiv_rn(dz, dn), 1.0);
 
-        // ---- keys: table by emitter index, +inf padding ----
-        double kmin = __longlong_as_double(0x7FF0000000000000ll), kmax = -kmin;
-        for (int j = tid; j < kTimeMaxN; j += kTimeThreads) {
-            double t = __longlong_as_double(0x7FF0000000000000ll);  // +inf
-            if (j < n) {
-                const double4 a = reinterpret_cast<const double4 *>(atoms)[j];
-                double s, dist;
-                arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, ic, t, s, dist);
-                kmin = fmin(kmin, t);
-                kmax = fmax(kmax, t);
+            // ---- sort: warm start from the previous pixel's order ----
+            bool sorted = false;
+            if (have && fails < kWarmMaxFails) {
+                keys_by_position<NF, SCALE>(g, atoms4, times, n, dx, dy, dz, dn, q0, q1, q2, c, ic, K, P);
+                // thread t's window: [40t, 40t+40) on even passes, [40t-20, 40t+20) on odd
+                // ones (the last thread's odd window runs to the end); the first even
+                // window is the thread's own run, whose keys it has just written
+                for (int pass = 0; pass < kWarmPasses; ++pass) {
+                    const int sh = (pass & 1) ? kTimeIPT / 2 : 0;
+                    const int lo = max(tid * kTimeIPT - sh, 0);
+                    const int hi = min(tid == kTimeThreads - 1 ? kTimeMaxN : (tid + 1) * kTimeIPT - sh, n);
+                    // (the previous pass's __syncthreads_or ordered its reads before these writes)
+                    if (lo < hi) window_sort(K, P, lo, hi);
+                    __syncthreads();
+                    bool bad = false;
+                    if (lo >= 1 && lo < n)
+                        bad = !before(K[slot(lo - 1)], P[slot(lo - 1)], K[slot(lo)], P[slot(lo)]);
+                    if (!__syncthreads_or(bad)) {
+                        sorted = true;
+                        break;
+                    }
+                }
+                fails = sorted ? 0 : fails + 1;
+                if (!sorted && tid == 0) atomicAdd(&hdr->work_counter3, 1u);  // warm starts given up
             }
-            keytab[j] = t;
-        }
-        block_minmax(kmin, kmax, scratch + 96);
-        if (!bucket_sort(keytab, perm, reinterpret_cast<uint32_t *>(H), coarse, n, kmin, kmax, scratch, &s_flag)) {
-            radix_sort(keytab, perm, H, base);
-        }
-        // perm[m] = emitter at sorted position m (positions >= n hold padding)
-
-        if (p == order_pixel) {
-            for (int m = tid; m < n; m += kTimeThreads) {
-                order_out[m] = perm[m];
-                keys_out[m] = keytab[perm[m]];
-            }
-        }
-
-        // ---- decaying scan over the sorted sequence, one pass ----
-        // Thread t owns positions [40t, 40t+40).  Inside its run
-        //   x_m = D_m X + B_m,  D_m = prod of the run's decays up to m,
-        // with X the value entering the run (known only after the block scan),
-        // so sum_m w_m |x_m|^2 = |X|^2 S1 + 2 Re(X conj(S2)) + S3 with
-        //   S1 = sum w D^2, S2 = sum w D B, S3 = sum w |B|^2
-        // and w_m = -tau/2 expm1(-2 (t_{m+1} - t_m)/tau), w_{n-1} = tau/2
-        // (the interval integral of time.py:36-45).  Each gap g enters twice:
-        // as the decay exp(-g/tau) = 1 + em of the later position and as the
-        // weight -tau/2 expm1(-2 g/tau) = -tau/2 em (2 + em) of the earlier one,
-        // with em = expm1(-g/tau): one polynomial per gap, no cancellation.
-        const int m0 = tid * kTimeIPT;
-        double Dm = 1.0, Br = 0.0, Bi = 0.0;
-        double S1 = 0.0, S2r = 0.0, S2i = 0.0, S3 = 0.0;
-        uint64_t h = 0, pw = DIGEST && m0 < n ? digest_pow(m0) : 0;
-        // the neighbours' keys travel in registers from one position to the
-        // next, and the next position's emitter row is loaded one step ahead
-        const double4 *atoms4 = reinterpret_cast<const double4 *>(atoms);
-        int j_next = 0;
-        double t_next = 0.0, em_in = 0.0;
-        double4 a_next = make_double4(0.0, 0.0, 0.0, 0.0);
-        if (m0 < n) {
-            j_next = perm[m0];
-            t_next = keytab[j_next];
-            a_next = atoms4[j_next];
-            if (m0 > 0) em_in = expm1_neg(__dsub_rn(t_next, keytab[perm[m0 - 1]]) * inv_tau);
-        }
-        for (int i = 0; i < kTimeIPT; ++i) {
-            const int m = m0 + i;
-            if (m >= n) break;
-            const double tj = t_next;
-            const double4 a = a_next;
-            if (DIGEST) {
-                h += (uint64_t)(j_next + 1) * pw;
-                pw *= kDigestBase;
-            }
-            if (m + 1 < n) {
-                j_next = perm[m + 1];
-                t_next = keytab[j_next];
-                if (i + 1 < kTimeIPT) a_next = atoms4[j_next];
-            }
-            double s, dist, re, im;
-            path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
-            amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
-            const double dec = m == 0 ? 0.0 : 1.0 + em_in;
-            Dm *= dec;
-            Br = fma(dec, Br, re);
-            Bi = fma(dec, Bi, im);
-            double w = tau / 2;
-            if (m < n - 1) {
-                em_in = expm1_neg(__dsub_rn(t_next, tj) * inv_tau);
-                w = (-tau / 2) * (em_in * (2.0 + em_in));
-            }
-            const double wD = w * Dm;
-            S1 = fma(wD, Dm, S1);
-            S2r = fma(wD, Br, S2r);
-            S2i = fma(wD, Bi, S2i);
-            S3 = fma(w, fma(Br, Br, Bi * Bi), S3);
-        }
-        const Affine agg = {Dm, Br, Bi};
-        // block exclusive scan of the run maps
-        Affine incl = agg;
+            if (!sorted) {
+                if (tid == 0) atomicAdd(&hdr->work_counter2, 1u);  // full sorts
+                // ---- full sort: keys by emitter index (K as a table), padding last ----
+                __syncthreads();
+                double kmin = __longlong_as_double(0x7FF0000000000000ll), kmax = -kmin;
+                for (int j = tid; j < kTimeMaxN; j += kTimeThreads) {
+                    double t = __longlong_as_double(kPadKeyBits);
+                    if (j < n) {
+                        const double4 a = atoms4[j];
+                        double s, dist;
+                        arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, ic, t, s, dist);
+                        kmin = fmin(kmin, t);
+                        kmax = fmax(kmax, t);
+                    }
+                    K[j] = t;
+                }
+                block_minmax(kmin, kmax, scratch + 96);
+                if (!bucket_sort(K, P, reinterpret_cast<uint32_t *>(H), coarse, n, kmin, kmax, scratch, &s_flag)) {
+                    radix_sort(K, P, H, base);
+                }
+                // P[m] (unpadded) = emitter at sorted position m: move to slots
+                uint32_t pk[kTimeIPT / 2];
+                const int m0 = tid * kTimeIPT;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            Affine y;
-            y.d = __shfl_up_sync(0xffffffffu, incl.d, o);
-            y.br = __shfl_up_sync(0xffffffffu, incl.br, o);
-            y.bi = __shfl_up_sync(0xffffffffu, incl.bi, o);
-            if (lane >= o) incl = compose(y, incl);
-        }
-        if (lane == 31) {
-            scratch[warp * 3 + 0] = incl.d;
-            scratch[warp * 3 + 1] = incl.br;
-            scratch[warp * 3 + 2] = incl.bi;
-        }
-        __syncthreads();
-        Affine wpre = {1.0, 0.0, 0.0};  // composition of all earlier warps
-        for (int w = 0; w < warp; ++w) {
-            const Affine y = {scratch[w * 3 + 0], scratch[w * 3 + 1], scratch[w * 3 + 2]};
-            wpre = compose(wpre, y);
-        }
-        Affine excl;
-        excl.d = __shfl_up_sync(0xffffffffu, incl.d, 1);
-        excl.br = __shfl_up_sync(0xffffffffu, incl.br, 1);
-        excl.bi = __shfl_up_sync(0xffffffffu, incl.bi, 1);
-        if (lane == 0) excl = Affine{1.0, 0.0, 0.0};
-        excl = compose(wpre, excl);
-        // X entering this thread's run = excl applied to x_{-1} = 0
-        const double Xr = excl.br, Xi = excl.bi;
-        double part = fma(fma(Xr, Xr, Xi * Xi), S1, fma(2.0, fma(Xr, S2r, Xi * S2i), S3));
-        // block sum (and of the order digest)
+                for (int i = 0; i < kTimeIPT / 2; ++i)
+                    pk[i] = (uint32_t)P[m0 + 2 * i] | ((uint32_t)P[m0 + 2 * i + 1] << 16);
+                __syncthreads();
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            part += __shfl_down_sync(0xffffffffu, part, o);
-            if (DIGEST) h += __shfl_down_sync(0xffffffffu, h, o);
-        }
-        __syncthreads();
-        if (lane == 0) {
-            scratch[64 + warp] = part;
-            if (DIGEST) s_dig[warp] = h;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            double tot = 0.0;
-            uint64_t hh = 0;
-            for (int w = 0; w < kTimeWarps; ++w) {
-                tot += scratch[64 + w];
-                if (DIGEST) hh += s_dig[w];
+                for (int i = 0; i < kTimeIPT / 2; ++i) {
+                    P[slot(m0) + 2 * i] = (uint16_t)(pk[i] & 0xFFFFu);
+                    P[slot(m0) + 2 * i + 1] = (uint16_t)(pk[i] >> 16);
+                }
+                __syncthreads();
+                keys_by_position<NF, SCALE>(g, atoms4, times, n, dx, dy, dz, dn, q0, q1, q2, c, ic, K, P);
+                __syncthreads();
             }
-            out[order_pixel >= 0 ? 0 : p] = tot;
-            if (DIGEST && order_pixel < 0) digest[p] = hh;
+            have = true;
+            // K[slot(m)], P[slot(m)]: key and emitter at sorted position m < n
+
+            if (order_pixel >= 0) {
+                for (int m = tid; m < n; m += kTimeThreads) {
+                    order_out[m] = P[slot(m)];
+                    keys_out[m] = K[slot(m)];
+                }
+            }
+
+            // ---- decaying scan over the sorted sequence, one pass ----
+            // Thread t owns positions [40t, 40t+40).  Inside its run
+            //   x_m = D_m X + B_m,  D_m = prod of the run's decays up to m,
+            // with X the value entering the run (known only after the block scan),
+            // so sum_m w_m |x_m|^2 = |X|^2 S1 + 2 Re(X conj(S2)) + S3 with
+            //   S1 = sum w D^2, S2 = sum w D B, S3 = sum w |B|^2
+            // and w_m = -tau/2 expm1(-2 (t_{m+1} - t_m)/tau), w_{n-1} = tau/2
+            // (the interval integral of time.py:36-45).  Each gap g enters twice:
+            // as the decay exp(-g/tau) = 1 + em of the later position and as the
+            // weight -tau/2 expm1(-2 g/tau) = -tau/2 em (2 + em) of the earlier one,
+            // with em = expm1(-g/tau): one polynomial per gap, no cancellation.
+            const int m0 = tid * kTimeIPT;
+            const double *Kr = K + slot(m0);  // the run's slots are contiguous
+            const uint16_t *Pr = P + slot(m0);
+            double Dm = 1.0, Br = 0.0, Bi = 0.0;
+            double S1 = 0.0, S2r = 0.0, S2i = 0.0, S3 = 0.0;
+            uint64_t h = 0, pw = DIGEST && m0 < n ? digest_pow(m0) : 0;
+            // the neighbours' keys travel in registers from one position to the
+            // next, and the next position's emitter row is loaded one step ahead
+            int j_next = 0;
+            double t_next = 0.0, em_in = 0.0;
+            double4 a_next = make_double4(0.0, 0.0, 0.0, 0.0);
+            if (m0 < n) {
+                j_next = Pr[0];
+                t_next = Kr[0];
+                a_next = atoms4[j_next];
+                if (m0 > 0) em_in = expm1_neg(__dsub_rn(t_next, K[slot(m0 - 1)]) * inv_tau);
+            }
+            for (int i = 0; i < kTimeIPT; ++i) {
+                const int m = m0 + i;
+                if (m >= n) break;
+                const double tj = t_next;
+                const double4 a = a_next;
+                if (DIGEST) {
+                    h += (uint64_t)(j_next + 1) * pw;
+                    pw *= kDigestBase;
+                }
+                if (m + 1 < n) {
+                    const bool in_run = i + 1 < kTimeIPT;
+                    j_next = in_run ? Pr[i + 1] : P[slot(m + 1)];
+                    t_next = in_run ? Kr[i + 1] : K[slot(m + 1)];
+                    if (in_run) a_next = atoms4[j_next];
+                }
+                double s, dist, re, im;
+                path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
+                amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
+                const double dec = m == 0 ? 0.0 : 1.0 + em_in;
+                Dm *= dec;
+                Br = fma(dec, Br, re);
+                Bi = fma(dec, Bi, im);
+                double w = tau / 2;
+                if (m < n - 1) {
+                    em_in = expm1_neg(__dsub_rn(t_next, tj) * inv_tau);
+                    w = (-tau / 2) * (em_in * (2.0 + em_in));
+                }
+                const double wD = w * Dm;
+                S1 = fma(wD, Dm, S1);
+                S2r = fma(wD, Br, S2r);
+                S2i = fma(wD, Bi, S2i);
+                S3 = fma(w, fma(Br, Br, Bi * Bi), S3);
+            }
+            const Affine agg = {Dm, Br, Bi};
+            // block exclusive scan of the run maps
+            Affine incl = agg;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                Affine y;
+                y.d = __shfl_up_sync(0xffffffffu, incl.d, o);
+                y.br = __shfl_up_sync(0xffffffffu, incl.br, o);
+                y.bi = __shfl_up_sync(0xffffffffu, incl.bi, o);
+                if (lane >= o) incl = compose(y, incl);
+            }
+            if (lane == 31) {
+                scratch[warp * 3 + 0] = incl.d;
+                scratch[warp * 3 + 1] = incl.br;
+                scratch[warp * 3 + 2] = incl.bi;
+            }
+            __syncthreads();
+            Affine wpre = {1.0, 0.0, 0.0};  // composition of all earlier warps
+            for (int w = 0; w < warp; ++w) {
+                const Affine y = {scratch[w * 3 + 0], scratch[w * 3 + 1], scratch[w * 3 + 2]};
+                wpre = compose(wpre, y);
+            }
+            Affine excl;
+            excl.d = __shfl_up_sync(0xffffffffu, incl.d, 1);
+            excl.br = __shfl_up_sync(0xffffffffu, incl.br, 1);
+            excl.bi = __shfl_up_sync(0xffffffffu, incl.bi, 1);
+            if (lane == 0) excl = Affine{1.0, 0.0, 0.0};
+            excl = compose(wpre, excl);
+            // X entering this thread's run = excl applied to x_{-1} = 0
+            const double Xr = excl.br, Xi = excl.bi;
+            double part = fma(fma(Xr, Xr, Xi * Xi), S1, fma(2.0, fma(Xr, S2r, Xi * S2i), S3));
+            // block sum (and of the order digest)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                part += __shfl_down_sync(0xffffffffu, part, o);
+                if (DIGEST) h += __shfl_down_sync(0xffffffffu, h, o);
+            }
+            __syncthreads();
+            if (lane == 0) {
+                scratch[64 + warp] = part;
+                if (DIGEST) s_dig[warp] = h;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                double tot = 0.0;
+                uint64_t hh = 0;
+                for (int w = 0; w < kTimeWarps; ++w) {
+                    tot += scratch[64 + w];
+                    if (DIGEST) hh += s_dig[w];
+                }
+                out[order_pixel >= 0 ? 0 : p] = tot;
+                if (DIGEST && order_pixel < 0) digest[p] = hh;
+            }
+            // the next pixel's key pass overwrites K and P, which the scan reads
+            // across runs, and scratch, which thread 0 has just read
+            __syncthreads();
         }
     }
 }
@@ -1111,15 +1284,19 @@ static idiwf_status time_launch(const idiwf_geom *geom, const double *atoms, con
     void *fn = nf ? (sc ? time_kernel_ptr<true, true>(dg) : time_kernel_ptr<true, false>(dg))
                   : (sc ? time_kernel_ptr<false, true>(dg) : time_kernel_ptr<false, false>(dg));
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTimeSmem));
-    IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 2 * sizeof(uint32_t), stream));  // counter + error word
+    // queue counter, error word, and the full-sort / given-up warm-start counts
+    IDIWF_CUDA_CHECK(cudaMemsetAsync(hdr, 0, 5 * sizeof(uint32_t), stream));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int npix = geom->nx * geom->ny;
     const int grid = order_pixel >= 0 ? 1 : std::min(npix, sms);
+    // pixels per queue claim: runs of neighbours for the warm-started sort,
+    // short enough that the last claims balance (about 8 per CTA at least)
+    int chunk = std::max(1, std::min(16, npix / (8 * grid)));
     int ni = (int)n;
     void *args[] = {(void *)&g, &atoms, &times, &ni, &c, &tau, &out, &hdr, &order_pixel, &order_out, &keys_out,
-                    &digest};
+                    &digest, &chunk};
     IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(kTimeThreads), args, kTimeSmem, stream));
     return IDIWF_OK;
 }

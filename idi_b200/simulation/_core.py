@@ -371,10 +371,12 @@ def time_max_emitters() -> int:
 
 
 def time_forward(atoms: torch.Tensor, times: torch.Tensor, geom: nat.Geom, c: float, tau: float,
-                 out: Optional[torch.Tensor] = None, digest: bool = False):
+                 out: Optional[torch.Tensor] = None, digest: bool = False, stats: Optional[dict] = None):
     """Time-dependent intensity (nx, ny) float64 of one image.  With ``digest``,
     returns (intensity, per-pixel order digests as (nx, ny) int64 holding the
-    uint64 bits)."""
+    uint64 bits).  A ``stats`` dict receives (synchronising) how many pixels
+    took the full sort and how many warm-started sorts were given up (on-chip
+    kernel, up to 20480 emitters; both 0 for larger counts)."""
     lib = nat.load()
     _require_cuda(atoms, "atoms", torch.float64)
     _require_cuda(times, "times", torch.float64)
@@ -392,12 +394,16 @@ def time_forward(atoms: torch.Tensor, times: torch.Tensor, geom: nat.Geom, c: fl
                                                 float(tau), ctypes.c_void_p(out.data_ptr()),
                                                 ctypes.c_void_p(dig.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
                                                 ws.numel(), _stream(dev)))
-        return out, dig
-    nat.check(lib.idiwf_time_forward(ctypes.byref(geom), ctypes.c_void_p(atoms.data_ptr()),
-                                     ctypes.c_void_p(times.data_ptr()), atoms.shape[0], float(c), float(tau),
-                                     ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
-                                     _stream(dev)))
-    return out
+    else:
+        nat.check(lib.idiwf_time_forward(ctypes.byref(geom), ctypes.c_void_p(atoms.data_ptr()),
+                                         ctypes.c_void_p(times.data_ptr()), atoms.shape[0], float(c), float(tau),
+                                         ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
+                                         ws.numel(), _stream(dev)))
+    if stats is not None:
+        # workspace header words 3 and 4 (uint32)
+        w = ws[12:20].cpu().numpy().view(np.uint32)
+        stats["full_sorts"], stats["warm_given_up"] = int(w[0]), int(w[1])
+    return (out, dig) if digest else out
 
 
 def time_order(atoms: torch.Tensor, times: torch.Tensor, geom: nat.Geom, c: float, ix: int, iy: int):

@@ -196,3 +196,48 @@ def test_time_large_emitter_counts_many_pixels():
     img = _core.time_forward(_gpu(at), _gpu(times), geom, 0.3, 2.0).cpu().numpy()
     ref = oracle.time_image(oracle.geometry([20, 20], 75.0, 1e5, K64), 0, at, times, 0.3, 2.0)
     assert np.max(np.abs(img - ref) / np.abs(ref)) < 1e-9
+
+
+def _all_pixels_vs_oracle(at, times, nd, c, tau, settings="", tol=1e-10):
+    flags, _, _ = _core.parse_settings(settings)
+    geom = _core.make_geom(nd, 75.0, 1e5, K64, (0, 0), (0, 0), flags)
+    og = oracle.geometry(nd, 75.0, 1e5, K64)
+    stats = {}
+    img, dig = _core.time_forward(_gpu(at), _gpu(times), geom, c, tau, digest=True, stats=stats)
+    ref, ref_dig, ties = oracle.time_image_digest(og, oracle.flags_from_settings(settings), at, times, c, tau)
+    assert np.array_equal(dig.cpu().numpy().view(np.uint64), ref_dig), int(np.sum(dig.cpu().numpy().view(np.uint64) != ref_dig))
+    assert np.max(np.abs(img.cpu().numpy() - ref) / np.abs(ref)) < tol
+    return stats, ties
+
+
+def test_time_warm_start_with_ties():
+    """Each CTA starts a pixel's sort from its previous pixel's order and
+    repairs it with window insertion sorts.  Every emitter twice (same
+    position, phase and emission time) makes every key appear twice, so each
+    pixel's order depends on the (key, emitter index) tie rule; 144x144 pixels
+    give the kernel claims of 16 neighbouring pixels.  Every pixel's order
+    digest and intensity against the oracle, and most pixels warm-started."""
+    g0 = rng(303)
+    n0 = 1500
+    pos = sphere(g0, n0, 0.01)
+    ph = g0.uniform(0, 2 * np.pi, n0)
+    t0 = g0.normal(0, 5.0 / 2.35, n0)
+    at = atoms(np.concatenate([pos, pos]), np.concatenate([ph, ph]))
+    times = np.concatenate([t0, t0])
+    stats, ties = _all_pixels_vs_oracle(at, times, 144, 0.3, 2.0)
+    assert ties.min() >= n0  # every key appears (at least) twice
+    assert stats["full_sorts"] < 144 * 144 // 4, stats
+
+
+@pytest.mark.parametrize("settings", ["", "nf scale"])
+def test_time_warm_start_given_up_for_geometric_keys(settings):
+    """All emission times equal: the keys are the geometric path differences
+    alone, whose order turns with the pixel direction (fastest near the beam
+    axis), so the window passes cannot always repair the previous order and
+    the kernel falls back to the full sort.  Every pixel against the oracle."""
+    g0 = rng(404)
+    n = 3000
+    at = atoms(sphere(g0, n, 0.5), g0.uniform(0, 2 * np.pi, n))
+    times = np.zeros(n)
+    stats, _ = _all_pixels_vs_oracle(at, times, 48, 0.3, 0.5, settings, tol=1e-9)
+    assert stats["full_sorts"] > 148, stats  # beyond each CTA's first pixel
