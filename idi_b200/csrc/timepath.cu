@@ -47,15 +47,14 @@ constexpr int kTimeWarps = kTimeThreads / 32;
 constexpr int kTimeIPT = 40;                                 // items per thread
 constexpr int kTimeMaxN = kTimeThreads * kTimeIPT;           // 20480
 constexpr int kCoarse = 1024;                                 // coarse bins of the bucket map
-// Slots of the position-ordered arrays: one pad slot after every 80
-// positions, so that the 40-position runs of the 16 threads of a half-warp
-// start in 16 different bank pairs (conflict-free 64-bit loads when every
-// thread walks its own run).
+// Slots of the position-ordered index array: one pad slot after every 80
+// positions, so that the 40-position runs of a warp's threads start in
+// different banks when every thread walks its own run.
 constexpr int kSlotGroup = 2 * kTimeIPT;
 constexpr int kTimeSlots = kTimeMaxN + kTimeMaxN / kSlotGroup;
 __device__ __forceinline__ int slot(int m) { return m + m / kSlotGroup; }
-constexpr size_t kTimeSmem = (size_t)kTimeSlots * 8          // keys (by position; by emitter in a full sort)
-                             + (size_t)kTimeSlots * 2        // emitter index per position
+constexpr size_t kTimeSmem = (size_t)kTimeMaxN * 8           // key table (by emitter index)
+                             + (size_t)kTimeSlots * 2        // emitter index per sorted position
                              + (size_t)kTimeWarps * 256 * 4  // per-warp digit counters
                              + 256 * 4 + 1024                // digit bases + scan scratch
                              + (kCoarse + 4) * 4;            // first fine bucket per coarse bin
@@ -121,6 +120,14 @@ __device__ __forceinline__ double div_rn(double a, double c, double ic) {
 // MK: divide by c with div_rn (the on-chip kernel) or the library division (the
 // large-count kernel, whose 64 registers the inlined correction would spill);
 // both give the correctly rounded quotient.
+// One 32-byte emitter row (x, y, z, phase) in a single 256-bit load; the
+// rows are 32-byte aligned (the entry points require it of the emitter array).
+__device__ __forceinline__ double4 ld_row(const double4 *p) {
+    double4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+    return r;
+}
+
 template <bool NF, bool SCALE, bool MK = true>
 __device__ __forceinline__ void arrival(const GeomParams &g, double dx, double dy, double dz, double dn,
                                         double q0, double q1, double q2, const double4 &a, double t0,
@@ -497,72 +504,40 @@ __device__ __forceinline__ bool before(double ka, int ja, double kb, int jb) {
 }
 
 // Insertion sort of positions [lo, hi) (hi - lo < kSlotGroup) of the
-// position-ordered keys K and emitter indices P by (key, emitter index).
-// The arrays come from the previous pixel's order, so the inner loop rarely
-// runs; kprev is the key at position m - 1 throughout.
-__device__ __forceinline__ void window_sort(double *K, uint16_t *P, int lo, int hi) {
+// position-ordered emitter indices P by (key, emitter index), keys from the
+// table by emitter.  P comes from the previous pixel's order, so the inner
+// loop rarely runs; (kprev, jprev) is the entry at position m - 1
+// throughout, and the next position's entry is loaded one step ahead (an
+// insertion only rewrites positions up to m).
+__device__ __forceinline__ void window_sort(const double *keytab, uint16_t *P, int lo, int hi) {
     // slots of [lo, hi): contiguous except for one pad slot at the next
     // multiple of kSlotGroup
     const int off = lo / kSlotGroup, cut = (off + 1) * kSlotGroup;
     auto sl = [&](int m) { return m + off + (m >= cut ? 1 : 0); };
-    double kprev = K[sl(lo)];
+    int jprev = P[sl(lo)];
+    double kprev = keytab[jprev];
+    int v = lo + 1 < hi ? P[sl(lo + 1)] : 0;
+    double kv = keytab[v];
     for (int m = lo + 1; m < hi; ++m) {
-        const double kv = K[sl(m)];
-        if (kv > kprev) {
+        const int vn = m + 1 < hi ? P[sl(m + 1)] : 0;
+        const double kn = keytab[vn];
+        if (before(kprev, jprev, kv, v)) {
             kprev = kv;
-            continue;
-        }
-        const int v = P[sl(m)];
-        if (kv == kprev && (int)P[sl(m - 1)] < v) continue;
-        // position m-1 is behind kv: shift the greater entries up by one
-        int q = m - 1;
-        while (q >= lo) {
-            const double ku = K[sl(q)];
-            const int u = P[sl(q)];
-            if (before(ku, u, kv, v)) break;
-            K[sl(q + 1)] = ku;
-            P[sl(q + 1)] = (uint16_t)u;
-            --q;
-        }
-        K[sl(q + 1)] = kv;
-        P[sl(q + 1)] = (uint16_t)v;
-        // position m now holds the old entry of m - 1, whose key is kprev
-    }
-}
-
-// Keys of positions [40t, 40t+40) of the thread's run, in the order P: the
-// emitter rows are gathered (the loads of eight positions in flight at a time,
-// four in the near-field and scaled kernels, whose scans need more registers).
-template <bool NF, bool SCALE>
-__device__ __forceinline__ void keys_by_position(const GeomParams &g, const double4 *__restrict__ atoms4,
-                                                 const double *__restrict__ times, int n, double dx, double dy,
-                                                 double dz, double dn, double q0, double q1, double q2, double c,
-                                                 double ic, double *K, const uint16_t *P) {
-    const int m0 = threadIdx.x * kTimeIPT;
-    if (m0 >= n) return;
-    double *Kr = K + slot(m0);  // a run never crosses a pad slot
-    const uint16_t *Pr = P + slot(m0);
-    constexpr int B = (NF || SCALE) ? 4 : 8;
-#pragma unroll 1
-    for (int b = 0; b < kTimeIPT; b += B) {
-        int jj[B];
-        double4 aa[B];
-        double tt[B];
-#pragma unroll
-        for (int u = 0; u < B; ++u) jj[u] = m0 + b + u < n ? (int)Pr[b + u] : 0;
-#pragma unroll
-        for (int u = 0; u < B; ++u) {
-            aa[u] = atoms4[jj[u]];
-            tt[u] = times[jj[u]];
-        }
-#pragma unroll
-        for (int u = 0; u < B; ++u) {
-            if (m0 + b + u < n) {
-                double t, s, dist;
-                arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, aa[u], tt[u], c, ic, t, s, dist);
-                Kr[b + u] = t;
+            jprev = v;
+        } else {
+            // shift the entries behind v up by one
+            int q = m - 1;
+            P[sl(m)] = (uint16_t)jprev;
+            while (--q >= lo) {
+                const int u = P[sl(q)];
+                if (before(keytab[u], u, kv, v)) break;
+                P[sl(q + 1)] = (uint16_t)u;
             }
+            P[sl(q + 1)] = (uint16_t)v;
+            // position m now holds (kprev, jprev)
         }
+        v = vn;
+        kv = kn;
     }
 }
 
@@ -575,9 +550,9 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
                                                                 double *__restrict__ keys_out,
                                                                 uint64_t *__restrict__ digest, int chunk) {
     extern __shared__ __align__(16) unsigned char smem[];
-    double *K = reinterpret_cast<double *>(smem);
-    uint16_t *P = reinterpret_cast<uint16_t *>(smem + (size_t)kTimeSlots * 8);
-    uint32_t *H = reinterpret_cast<uint32_t *>(smem + (size_t)kTimeSlots * 10);
+    double *keytab = reinterpret_cast<double *>(smem);
+    uint16_t *P = reinterpret_cast<uint16_t *>(smem + (size_t)kTimeMaxN * 8);
+    uint32_t *H = reinterpret_cast<uint32_t *>(smem + (size_t)kTimeMaxN * 8 + (size_t)kTimeSlots * 2);
     uint32_t *base = H + kTimeWarps * 256;
     double *scratch = reinterpret_cast<double *>(base + 256);  // 128 doubles
     uint32_t *coarse = reinterpret_cast<uint32_t *>(scratch + 128);
@@ -627,50 +602,137 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
                 __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
             const double q0 = __ddiv_rn(dx, dn), q1 = __ddiv_rn(dy, dn), q2 = __dsub_rn(__ddiv_rn(dz, dn), 1.0);
 
+            // ---- keys: table by emitter index (coalesced), padding last ----
+            // (the rows of KB emitters per thread are loaded before any is used)
+            double kmin = __longlong_as_double(0x7FF0000000000000ll), kmax = -kmin;
+            {
+                constexpr int KB = NF ? 4 : 8;
+#pragma unroll 1
+                for (int b = 0; b < kTimeIPT; b += KB) {
+                    double4 aa[KB];
+                    double tt[KB];
+#pragma unroll
+                    for (int u = 0; u < KB; ++u) {
+                        const int j = tid + (b + u) * kTimeThreads;
+                        aa[u] = j < n ? ld_row(atoms4 + j) : make_double4(0.0, 0.0, 0.0, 0.0);
+                        tt[u] = j < n ? times[j] : 0.0;
+                    }
+                    if (!NF) {
+                        // far field without branches: the Markstein quotient of every
+                        // row, and the IEEE division after the batch for a quotient out of
+                        // div_rn's range (a zero path difference, say); the padding keys
+                        // (a NaN) leave min and max alone
+                        double tq[KB];
+                        bool redo = false;
+#pragma unroll
+                        for (int u = 0; u < KB; ++u) {
+                            const double sp = __fma_rn(q2, aa[u].z, __fma_rn(q1, aa[u].y, __dmul_rn(q0, aa[u].x)));
+                            const double qa = __dmul_rn(-sp, ic);
+                            tq[u] = __fma_rn(__fma_rn(-c, qa, -sp), ic, qa);
+                            redo |= tid + (b + u) * kTimeThreads < n && !(fabs(qa) >= 0x1p-960 && fabs(qa) <= 0x1p1000);
+                        }
+                        if (redo) {
+#pragma unroll
+                            for (int u = 0; u < KB; ++u) {
+                                const double sp =
+                                    __fma_rn(q2, aa[u].z, __fma_rn(q1, aa[u].y, __dmul_rn(q0, aa[u].x)));
+                                tq[u] = div_rn(-sp, c, ic);
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < KB; ++u) {
+                            const int j = tid + (b + u) * kTimeThreads;
+                            const double t = j < n ? __dadd_rn(tq[u], tt[u]) : __longlong_as_double(kPadKeyBits);
+                            kmin = fmin(kmin, t);
+                            kmax = fmax(kmax, t);
+                            keytab[j] = t;
+                        }
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < KB; ++u) {
+                            const int j = tid + (b + u) * kTimeThreads;
+                            double t = __longlong_as_double(kPadKeyBits);
+                            if (j < n) {
+                                double s, dist;
+                                arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, aa[u], tt[u], c, ic, t, s, dist);
+                                kmin = fmin(kmin, t);
+                                kmax = fmax(kmax, t);
+                            }
+                            keytab[j] = t;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+
             // ---- sort: warm start from the previous pixel's order ----
             bool sorted = false;
             if (have && fails < kWarmMaxFails) {
-                keys_by_position<NF, SCALE>(g, atoms4, times, n, dx, dy, dz, dn, q0, q1, q2, c, ic, K, P);
                 // thread t's window: [40t, 40t+40) on even passes, [40t-20, 40t+20) on odd
-                // ones (the last thread's odd window runs to the end); the first even
-                // window is the thread's own run, whose keys it has just written
+                // ones (the last thread's odd window runs to the end).  After a pass every
+                // window is sorted, so a window of the other grid -- two sorted halves --
+                // is out of order only if the boundary at its middle is: a thread sorts its
+                // window in the first pass, and later only when that boundary was found out
+                // of order (dirty).  The boundary a thread checks is the middle of its next
+                // window; together the threads check every boundary of the pass's grid.
+                bool dirty = true;
                 for (int pass = 0; pass < kWarmPasses; ++pass) {
                     const int sh = (pass & 1) ? kTimeIPT / 2 : 0;
                     const int lo = max(tid * kTimeIPT - sh, 0);
                     const int hi = min(tid == kTimeThreads - 1 ? kTimeMaxN : (tid + 1) * kTimeIPT - sh, n);
                     // (the previous pass's __syncthreads_or ordered its reads before these writes)
-                    if (lo < hi) window_sort(K, P, lo, hi);
+                    if (dirty && lo < hi) window_sort(keytab, P, lo, hi);
                     __syncthreads();
+                    const int b = (pass & 1) ? (tid + 1) * kTimeIPT - sh : tid * kTimeIPT;
                     bool bad = false;
-                    if (lo >= 1 && lo < n)
-                        bad = !before(K[slot(lo - 1)], P[slot(lo - 1)], K[slot(lo)], P[slot(lo)]);
+                    if (b >= 1 && b < n) {
+                        const int u = P[slot(b - 1)], v = P[slot(b)];
+                        bad = !before(keytab[u], u, keytab[v], v);
+                    }
+                    dirty = bad;
                     if (!__syncthreads_or(bad)) {
                         sorted = true;
                         break;
+                    }
+                    if (pass == 0) {
+                        // Between neighbouring pixels the few pairs still out of order sit
+                        // at even boundaries and have moved by a position or two: first a
+                        // window of 2 kPatch positions around each such boundary.  Only
+                        // the pairs at those windows' ends can then be out of order; where
+                        // one is, the odd window around it (which holds the short one)
+                        // takes over in the next pass.
+                        constexpr int kPatch = 8;
+                        const int plo = max(b - kPatch, 0), phi = min(b + kPatch, n);
+                        if (bad) window_sort(keytab, P, plo, phi);
+                        __syncthreads();
+                        bool pbad = false;
+                        if (bad) {
+                            if (plo >= 1) {
+                                const int u = P[slot(plo - 1)], v = P[slot(plo)];
+                                pbad = !before(keytab[u], u, keytab[v], v);
+                            }
+                            if (phi < n) {
+                                const int u = P[slot(phi - 1)], v = P[slot(phi)];
+                                pbad = pbad || !before(keytab[u], u, keytab[v], v);
+                            }
+                        }
+                        dirty = pbad;
+                        if (!__syncthreads_or(pbad)) {
+                            sorted = true;
+                            break;
+                        }
                     }
                 }
                 fails = sorted ? 0 : fails + 1;
                 if (!sorted && tid == 0) atomicAdd(&hdr->work_counter3, 1u);  // warm starts given up
             }
             if (!sorted) {
+                // ---- full sort ----
                 if (tid == 0) atomicAdd(&hdr->work_counter2, 1u);  // full sorts
-                // ---- full sort: keys by emitter index (K as a table), padding last ----
-                __syncthreads();
-                double kmin = __longlong_as_double(0x7FF0000000000000ll), kmax = -kmin;
-                for (int j = tid; j < kTimeMaxN; j += kTimeThreads) {
-                    double t = __longlong_as_double(kPadKeyBits);
-                    if (j < n) {
-                        const double4 a = atoms4[j];
-                        double s, dist;
-                        arrival<NF, SCALE>(g, dx, dy, dz, dn, q0, q1, q2, a, times[j], c, ic, t, s, dist);
-                        kmin = fmin(kmin, t);
-                        kmax = fmax(kmax, t);
-                    }
-                    K[j] = t;
-                }
                 block_minmax(kmin, kmax, scratch + 96);
-                if (!bucket_sort(K, P, reinterpret_cast<uint32_t *>(H), coarse, n, kmin, kmax, scratch, &s_flag)) {
-                    radix_sort(K, P, H, base);
+                if (!bucket_sort(keytab, P, reinterpret_cast<uint32_t *>(H), coarse, n, kmin, kmax, scratch,
+                                 &s_flag)) {
+                    radix_sort(keytab, P, H, base);
                 }
                 // P[m] (unpadded) = emitter at sorted position m: move to slots
                 uint32_t pk[kTimeIPT / 2];
@@ -685,16 +747,14 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
                     P[slot(m0) + 2 * i + 1] = (uint16_t)(pk[i] >> 16);
                 }
                 __syncthreads();
-                keys_by_position<NF, SCALE>(g, atoms4, times, n, dx, dy, dz, dn, q0, q1, q2, c, ic, K, P);
-                __syncthreads();
             }
             have = true;
-            // K[slot(m)], P[slot(m)]: key and emitter at sorted position m < n
+            // P[slot(m)]: emitter at sorted position m < n
 
             if (order_pixel >= 0) {
                 for (int m = tid; m < n; m += kTimeThreads) {
                     order_out[m] = P[slot(m)];
-                    keys_out[m] = K[slot(m)];
+                    keys_out[m] = keytab[P[slot(m)]];
                 }
             }
 
@@ -710,37 +770,37 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
             // weight -tau/2 expm1(-2 g/tau) = -tau/2 em (2 + em) of the earlier one,
             // with em = expm1(-g/tau): one polynomial per gap, no cancellation.
             const int m0 = tid * kTimeIPT;
-            const double *Kr = K + slot(m0);  // the run's slots are contiguous
-            const uint16_t *Pr = P + slot(m0);
+            const uint16_t *Pr = P + slot(m0);  // the run's slots are contiguous
             double Dm = 1.0, Br = 0.0, Bi = 0.0;
             double S1 = 0.0, S2r = 0.0, S2i = 0.0, S3 = 0.0;
             uint64_t h = 0, pw = DIGEST && m0 < n ? digest_pow(m0) : 0;
             // the neighbours' keys travel in registers from one position to the
-            // next, and the next position's emitter row is loaded one step ahead
+            // next, and the emitter rows are loaded two positions ahead
             int j_next = 0;
             double t_next = 0.0, em_in = 0.0;
-            double4 a_next = make_double4(0.0, 0.0, 0.0, 0.0);
+            double4 a_next = make_double4(0.0, 0.0, 0.0, 0.0), a_next2 = a_next;
             if (m0 < n) {
                 j_next = Pr[0];
-                t_next = Kr[0];
-                a_next = atoms4[j_next];
-                if (m0 > 0) em_in = expm1_neg(__dsub_rn(t_next, K[slot(m0 - 1)]) * inv_tau);
+                t_next = keytab[j_next];
+                a_next = ld_row(atoms4 + j_next);
+                if (m0 + 1 < n) a_next2 = ld_row(atoms4 + Pr[1]);
+                if (m0 > 0) em_in = expm1_neg(__dsub_rn(t_next, keytab[P[slot(m0 - 1)]]) * inv_tau);
             }
             for (int i = 0; i < kTimeIPT; ++i) {
                 const int m = m0 + i;
                 if (m >= n) break;
                 const double tj = t_next;
                 const double4 a = a_next;
+                a_next = a_next2;
                 if (DIGEST) {
                     h += (uint64_t)(j_next + 1) * pw;
                     pw *= kDigestBase;
                 }
                 if (m + 1 < n) {
-                    const bool in_run = i + 1 < kTimeIPT;
-                    j_next = in_run ? Pr[i + 1] : P[slot(m + 1)];
-                    t_next = in_run ? Kr[i + 1] : K[slot(m + 1)];
-                    if (in_run) a_next = atoms4[j_next];
+                    j_next = i + 1 < kTimeIPT ? Pr[i + 1] : P[slot(m + 1)];
+                    t_next = keytab[j_next];
                 }
+                if (i + 2 < kTimeIPT && m + 2 < n) a_next2 = ld_row(atoms4 + Pr[i + 2]);
                 double s, dist, re, im;
                 path_only<NF>(dx, dy, dz, dn, q0, q1, q2, a, s, dist);
                 amplitude<NF, SCALE>(g.k, s, a.w, dist, re, im);
@@ -812,7 +872,7 @@ __global__ void __launch_bounds__(kTimeThreads, 1) time_kernel(const GeomParams 
                 out[order_pixel >= 0 ? 0 : p] = tot;
                 if (DIGEST && order_pixel < 0) digest[p] = hh;
             }
-            // the next pixel's key pass overwrites K and P, which the scan reads
+            // the next pixel's key pass overwrites the key table and P, which the scan reads
             // across runs, and scratch, which thread 0 has just read
             __syncthreads();
         }
@@ -1291,9 +1351,11 @@ static idiwf_status time_launch(const idiwf_geom *geom, const double *atoms, con
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int npix = geom->nx * geom->ny;
     const int grid = order_pixel >= 0 ? 1 : std::min(npix, sms);
-    // pixels per queue claim: runs of neighbours for the warm-started sort,
-    // short enough that the last claims balance (about 8 per CTA at least)
-    int chunk = std::max(1, std::min(16, npix / (8 * grid)));
+    // pixels per queue claim: an equal share of the detector per CTA, walked in
+    // serpentine order (every pixel of a CTA but its first warm-starts from a
+    // neighbour's order; the per-pixel cost hardly varies, so equal shares
+    // balance)
+    int chunk = (npix + grid - 1) / grid;
     int ni = (int)n;
     void *args[] = {(void *)&g, &atoms, &times, &ni, &c, &tau, &out, &hdr, &order_pixel, &order_out, &keys_out,
                     &digest, &chunk};
