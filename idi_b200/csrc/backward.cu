@@ -41,7 +41,7 @@ namespace idiwf {
 
 constexpr int kBwdThreads = 128;
 constexpr int kBwdTP = 128;                      // pixels per shared-memory tile
-constexpr int kBwdChunk = 2048;                  // pixels per work unit
+constexpr int kBwdChunk = 2048;                  // largest number of pixels per work unit
 constexpr int kBwdNAcc = 6;                      // partial sums per emitter
 constexpr int kBwdMaxPE = 8;                     // largest emitters-per-thread instantiation
 
@@ -76,17 +76,49 @@ static_assert(kBwdTP % kRun == 0 && kBwdChunk % kRun == 0, "tiles hold whole run
 
 struct BwdLayout {
     int npix_pad;          // pixels rounded up to the chunk size
-    int n_chunks;
+    int n_chunks, chunk_px;
     int64_t nrec;          // emitter records (images padded to the emitter block)
     size_t off_p64, off_pf, off_pg, off_pd, off_rb64, off_rbf, off_px, off_rmax, off_erec64, off_erecf, off_part, total;
 };
+
+// Pixels per work unit: 2048, 1024 or 512, whichever gives the shortest
+// estimated makespan of the persistent adjoint -- the number of unit waves
+// over the resident CTAs (4 per SM, the default shape) times the unit's
+// pixels plus one tile of pipeline fill.  With few units per CTA the last
+// wave runs part-empty: 10k emitters on 512^2 pixels make 20 emitter blocks x
+// 128 chunks of 2048 = 4.3 waves on 592 CTAs (5 waves' time), but 8.6 of 1024
+// (9).  Ties keep the larger unit (fewer partial sums).
+static int bwd_chunk_px(const idiwf_geom *g, const idiwf_batch *b) {
+    const int64_t npix = (int64_t)g->nx * g->ny;
+    int64_t nb = 0;
+    for (int i = 0; i < b->n_images; ++i) {
+        const int64_t n = b->offsets[i + 1] - b->offsets[i];
+        nb += (n + kBwdThreads * 4 - 1) / (kBwdThreads * 4);
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t slots = (int64_t)std::max(sms, 1) * 4;
+    int best = kBwdChunk;
+    int64_t best_cost = -1;
+    for (const int c : {kBwdChunk, kBwdChunk / 2, kBwdChunk / 4}) {
+        const int64_t units = std::max<int64_t>(nb, 1) * ((npix + c - 1) / c);
+        const int64_t cost = (units + slots - 1) / slots * (c + kBwdTP);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    }
+    return best;
+}
 
 static BwdLayout bwd_layout(const idiwf_geom *g, const idiwf_batch *b) {
     BwdLayout L;
     const int64_t npix = (int64_t)g->nx * g->ny;
     const int eb = kBwdThreads * kBwdMaxPE;
-    L.npix_pad = (int)((npix + kBwdChunk - 1) / kBwdChunk * kBwdChunk);
-    L.n_chunks = L.npix_pad / kBwdChunk;
+    L.chunk_px = bwd_chunk_px(g, b);
+    L.npix_pad = (int)((npix + L.chunk_px - 1) / L.chunk_px * L.chunk_px);
+    L.n_chunks = L.npix_pad / L.chunk_px;
     L.nrec = 0;
     for (int i = 0; i < b->n_images; ++i) {
         const int64_t n = b->offsets[i + 1] - b->offsets[i];
@@ -115,7 +147,8 @@ struct BwdImage {
 };
 struct BwdParams {
     int32_t n_images, n_chunks, npix, npix_pad, total_units, eb;
-    int32_t runs, pad;  // runs: pixel runs allowed (rows hold whole runs)
+    int32_t runs;      // pixel runs allowed (rows hold whole runs)
+    int32_t chunk_px;  // pixels per work unit (a multiple of kBwdTP)
     BwdImage img[kMaxImagesPerLaunch];
     int32_t unit_img[kMaxImagesPerLaunch];   // images by descending emitter count
 };
@@ -317,8 +350,8 @@ __device__ __forceinline__ bool bwd_unit(const BwdParams &bp, const BwdRecs &R, 
 #pragma unroll
         for (int q = 0; q < PH; ++q) ac[a][q] = g2(0.f, 0.f);
 
-    const int p_begin = chunk * kBwdChunk;
-    constexpr int nt = kBwdChunk / kBwdTP;
+    const int p_begin = chunk * bp.chunk_px;
+    const int nt = bp.chunk_px / kBwdTP;
     auto issue = [&](int t) {
         const uint32_t slot = issued & 1;
         unsigned char *st = smem + slot * kStage;
@@ -660,42 +693,66 @@ __global__ void __launch_bounds__(kBwdThreads) bwd_split_kernel(const __grid_con
 // acc[5] multiplies all of r, the paraxial one (x, y, 0); images outside the
 // split range get zero gradients (the call reports kErrGeometry).
 template <bool KAPPA>
-__global__ void bwd_reduce_kernel(const __grid_constant__ BwdParams bp, const float *__restrict__ part,
-                                  int64_t nrec, const double *__restrict__ atoms, const void *__restrict__ amps,
-                                  int amp_dtype, double *__restrict__ grad_atoms, double *__restrict__ grad_amp,
-                                  const GeomParams g, const uint32_t *__restrict__ rmax2) {
+__global__ void __launch_bounds__(256) bwd_reduce_kernel(const __grid_constant__ BwdParams bp,
+                                                         const float *__restrict__ part, int64_t nrec,
+                                                         const double *__restrict__ atoms,
+                                                         const void *__restrict__ amps, int amp_dtype,
+                                                         double *__restrict__ grad_atoms,
+                                                         double *__restrict__ grad_amp, const GeomParams g,
+                                                         const uint32_t *__restrict__ rmax2) {
+    // 32 emitters per block (one per lane); the 8 warps take every 8th chunk,
+    // so the partial sums of a chunk are read as 32 consecutive records; the
+    // 8 warp sums are added in warp order (a fixed order: the result does not
+    // depend on timing)
+    __shared__ double red[8][32][kBwdNAcc + 1];
     const int b = blockIdx.y;
     const BwdImage d = bp.img[b];
     const int path = split_path(g, rmax2[b], bp.runs != 0, true);
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < d.n; j += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = d.rec + j;
-        const int64_t s = d.src + j;
-        if (path == kPathReject) {
-            reinterpret_cast<double4 *>(grad_atoms)[s] = make_double4(0.0, 0.0, 0.0, 0.0);
-            if (grad_amp) grad_amp[s] = 0.0;
-            continue;
-        }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t j0 = (int64_t)blockIdx.x * 32; j0 < d.n; j0 += (int64_t)gridDim.x * 32) {
+        const int64_t j = j0 + lane;
         double acc[kBwdNAcc];
 #pragma unroll
         for (int a = 0; a < kBwdNAcc; ++a) acc[a] = 0.0;
-        for (int c = 0; c < bp.n_chunks; ++c) {
-            const float *src = part + ((size_t)c * nrec + r) * kBwdNAcc;
+        if (j < d.n && path != kPathReject) {
+            const int64_t r = d.rec + j;
+            for (int c = w; c < bp.n_chunks; c += 8) {
+                const float *src = part + ((size_t)c * nrec + r) * kBwdNAcc;
 #pragma unroll
-            for (int a = 0; a < kBwdNAcc; ++a) acc[a] += (double)src[a];
+                for (int a = 0; a < kBwdNAcc; ++a) acc[a] += (double)src[a];
+            }
         }
-        const double4 at = reinterpret_cast<const double4 *>(atoms)[s];
-        double aj = 1.0;
-        if (amps) aj = amp_dtype == IDIWF_F32 ? (double)static_cast<const float *>(amps)[s]
-                                             : static_cast<const double *>(amps)[s];
-        // dL/dr = -a sum w Im z grad(phi) [+ a sum Re z grad w] = a (Q - K (x, y, 0 or z))
-        double gx = acc[2], gy = acc[3], gz = acc[4];
-        if (KAPPA) {
-            gx -= acc[5] * at.x;
-            gy -= acc[5] * at.y;
-            if (path == kPathExact) gz -= acc[5] * at.z;
+#pragma unroll
+        for (int a = 0; a < kBwdNAcc; ++a) red[w][lane][a] = acc[a];
+        __syncthreads();
+        if (w == 0 && j < d.n) {
+            const int64_t s = d.src + j;
+            if (path == kPathReject) {
+                reinterpret_cast<double4 *>(grad_atoms)[s] = make_double4(0.0, 0.0, 0.0, 0.0);
+                if (grad_amp) grad_amp[s] = 0.0;
+            } else {
+#pragma unroll
+                for (int a = 0; a < kBwdNAcc; ++a) {
+                    double t = red[0][lane][a];
+                    for (int ww = 1; ww < 8; ++ww) t += red[ww][lane][a];
+                    acc[a] = t;
+                }
+                const double4 at = reinterpret_cast<const double4 *>(atoms)[s];
+                double aj = 1.0;
+                if (amps) aj = amp_dtype == IDIWF_F32 ? (double)static_cast<const float *>(amps)[s]
+                                                     : static_cast<const double *>(amps)[s];
+                // dL/dr = -a sum w Im z grad(phi) [+ a sum Re z grad w] = a (Q - K (x, y, 0 or z))
+                double gx = acc[2], gy = acc[3], gz = acc[4];
+                if (KAPPA) {
+                    gx -= acc[5] * at.x;
+                    gy -= acc[5] * at.y;
+                    if (path == kPathExact) gz -= acc[5] * at.z;
+                }
+                reinterpret_cast<double4 *>(grad_atoms)[s] = make_double4(aj * gx, aj * gy, aj * gz, -aj * acc[1]);
+                if (grad_amp) grad_amp[s] = acc[0];
+            }
         }
-        reinterpret_cast<double4 *>(grad_atoms)[s] = make_double4(aj * gx, aj * gy, aj * gz, -aj * acc[1]);
-        if (grad_amp) grad_amp[s] = acc[0];
+        __syncthreads();
     }
 }
 
@@ -778,6 +835,7 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
     std::memset(&bp, 0, sizeof(bp));
     bp.n_images = batch->n_images;
     bp.n_chunks = L.n_chunks;
+    bp.chunk_px = L.chunk_px;
     bp.npix = npix;
     bp.npix_pad = L.npix_pad;
     bp.eb = eb;
@@ -847,7 +905,9 @@ extern "C" idiwf_status idiwf_backward(const idiwf_geom *geom, const idiwf_batch
         IDIWF_CUDA_CHECK(cudaLaunchKernel(fn, dim3(grid), dim3(kBwdThreads), args, smem, stream));
     }
     {
-        dim3 rgrid((unsigned)std::max<int64_t>(1, (max_blocks * eb + 255) / 256), batch->n_images);
+        int64_t max_n = 1;
+        for (int i = 0; i < batch->n_images; ++i) max_n = std::max<int64_t>(max_n, bp.img[i].n);
+        dim3 rgrid((unsigned)std::min<int64_t>((max_n + 31) / 32, 65535), batch->n_images);
         if (nf || so)
             bwd_reduce_kernel<true><<<rgrid, 256, 0, stream>>>(bp, part, nrec, batch->atoms, batch->amplitudes,
                                                                 batch->amp_dtype, grad_atoms, grad_amp, g, rmax2);
