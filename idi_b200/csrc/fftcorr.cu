@@ -1,8 +1,11 @@
-// Elementwise steps of the FFT autocorrelation (idi/reconstruction/cusimple.py):
-// the power spectrum in place, the fftshift + centre crop fused with the
-// normalisation, and the correlator's running mean / variance.  HBM-bound,
-// one pass each; the transforms themselves are cuFFT's.
+// FFT autocorrelation (idi/reconstruction/cusimple.py): for power-of-two
+// shapes the whole autocorrelation by hand-written shared-memory FFTs (three
+// passes per image, below); for other lengths the elementwise steps around
+// cuFFT's transforms -- the power spectrum in place, the fftshift + centre crop
+// fused with the normalisation -- and the correlator's running mean /
+// variance.
 #include <cmath>
+#include <type_traits>
 
 #include "idiwf_internal.cuh"
 
@@ -10,10 +13,14 @@ namespace idiwf {
 
 template <typename T>
 __global__ void power_kernel(T *__restrict__ z, int64_t n) {
+    // one vector load and store per complex value
+    using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    V *zv = reinterpret_cast<V *>(z);
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const T re = z[2 * i], im = z[2 * i + 1];
-        z[2 * i] = re * re + im * im;
-        z[2 * i + 1] = T(0);
+        V v = zv[i];
+        v.x = v.x * v.x + v.y * v.y;
+        v.y = T(0);
+        zv[i] = v;
     }
 }
 
@@ -57,6 +64,33 @@ __global__ void crop_kernel(const T *__restrict__ full, int64_t batch, const Cro
     }
 }
 
+// The 2D case of crop_kernel without divisions: blockIdx.y is the output
+// row (batch-major), threads run along the row.
+template <typename T>
+__global__ void crop2d_kernel(const T *__restrict__ full, int g0, int g1, int n0, int n1, const T *__restrict__ norm,
+                              int mode, T threshold, T *__restrict__ out) {
+    const int row = blockIdx.y;  // b * 2 n0 + i
+    const int b = row / (2 * n0), i = row - b * 2 * n0;
+    int j0 = (i - n0) % g0;
+    if (j0 < 0) j0 += g0;
+    const T *src = full + ((size_t)b * g0 + j0) * g1;
+    T *dst = out + (size_t)row * 2 * n1;
+    const T *nrm = norm ? norm + (size_t)i * 2 * n1 : nullptr;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < 2 * n1; c += gridDim.x * blockDim.x) {
+        int j1 = (c - n1) % g1;
+        if (j1 < 0) j1 += g1;
+        T y = src[j1];
+        if (nrm) {
+            const T cn = nrm[c];
+            if (mode == 0)
+                y = cn < threshold ? T(NAN) : y / cn;
+            else
+                y = cn > threshold ? y / cn : T(0);
+        }
+        dst[c] = y;
+    }
+}
+
 __global__ void welford_kernel(const float *__restrict__ x, float *__restrict__ mean, float *__restrict__ nvar,
                                int64_t n, int64_t count) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -71,6 +105,405 @@ __global__ void welford_kernel(const float *__restrict__ x, float *__restrict__ 
             nvar[i] = nvar[i] + delta * (v - m);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Hand-written FFT autocorrelation for power-of-two shapes: out =
+// fftshift(irfft2(|rfft2(x, (2 n0, 2 n1))|^2)) -- the reference's padded
+// length fastlen(2 n) is exactly 2 n for these shapes, so its centre crop is
+// the whole shifted array -- optionally divided by a normalisation.  Three
+// kernels per group of images, each made of shared-memory FFTs:
+//   A  rows:    the real FFT of each input row (length G1 = 2 n1, zero-padded)
+//               through a complex FFT of length H = n1 of (x[2k] + i x[2k+1])
+//               and the split into even and odd parts; written transposed,
+//               T[k][r] for k = 0..H (H + 1 columns of n0 rows);
+//   B  columns: per column k, the complex FFT of length G0 = 2 n0 of T[k][.]
+//               (rows n0.. are zero), the power |.|^2 and the inverse FFT (two
+//               columns' real power spectra packed into one complex inverse),
+//               written C[k][r] for rows r = 0..n0;
+//   C  rows:    per row r = 0..n0, the inverse real FFT of the half spectrum
+//               C[.][r] through a complex inverse FFT of length H, written with
+//               the fftshift and the normalisation, twice: the autocorrelation
+//               is point-symmetric, so row r also gives the mirrored row.
+// The FFTs are Stockham auto-sort passes (Govindaraju et al., "High
+// performance discrete Fourier transforms on graphics processors", SC 2008):
+// natural order in and out, each pass a radix-16 (or 2/4/8 for the remainder)
+// DFT of values held in registers, 16 per thread, with one shared-memory read
+// and write per value per pass; slots are XOR-swizzled so that every pass's
+// reads and writes are free of bank conflicts.  Inter-pass twiddles: one
+// value exp(-2 pi i m / N) from a table (sincospi) per butterfly, its powers by
+// multiplication in double precision.
+// ---------------------------------------------------------------------------
+template <typename T> struct Cx;
+template <> struct Cx<double> { using t = double2; };
+template <> struct Cx<float> { using t = float2; };
+
+template <typename V> __device__ __forceinline__ V cx_mul(V a, V b) {
+    V r;
+    r.x = a.x * b.x - a.y * b.y;
+    r.y = a.x * b.y + a.y * b.x;
+    return r;
+}
+template <typename V> __device__ __forceinline__ V cx_add(V a, V b) {
+    V r;
+    r.x = a.x + b.x;
+    r.y = a.y + b.y;
+    return r;
+}
+template <typename V> __device__ __forceinline__ V cx_sub(V a, V b) {
+    V r;
+    r.x = a.x - b.x;
+    r.y = a.y - b.y;
+    return r;
+}
+template <typename V> __device__ __forceinline__ V cx_conj(V a) {
+    a.y = -a.y;
+    return a;
+}
+template <typename V> __device__ __forceinline__ V cx_zero() {
+    V r;
+    r.x = 0;
+    r.y = 0;
+    return r;
+}
+
+// Complex values per block of the FFT kernels (one 8192-point column takes
+// 8192); values per thread E: 8 in FP64 (16 for the 8192-point column), 16
+// in FP32 -- the block's values live in registers during a pass.
+constexpr int kFcBlockElems = 4096;
+
+// Shared-memory slot of complex value w: a 128-byte bank row holds 8 (FP64)
+// or 16 (FP32) values, and the row index XOR'ed into the slot spreads the
+// strided accesses of the passes over all banks.
+template <typename V> __device__ __forceinline__ int fsw(int w) {
+    return sizeof(V) == 16 ? (w ^ ((w >> 4) & 7)) : (w ^ ((w >> 5) & 15));
+}
+
+// d * exp(-/+ 2 pi i e / 16) for e = 0..7 (a constant after unrolling).
+template <bool INV, typename V> __device__ __forceinline__ V mul_w16(V d, int e) {
+    using T = decltype(d.x);
+    constexpr double kC1 = 0.92387953251128675613;  // cos(pi / 8)
+    constexpr double kS1 = 0.38268343236508977173;  // sin(pi / 8)
+    constexpr double kH = 0.70710678118654752440;   // sqrt(1 / 2)
+    double c, s;
+    switch (e) {
+        case 0: return d;
+        case 4: {
+            V r;
+            r.x = INV ? -d.y : d.y;
+            r.y = INV ? d.x : -d.x;
+            return r;
+        }
+        case 1: c = kC1; s = kS1; break;
+        case 2: c = kH; s = kH; break;
+        case 3: c = kS1; s = kC1; break;
+        case 5: c = -kS1; s = kC1; break;
+        case 6: c = -kH; s = kH; break;
+        default: c = -kC1; s = kS1; break;
+    }
+    const T tc = (T)c, ts = INV ? (T)s : (T)-s;
+    V r;
+    r.x = d.x * tc - d.y * ts;
+    r.y = d.x * ts + d.y * tc;
+    return r;
+}
+
+__host__ __device__ constexpr int brevc(int r, int R) {
+    int o = 0;
+    for (int b = 1; b < R; b <<= 1) o = (o << 1) | ((r & b) ? 1 : 0);
+    return o;
+}
+
+// In-register R-point DFT (R = 2, 4, 8, 16): radix-2 decimation in frequency,
+// X[q] ends in v[brevc(q, R)].
+template <int R, bool INV, typename V> __device__ __forceinline__ void dft_reg(V *v) {
+#pragma unroll
+    for (int half = R / 2; half >= 1; half >>= 1) {
+#pragma unroll
+        for (int base = 0; base < R; base += 2 * half) {
+#pragma unroll
+            for (int j = 0; j < half; ++j) {
+                const V a = v[base + j], b = v[base + j + half];
+                v[base + j] = cx_add(a, b);
+                v[base + j + half] = mul_w16<INV>(cx_sub(a, b), j * (16 / (2 * half)));
+            }
+        }
+    }
+}
+
+// v[r] *= w^r, r = 1..R-1; the powers in double precision.
+template <int R, typename V> __device__ __forceinline__ void twiddle_powers(V *v, double2 w) {
+    using T = decltype(v[0].x);
+    double2 p = w;
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+        V q;
+        q.x = (T)p.x;
+        q.y = (T)p.y;
+        v[r] = cx_mul(v[r], q);
+        if (r + 1 < R) p = cx_mul(p, w);
+    }
+}
+
+// Loader of a pass that reads shared memory (never called).
+template <typename V> struct FcNoLoad {
+    __device__ V operator()(int, int) const { return cx_zero<V>(); }
+};
+
+// One Stockham pass over `count` sequences of length n = 2^logn at S: each
+// butterfly g (thread t takes g = t, t + blockDim, ...) reads
+// in[j + r n/R] (from shared memory, or from `ld(sequence, index)` for a first
+// pass), multiplies by exp(-/+ 2 pi i (j mod Ns) r / (Ns R)), takes the R-point
+// DFT and writes out[(j - j mod Ns) R + j mod Ns + q Ns].
+template <typename V, int R, int E, bool INV, bool LOADER, class Ld>
+__device__ __forceinline__ void fc_pass(V *S, int logn, int count, int Ns, const double2 *__restrict__ tw, int N,
+                                        const Ld &ld) {
+    constexpr int NB = E / R;
+    constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
+    const int n = 1 << logn, lognb = logn - LR, nb = 1 << lognb, total = count << lognb;
+    V v[E];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const int g = threadIdx.x + b * blockDim.x;
+        if (g < total) {
+            const int q = g >> lognb, j = g & (nb - 1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if constexpr (LOADER)
+                    v[b * R + r] = ld(q, j + r * nb);
+                else
+                    v[b * R + r] = S[fsw<V>(q * n + j + r * nb)];
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const int g = threadIdx.x + b * blockDim.x;
+        if (g < total) {
+            const int q = g >> lognb, j = g & (nb - 1), k = j & (Ns - 1);
+            if (Ns > 1) {
+                double2 w = __ldg(&tw[k * (N / (Ns * R))]);
+                if (INV) w.y = -w.y;
+                twiddle_powers<R>(&v[b * R], w);
+            }
+            dft_reg<R, INV>(&v[b * R]);
+            const int base = q * n + (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) S[fsw<V>(base + r * Ns)] = v[b * R + brevc(r, R)];
+        }
+    }
+    __syncthreads();
+}
+
+// The FFT of `count` sequences of length 2^logn in place at S (natural order
+// in and out), E values per thread (count << logn <= E * blockDim.x); the
+// first pass reads through `ld` when from_loader.
+template <typename V, int E, bool INV, class Ld>
+__device__ __forceinline__ void fc_fft(V *S, int logn, int count, const double2 *__restrict__ tw, int N, const Ld &ld,
+                                       bool from_loader) {
+    constexpr int LMAX = E >= 16 ? 4 : 3;
+    int Ns = 1;
+    bool first = from_loader;
+    const int rem = logn % LMAX;
+#define FC_RUN(RR)                                                                          \
+    do {                                                                                    \
+        if (first)                                                                          \
+            fc_pass<V, RR, E, INV, true>(S, logn, count, Ns, tw, N, ld);                    \
+        else                                                                                \
+            fc_pass<V, RR, E, INV, false>(S, logn, count, Ns, tw, N, ld);                   \
+        first = false;                                                                      \
+        Ns *= RR;                                                                           \
+    } while (0)
+    if (rem == 1) FC_RUN(2);
+    else if (rem == 2) FC_RUN(4);
+    else if (rem == 3) { if constexpr (LMAX == 4) FC_RUN(8); }
+    for (int p = 0; p < logn / LMAX; ++p) FC_RUN(1 << LMAX);
+#undef FC_RUN
+}
+
+// Pass A: rpb rows per block, one image per blockIdx.y.  x: n0 x n1 real per
+// image; T: (H+1) x n0 complex per image (t_img values apart).
+template <typename T, int E>
+__global__ void __launch_bounds__(512) fc_rows_fwd(const T *__restrict__ x, int n0, int n1, int logh, int rpb,
+                                                   const double2 *__restrict__ tw, int N,
+                                                   typename Cx<T>::t *__restrict__ Tt, size_t t_img) {
+    using V = typename Cx<T>::t;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    V *S = reinterpret_cast<V *>(fsm);
+    const int H = 1 << logh, r0 = blockIdx.x * rpb;
+    x += (size_t)blockIdx.y * n0 * n1;
+    Tt += (size_t)blockIdx.y * t_img;
+    // (x[2k], x[2k+1]) in one load: n1 is even and x is aligned to two values;
+    // k >= H/2 is the zero padding
+    auto ld = [&](int q, int k) -> V {
+        V z = cx_zero<V>();
+        const int r = r0 + q;
+        if (r < n0 && k < (H >> 1)) z = reinterpret_cast<const V *>(x + (size_t)r * n1)[k];
+        return z;
+    };
+    fc_fft<V, E, false>(S, logh, rpb, tw, N, ld, true);
+    // X[k] = (Z[k] + conj Z[H-k]) / 2 + W^k (Z[k] - conj Z[H-k]) / (2i), W = exp(-2 pi i / G1)
+    const int wstep = N / (2 * H);
+    for (int idx = threadIdx.x; idx < (H + 1) * rpb; idx += blockDim.x) {
+        const int k = idx / rpb, rr = idx - k * rpb, r = r0 + rr;
+        if (r >= n0) continue;
+        const V zk = S[fsw<V>(rr * H + (k & (H - 1)))], zc = cx_conj(S[fsw<V>(rr * H + ((H - k) & (H - 1)))]);
+        const V e = cx_add(zk, zc), d = cx_sub(zk, zc);
+        V o;  // d / (2i) = (d.y, -d.x) / 2
+        o.x = d.y;
+        o.y = -d.x;
+        const double2 wd = __ldg(&tw[k * wstep]);
+        V w;
+        w.x = (T)wd.x;
+        w.y = (T)wd.y;
+        const V wo = cx_mul(w, o);
+        V X;
+        X.x = T(0.5) * (e.x + wo.x);
+        X.y = T(0.5) * (e.y + wo.y);
+        Tt[(size_t)k * n0 + r] = X;
+    }
+}
+
+// Pass B: cpb columns per block (cpb = 1 for 8192-point columns), one image
+// per blockIdx.y.  The forward FFTs of the cpb columns (first pass straight
+// from T), then one inverse FFT per pair of columns of the packed power
+// spectra Z = P_k + i P_k+1 (both real; P_k+1 = 0 without a partner),
+// unpacked by Hermitian symmetry:
+// IFFT(P_k)[r] = (z[r] + conj z[-r]) / 2, IFFT(P_k+1)[r] = (z[r] - conj z[-r]) / (2i);
+// rows 0..n0 only (the rest follows from the point symmetry in pass C).
+// The inverse runs on the first npair * G0 / E threads.
+template <typename T, int E>
+__global__ void __launch_bounds__(512) fc_cols(const typename Cx<T>::t *__restrict__ Tt, size_t t_img, int n0,
+                                               int ncols, int logg0, int cpb, const double2 *__restrict__ tw, int N,
+                                               typename Cx<T>::t *__restrict__ C, size_t c_img) {
+    using V = typename Cx<T>::t;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    V *S = reinterpret_cast<V *>(fsm);
+    const int G0 = 1 << logg0, k0 = blockIdx.x * cpb;
+    Tt += (size_t)blockIdx.y * t_img;
+    C += (size_t)blockIdx.y * c_img;
+    auto ldT = [&](int q, int r) -> V {
+        V z = cx_zero<V>();
+        const int col = k0 + q;
+        if (r < n0 && col < ncols) z = Tt[(size_t)col * n0 + r];
+        return z;
+    };
+    fc_fft<V, E, false>(S, logg0, cpb, tw, N, ldT, true);
+    const int npair = (cpb + 1) >> 1;
+    auto ldP = [&](int q, int r) -> V {
+        const V u = S[fsw<V>(2 * q * G0 + r)];
+        V z;
+        z.x = u.x * u.x + u.y * u.y;
+        z.y = T(0);
+        if (2 * q + 1 < cpb) {
+            const V w = S[fsw<V>((2 * q + 1) * G0 + r)];
+            z.y = w.x * w.x + w.y * w.y;
+        }
+        return z;
+    };
+    fc_fft<V, E, true>(S, logg0, npair, tw, N, ldP, true);
+    const T half = T(0.5) / (T)G0;
+    for (int idx = threadIdx.x; idx < npair * (n0 + 1); idx += blockDim.x) {
+        const int q = idx / (n0 + 1), r = idx - q * (n0 + 1);
+        const V zp = S[fsw<V>(q * G0 + r)], zm = cx_conj(S[fsw<V>(q * G0 + ((G0 - r) & (G0 - 1)))]);
+        const int col = k0 + 2 * q;
+        if (col < ncols) {
+            V c0;
+            c0.x = (zp.x + zm.x) * half;
+            c0.y = (zp.y + zm.y) * half;
+            C[(size_t)col * (n0 + 1) + r] = c0;
+        }
+        if (2 * q + 1 < cpb && col + 1 < ncols) {
+            V c1;  // (zp - zm) / (2i) = ((zp - zm).y, -(zp - zm).x) / 2
+            c1.x = (zp.y - zm.y) * half;
+            c1.y = -(zp.x - zm.x) * half;
+            C[(size_t)(col + 1) * (n0 + 1) + r] = c1;
+        }
+    }
+}
+
+// Pass C: rpb rows per block of rows 0..n0, one image per blockIdx.y; the
+// inverse real FFT of each row's half spectrum, then the fftshift (row r to
+// (r + n0) mod G0, column c to (c + n1) mod G1) and, by the point symmetry of
+// an autocorrelation (A[-d] = A[d]), the mirrored row n0 - r with column c at
+// (n1 - c) mod G1; each thread stores two adjacent columns at once.  The
+// normalisation at each output position: mode 0 divides by norm (NaN below
+// threshold), mode 1 divides by norm (0 at or below threshold), mode 2 by the
+// pair count (n0 - |i - n0|)(n1 - |j - n1|) (NaN below threshold), mode -1
+// none.
+template <typename T, int E>
+__global__ void __launch_bounds__(512) fc_rows_inv(const typename Cx<T>::t *__restrict__ C, size_t c_img, int n0,
+                                                   int n1, int logh, int rpb, const double2 *__restrict__ tw, int N,
+                                                   const T *__restrict__ norm, int mode, T threshold,
+                                                   T *__restrict__ out) {
+    using V = typename Cx<T>::t;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    V *S = reinterpret_cast<V *>(fsm);
+    const int H = 1 << logh, G1 = 2 * H, G0 = 2 * n0, r0 = blockIdx.x * rpb;
+    C += (size_t)blockIdx.y * c_img;
+    out += (size_t)blockIdx.y * G0 * G1;
+    const int wstep = N / G1;
+    // Z[k] = (Y[k] + conj Y[H-k]) + i W^-k (Y[k] - conj Y[H-k]); rows fastest,
+    // the rpb rows of one k are contiguous in C
+    for (int idx = threadIdx.x; idx < rpb * H; idx += blockDim.x) {
+        const int k = idx / rpb, rr = idx - k * rpb, r = r0 + rr;
+        V z = cx_zero<V>();
+        if (r <= n0) {
+            const V yk = C[(size_t)k * (n0 + 1) + r], yc = cx_conj(C[(size_t)(H - k) * (n0 + 1) + r]);
+            const V e = cx_add(yk, yc), d = cx_sub(yk, yc);
+            const double2 wdd = __ldg(&tw[k * wstep]);
+            V w;
+            w.x = (T)wdd.x;
+            w.y = (T)-wdd.y;
+            const V wd = cx_mul(w, d);
+            z.x = e.x - wd.y;
+            z.y = e.y + wd.x;
+        }
+        S[fsw<V>(rr * H + k)] = z;
+    }
+    __syncthreads();
+    fc_fft<V, E, true>(S, logh, rpb, tw, N, FcNoLoad<V>{}, false);
+    const T scale = T(1) / (T)G1;  // the inverse's 1/H and the split's 1/2
+    auto fix = [&](int i, int j, T y) -> T {
+        if (mode == 0 || mode == 1) {
+            const T cn = norm[(size_t)i * G1 + j];
+            return mode == 0 ? (cn < threshold ? T(NAN) : y / cn) : (cn > threshold ? y / cn : T(0));
+        }
+        if (mode == 2) {
+            const T cn = (T)((int64_t)(n0 - abs(i - n0)) * (n1 - abs(j - n1)));
+            return cn < threshold ? T(NAN) : y / cn;
+        }
+        return y;
+    };
+    auto put2 = [&](int i, int j, T y0, T y1) {  // columns j (even), j + 1
+        V p;
+        p.x = fix(i, j, y0);
+        p.y = fix(i, j + 1, y1);
+        *reinterpret_cast<V *>(out + (size_t)i * G1 + j) = p;
+    };
+    for (int idx = threadIdx.x; idx < rpb * H; idx += blockDim.x) {
+        const int rr = idx >> logh, k = idx & (H - 1), r = r0 + rr;
+        if (r > n0) continue;
+        // value k holds columns c = 2k (x) and 2k + 1 (y)
+        const V z = S[fsw<V>(rr * H + k)];
+        const int i = (r + n0) & (G0 - 1), im = (n0 - r) & (G0 - 1);
+        put2(i, (2 * k + n1) & (G1 - 1), z.x * scale, z.y * scale);
+        if (im != i) {
+            // mirrored columns (n1 - 2k, n1 - 2k + 1) hold c = 2k and c = 2k - 1
+            const V zp = S[fsw<V>(rr * H + ((k - 1) & (H - 1)))];
+            put2(im, (n1 - 2 * k) & (G1 - 1), z.x * scale, zp.y * scale);
+        }
+    }
+}
+
+// tw[m] = exp(-2 pi i m / N), m = 0..N-1, in double precision for both dtypes
+__global__ void fc_twiddle_kernel(double2 *tw, int N) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= N) return;
+    double sn, cs;
+    sincospi(-2.0 * (double)m / (double)N, &sn, &cs);
+    tw[m] = make_double2(cs, sn);
 }
 
 static int ew_blocks(int64_t n) {
@@ -113,6 +546,22 @@ extern "C" idiwf_status idiwf_corr_crop(const void *full, int32_t dtype, int64_t
         D.n[k] = n[k];
         total *= 2 * (int64_t)n[k];
     }
+    if (ndim == 2 && batch * 2 * (int64_t)n[0] <= 65535) {
+        const dim3 grid((unsigned)std::min<int64_t>((2 * (int64_t)n[1] + 255) / 256, 64),
+                        (unsigned)(batch * 2 * n[0]));
+        if (dtype == IDIWF_F64)
+            crop2d_kernel<double><<<grid, 256, 0, stream>>>(static_cast<const double *>(full), g[0], g[1], n[0], n[1],
+                                                            static_cast<const double *>(norm), mode, threshold,
+                                                            static_cast<double *>(out));
+        else if (dtype == IDIWF_F32)
+            crop2d_kernel<float><<<grid, 256, 0, stream>>>(static_cast<const float *>(full), g[0], g[1], n[0], n[1],
+                                                           static_cast<const float *>(norm), mode, (float)threshold,
+                                                           static_cast<float *>(out));
+        else
+            return set_error(IDIWF_ERR_INVALID_ARGUMENT, "dtype must be IDIWF_F64 or IDIWF_F32");
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+        return IDIWF_OK;
+    }
     if (dtype == IDIWF_F64)
         crop_kernel<double><<<ew_blocks(total), 256, 0, stream>>>(static_cast<const double *>(full), batch, D,
                                                                   static_cast<const double *>(norm), mode, threshold,
@@ -135,4 +584,126 @@ extern "C" idiwf_status idiwf_welford_update(const float *x, float *mean, float 
     welford_kernel<<<ew_blocks(n), 256, 0, stream>>>(x, mean, nvar, n, count);
     IDIWF_CUDA_CHECK(cudaGetLastError());
     return IDIWF_OK;
+}
+
+// Workspace of idiwf_fft_autocorr: the twiddle table, then T and C of one
+// group of images, each 256-byte aligned.
+static size_t fc_align(size_t b) { return (b + 255) & ~(size_t)255; }
+static bool fc_pow2(int v) { return v >= 4 && v <= 4096 && (v & (v - 1)) == 0; }
+static int fc_log2(int v) {
+    int l = 0;
+    while ((1 << l) < v) ++l;
+    return l;
+}
+struct FcPlan {
+    int n0, n1, H, G0, G1, N, logh, logg0;
+    int rpb, cpb;         // rows per block (passes A and C), columns per block (pass B)
+    size_t vsz;           // bytes per complex value
+    size_t t_img, c_img;  // complex values of T and C per image
+    size_t tw_bytes, t_bytes, c_bytes;
+    int64_t group;        // images per launch
+};
+// Images per launch: all of them while T and C of the group stay within
+// 256 MB, else equal groups under that.
+static FcPlan fc_plan(int64_t batch, int n0, int n1, int dtype) {
+    FcPlan p{};
+    p.n0 = n0;
+    p.n1 = n1;
+    p.H = n1;
+    p.G0 = 2 * n0;
+    p.G1 = 2 * n1;
+    p.N = std::max(p.G0, p.G1);
+    p.logh = fc_log2(p.H);
+    p.logg0 = fc_log2(p.G0);
+    p.vsz = dtype == IDIWF_F64 ? 16 : 8;
+    p.rpb = std::max(1, std::min(kFcBlockElems / p.H, n0));
+    p.cpb = std::max(1, std::min(kFcBlockElems / p.G0, 1 << fc_log2(p.H + 1)));
+    p.t_img = (size_t)(p.H + 1) * n0;
+    p.c_img = (size_t)(p.H + 1) * (n0 + 1);
+    p.tw_bytes = fc_align((size_t)p.N * sizeof(double2));
+    const size_t per = (p.t_img + p.c_img) * p.vsz;
+    const int64_t gmax = std::max<int64_t>(1, std::min<int64_t>(65535, (int64_t)((256u << 20) / per)));
+    const int64_t ngroups = (std::max<int64_t>(batch, 1) + gmax - 1) / gmax;
+    p.group = (std::max<int64_t>(batch, 1) + ngroups - 1) / ngroups;
+    p.t_bytes = fc_align(p.t_img * p.vsz * p.group);
+    p.c_bytes = fc_align(p.c_img * p.vsz * p.group);
+    return p;
+}
+
+extern "C" size_t idiwf_fft_autocorr_workspace_size(int64_t batch, int32_t n0, int32_t n1, int32_t dtype) {
+    if (batch <= 0 || !fc_pow2(n0) || !fc_pow2(n1) || (dtype != IDIWF_F64 && dtype != IDIWF_F32)) return 0;
+    const FcPlan p = fc_plan(batch, n0, n1, dtype);
+    return p.tw_bytes + p.t_bytes + p.c_bytes;
+}
+
+template <typename T, int EA, int EB>
+static idiwf_status fc_launch(const T *x, int64_t batch, const FcPlan &p, const T *norm, int mode, double threshold,
+                              T *out, const double2 *tw, typename Cx<T>::t *Tt, typename Cx<T>::t *C,
+                              cudaStream_t stream) {
+    using V = typename Cx<T>::t;
+    const int thrA = std::max(1, p.rpb * p.H / EA), thrB = std::max(1, p.cpb * p.G0 / EB);
+    const size_t smA = (size_t)p.rpb * p.H * sizeof(V), smB = (size_t)p.cpb * p.G0 * sizeof(V);
+    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fc_rows_fwd<T, EA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
+    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fc_rows_inv<T, EA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
+    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fc_cols<T, EB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
+    const unsigned blkA = (unsigned)((p.n0 + p.rpb - 1) / p.rpb), blkC = (unsigned)((p.n0 + 1 + p.rpb - 1) / p.rpb);
+    const unsigned blkB = (unsigned)((p.H + 1 + p.cpb - 1) / p.cpb);
+    const size_t in_img = (size_t)p.n0 * p.n1, out_img = (size_t)p.G0 * p.G1;
+    for (int64_t b0 = 0; b0 < batch; b0 += p.group) {
+        const unsigned g = (unsigned)std::min<int64_t>(p.group, batch - b0);
+        fc_rows_fwd<T, EA><<<dim3(blkA, g), thrA, smA, stream>>>(x + b0 * in_img, p.n0, p.n1, p.logh, p.rpb, tw, p.N,
+                                                                    Tt, p.t_img);
+        fc_cols<T, EB><<<dim3(blkB, g), thrB, smB, stream>>>(Tt, p.t_img, p.n0, p.H + 1, p.logg0, p.cpb, tw, p.N, C,
+                                                             p.c_img);
+        fc_rows_inv<T, EA><<<dim3(blkC, g), thrA, smA, stream>>>(C, p.c_img, p.n0, p.n1, p.logh, p.rpb, tw, p.N, norm,
+                                                                    mode, (T)threshold, out + b0 * out_img);
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+    }
+    return IDIWF_OK;
+}
+
+template <typename T>
+static idiwf_status fc_run(const T *x, int64_t batch, const FcPlan &p, const T *norm, int mode, double threshold,
+                           T *out, unsigned char *ws, cudaStream_t stream) {
+    using V = typename Cx<T>::t;
+    double2 *tw = reinterpret_cast<double2 *>(ws);
+    V *Tt = reinterpret_cast<V *>(ws + p.tw_bytes);
+    V *C = reinterpret_cast<V *>(ws + p.tw_bytes + p.t_bytes);
+    fc_twiddle_kernel<<<(p.N + 255) / 256, 256, 0, stream>>>(tw, p.N);
+    IDIWF_CUDA_CHECK(cudaGetLastError());
+    if constexpr (sizeof(T) == 4) {
+        return fc_launch<T, 16, 16>(x, batch, p, norm, mode, threshold, out, tw, Tt, C, stream);
+    } else {
+        if (p.G0 > kFcBlockElems)  // one 8192-point column per block: 16 values per thread keep it at 512 threads
+            return fc_launch<T, 8, 16>(x, batch, p, norm, mode, threshold, out, tw, Tt, C, stream);
+        return fc_launch<T, 8, 8>(x, batch, p, norm, mode, threshold, out, tw, Tt, C, stream);
+    }
+}
+
+extern "C" idiwf_status idiwf_fft_autocorr(const void *x, int32_t dtype, int64_t batch, int32_t n0, int32_t n1,
+                                           const void *norm, int32_t mode, double threshold, void *out,
+                                           void *workspace, size_t workspace_bytes, cudaStream_t stream) {
+    if (!x || !out) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (batch <= 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "batch must be positive");
+    if (!fc_pow2(n0) || !fc_pow2(n1))
+        return set_error(IDIWF_ERR_UNSUPPORTED, "the hand-written autocorrelation takes powers of two from 4 to 4096");
+    if (mode < -1 || mode > 2) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "mode must be -1, 0, 1 or 2");
+    if ((mode == 0 || mode == 1) && !norm) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "modes 0 and 1 need norm");
+    const size_t need = idiwf_fft_autocorr_workspace_size(batch, n0, n1, dtype);
+    if (need == 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "dtype must be IDIWF_F64 or IDIWF_F32");
+    if (!workspace || workspace_bytes < need)
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_fft_autocorr_workspace_size()");
+    if (reinterpret_cast<uintptr_t>(workspace) & 255)
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    // rows are read and written as pairs of values
+    const uintptr_t pair = dtype == IDIWF_F64 ? 15 : 7;
+    if ((reinterpret_cast<uintptr_t>(x) & pair) || (reinterpret_cast<uintptr_t>(out) & pair))
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "x and out must be aligned to two elements");
+    const FcPlan p = fc_plan(batch, n0, n1, dtype);
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    if (dtype == IDIWF_F64)
+        return fc_run<double>(static_cast<const double *>(x), batch, p, static_cast<const double *>(norm), mode,
+                              threshold, static_cast<double *>(out), ws, stream);
+    return fc_run<float>(static_cast<const float *>(x), batch, p, static_cast<const float *>(norm), mode, threshold,
+                         static_cast<float *>(out), ws, stream);
 }

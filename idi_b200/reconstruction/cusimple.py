@@ -1,11 +1,14 @@
 """Drop-in for ``idi.reconstruction.cusimple``: FFT autocorrelation on the GPU
 (``idi/reconstruction/cusimple.py:6-121``).
 
-The transforms are cuFFT's (through ``torch.fft``); the power spectrum, the
-fftshift + centre crop with its normalisation and the correlator's running
-mean / variance are this library's kernels (``idiwf_power_spectrum``,
-``idiwf_corr_crop``, ``idiwf_welford_update``).  Inputs may be numpy arrays
-or CUDA tensors; results are numpy unless ``returngpu``.
+Two correlated axes of power-of-two lengths (4 to 4096) go through this
+library's own FFTs end to end (``idiwf_fft_autocorr``: the padded transform,
+the power spectrum, the inverse, the fftshift and the normalisation).  Other
+shapes use cuFFT's transforms (through ``torch.fft``) with this library's
+power-spectrum and crop kernels around them (``idiwf_power_spectrum``,
+``idiwf_corr_crop``).  The correlator's running mean / variance is
+``idiwf_welford_update``.  Inputs may be numpy arrays or CUDA tensors;
+results are numpy unless ``returngpu``.
 """
 
 from __future__ import annotations
@@ -84,6 +87,36 @@ def _autocorr(x, nax, fftshape):
     return torch.fft.irfftn(spec, dim=dims)
 
 
+def _hand_ok(shape, dtype):
+    """Whether ``idiwf_fft_autocorr`` takes these two correlated axes."""
+    return (len(shape) == 2 and dtype in (torch.float32, torch.float64)
+            and all(4 <= int(s) <= 4096 and (int(s) & (int(s) - 1)) == 0 for s in shape))
+
+
+def _hand_autocorr(x, mode=-1, norm=None, threshold=0.0):
+    """Shifted autocorrelation ((2 n0) x (2 n1), no crop needed) of the last two axes of
+    ``x`` (power-of-two lengths) by ``idiwf_fft_autocorr``; ``mode`` as there
+    (-1 none, 0 / 1 divide by ``norm``, 2 divide by the pair count)."""
+    x = x.contiguous()
+    if x.data_ptr() % (2 * x.element_size()):
+        x = x.clone()  # rows are read as pairs of values
+    n0, n1 = int(x.shape[-2]), int(x.shape[-1])
+    lead = tuple(x.shape[:-2])
+    batch = int(np.prod(lead)) if lead else 1
+    out = torch.empty(lead + (2 * n0, 2 * n1), dtype=x.dtype, device=x.device)
+    if norm is not None:
+        norm = norm.to(x.dtype).contiguous()
+    lib = nat.load()
+    code = _code(x)
+    nbytes = lib.idiwf_fft_autocorr_workspace_size(batch, n0, n1, code)
+    ws = _core.WORKSPACES.get(nbytes, x.device, "fftcorr")
+    nat.check(lib.idiwf_fft_autocorr(
+        ctypes.c_void_p(x.data_ptr()), code, batch, n0, n1,
+        ctypes.c_void_p(norm.data_ptr()) if norm is not None else None, int(mode), float(threshold),
+        ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(), _stream(x.device)))
+    return out
+
+
 def corr(input, axes=(-1, -2), norm=False, returngpu=False, **kwargs):
     """Autocorrelation of ``input`` along ``axes`` (default the last two),
     output 2n per correlated axis with zero shift at index n.  ``norm``
@@ -100,12 +133,17 @@ def corr(input, axes=(-1, -2), norm=False, returngpu=False, **kwargs):
     if norm:
         x = x * (1 / x.mean(dim=others if others else None, keepdim=bool(others)))
     moved = torch.movedim(x, axes, list(range(x.ndim - len(axes), x.ndim))).contiguous()
-    full = _autocorr(moved, len(axes), fftshape)
-    pairs = None
-    if norm:
-        ones = torch.ones(sizes, dtype=x.dtype, device=x.device)
-        pairs = _crop(_autocorr(ones, len(axes), fftshape), len(axes), sizes)
-    ret = _crop(full, len(axes), sizes, norm=pairs, mode=0, threshold=0.9)
+    if _hand_ok(sizes, x.dtype):
+        # the pair count in closed form: the transform of ones in the
+        # reference rounds to the same integers, and the same < 0.9 positions
+        ret = _hand_autocorr(moved, mode=2 if norm else -1, threshold=0.9)
+    else:
+        full = _autocorr(moved, len(axes), fftshape)
+        pairs = None
+        if norm:
+            ones = torch.ones(sizes, dtype=x.dtype, device=x.device)
+            pairs = _crop(_autocorr(ones, len(axes), fftshape), len(axes), sizes)
+        ret = _crop(full, len(axes), sizes, norm=pairs, mode=0, threshold=0.9)
     ret = torch.movedim(ret, list(range(x.ndim - len(axes), x.ndim)), axes)
     if returngpu:
         return ret
@@ -135,6 +173,8 @@ class correlator2d:
     def _corr(self, x):
         if self._fftshape is None:
             self._fftshape = [fastlen(2 * s) for s in x.shape[-2:]]
+        if _hand_ok(x.shape[-2:], x.dtype):
+            return _hand_autocorr(x)
         return _crop(_autocorr(x, 2, self._fftshape), 2, list(x.shape[-2:]))
 
     def add(self, input, mask=None) -> None:
@@ -157,8 +197,11 @@ class correlator2d:
         else:
             maskcorr = self._corr(torch.ones_like(x))
             self._maskcorr = maskcorr
-        c = _crop(_autocorr(x, 2, self._fftshape or [fastlen(2 * s) for s in x.shape]), 2, list(x.shape),
-                  norm=maskcorr, mode=1, threshold=0.5)
+        if _hand_ok(x.shape, x.dtype):
+            c = _hand_autocorr(x, mode=1, norm=maskcorr, threshold=0.5)
+        else:
+            c = _crop(_autocorr(x, 2, self._fftshape or [fastlen(2 * s) for s in x.shape]), 2, list(x.shape),
+                      norm=maskcorr, mode=1, threshold=0.5)
         if self._mean is None:
             self._mean = torch.empty_like(c)
             self._nvar = torch.empty_like(c)

@@ -459,8 +459,33 @@ idiwf_status idiwf_qcorr_3d(const float *zd, const float *images, int32_t n_imag
                             void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
-/* FFT autocorrelation helpers (the transforms are the caller's, e.g. cuFFT)  */
+/* FFT autocorrelation                                                      */
 /* ------------------------------------------------------------------------ */
+
+/*
+ * The whole autocorrelation of idi/reconstruction/cusimple.py:6-38 for 2D
+ * power-of-two shapes, by this library's own FFTs: for each of `batch` images
+ * x[b] (n0 x n1 of dtype, row-major, contiguous, batch-major),
+ *     out[b] = fftshift(irfft2(|rfft2(x[b], (2 n0, 2 n1))|^2))
+ * ((2 n0) x (2 n1) of dtype) -- the reference's padded length fastlen(2 n) is
+ * 2 n for these shapes, so its centre crop is the whole shifted array.  Then,
+ * per output position (i, j): mode -1 nothing; mode 0 y / norm, NaN where
+ * norm < threshold; mode 1 y / norm where norm > threshold, else 0 (norm:
+ * (2 n0) x (2 n1) of dtype); mode 2 y / count with the pair count
+ * count = (n0 - |i - n0|)(n1 - |j - n1|), NaN where count < threshold (the
+ * norm=True result of cusimple.py:23-34 without a second transform).
+ * n0, n1: powers of two from 4 to 4096 (else IDIWF_ERR_UNSUPPORTED); x and
+ * out aligned to two elements; workspace: idiwf_fft_autocorr_workspace_size()
+ * bytes for this batch and shape, 256-byte aligned (the twiddle table and the
+ * intermediates of one group of images; groups run one after another, 0 for
+ * unsupported arguments).
+ */
+size_t idiwf_fft_autocorr_workspace_size(int64_t batch, int32_t n0, int32_t n1, int32_t dtype);
+idiwf_status idiwf_fft_autocorr(const void *x, int32_t dtype, int64_t batch, int32_t n0, int32_t n1,
+                                const void *norm, int32_t mode, double threshold, void *out, void *workspace,
+                                size_t workspace_bytes, cudaStream_t stream);
+
+/* Helpers around a library FFT (other shapes). */
 
 /* In place |X|^2 of n complex values (dtype IDIWF_F64: complex128, IDIWF_F32:
  * complex64): re <- re^2 + im^2, im <- 0.  The `ret = abs(ret) ** 2` of

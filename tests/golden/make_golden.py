@@ -289,6 +289,21 @@ def make_fftcorr(ref):
             c.add(im, mask=per_add) if per_add is not None else c.add(im)
         out[f"c2d_{name}__mean"] = c.mean
         out[f"c2d_{name}__std"] = c.std
+    # power-of-two shapes (the GPU library's own FFTs take these)
+    st2 = g.exponential(1.0, (2, 32, 64))
+    out["corr_pow2__in"] = st2
+    out["corr_pow2__out"] = simple.corr(st2)
+    out["corr_pow2_norm__out"] = simple.corr(st2, axes=(1, 2), norm=True)
+    imgs2 = g.exponential(1.0, (3, 16, 32)).astype(np.float32)
+    mask2 = (g.uniform(0, 1, (16, 32)) > 0.2).astype(np.float32)
+    out["c2dp__images"] = imgs2
+    out["c2dp__mask"] = mask2
+    for name, kw, per_add in (("plain", {}, None), ("mask", {"mask": mask2}, None), ("addmask", {}, mask2)):
+        c = simple.correlator2d(**kw)
+        for im in imgs2:
+            c.add(im, mask=per_add) if per_add is not None else c.add(im)
+        out[f"c2dp_{name}__mean"] = c.mean
+        out[f"c2dp_{name}__std"] = c.std
     return out
 
 

@@ -147,3 +147,56 @@ def test_product_has_no_cpu_fallback(monkeypatch):
     with pytest.raises(nat.NativeLibraryMissing):
         nat.load()
     importlib.reload(nat)
+
+
+def test_fft_autocorr_validation(lib):
+    """``idiwf_fft_autocorr``: its workspace size and the argument checks
+    that come before any device work."""
+    vp = ctypes.c_void_p
+    al = lambda b: (b + 255) // 256 * 256  # noqa: E731
+    # twiddles (N = max(2 n0, 2 n1) double pairs), then T (n1 + 1) x n0 and
+    # C (n1 + 1) x (n0 + 1) complex values per image of a group
+    need = lib.idiwf_fft_autocorr_workspace_size(1, 8, 16, nat.F64)
+    assert need == al(32 * 16) + al(17 * 8 * 16) + al(17 * 9 * 16)
+    assert lib.idiwf_fft_autocorr_workspace_size(3, 8, 16, nat.F32) == al(32 * 16) + al(3 * 17 * 8 * 8) + al(
+        3 * 17 * 9 * 8)
+    # 1024^2 FP64: 33.6 MB of T and C per image, groups of at most 7 images
+    # (256 MB), balanced: 8 images run as two groups of 4
+    assert lib.idiwf_fft_autocorr_workspace_size(8, 1024, 1024, nat.F64) == al(2048 * 16) + al(
+        4 * 1025 * 1024 * 16) + al(4 * 1025 * 1025 * 16)
+    for n0, n1 in ((6, 8), (8, 2), (8, 8192), (0, 8), (3, 4)):
+        assert lib.idiwf_fft_autocorr_workspace_size(1, n0, n1, nat.F64) == 0
+    assert lib.idiwf_fft_autocorr_workspace_size(1, 8, 8, 7) == 0
+    assert lib.idiwf_fft_autocorr_workspace_size(0, 8, 8, nat.F64) == 0
+
+    def call(x=4096, dtype=nat.F64, batch=1, n0=8, n1=16, norm=None, mode=-1, ws=4096, ws_bytes=need, out=8192):
+        return lib.idiwf_fft_autocorr(vp(x), dtype, batch, n0, n1, vp(norm) if norm else None, mode, 0.5, vp(out),
+                                      vp(ws), ws_bytes, None)
+
+    assert call(x=0) == nat.ERR_INVALID_ARGUMENT
+    assert call(out=0) == nat.ERR_INVALID_ARGUMENT
+    assert call(batch=0) == nat.ERR_INVALID_ARGUMENT
+    assert call(n0=12) == nat.ERR_UNSUPPORTED
+    assert b"powers of two" in lib.idiwf_last_error_string()
+    assert call(mode=3) == nat.ERR_INVALID_ARGUMENT
+    assert call(mode=0) == nat.ERR_INVALID_ARGUMENT  # no norm
+    assert call(ws_bytes=need - 1) == nat.ERR_WORKSPACE
+    assert call(batch=2) == nat.ERR_WORKSPACE  # sized for one image
+    assert call(ws=4096 + 128) == nat.ERR_WORKSPACE
+    assert call(x=4096 + 8) == nat.ERR_INVALID_ARGUMENT
+    assert call(out=8192 + 8) == nat.ERR_INVALID_ARGUMENT
+    assert call(dtype=9) == nat.ERR_INVALID_ARGUMENT
+
+
+def test_fft_autocorr_shape_predicate():
+    import torch
+
+    from idi_b200.reconstruction import cusimple
+
+    assert cusimple._hand_ok((1024, 1024), torch.float64)
+    assert cusimple._hand_ok((4, 4096), torch.float32)
+    assert not cusimple._hand_ok((2, 8), torch.float64)
+    assert not cusimple._hand_ok((8, 8192), torch.float64)
+    assert not cusimple._hand_ok((24, 32), torch.float64)
+    assert not cusimple._hand_ok((8, 8, 8), torch.float64)
+    assert not cusimple._hand_ok((8, 8), torch.float16)

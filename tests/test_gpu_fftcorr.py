@@ -67,3 +67,65 @@ def test_correlator2d_reference(golden, name):
     for attr in ("mean", "std"):
         ref = golden[f"c2d_{name}__{attr}"]
         np.testing.assert_allclose(getattr(c, attr), ref, rtol=2e-4, atol=2e-4 * np.abs(ref).max())
+
+
+def test_corr_pow2_reference(golden):
+    """Power-of-two shapes: this library's own FFTs (idiwf_fft_autocorr)."""
+    st = golden["corr_pow2__in"]
+    for key, kw in (("corr_pow2__out", {}), ("corr_pow2_norm__out", {"norm": True})):
+        ref = golden[key]
+        out = cusimple.corr(st, **kw)
+        assert out.shape == ref.shape
+        np.testing.assert_array_equal(np.isnan(out), np.isnan(ref))
+        np.testing.assert_allclose(out, ref, rtol=1e-10, atol=1e-10 * np.nanmax(np.abs(ref)))
+
+
+@pytest.mark.parametrize("name", ["plain", "mask", "addmask"])
+def test_correlator2d_pow2_reference(golden, name):
+    imgs, mask = golden["c2dp__images"], golden["c2dp__mask"]
+    c = cusimple.correlator2d(mask=mask) if name == "mask" else cusimple.correlator2d()
+    for im in imgs:
+        if name == "addmask":
+            c.add(im, mask=mask)
+        else:
+            c.add(im)
+    for attr in ("mean", "std"):
+        ref = golden[f"c2dp_{name}__{attr}"]
+        np.testing.assert_allclose(getattr(c, attr), ref, rtol=2e-4, atol=2e-4 * np.abs(ref).max())
+
+
+def _pair_count(n0, n1, dtype):
+    i = torch.arange(2 * n0, dtype=torch.float64)
+    j = torch.arange(2 * n1, dtype=torch.float64)
+    c = (n0 - (i - n0).abs())[:, None] * (n1 - (j - n1).abs())[None, :]
+    return c.to(dtype).cuda()
+
+
+@pytest.mark.parametrize("shape,dtype", [((4, 4), torch.float64), ((8, 64), torch.float64),
+                                         ((256, 128), torch.float64), ((1024, 1024), torch.float64),
+                                         ((2048, 16), torch.float64), ((64, 32), torch.float32),
+                                         ((512, 512), torch.float32)])
+def test_hand_fft_vs_cufft(shape, dtype):
+    """The hand-written FFT autocorrelation against cuFFT's transforms with the
+    same crop, on a batch of 3, plain and divided by the pair count."""
+    g = torch.Generator(device="cuda").manual_seed(sum(shape))
+    x = torch.empty((3,) + shape, dtype=dtype, device="cuda").exponential_(1.0, generator=g)
+    tol = 1e-12 if dtype == torch.float64 else 2e-5
+    ref = cusimple._crop(cusimple._autocorr(x, 2, [2 * s for s in shape]), 2, list(shape))
+    hand = cusimple._hand_autocorr(x)
+    assert hand.shape == ref.shape
+    assert (hand - ref).abs().max().item() <= tol * ref.abs().max().item()
+    count = _pair_count(*shape, dtype)
+    hn = cusimple._hand_autocorr(x, mode=2, threshold=0.9)
+    rn = torch.where(count < 0.9, torch.full_like(ref, float("nan")), ref / count)
+    assert torch.equal(torch.isnan(hn), torch.isnan(rn))
+    ok = ~torch.isnan(rn)
+    assert ((hn - rn).abs() * count)[ok].max().item() <= 2 * tol * ref.abs().max().item()
+
+
+def test_other_shapes_take_cufft():
+    assert not cusimple._hand_ok((12, 8), torch.float64)
+    x = torch.ones((12, 8), dtype=torch.float64, device="cuda")
+    # a non-power-of-two shape still goes through cuFFT
+    c = cusimple.corr(x, returngpu=True)
+    assert c.shape == (24, 16)
