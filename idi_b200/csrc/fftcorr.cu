@@ -172,11 +172,31 @@ template <typename V> __device__ __forceinline__ V cx_zero() {
 // in FP32 -- the block's values live in registers during a pass.
 constexpr int kFcBlockElems = 4096;
 
-// Shared-memory slot of complex value w: a 128-byte bank row holds 8 (FP64)
-// or 16 (FP32) values, and the row index XOR'ed into the slot spreads the
-// strided accesses of the passes over all banks.
-template <typename V> __device__ __forceinline__ int fsw(int w) {
-    return sizeof(V) == 16 ? (w ^ ((w >> 4) & 7)) : (w ^ ((w >> 5) & 15));
+// Shared-memory slot of complex value w.  A 128-byte bank row holds 8 (FP64)
+// or 16 (FP32) values, and shared memory serves 8 (FP64) or 16 (FP32) threads
+// of a warp at a time: one spare slot after every bank row of values makes
+// the strided writes of every pass hit distinct banks within each such
+// group, and rp spare slots per sequence (q = w >> logn) do the same for the
+// row-interleaved loops that touch the same column of rpb rows at once.
+struct FcSwz {
+    int logn;  // sequence length (31: no sequence term)
+    int rp;
+};
+template <typename V> __host__ __device__ constexpr int fc_lkc() { return sizeof(V) == 16 ? 3 : 4; }
+template <typename V> __device__ __forceinline__ int fsw(int w, FcSwz z) {
+    return w + (w >> fc_lkc<V>()) + (w >> z.logn) * z.rp;
+}
+// Layout of rpb interleaved rows of length 2^logn (rows shorter than a bank
+// row get no row term).
+template <typename V> __host__ __device__ inline FcSwz fc_rows_swz(int logn, int rpb) {
+    const int kc = 1 << fc_lkc<V>();
+    if (logn < fc_lkc<V>()) return FcSwz{31, 0};
+    return FcSwz{logn, rpb < kc ? kc / rpb : 1};
+}
+// Shared-memory values for count sequences of 2^logn with layout z.
+template <typename V> __host__ inline size_t fc_smem_values(int count, int logn, FcSwz z) {
+    const size_t tot = (size_t)count << logn;
+    return tot + (tot >> fc_lkc<V>()) + (z.logn == 31 ? 0 : (size_t)count * z.rp);
 }
 
 // d * exp(-/+ 2 pi i e / 16) for e = 0..7 (a constant after unrolling).
@@ -245,6 +265,11 @@ template <int R, typename V> __device__ __forceinline__ void twiddle_powers(V *v
     }
 }
 
+// First passes from global memory take one butterfly at a time in FP64,
+// where registers bound the blocks per SM; FP32 keeps all its loads in
+// flight.
+template <typename T> constexpr bool kFcOneAtATime = sizeof(T) == 8;
+
 // Loader of a pass that reads shared memory (never called).
 template <typename V> struct FcNoLoad {
     __device__ V operator()(int, int) const { return cx_zero<V>(); }
@@ -254,54 +279,75 @@ template <typename V> struct FcNoLoad {
 // butterfly g (thread t takes g = t, t + blockDim, ...) reads
 // in[j + r n/R] (from shared memory, or from `ld(sequence, index)` for a first
 // pass), multiplies by exp(-/+ 2 pi i (j mod Ns) r / (Ns R)), takes the R-point
-// DFT and writes out[(j - j mod Ns) R + j mod Ns + q Ns].
-template <typename V, int R, int E, bool INV, bool LOADER, class Ld>
-__device__ __forceinline__ void fc_pass(V *S, int logn, int count, int Ns, const double2 *__restrict__ tw, int N,
-                                        const Ld &ld) {
+// DFT and writes out[(j - j mod Ns) R + j mod Ns + q Ns].  In place: all reads
+// of the block come before its writes, except for a first pass whose loader
+// reads global memory only (LD_GLOBAL), which takes one butterfly at a time.
+template <typename V, int R, int E, bool INV, bool LOADER, bool LD_GLOBAL, class Ld>
+__device__ __forceinline__ void fc_pass(V *S, FcSwz z, int logn, int count, int Ns, const double2 *__restrict__ tw,
+                                        int N, const Ld &ld) {
     constexpr int NB = E / R;
     constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
     const int n = 1 << logn, lognb = logn - LR, nb = 1 << lognb, total = count << lognb;
-    V v[E];
+    if constexpr (LOADER && LD_GLOBAL) {
+        // Ns = 1: no twiddles
 #pragma unroll
-    for (int b = 0; b < NB; ++b) {
-        const int g = threadIdx.x + b * blockDim.x;
-        if (g < total) {
-            const int q = g >> lognb, j = g & (nb - 1);
+        for (int b = 0; b < NB; ++b) {
+            const int g = threadIdx.x + b * blockDim.x;
+            if (g < total) {
+                const int q = g >> lognb, j = g & (nb - 1);
+                V v[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if constexpr (LOADER)
-                    v[b * R + r] = ld(q, j + r * nb);
-                else
-                    v[b * R + r] = S[fsw<V>(q * n + j + r * nb)];
+                for (int r = 0; r < R; ++r) v[r] = ld(q, j + r * nb);
+                dft_reg<R, INV>(v);
+                const int base = q * n + j * R;
+#pragma unroll
+                for (int r = 0; r < R; ++r) S[fsw<V>(base + r, z)] = v[brevc(r, R)];
             }
         }
-    }
-    __syncthreads();
+        __syncthreads();
+    } else {
+        V v[E];
 #pragma unroll
-    for (int b = 0; b < NB; ++b) {
-        const int g = threadIdx.x + b * blockDim.x;
-        if (g < total) {
-            const int q = g >> lognb, j = g & (nb - 1), k = j & (Ns - 1);
-            if (Ns > 1) {
-                double2 w = __ldg(&tw[k * (N / (Ns * R))]);
-                if (INV) w.y = -w.y;
-                twiddle_powers<R>(&v[b * R], w);
+        for (int b = 0; b < NB; ++b) {
+            const int g = threadIdx.x + b * blockDim.x;
+            if (g < total) {
+                const int q = g >> lognb, j = g & (nb - 1);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if constexpr (LOADER)
+                        v[b * R + r] = ld(q, j + r * nb);
+                    else
+                        v[b * R + r] = S[fsw<V>(q * n + j + r * nb, z)];
+                }
             }
-            dft_reg<R, INV>(&v[b * R]);
-            const int base = q * n + (j - k) * R + k;
-#pragma unroll
-            for (int r = 0; r < R; ++r) S[fsw<V>(base + r * Ns)] = v[b * R + brevc(r, R)];
         }
+        __syncthreads();
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int g = threadIdx.x + b * blockDim.x;
+            if (g < total) {
+                const int q = g >> lognb, j = g & (nb - 1), k = j & (Ns - 1);
+                if (Ns > 1) {
+                    double2 w = __ldg(&tw[k * (N / (Ns * R))]);
+                    if (INV) w.y = -w.y;
+                    twiddle_powers<R>(&v[b * R], w);
+                }
+                dft_reg<R, INV>(&v[b * R]);
+                const int base = q * n + (j - k) * R + k;
+#pragma unroll
+                for (int r = 0; r < R; ++r) S[fsw<V>(base + r * Ns, z)] = v[b * R + brevc(r, R)];
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
 }
 
 // The FFT of `count` sequences of length 2^logn in place at S (natural order
 // in and out), E values per thread (count << logn <= E * blockDim.x); the
 // first pass reads through `ld` when from_loader.
-template <typename V, int E, bool INV, class Ld>
-__device__ __forceinline__ void fc_fft(V *S, int logn, int count, const double2 *__restrict__ tw, int N, const Ld &ld,
-                                       bool from_loader) {
+template <typename V, int E, bool INV, bool LD_GLOBAL, class Ld>
+__device__ __forceinline__ void fc_fft(V *S, FcSwz z, int logn, int count, const double2 *__restrict__ tw, int N,
+                                       const Ld &ld, bool from_loader) {
     constexpr int LMAX = E >= 16 ? 4 : 3;
     int Ns = 1;
     bool first = from_loader;
@@ -309,9 +355,9 @@ __device__ __forceinline__ void fc_fft(V *S, int logn, int count, const double2 
 #define FC_RUN(RR)                                                                          \
     do {                                                                                    \
         if (first)                                                                          \
-            fc_pass<V, RR, E, INV, true>(S, logn, count, Ns, tw, N, ld);                    \
+            fc_pass<V, RR, E, INV, true, LD_GLOBAL>(S, z, logn, count, Ns, tw, N, ld);      \
         else                                                                                \
-            fc_pass<V, RR, E, INV, false>(S, logn, count, Ns, tw, N, ld);                   \
+            fc_pass<V, RR, E, INV, false, false>(S, z, logn, count, Ns, tw, N, ld);         \
         first = false;                                                                      \
         Ns *= RR;                                                                           \
     } while (0)
@@ -325,7 +371,7 @@ __device__ __forceinline__ void fc_fft(V *S, int logn, int count, const double2 
 // Pass A: rpb rows per block, one image per blockIdx.y.  x: n0 x n1 real per
 // image; T: (H+1) x n0 complex per image (t_img values apart).
 template <typename T, int E>
-__global__ void __launch_bounds__(512) fc_rows_fwd(const T *__restrict__ x, int n0, int n1, int logh, int rpb,
+__global__ void __launch_bounds__(512, (sizeof(T) == 8 && E == 8) ? 2 : 1) fc_rows_fwd(const T *__restrict__ x, int n0, int n1, int logh, int rpb,
                                                    const double2 *__restrict__ tw, int N,
                                                    typename Cx<T>::t *__restrict__ Tt, size_t t_img) {
     using V = typename Cx<T>::t;
@@ -342,13 +388,14 @@ __global__ void __launch_bounds__(512) fc_rows_fwd(const T *__restrict__ x, int 
         if (r < n0 && k < (H >> 1)) z = reinterpret_cast<const V *>(x + (size_t)r * n1)[k];
         return z;
     };
-    fc_fft<V, E, false>(S, logh, rpb, tw, N, ld, true);
+    const FcSwz z = fc_rows_swz<V>(logh, rpb);
+    fc_fft<V, E, false, kFcOneAtATime<T>>(S, z, logh, rpb, tw, N, ld, true);
     // X[k] = (Z[k] + conj Z[H-k]) / 2 + W^k (Z[k] - conj Z[H-k]) / (2i), W = exp(-2 pi i / G1)
-    const int wstep = N / (2 * H);
+    const int wstep = N / (2 * H), lrpb = 31 - __clz(rpb);
     for (int idx = threadIdx.x; idx < (H + 1) * rpb; idx += blockDim.x) {
-        const int k = idx / rpb, rr = idx - k * rpb, r = r0 + rr;
+        const int k = idx >> lrpb, rr = idx & (rpb - 1), r = r0 + rr;
         if (r >= n0) continue;
-        const V zk = S[fsw<V>(rr * H + (k & (H - 1)))], zc = cx_conj(S[fsw<V>(rr * H + ((H - k) & (H - 1)))]);
+        const V zk = S[fsw<V>(rr * H + (k & (H - 1)), z)], zc = cx_conj(S[fsw<V>(rr * H + ((H - k) & (H - 1)), z)]);
         const V e = cx_add(zk, zc), d = cx_sub(zk, zc);
         V o;  // d / (2i) = (d.y, -d.x) / 2
         o.x = d.y;
@@ -374,7 +421,7 @@ __global__ void __launch_bounds__(512) fc_rows_fwd(const T *__restrict__ x, int 
 // rows 0..n0 only (the rest follows from the point symmetry in pass C).
 // The inverse runs on the first npair * G0 / E threads.
 template <typename T, int E>
-__global__ void __launch_bounds__(512) fc_cols(const typename Cx<T>::t *__restrict__ Tt, size_t t_img, int n0,
+__global__ void __launch_bounds__(512, (sizeof(T) == 8 && E == 8) ? 2 : 1) fc_cols(const typename Cx<T>::t *__restrict__ Tt, size_t t_img, int n0,
                                                int ncols, int logg0, int cpb, const double2 *__restrict__ tw, int N,
                                                typename Cx<T>::t *__restrict__ C, size_t c_img) {
     using V = typename Cx<T>::t;
@@ -389,24 +436,25 @@ __global__ void __launch_bounds__(512) fc_cols(const typename Cx<T>::t *__restri
         if (r < n0 && col < ncols) z = Tt[(size_t)col * n0 + r];
         return z;
     };
-    fc_fft<V, E, false>(S, logg0, cpb, tw, N, ldT, true);
+    const FcSwz sz{31, 0};
+    fc_fft<V, E, false, kFcOneAtATime<T>>(S, sz, logg0, cpb, tw, N, ldT, true);
     const int npair = (cpb + 1) >> 1;
     auto ldP = [&](int q, int r) -> V {
-        const V u = S[fsw<V>(2 * q * G0 + r)];
+        const V u = S[fsw<V>(2 * q * G0 + r, sz)];
         V z;
         z.x = u.x * u.x + u.y * u.y;
         z.y = T(0);
         if (2 * q + 1 < cpb) {
-            const V w = S[fsw<V>((2 * q + 1) * G0 + r)];
+            const V w = S[fsw<V>((2 * q + 1) * G0 + r, sz)];
             z.y = w.x * w.x + w.y * w.y;
         }
         return z;
     };
-    fc_fft<V, E, true>(S, logg0, npair, tw, N, ldP, true);
+    fc_fft<V, E, true, false>(S, sz, logg0, npair, tw, N, ldP, true);
     const T half = T(0.5) / (T)G0;
-    for (int idx = threadIdx.x; idx < npair * (n0 + 1); idx += blockDim.x) {
-        const int q = idx / (n0 + 1), r = idx - q * (n0 + 1);
-        const V zp = S[fsw<V>(q * G0 + r)], zm = cx_conj(S[fsw<V>(q * G0 + ((G0 - r) & (G0 - 1)))]);
+    int q = threadIdx.x / (n0 + 1), r = threadIdx.x - q * (n0 + 1);
+    for (; q < npair; r += blockDim.x, q += r / (n0 + 1), r %= (n0 + 1)) {
+        const V zp = S[fsw<V>(q * G0 + r, sz)], zm = cx_conj(S[fsw<V>(q * G0 + ((G0 - r) & (G0 - 1)), sz)]);
         const int col = k0 + 2 * q;
         if (col < ncols) {
             V c0;
@@ -433,7 +481,7 @@ __global__ void __launch_bounds__(512) fc_cols(const typename Cx<T>::t *__restri
 // pair count (n0 - |i - n0|)(n1 - |j - n1|) (NaN below threshold), mode -1
 // none.
 template <typename T, int E>
-__global__ void __launch_bounds__(512) fc_rows_inv(const typename Cx<T>::t *__restrict__ C, size_t c_img, int n0,
+__global__ void __launch_bounds__(512, (sizeof(T) == 8 && E == 8) ? 2 : 1) fc_rows_inv(const typename Cx<T>::t *__restrict__ C, size_t c_img, int n0,
                                                    int n1, int logh, int rpb, const double2 *__restrict__ tw, int N,
                                                    const T *__restrict__ norm, int mode, T threshold,
                                                    T *__restrict__ out) {
@@ -444,10 +492,12 @@ __global__ void __launch_bounds__(512) fc_rows_inv(const typename Cx<T>::t *__re
     C += (size_t)blockIdx.y * c_img;
     out += (size_t)blockIdx.y * G0 * G1;
     const int wstep = N / G1;
+    const FcSwz sz = fc_rows_swz<V>(logh, rpb);
     // Z[k] = (Y[k] + conj Y[H-k]) + i W^-k (Y[k] - conj Y[H-k]); rows fastest,
     // the rpb rows of one k are contiguous in C
+    const int lrpb = 31 - __clz(rpb);
     for (int idx = threadIdx.x; idx < rpb * H; idx += blockDim.x) {
-        const int k = idx / rpb, rr = idx - k * rpb, r = r0 + rr;
+        const int k = idx >> lrpb, rr = idx & (rpb - 1), r = r0 + rr;
         V z = cx_zero<V>();
         if (r <= n0) {
             const V yk = C[(size_t)k * (n0 + 1) + r], yc = cx_conj(C[(size_t)(H - k) * (n0 + 1) + r]);
@@ -460,10 +510,10 @@ __global__ void __launch_bounds__(512) fc_rows_inv(const typename Cx<T>::t *__re
             z.x = e.x - wd.y;
             z.y = e.y + wd.x;
         }
-        S[fsw<V>(rr * H + k)] = z;
+        S[fsw<V>(rr * H + k, sz)] = z;
     }
     __syncthreads();
-    fc_fft<V, E, true>(S, logh, rpb, tw, N, FcNoLoad<V>{}, false);
+    fc_fft<V, E, true, false>(S, sz, logh, rpb, tw, N, FcNoLoad<V>{}, false);
     const T scale = T(1) / (T)G1;  // the inverse's 1/H and the split's 1/2
     auto fix = [&](int i, int j, T y) -> T {
         if (mode == 0 || mode == 1) {
@@ -486,12 +536,12 @@ __global__ void __launch_bounds__(512) fc_rows_inv(const typename Cx<T>::t *__re
         const int rr = idx >> logh, k = idx & (H - 1), r = r0 + rr;
         if (r > n0) continue;
         // value k holds columns c = 2k (x) and 2k + 1 (y)
-        const V z = S[fsw<V>(rr * H + k)];
+        const V z = S[fsw<V>(rr * H + k, sz)];
         const int i = (r + n0) & (G0 - 1), im = (n0 - r) & (G0 - 1);
         put2(i, (2 * k + n1) & (G1 - 1), z.x * scale, z.y * scale);
         if (im != i) {
             // mirrored columns (n1 - 2k, n1 - 2k + 1) hold c = 2k and c = 2k - 1
-            const V zp = S[fsw<V>(rr * H + ((k - 1) & (H - 1)))];
+            const V zp = S[fsw<V>(rr * H + ((k - 1) & (H - 1)), sz)];
             put2(im, (n1 - 2 * k) & (G1 - 1), z.x * scale, zp.y * scale);
         }
     }
@@ -642,7 +692,8 @@ static idiwf_status fc_launch(const T *x, int64_t batch, const FcPlan &p, const 
                               cudaStream_t stream) {
     using V = typename Cx<T>::t;
     const int thrA = std::max(1, p.rpb * p.H / EA), thrB = std::max(1, p.cpb * p.G0 / EB);
-    const size_t smA = (size_t)p.rpb * p.H * sizeof(V), smB = (size_t)p.cpb * p.G0 * sizeof(V);
+    const size_t smA = fc_smem_values<V>(p.rpb, p.logh, fc_rows_swz<V>(p.logh, p.rpb)) * sizeof(V);
+    const size_t smB = fc_smem_values<V>(p.cpb, p.logg0, FcSwz{31, 0}) * sizeof(V);
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fc_rows_fwd<T, EA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fc_rows_inv<T, EA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fc_cols<T, EB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
