@@ -556,6 +556,356 @@ __global__ void fc_twiddle_kernel(double2 *tw, int N) {
     tw[m] = make_double2(cs, sn);
 }
 
+// ---------------------------------------------------------------------------
+// General lengths: the reference pads each axis to fastlen(2 n) (factors 2,
+// 3, 5, 7, 11).  The same three kernels, with mixed-radix Stockham passes
+// (radix 8/4/2 and 3, 5, 7, 11), rows packed in pairs as x_a + i x_b for the
+// row FFT, and the inverse along rows of length L1 = G1 through a complex
+// inverse of L1/2 values (the real parts only at frequencies 0 and L1/2, as
+// a c2r transform).  The output is the centre crop (i - n0) mod G0,
+// (j - n1) mod L1 of the shifted array.  An odd G1 is not taken: the
+// reference's inverse then has length G1 - 1, which is never a product of 2,
+// 3, 5, 7, 11 (it would be a smaller padded length).
+// ---------------------------------------------------------------------------
+// {cos, sin}(2 pi m / R) for R = 3, 5, 7, 11, m = 0..R-1 (offsets 0, 3, 8, 15)
+__constant__ double2 kFcgOdd[26] = {
+    {1.0, 0.0},
+    {-5.0e-1, 8.66025403784438646764e-1},
+    {-5.0e-1, -8.66025403784438646764e-1},
+    {1.0, 0.0},
+    {3.09016994374947424102e-1, 9.51056516295153572116e-1},
+    {-8.09016994374947424102e-1, 5.87785252292473129169e-1},
+    {-8.09016994374947424102e-1, -5.87785252292473129169e-1},
+    {3.09016994374947424102e-1, -9.51056516295153572116e-1},
+    {1.0, 0.0},
+    {6.23489801858733530525e-1, 7.81831482468029808708e-1},
+    {-2.22520933956314404289e-1, 9.74927912181823607018e-1},
+    {-9.00968867902419126236e-1, 4.33883739117558120476e-1},
+    {-9.00968867902419126236e-1, -4.33883739117558120476e-1},
+    {-2.22520933956314404289e-1, -9.74927912181823607018e-1},
+    {6.23489801858733530525e-1, -7.81831482468029808708e-1},
+    {1.0, 0.0},
+    {8.41253532831181168862e-1, 5.40640817455597582108e-1},
+    {4.15415013001886425529e-1, 9.09631995354518371412e-1},
+    {-1.42314838273285140444e-1, 9.89821441880932732376e-1},
+    {-6.54860733945285064057e-1, 7.55749574354258283774e-1},
+    {-9.5949297361449738989e-1, 2.81732556841429697711e-1},
+    {-9.5949297361449738989e-1, -2.81732556841429697711e-1},
+    {-6.54860733945285064057e-1, -7.55749574354258283774e-1},
+    {-1.42314838273285140444e-1, -9.89821441880932732376e-1},
+    {4.15415013001886425529e-1, -9.09631995354518371412e-1},
+    {8.41253532831181168862e-1, -5.40640817455597582108e-1},
+};
+template <int R> __host__ __device__ constexpr int fcg_odd_off() { return R == 3 ? 0 : R == 5 ? 3 : R == 7 ? 8 : 15; }
+
+// Register holding output q of fcg_dft<R>: bit-reversed for R = 2^m.
+template <int R> __host__ __device__ constexpr int fcg_out(int q) { return (R & (R - 1)) == 0 ? brevc(q, R) : q; }
+
+// R-point DFT in registers, output q in v[fcg_out<R>(q)]; odd R by the
+// symmetric pairs x_k +- x_{R-k} (real and imaginary halves), R = 2^m by
+// dft_reg.
+template <int R, bool INV, typename V> __device__ __forceinline__ void fcg_dft(V *v) {
+    using T = decltype(v[0].x);
+    if constexpr ((R & (R - 1)) == 0) {
+        dft_reg<R, INV>(v);
+    } else {
+        constexpr int h = (R - 1) / 2, off = fcg_odd_off<R>();
+        V a[h], b[h];
+        V x0 = v[0], X0 = v[0];
+#pragma unroll
+        for (int k = 1; k <= h; ++k) {
+            a[k - 1] = cx_add(v[k], v[R - k]);
+            b[k - 1] = cx_sub(v[k], v[R - k]);
+            X0 = cx_add(X0, a[k - 1]);
+        }
+        v[0] = X0;
+#pragma unroll
+        for (int q = 1; q <= h; ++q) {
+            V re = x0, im = cx_zero<V>();
+#pragma unroll
+            for (int k = 1; k <= h; ++k) {
+                const double2 cs = kFcgOdd[off + (k * q) % R];
+                re.x += a[k - 1].x * (T)cs.x;
+                re.y += a[k - 1].y * (T)cs.x;
+                im.x += b[k - 1].x * (T)cs.y;
+                im.y += b[k - 1].y * (T)cs.y;
+            }
+            // sum_k x_k W^{kq} = re -/+ i im (W = exp(-/+ 2 pi i / R))
+            V mi;  // -i * im
+            mi.x = im.y;
+            mi.y = -im.x;
+            v[q] = INV ? cx_sub(re, mi) : cx_add(re, mi);
+            v[R - q] = INV ? cx_add(re, mi) : cx_sub(re, mi);
+        }
+    }
+}
+
+// Radices of one general length n (pass order: 11, 7, 5, 3, then 8s, then
+// the remaining 4 or 2).
+constexpr int kFcgMaxPasses = 14;
+struct FcgRad {
+    int n, np;
+    int r[kFcgMaxPasses];
+};
+
+// Slot of value i of sequence q: sequences `stride` slots apart, one spare
+// slot per 8 (FP64) or 16 (FP32) values.
+template <typename V> __device__ __forceinline__ int fcg_slot(int q, int i, int stride) {
+    return q * stride + i + (i >> fc_lkc<V>());
+}
+
+// (a, b) = divmod(i, nb) for i = start, start + step, ...: one division at
+// the start, then additions.
+struct FcgIdx {
+    int a, b, da, db, nb;
+    __device__ __forceinline__ FcgIdx(int start, int step, int nb_) : nb(nb_) {
+        a = start / nb;
+        b = start - a * nb;
+        da = step / nb;
+        db = step - da * nb;
+    }
+    __device__ __forceinline__ void next() {
+        a += da;
+        b += db;
+        if (b >= nb) {
+            b -= nb;
+            ++a;
+        }
+    }
+};
+
+// Out-of-place Stockham pass of radix R (in -> out), one butterfly of R
+// values in registers per loop iteration.
+template <typename V, int R, bool INV>
+__device__ __forceinline__ void fcg_pass(const V *in, V *out, int stride, int n, int count, int Ns,
+                                         const double2 *__restrict__ tab, int ntab) {
+    const int nb = n / R, total = count * nb, tstep = ntab / (Ns * R);
+    FcgIdx it(threadIdx.x, blockDim.x, nb);
+    // k = j mod Ns (nb is a multiple of Ns, so the wrap of j keeps k)
+    const int dk = it.db % Ns;
+    int k = it.b % Ns;
+    for (int g = threadIdx.x; g < total; g += blockDim.x, it.next(), k = (k + dk >= Ns) ? k + dk - Ns : k + dk) {
+        const int q = it.a, j = it.b;
+        V v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = in[fcg_slot<V>(q, j + r * nb, stride)];
+        if (Ns > 1) {
+            double2 w = __ldg(&tab[k * tstep]);
+            if (INV) w.y = -w.y;
+            twiddle_powers<R>(v, w);
+        }
+        fcg_dft<R, INV>(v);
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) out[fcg_slot<V>(q, base + r * Ns, stride)] = v[fcg_out<R>(r)];
+    }
+}
+
+// The FFT of `count` sequences of length rad.n: the values from `ld` (or
+// already in A) go through the passes between buffers A and B; returns the
+// buffer holding the result.
+template <typename V, bool INV, class Ld>
+__device__ __forceinline__ V *fcg_fft(V *A, V *B, int stride, const FcgRad &rad, int count,
+                                      const double2 *__restrict__ tab, int ntab, const Ld &ld, bool from_loader) {
+    const int n = rad.n;
+    if (from_loader) {
+        FcgIdx it(threadIdx.x, blockDim.x, n);
+        for (int idx = threadIdx.x; idx < count * n; idx += blockDim.x, it.next())
+            A[fcg_slot<V>(it.a, it.b, stride)] = ld(it.a, it.b);
+        __syncthreads();
+    }
+    V *in = A, *out = B;
+    int Ns = 1;
+    for (int p = 0; p < rad.np; ++p) {
+        const int R = rad.r[p];
+        switch (R) {
+            case 2: fcg_pass<V, 2, INV>(in, out, stride, n, count, Ns, tab, ntab); break;
+            case 3: fcg_pass<V, 3, INV>(in, out, stride, n, count, Ns, tab, ntab); break;
+            case 4: fcg_pass<V, 4, INV>(in, out, stride, n, count, Ns, tab, ntab); break;
+            case 5: fcg_pass<V, 5, INV>(in, out, stride, n, count, Ns, tab, ntab); break;
+            case 7: fcg_pass<V, 7, INV>(in, out, stride, n, count, Ns, tab, ntab); break;
+            case 8: fcg_pass<V, 8, INV>(in, out, stride, n, count, Ns, tab, ntab); break;
+            default: fcg_pass<V, 11, INV>(in, out, stride, n, count, Ns, tab, ntab); break;
+        }
+        __syncthreads();
+        V *t = in;
+        in = out;
+        out = t;
+        Ns *= R;
+    }
+    return in;
+}
+
+// Pass A (general): ppb pairs of rows per block, one image per blockIdx.y;
+// rows 2p, 2p+1 as one complex sequence of length G1 (zero-padded from n1),
+// split by Hermitian symmetry into the two real spectra, columns k = 0..m-1
+// (m = G1/2 + 1) written to T[k][r].
+template <typename T>
+__global__ void __launch_bounds__(512) fcg_rows_fwd(const T *__restrict__ x, int n0, int n1, int ppb, FcgRad rad,
+                                                    int stride, const double2 *__restrict__ twg1, int m,
+                                                    typename Cx<T>::t *__restrict__ Tt, size_t t_img) {
+    using V = typename Cx<T>::t;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    V *S = reinterpret_cast<V *>(fsm);
+    const int G1 = rad.n, p0 = blockIdx.x * ppb;
+    x += (size_t)blockIdx.y * n0 * n1;
+    Tt += (size_t)blockIdx.y * t_img;
+    auto ld = [&](int q, int c) -> V {
+        V z = cx_zero<V>();
+        const int ra = 2 * (p0 + q);
+        if (c < n1) {
+            if (ra < n0) z.x = x[(size_t)ra * n1 + c];
+            if (ra + 1 < n0) z.y = x[(size_t)(ra + 1) * n1 + c];
+        }
+        return z;
+    };
+    const V *Z = fcg_fft<V, false>(S, S + ppb * stride, stride, rad, ppb, twg1, G1, ld, true);
+    // X_a[k] = (Z[k] + conj Z[-k]) / 2, X_b[k] = (Z[k] - conj Z[-k]) / (2i); pairs fastest
+    FcgIdx it(threadIdx.x, blockDim.x, ppb);
+    for (int idx = threadIdx.x; idx < m * ppb; idx += blockDim.x, it.next()) {
+        const int k = it.a, q = it.b, ra = 2 * (p0 + q);
+        if (ra >= n0) continue;
+        const V zk = Z[fcg_slot<V>(q, k, stride)];
+        const V zc = cx_conj(Z[fcg_slot<V>(q, k == 0 ? 0 : G1 - k, stride)]);
+        V xa;
+        xa.x = T(0.5) * (zk.x + zc.x);
+        xa.y = T(0.5) * (zk.y + zc.y);
+        Tt[(size_t)k * n0 + ra] = xa;
+        if (ra + 1 < n0) {
+            V xb;
+            xb.x = T(0.5) * (zk.y - zc.y);
+            xb.y = -T(0.5) * (zk.x - zc.x);
+            Tt[(size_t)k * n0 + ra + 1] = xb;
+        }
+    }
+}
+
+// Pass B (general): as fc_cols for a column length G0 = rad.n of any
+// factorisation.
+template <typename T>
+__global__ void __launch_bounds__(512) fcg_cols(const typename Cx<T>::t *__restrict__ Tt, size_t t_img, int n0,
+                                                int ncols, int cpb, FcgRad rad, int stride,
+                                                const double2 *__restrict__ twg0, typename Cx<T>::t *__restrict__ C,
+                                                size_t c_img) {
+    using V = typename Cx<T>::t;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    V *S = reinterpret_cast<V *>(fsm);
+    const int G0 = rad.n, k0 = blockIdx.x * cpb;
+    Tt += (size_t)blockIdx.y * t_img;
+    C += (size_t)blockIdx.y * c_img;
+    auto ldT = [&](int q, int r) -> V {
+        V z = cx_zero<V>();
+        const int col = k0 + q;
+        if (r < n0 && col < ncols) z = Tt[(size_t)col * n0 + r];
+        return z;
+    };
+    V *S2 = S + cpb * stride;
+    V *F = fcg_fft<V, false>(S, S2, stride, rad, cpb, twg0, G0, ldT, true);
+    const int npair = (cpb + 1) >> 1;
+    auto ldP = [&](int q, int r) -> V {
+        const V u = F[fcg_slot<V>(2 * q, r, stride)];
+        V z;
+        z.x = u.x * u.x + u.y * u.y;
+        z.y = T(0);
+        if (2 * q + 1 < cpb) {
+            const V w = F[fcg_slot<V>(2 * q + 1, r, stride)];
+            z.y = w.x * w.x + w.y * w.y;
+        }
+        return z;
+    };
+    // the packed spectra load into the other buffer, then the passes run
+    // between it and F
+    const V *P = fcg_fft<V, true>(F == S ? S2 : S, F, stride, rad, npair, twg0, G0, ldP, true);
+    const T half = T(0.5) / (T)G0;
+    FcgIdx it(threadIdx.x, blockDim.x, n0 + 1);
+    for (int idx = threadIdx.x; idx < npair * (n0 + 1); idx += blockDim.x, it.next()) {
+        const int q = it.a, r = it.b;
+        const V zp = P[fcg_slot<V>(q, r, stride)];
+        const V zm = cx_conj(P[fcg_slot<V>(q, r == 0 ? 0 : G0 - r, stride)]);
+        const int col = k0 + 2 * q;
+        if (col < ncols) {
+            V c0;
+            c0.x = (zp.x + zm.x) * half;
+            c0.y = (zp.y + zm.y) * half;
+            C[(size_t)col * (n0 + 1) + r] = c0;
+        }
+        if (2 * q + 1 < cpb && col + 1 < ncols) {
+            V c1;
+            c1.x = (zp.y - zm.y) * half;
+            c1.y = -(zp.x - zm.x) * half;
+            C[(size_t)(col + 1) * (n0 + 1) + r] = c1;
+        }
+    }
+}
+
+// Pass C (general): rpb rows per block of rows 0..n0; the inverse real FFT
+// of length L1 = 2 rad.n through a complex inverse FFT of length rad.n (the
+// real parts only at frequencies 0 and L1/2, as a c2r transform), then the
+// centre crop: output (i, j) of row r is column (j - n1) mod L1 for
+// i = n0 + r (r < n0), and by point symmetry column (n1 - j) mod L1 for the
+// mirrored row i = n0 - r.  Normalisation modes as fc_rows_inv.
+template <typename T>
+__global__ void __launch_bounds__(512) fcg_rows_inv(const typename Cx<T>::t *__restrict__ C, size_t c_img, int n0,
+                                                    int n1, int rpb, FcgRad rad, int stride,
+                                                    const double2 *__restrict__ twl1, const T *__restrict__ norm,
+                                                    int mode, T threshold, T *__restrict__ out) {
+    using V = typename Cx<T>::t;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    V *S = reinterpret_cast<V *>(fsm);
+    const int Hp = rad.n, L1 = 2 * Hp, r0 = blockIdx.x * rpb, W = 2 * n1;
+    C += (size_t)blockIdx.y * c_img;
+    out += (size_t)blockIdx.y * (2 * n0) * W;
+    // Z[k] = (Y[k] + conj Y[Hp-k]) + i W^-k (Y[k] - conj Y[Hp-k]); rows fastest
+    FcgIdx it(threadIdx.x, blockDim.x, rpb);
+    for (int idx = threadIdx.x; idx < rpb * Hp; idx += blockDim.x, it.next()) {
+        const int k = it.a, rr = it.b, r = r0 + rr;
+        V z = cx_zero<V>();
+        if (r <= n0) {
+            V yk = C[(size_t)k * (n0 + 1) + r], yc = cx_conj(C[(size_t)(Hp - k) * (n0 + 1) + r]);
+            if (k == 0) {
+                yk.y = T(0);
+                yc.y = T(0);
+            }
+            const V e = cx_add(yk, yc), d = cx_sub(yk, yc);
+            const double2 wdd = __ldg(&twl1[k]);
+            V w;
+            w.x = (T)wdd.x;
+            w.y = (T)-wdd.y;
+            const V wd = cx_mul(w, d);
+            z.x = e.x - wd.y;
+            z.y = e.y + wd.x;
+        }
+        S[fcg_slot<V>(rr, k, stride)] = z;
+    }
+    __syncthreads();
+    const V *Z = fcg_fft<V, true>(S, S + rpb * stride, stride, rad, rpb, twl1, L1, FcNoLoad<V>{}, false);
+    const T scale = T(1) / (T)L1;
+    auto val = [&](int rr, int c) -> T {
+        const V z = Z[fcg_slot<V>(rr, c >> 1, stride)];
+        return ((c & 1) ? z.y : z.x) * scale;
+    };
+    auto put = [&](int i, int j, T y) {
+        const size_t o = (size_t)i * W + j;
+        if (mode == 0 || mode == 1) {
+            const T cn = norm[o];
+            y = mode == 0 ? (cn < threshold ? T(NAN) : y / cn) : (cn > threshold ? y / cn : T(0));
+        } else if (mode == 2) {
+            const T cn = (T)((int64_t)(n0 - abs(i - n0)) * (n1 - abs(j - n1)));
+            y = cn < threshold ? T(NAN) : y / cn;
+        }
+        out[o] = y;
+    };
+    FcgIdx ot(threadIdx.x, blockDim.x, W);
+    for (int idx = threadIdx.x; idx < rpb * W; idx += blockDim.x, ot.next()) {
+        const int rr = ot.a, j = ot.b, r = r0 + rr;
+        if (r > n0) continue;
+        // |j - n1| <= n1 <= L1 / 2: one conditional add gives the residue
+        const int c = j - n1 < 0 ? j - n1 + L1 : j - n1;
+        if (r < n0) put(n0 + r, j, val(rr, c));
+        if (r > 0) put(n0 - r, j, val(rr, n1 - j < 0 ? n1 - j + L1 : n1 - j));
+    }
+}
+
 static int ew_blocks(int64_t n) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -680,10 +1030,143 @@ static FcPlan fc_plan(int64_t batch, int n0, int n1, int dtype) {
     return p;
 }
 
+// ---- general lengths: host side ----
+// Smallest N >= x whose prime factors are 2, 3, 5, 7, 11 (the reference's
+// idi.util.fastlen).
+static int fcg_fastlen(int x) {
+    for (int n = std::max(1, x);; ++n) {
+        int m = n;
+        for (int f : {2, 3, 5, 7, 11})
+            while (m % f == 0) m /= f;
+        if (m == 1) return n;
+    }
+}
+// Radices of n (11, 7, 5, 3, then 8s, then 4 or 2); false if n has another
+// prime factor or needs too many passes.
+static bool fcg_radices(int n, FcgRad &rad) {
+    rad = FcgRad{};
+    rad.n = n;
+    int m = n;
+    for (int f : {11, 7, 5, 3})
+        while (m % f == 0) {
+            if (rad.np == kFcgMaxPasses) return false;
+            rad.r[rad.np++] = f;
+            m /= f;
+        }
+    while (m % 8 == 0 && m > 1) {
+        if (rad.np == kFcgMaxPasses) return false;
+        rad.r[rad.np++] = 8;
+        m /= 8;
+    }
+    if (m == 2 || m == 4) {
+        if (rad.np == kFcgMaxPasses) return false;
+        rad.r[rad.np++] = m;
+        m = 1;
+    }
+    return m == 1;
+}
+// Threads of a general-path block holding `values` complex values in
+// `smem` bytes (every pass loops over its butterflies, so any count works):
+// 256 where two or more blocks fit in an SM's shared memory, else 512 (more
+// warps per SM either way), fewer for small blocks.
+static int fcg_threads(int values, size_t smem) {
+    const int cap = 2 * smem <= 227 * 1024 ? 256 : 512;
+    return std::min(cap, std::max(32, (values / 4 + 31) / 32 * 32));
+}
+static int fcg_stride(int n, int lkc) { return n + ((n - 1) >> lkc) + 1; }
+
+constexpr int kFcgMaxLen = 4096;  // G0, G1 and L1 of the general path
+struct FcgPlan {
+    int n0, n1, G0, G1, L1, m;
+    int ppb, cpb, rpb;  // row pairs (pass A), columns (B), rows (C) per block
+    FcgRad radA, radB, radC;
+    int thrA, thrB, thrC, strA, strB, strC;
+    size_t vsz, t_img, c_img;
+    size_t twA_bytes, twB_bytes, twC_bytes, t_bytes, c_bytes;
+    int64_t group;
+};
+static bool fcg_plan(int64_t batch, int n0, int n1, int dtype, FcgPlan &p) {
+    if (n0 < 1 || n1 < 1 || n0 > kFcgMaxLen || n1 > kFcgMaxLen) return false;
+    p = FcgPlan{};
+    p.n0 = n0;
+    p.n1 = n1;
+    p.G0 = fcg_fastlen(2 * n0);
+    p.G1 = fcg_fastlen(2 * n1);
+    p.L1 = p.G1;
+    p.m = p.G1 / 2 + 1;
+    if (p.G0 > kFcgMaxLen || p.G1 > kFcgMaxLen || p.G1 % 2) return false;
+    if (!fcg_radices(p.G1, p.radA) || !fcg_radices(p.G0, p.radB) || !fcg_radices(p.L1 / 2, p.radC)) return false;
+    p.vsz = dtype == IDIWF_F64 ? 16 : 8;
+    const int lkc = p.vsz == 16 ? 3 : 4;
+    p.ppb = std::max(1, std::min(kFcBlockElems / p.G1, (n0 + 1) / 2));
+    p.cpb = std::max(1, std::min(kFcBlockElems / p.G0, p.m));
+    p.rpb = std::max(1, std::min(kFcBlockElems / (p.L1 / 2), n0 + 1));
+    p.strA = fcg_stride(p.G1, lkc);
+    p.strB = fcg_stride(p.G0, lkc);
+    p.strC = fcg_stride(p.L1 / 2, lkc);
+    // ping-pong buffers of count sequences each
+    p.thrA = fcg_threads(p.ppb * p.G1, 2 * (size_t)p.ppb * p.strA * p.vsz);
+    p.thrB = fcg_threads(p.cpb * p.G0, 2 * (size_t)p.cpb * p.strB * p.vsz);
+    p.thrC = fcg_threads(p.rpb * (p.L1 / 2), 2 * (size_t)p.rpb * p.strC * p.vsz);
+    p.t_img = (size_t)p.m * n0;
+    p.c_img = (size_t)p.m * (n0 + 1);
+    p.twA_bytes = fc_align((size_t)p.G1 * sizeof(double2));
+    p.twB_bytes = fc_align((size_t)p.G0 * sizeof(double2));
+    p.twC_bytes = fc_align((size_t)p.L1 * sizeof(double2));
+    const size_t per = (p.t_img + p.c_img) * p.vsz;
+    const int64_t gmax = std::max<int64_t>(1, std::min<int64_t>(65535, (int64_t)((256u << 20) / per)));
+    const int64_t ngroups = (std::max<int64_t>(batch, 1) + gmax - 1) / gmax;
+    p.group = (std::max<int64_t>(batch, 1) + ngroups - 1) / ngroups;
+    p.t_bytes = fc_align(p.t_img * p.vsz * p.group);
+    p.c_bytes = fc_align(p.c_img * p.vsz * p.group);
+    return true;
+}
+
+template <typename T>
+static idiwf_status fcg_run(const T *x, int64_t batch, const FcgPlan &p, const T *norm, int mode, double threshold,
+                            T *out, unsigned char *ws, cudaStream_t stream) {
+    using V = typename Cx<T>::t;
+    double2 *twA = reinterpret_cast<double2 *>(ws);
+    double2 *twB = reinterpret_cast<double2 *>(ws + p.twA_bytes);
+    double2 *twC = reinterpret_cast<double2 *>(ws + p.twA_bytes + p.twB_bytes);
+    unsigned char *rest = ws + p.twA_bytes + p.twB_bytes + p.twC_bytes;
+    V *Tt = reinterpret_cast<V *>(rest);
+    V *C = reinterpret_cast<V *>(rest + p.t_bytes);
+    fc_twiddle_kernel<<<(p.G1 + 255) / 256, 256, 0, stream>>>(twA, p.G1);
+    fc_twiddle_kernel<<<(p.G0 + 255) / 256, 256, 0, stream>>>(twB, p.G0);
+    fc_twiddle_kernel<<<(p.L1 + 255) / 256, 256, 0, stream>>>(twC, p.L1);
+    IDIWF_CUDA_CHECK(cudaGetLastError());
+    const size_t smA = 2 * (size_t)p.ppb * p.strA * sizeof(V), smB = 2 * (size_t)p.cpb * p.strB * sizeof(V);
+    const size_t smC = 2 * (size_t)p.rpb * p.strC * sizeof(V);
+    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fcg_rows_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
+    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fcg_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
+    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fcg_rows_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
+    const int npairs = (p.n0 + 1) / 2;
+    const unsigned blkA = (unsigned)((npairs + p.ppb - 1) / p.ppb), blkB = (unsigned)((p.m + p.cpb - 1) / p.cpb);
+    const unsigned blkC = (unsigned)((p.n0 + 1 + p.rpb - 1) / p.rpb);
+    const size_t in_img = (size_t)p.n0 * p.n1, out_img = (size_t)(2 * p.n0) * (2 * p.n1);
+    for (int64_t b0 = 0; b0 < batch; b0 += p.group) {
+        const unsigned g = (unsigned)std::min<int64_t>(p.group, batch - b0);
+        fcg_rows_fwd<T><<<dim3(blkA, g), p.thrA, smA, stream>>>(x + b0 * in_img, p.n0, p.n1, p.ppb, p.radA, p.strA,
+                                                                  twA, p.m, Tt, p.t_img);
+        fcg_cols<T><<<dim3(blkB, g), p.thrB, smB, stream>>>(Tt, p.t_img, p.n0, p.m, p.cpb, p.radB, p.strB, twB, C,
+                                                              p.c_img);
+        fcg_rows_inv<T><<<dim3(blkC, g), p.thrC, smC, stream>>>(C, p.c_img, p.n0, p.n1, p.rpb, p.radC, p.strC, twC,
+                                                                  norm, mode, (T)threshold, out + b0 * out_img);
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+    }
+    return IDIWF_OK;
+}
+
 extern "C" size_t idiwf_fft_autocorr_workspace_size(int64_t batch, int32_t n0, int32_t n1, int32_t dtype) {
-    if (batch <= 0 || !fc_pow2(n0) || !fc_pow2(n1) || (dtype != IDIWF_F64 && dtype != IDIWF_F32)) return 0;
-    const FcPlan p = fc_plan(batch, n0, n1, dtype);
-    return p.tw_bytes + p.t_bytes + p.c_bytes;
+    if (batch <= 0 || (dtype != IDIWF_F64 && dtype != IDIWF_F32)) return 0;
+    if (fc_pow2(n0) && fc_pow2(n1)) {
+        const FcPlan p = fc_plan(batch, n0, n1, dtype);
+        return p.tw_bytes + p.t_bytes + p.c_bytes;
+    }
+    FcgPlan g;
+    if (!fcg_plan(batch, n0, n1, dtype, g)) return 0;
+    return g.twA_bytes + g.twB_bytes + g.twC_bytes + g.t_bytes + g.c_bytes;
 }
 
 template <typename T, int EA, int EB>
@@ -736,8 +1219,10 @@ extern "C" idiwf_status idiwf_fft_autocorr(const void *x, int32_t dtype, int64_t
                                            void *workspace, size_t workspace_bytes, cudaStream_t stream) {
     if (!x || !out) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "NULL argument");
     if (batch <= 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "batch must be positive");
-    if (!fc_pow2(n0) || !fc_pow2(n1))
-        return set_error(IDIWF_ERR_UNSUPPORTED, "the hand-written autocorrelation takes powers of two from 4 to 4096");
+    if ((dtype == IDIWF_F64 || dtype == IDIWF_F32) && idiwf_fft_autocorr_workspace_size(batch, n0, n1, dtype) == 0)
+        return set_error(IDIWF_ERR_UNSUPPORTED,
+                         "shape not supported by the hand-written autocorrelation (powers of two from 4 to 4096, or "
+                         "fastlen(2 n0) <= 4096 and an even fastlen(2 n1) <= 4096)");
     if (mode < -1 || mode > 2) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "mode must be -1, 0, 1 or 2");
     if ((mode == 0 || mode == 1) && !norm) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "modes 0 and 1 need norm");
     const size_t need = idiwf_fft_autocorr_workspace_size(batch, n0, n1, dtype);
@@ -746,12 +1231,21 @@ extern "C" idiwf_status idiwf_fft_autocorr(const void *x, int32_t dtype, int64_t
         return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_fft_autocorr_workspace_size()");
     if (reinterpret_cast<uintptr_t>(workspace) & 255)
         return set_error(IDIWF_ERR_WORKSPACE, "workspace must be 256-byte aligned");
-    // rows are read and written as pairs of values
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    if (!(fc_pow2(n0) && fc_pow2(n1))) {
+        FcgPlan g;
+        fcg_plan(batch, n0, n1, dtype, g);
+        if (dtype == IDIWF_F64)
+            return fcg_run<double>(static_cast<const double *>(x), batch, g, static_cast<const double *>(norm), mode,
+                                   threshold, static_cast<double *>(out), ws, stream);
+        return fcg_run<float>(static_cast<const float *>(x), batch, g, static_cast<const float *>(norm), mode,
+                              threshold, static_cast<float *>(out), ws, stream);
+    }
+    // power-of-two shapes: rows are read and written as pairs of values
     const uintptr_t pair = dtype == IDIWF_F64 ? 15 : 7;
     if ((reinterpret_cast<uintptr_t>(x) & pair) || (reinterpret_cast<uintptr_t>(out) & pair))
         return set_error(IDIWF_ERR_INVALID_ARGUMENT, "x and out must be aligned to two elements");
     const FcPlan p = fc_plan(batch, n0, n1, dtype);
-    unsigned char *ws = static_cast<unsigned char *>(workspace);
     if (dtype == IDIWF_F64)
         return fc_run<double>(static_cast<const double *>(x), batch, p, static_cast<const double *>(norm), mode,
                               threshold, static_cast<double *>(out), ws, stream);

@@ -1,12 +1,14 @@
 """Drop-in for ``idi.reconstruction.cusimple``: FFT autocorrelation on the GPU
 (``idi/reconstruction/cusimple.py:6-121``).
 
-Two correlated axes of power-of-two lengths (4 to 4096) go through this
-library's own FFTs end to end (``idiwf_fft_autocorr``: the padded transform,
-the power spectrum, the inverse, the fftshift and the normalisation).  Other
-shapes use cuFFT's transforms (through ``torch.fft``) with this library's
-power-spectrum and crop kernels around them (``idiwf_power_spectrum``,
-``idiwf_corr_crop``).  The correlator's running mean / variance is
+One or two correlated axes go through this library's own FFTs end to end
+(``idiwf_fft_autocorr``: the padded transform, the power spectrum, the
+inverse, the fftshift, the crop and the normalisation) whenever the library
+takes the shape: powers of two from 4 to 4096, or padded lengths
+``fastlen(2 n)`` up to 4096 with an even one along the last axis.
+Other shapes (and three axes) use cuFFT's transforms (through ``torch.fft``)
+with this library's power-spectrum and crop kernels around them
+(``idiwf_power_spectrum``, ``idiwf_corr_crop``).  The correlator's running mean / variance is
 ``idiwf_welford_update``.  Inputs may be numpy arrays or CUDA tensors;
 results are numpy unless ``returngpu``.
 """
@@ -88,9 +90,21 @@ def _autocorr(x, nax, fftshape):
 
 
 def _hand_ok(shape, dtype):
-    """Whether ``idiwf_fft_autocorr`` takes these two correlated axes."""
-    return (len(shape) == 2 and dtype in (torch.float32, torch.float64)
-            and all(4 <= int(s) <= 4096 and (int(s) & (int(s) - 1)) == 0 for s in shape))
+    """Whether ``idiwf_fft_autocorr`` takes these one or two correlated axes
+    (one axis of length n runs as a 1 x n image)."""
+    if len(shape) not in (1, 2) or dtype not in (torch.float32, torch.float64):
+        return False
+    n0, n1 = (1, int(shape[0])) if len(shape) == 1 else (int(shape[0]), int(shape[1]))
+    code = nat.F64 if dtype == torch.float64 else nat.F32
+    return nat.load().idiwf_fft_autocorr_workspace_size(1, n0, n1, code) > 0
+
+
+def _hand_autocorr_1d(x, mode=-1, threshold=0.0):
+    """Autocorrelation of the last axis (length n) as 1 x n images: row 1 of
+    the (2, 2n) result is the zero row shift."""
+    n = int(x.shape[-1])
+    out = _hand_autocorr(x.reshape(-1, 1, n), mode=mode, threshold=threshold)
+    return out[:, 1, :].reshape(tuple(x.shape[:-1]) + (2 * n,))
 
 
 def _hand_autocorr(x, mode=-1, norm=None, threshold=0.0):
@@ -136,7 +150,8 @@ def corr(input, axes=(-1, -2), norm=False, returngpu=False, **kwargs):
     if _hand_ok(sizes, x.dtype):
         # the pair count in closed form: the transform of ones in the
         # reference rounds to the same integers, and the same < 0.9 positions
-        ret = _hand_autocorr(moved, mode=2 if norm else -1, threshold=0.9)
+        f = _hand_autocorr if len(sizes) == 2 else _hand_autocorr_1d
+        ret = f(moved, mode=2 if norm else -1, threshold=0.9)
     else:
         full = _autocorr(moved, len(axes), fftshape)
         pairs = None

@@ -463,22 +463,27 @@ idiwf_status idiwf_qcorr_3d(const float *zd, const float *images, int32_t n_imag
 /* ------------------------------------------------------------------------ */
 
 /*
- * The whole autocorrelation of idi/reconstruction/cusimple.py:6-38 for 2D
- * power-of-two shapes, by this library's own FFTs: for each of `batch` images
- * x[b] (n0 x n1 of dtype, row-major, contiguous, batch-major),
- *     out[b] = fftshift(irfft2(|rfft2(x[b], (2 n0, 2 n1))|^2))
- * ((2 n0) x (2 n1) of dtype) -- the reference's padded length fastlen(2 n) is
- * 2 n for these shapes, so its centre crop is the whole shifted array.  Then,
+ * The whole autocorrelation of idi/reconstruction/cusimple.py:6-38 along two
+ * axes, by this library's own FFTs: for each of `batch` images x[b] (n0 x n1
+ * of dtype, row-major, contiguous, batch-major),
+ *     out[b] = crop(fftshift(irfft2(|rfft2(x[b], (G0, G1))|^2)))
+ * ((2 n0) x (2 n1) of dtype; for powers of two G = 2 n and the crop is the
+ * whole shifted array).  Then,
  * per output position (i, j): mode -1 nothing; mode 0 y / norm, NaN where
  * norm < threshold; mode 1 y / norm where norm > threshold, else 0 (norm:
  * (2 n0) x (2 n1) of dtype); mode 2 y / count with the pair count
  * count = (n0 - |i - n0|)(n1 - |j - n1|), NaN where count < threshold (the
  * norm=True result of cusimple.py:23-34 without a second transform).
- * n0, n1: powers of two from 4 to 4096 (else IDIWF_ERR_UNSUPPORTED); x and
- * out aligned to two elements; workspace: idiwf_fft_autocorr_workspace_size()
- * bytes for this batch and shape, 256-byte aligned (the twiddle table and the
- * intermediates of one group of images; groups run one after another, 0 for
- * unsupported arguments).
+ * Shapes: n0, n1 powers of two from 4 to 4096 (x and out aligned to two
+ * elements), or any n0, n1 >= 1 whose padded lengths G0 = fastlen(2 n0) and
+ * G1 = fastlen(2 n1) (smallest products of 2, 3, 5, 7, 11, as
+ * idi.util.fastlen) are at most 4096 with G1 even; out is then the centre
+ * crop (i - n0) mod G0, (j - n1) mod G1 of the shifted array, as the
+ * reference's slice.  Other shapes: IDIWF_ERR_UNSUPPORTED.  A 1D
+ * autocorrelation of length n is row 1 of the 1 x n image's result.
+ * workspace: idiwf_fft_autocorr_workspace_size() bytes for this batch and
+ * shape, 256-byte aligned (twiddle tables and the intermediates of one group
+ * of images; groups run one after another; 0 for unsupported arguments).
  */
 size_t idiwf_fft_autocorr_workspace_size(int64_t batch, int32_t n0, int32_t n1, int32_t dtype);
 idiwf_status idiwf_fft_autocorr(const void *x, int32_t dtype, int64_t batch, int32_t n0, int32_t n1,

@@ -164,8 +164,15 @@ def test_fft_autocorr_validation(lib):
     # (256 MB), balanced: 8 images run as two groups of 4
     assert lib.idiwf_fft_autocorr_workspace_size(8, 1024, 1024, nat.F64) == al(2048 * 16) + al(
         4 * 1025 * 1024 * 16) + al(4 * 1025 * 1025 * 16)
-    for n0, n1 in ((6, 8), (8, 2), (8, 8192), (0, 8), (3, 4)):
-        assert lib.idiwf_fft_autocorr_workspace_size(1, n0, n1, nat.F64) == 0
+    # other lengths: padded to fastlen(2 n); tables of G1, G0 and L1 values,
+    # T m x n0 and C m x (n0 + 1), m = G1 / 2 + 1.  6 x 8: G0 = 12, G1 = L1 = 16
+    assert lib.idiwf_fft_autocorr_workspace_size(1, 6, 8, nat.F64) == 3 * 256 + al(9 * 6 * 16) + al(9 * 7 * 16)
+    # 5 x 13: G1 = 27 is odd, the inverse length L1 = 26 has the factor 13
+    for n0, n1 in ((5, 13), (8, 8192), (0, 8), (3000, 8), (8, 0)):
+        assert lib.idiwf_fft_autocorr_workspace_size(1, n0, n1, nat.F64) == 0, (n0, n1)
+    # 5 x 14: G1 = 28; 4 x 17: G1 = 35 odd, L1 = 34 -> inverse of 17 values: not taken
+    assert lib.idiwf_fft_autocorr_workspace_size(1, 5, 14, nat.F64) > 0
+    assert lib.idiwf_fft_autocorr_workspace_size(1, 4, 17, nat.F64) == 0
     assert lib.idiwf_fft_autocorr_workspace_size(1, 8, 8, 7) == 0
     assert lib.idiwf_fft_autocorr_workspace_size(0, 8, 8, nat.F64) == 0
 
@@ -176,8 +183,8 @@ def test_fft_autocorr_validation(lib):
     assert call(x=0) == nat.ERR_INVALID_ARGUMENT
     assert call(out=0) == nat.ERR_INVALID_ARGUMENT
     assert call(batch=0) == nat.ERR_INVALID_ARGUMENT
-    assert call(n0=12) == nat.ERR_UNSUPPORTED
-    assert b"powers of two" in lib.idiwf_last_error_string()
+    assert call(n1=13) == nat.ERR_UNSUPPORTED
+    assert b"not supported" in lib.idiwf_last_error_string()
     assert call(mode=3) == nat.ERR_INVALID_ARGUMENT
     assert call(mode=0) == nat.ERR_INVALID_ARGUMENT  # no norm
     assert call(ws_bytes=need - 1) == nat.ERR_WORKSPACE
@@ -195,8 +202,11 @@ def test_fft_autocorr_shape_predicate():
 
     assert cusimple._hand_ok((1024, 1024), torch.float64)
     assert cusimple._hand_ok((4, 4096), torch.float32)
-    assert not cusimple._hand_ok((2, 8), torch.float64)
+    assert cusimple._hand_ok((2, 8), torch.float64)
+    assert cusimple._hand_ok((15, 33), torch.float64)
+    assert cusimple._hand_ok((30,), torch.float64)
+    assert not cusimple._hand_ok((13,), torch.float64)
+    assert not cusimple._hand_ok((8, 13), torch.float64)
     assert not cusimple._hand_ok((8, 8192), torch.float64)
-    assert not cusimple._hand_ok((24, 32), torch.float64)
     assert not cusimple._hand_ok((8, 8, 8), torch.float64)
     assert not cusimple._hand_ok((8, 8), torch.float16)

@@ -124,8 +124,55 @@ def test_hand_fft_vs_cufft(shape, dtype):
 
 
 def test_other_shapes_take_cufft():
-    assert not cusimple._hand_ok((12, 8), torch.float64)
-    x = torch.ones((12, 8), dtype=torch.float64, device="cuda")
-    # a non-power-of-two shape still goes through cuFFT
+    # fastlen(26) = 27 is odd: the reference's inverse then has length 26,
+    # which the hand-written FFTs do not take; cuFFT does
+    assert not cusimple._hand_ok((12, 13), torch.float64)
+    x = torch.ones((12, 13), dtype=torch.float64, device="cuda")
     c = cusimple.corr(x, returngpu=True)
-    assert c.shape == (24, 16)
+    assert c.shape == (24, 26)
+
+
+@pytest.mark.parametrize("shape,dtype", [((15, 33), torch.float64), ((13, 10), torch.float64),
+                                         ((1, 30), torch.float64), ((3, 5), torch.float64),
+                                         ((2, 9), torch.float64), ((7, 50), torch.float64),
+                                         ((40, 12), torch.float64), ((100, 75), torch.float64),
+                                         ((300, 500), torch.float64), ((1000, 1050), torch.float64),
+                                         ((1500, 7), torch.float64), ((6, 2000), torch.float64),
+                                         ((100, 75), torch.float32), ((300, 500), torch.float32)])
+def test_hand_fft_general_vs_cufft(shape, dtype):
+    """Other lengths: mixed-radix passes (2, 3, 4, 5, 7, 8, 11) on the padded
+    lengths fastlen(2 n), cropped, against cuFFT's transforms with the same
+    crop; plain and divided by the pair count."""
+    fs = [cusimple.fastlen(2 * s) for s in shape]
+    assert cusimple._hand_ok(shape, dtype) and fs[1] % 2 == 0
+    g = torch.Generator(device="cuda").manual_seed(sum(shape) + 7)
+    x = torch.empty((3,) + shape, dtype=dtype, device="cuda").exponential_(1.0, generator=g)
+    tol = 1e-12 if dtype == torch.float64 else 2e-5
+    ref = cusimple._crop(cusimple._autocorr(x, 2, fs), 2, list(shape))
+    hand = cusimple._hand_autocorr(x)
+    assert hand.shape == ref.shape
+    assert (hand - ref).abs().max().item() <= tol * ref.abs().max().item()
+    count = _pair_count(*shape, dtype)
+    hn = cusimple._hand_autocorr(x, mode=2, threshold=0.9)
+    rn = torch.where(count < 0.9, torch.full_like(ref, float("nan")), ref / count)
+    assert torch.equal(torch.isnan(hn), torch.isnan(rn))
+    ok = ~torch.isnan(rn)
+    assert ((hn - rn).abs() * count)[ok].max().item() <= 2 * tol * ref.abs().max().item()
+
+
+@pytest.mark.parametrize("n", [4, 30, 1000, 1024, 1500])
+def test_hand_fft_1d_vs_cufft(n):
+    """One correlated axis as 1 x n images, against cuFFT's 1D transforms."""
+    g = torch.Generator(device="cuda").manual_seed(n)
+    x = torch.empty((5, 2, n), dtype=torch.float64, device="cuda").exponential_(1.0, generator=g)
+    ref = cusimple._crop(cusimple._autocorr(x, 1, [cusimple.fastlen(2 * n)]), 1, [n])
+    hand = cusimple._hand_autocorr_1d(x)
+    assert hand.shape == ref.shape == (5, 2, 2 * n)
+    assert (hand - ref).abs().max().item() <= 1e-12 * ref.abs().max().item()
+    j = torch.arange(2 * n, dtype=torch.float64, device="cuda")
+    count = n - (j - n).abs()
+    hn = cusimple._hand_autocorr_1d(x, mode=2, threshold=0.9)
+    rn = torch.where(count < 0.9, torch.full_like(ref, float("nan")), ref / count)
+    assert torch.equal(torch.isnan(hn), torch.isnan(rn))
+    ok = ~torch.isnan(rn)
+    assert ((hn - rn).abs() * count)[ok].max().item() <= 2e-12 * ref.abs().max().item()
