@@ -81,6 +81,8 @@ EXPORTED = (
     "idiwf_welford_update",
     "idiwf_fft_autocorr_workspace_size",
     "idiwf_fft_autocorr",
+    "idiwf_fft_autocorr_1d_workspace_size",
+    "idiwf_fft_autocorr_1d",
     "idiwf_tune",
     "idiwf_workspace_error",
     "idiwf_microbench",
@@ -240,6 +242,11 @@ def load():
     L.idiwf_fft_autocorr.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, vp,
                                      ctypes.c_int32, ctypes.c_double, vp, vp, ctypes.c_size_t, vp]
     L.idiwf_fft_autocorr.restype = st
+    L.idiwf_fft_autocorr_1d_workspace_size.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32]
+    L.idiwf_fft_autocorr_1d_workspace_size.restype = ctypes.c_size_t
+    L.idiwf_fft_autocorr_1d.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, vp, ctypes.c_int32,
+                                        ctypes.c_double, vp, vp, ctypes.c_size_t, vp]
+    L.idiwf_fft_autocorr_1d.restype = st
     L.idiwf_tune.argtypes = [P(Geom), P(Batch), ctypes.c_int32, ctypes.c_int32, vp, vp, ctypes.c_size_t, vp,
                              P(Config)]
     L.idiwf_tune.restype = st

@@ -844,7 +844,10 @@ __global__ void __launch_bounds__(512) fcg_cols(const typename Cx<T>::t *__restr
 // centre crop: output (i, j) of row r is column (j - n1) mod L1 for
 // i = n0 + r (r < n0), and by point symmetry column (n1 - j) mod L1 for the
 // mirrored row i = n0 - r.  Normalisation modes as fc_rows_inv.
-template <typename T>
+// ONED: the autocorrelation of each of n0 lines on its own -- the half
+// spectrum is the line's power |T[k][r]|^2 (C is pass A's T), and line r's
+// result is output row r (pair count n1 - |j - n1|, norm of 2 n1 values).
+template <typename T, bool ONED>
 __global__ void __launch_bounds__(512) fcg_rows_inv(const typename Cx<T>::t *__restrict__ C, size_t c_img, int n0,
                                                     int n1, int rpb, FcgRad rad, int stride,
                                                     const double2 *__restrict__ twl1, const T *__restrict__ norm,
@@ -853,15 +856,24 @@ __global__ void __launch_bounds__(512) fcg_rows_inv(const typename Cx<T>::t *__r
     extern __shared__ __align__(16) unsigned char fsm[];
     V *S = reinterpret_cast<V *>(fsm);
     const int Hp = rad.n, L1 = 2 * Hp, r0 = blockIdx.x * rpb, W = 2 * n1;
+    const int rows = ONED ? n0 : n0 + 1, cst = ONED ? n0 : n0 + 1;
     C += (size_t)blockIdx.y * c_img;
-    out += (size_t)blockIdx.y * (2 * n0) * W;
+    out += (size_t)blockIdx.y * (ONED ? n0 : 2 * n0) * W;
+    auto spec = [&](int k, int r) -> V {
+        V y = C[(size_t)k * cst + r];
+        if constexpr (ONED) {
+            y.x = y.x * y.x + y.y * y.y;
+            y.y = T(0);
+        }
+        return y;
+    };
     // Z[k] = (Y[k] + conj Y[Hp-k]) + i W^-k (Y[k] - conj Y[Hp-k]); rows fastest
     FcgIdx it(threadIdx.x, blockDim.x, rpb);
     for (int idx = threadIdx.x; idx < rpb * Hp; idx += blockDim.x, it.next()) {
         const int k = it.a, rr = it.b, r = r0 + rr;
         V z = cx_zero<V>();
-        if (r <= n0) {
-            V yk = C[(size_t)k * (n0 + 1) + r], yc = cx_conj(C[(size_t)(Hp - k) * (n0 + 1) + r]);
+        if (r < rows) {
+            V yk = spec(k, r), yc = cx_conj(spec(Hp - k, r));
             if (k == 0) {
                 yk.y = T(0);
                 yc.y = T(0);
@@ -887,10 +899,10 @@ __global__ void __launch_bounds__(512) fcg_rows_inv(const typename Cx<T>::t *__r
     auto put = [&](int i, int j, T y) {
         const size_t o = (size_t)i * W + j;
         if (mode == 0 || mode == 1) {
-            const T cn = norm[o];
+            const T cn = norm[ONED ? (size_t)j : o];
             y = mode == 0 ? (cn < threshold ? T(NAN) : y / cn) : (cn > threshold ? y / cn : T(0));
         } else if (mode == 2) {
-            const T cn = (T)((int64_t)(n0 - abs(i - n0)) * (n1 - abs(j - n1)));
+            const T cn = (T)((int64_t)(ONED ? 1 : n0 - abs(i - n0)) * (n1 - abs(j - n1)));
             y = cn < threshold ? T(NAN) : y / cn;
         }
         out[o] = y;
@@ -898,11 +910,15 @@ __global__ void __launch_bounds__(512) fcg_rows_inv(const typename Cx<T>::t *__r
     FcgIdx ot(threadIdx.x, blockDim.x, W);
     for (int idx = threadIdx.x; idx < rpb * W; idx += blockDim.x, ot.next()) {
         const int rr = ot.a, j = ot.b, r = r0 + rr;
-        if (r > n0) continue;
+        if (r >= rows) continue;
         // |j - n1| <= n1 <= L1 / 2: one conditional add gives the residue
         const int c = j - n1 < 0 ? j - n1 + L1 : j - n1;
-        if (r < n0) put(n0 + r, j, val(rr, c));
-        if (r > 0) put(n0 - r, j, val(rr, n1 - j < 0 ? n1 - j + L1 : n1 - j));
+        if constexpr (ONED) {
+            put(r, j, val(rr, c));
+        } else {
+            if (r < n0) put(n0 + r, j, val(rr, c));
+            if (r > 0) put(n0 - r, j, val(rr, n1 - j < 0 ? n1 - j + L1 : n1 - j));
+        }
     }
 }
 
@@ -1084,10 +1100,12 @@ struct FcgPlan {
     size_t vsz, t_img, c_img;
     size_t twA_bytes, twB_bytes, twC_bytes, t_bytes, c_bytes;
     int64_t group;
+    bool oned;  // n0 independent lines: no column pass, no C
 };
-static bool fcg_plan(int64_t batch, int n0, int n1, int dtype, FcgPlan &p) {
-    if (n0 < 1 || n1 < 1 || n0 > kFcgMaxLen || n1 > kFcgMaxLen) return false;
+static bool fcg_plan(int64_t batch, int n0, int n1, int dtype, FcgPlan &p, bool oned = false) {
+    if (n0 < 1 || n1 < 1 || (!oned && n0 > kFcgMaxLen) || n1 > kFcgMaxLen) return false;
     p = FcgPlan{};
+    p.oned = oned;
     p.n0 = n0;
     p.n1 = n1;
     p.G0 = fcg_fastlen(2 * n0);
@@ -1095,12 +1113,14 @@ static bool fcg_plan(int64_t batch, int n0, int n1, int dtype, FcgPlan &p) {
     p.L1 = p.G1;
     p.m = p.G1 / 2 + 1;
     if (p.G0 > kFcgMaxLen || p.G1 > kFcgMaxLen || p.G1 % 2) return false;
-    if (!fcg_radices(p.G1, p.radA) || !fcg_radices(p.G0, p.radB) || !fcg_radices(p.L1 / 2, p.radC)) return false;
+    if (oned) p.G0 = 1;  // no column pass
+    if (!fcg_radices(p.G1, p.radA) || !fcg_radices(p.L1 / 2, p.radC)) return false;
+    if (!oned && !fcg_radices(p.G0, p.radB)) return false;
     p.vsz = dtype == IDIWF_F64 ? 16 : 8;
     const int lkc = p.vsz == 16 ? 3 : 4;
     p.ppb = std::max(1, std::min(kFcBlockElems / p.G1, (n0 + 1) / 2));
     p.cpb = std::max(1, std::min(kFcBlockElems / p.G0, p.m));
-    p.rpb = std::max(1, std::min(kFcBlockElems / (p.L1 / 2), n0 + 1));
+    p.rpb = std::max(1, std::min(kFcBlockElems / (p.L1 / 2), oned ? n0 : n0 + 1));
     p.strA = fcg_stride(p.G1, lkc);
     p.strB = fcg_stride(p.G0, lkc);
     p.strC = fcg_stride(p.L1 / 2, lkc);
@@ -1109,9 +1129,9 @@ static bool fcg_plan(int64_t batch, int n0, int n1, int dtype, FcgPlan &p) {
     p.thrB = fcg_threads(p.cpb * p.G0, 2 * (size_t)p.cpb * p.strB * p.vsz);
     p.thrC = fcg_threads(p.rpb * (p.L1 / 2), 2 * (size_t)p.rpb * p.strC * p.vsz);
     p.t_img = (size_t)p.m * n0;
-    p.c_img = (size_t)p.m * (n0 + 1);
+    p.c_img = oned ? 0 : (size_t)p.m * (n0 + 1);
     p.twA_bytes = fc_align((size_t)p.G1 * sizeof(double2));
-    p.twB_bytes = fc_align((size_t)p.G0 * sizeof(double2));
+    p.twB_bytes = oned ? 0 : fc_align((size_t)p.G0 * sizeof(double2));
     p.twC_bytes = fc_align((size_t)p.L1 * sizeof(double2));
     const size_t per = (p.t_img + p.c_img) * p.vsz;
     const int64_t gmax = std::max<int64_t>(1, std::min<int64_t>(65535, (int64_t)((256u << 20) / per)));
@@ -1133,26 +1153,36 @@ static idiwf_status fcg_run(const T *x, int64_t batch, const FcgPlan &p, const T
     V *Tt = reinterpret_cast<V *>(rest);
     V *C = reinterpret_cast<V *>(rest + p.t_bytes);
     fc_twiddle_kernel<<<(p.G1 + 255) / 256, 256, 0, stream>>>(twA, p.G1);
-    fc_twiddle_kernel<<<(p.G0 + 255) / 256, 256, 0, stream>>>(twB, p.G0);
+    if (!p.oned) fc_twiddle_kernel<<<(p.G0 + 255) / 256, 256, 0, stream>>>(twB, p.G0);
     fc_twiddle_kernel<<<(p.L1 + 255) / 256, 256, 0, stream>>>(twC, p.L1);
     IDIWF_CUDA_CHECK(cudaGetLastError());
     const size_t smA = 2 * (size_t)p.ppb * p.strA * sizeof(V), smB = 2 * (size_t)p.cpb * p.strB * sizeof(V);
     const size_t smC = 2 * (size_t)p.rpb * p.strC * sizeof(V);
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fcg_rows_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
-    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fcg_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
-    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fcg_rows_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
+    if (!p.oned)
+        IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fcg_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
+    IDIWF_CUDA_CHECK(
+        cudaFuncSetAttribute(fcg_rows_inv<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
+    IDIWF_CUDA_CHECK(
+        cudaFuncSetAttribute(fcg_rows_inv<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
     const int npairs = (p.n0 + 1) / 2;
     const unsigned blkA = (unsigned)((npairs + p.ppb - 1) / p.ppb), blkB = (unsigned)((p.m + p.cpb - 1) / p.cpb);
-    const unsigned blkC = (unsigned)((p.n0 + 1 + p.rpb - 1) / p.rpb);
-    const size_t in_img = (size_t)p.n0 * p.n1, out_img = (size_t)(2 * p.n0) * (2 * p.n1);
+    const int rowsC = p.oned ? p.n0 : p.n0 + 1;
+    const unsigned blkC = (unsigned)((rowsC + p.rpb - 1) / p.rpb);
+    const size_t in_img = (size_t)p.n0 * p.n1, out_img = (size_t)(p.oned ? p.n0 : 2 * p.n0) * (2 * p.n1);
     for (int64_t b0 = 0; b0 < batch; b0 += p.group) {
         const unsigned g = (unsigned)std::min<int64_t>(p.group, batch - b0);
         fcg_rows_fwd<T><<<dim3(blkA, g), p.thrA, smA, stream>>>(x + b0 * in_img, p.n0, p.n1, p.ppb, p.radA, p.strA,
                                                                   twA, p.m, Tt, p.t_img);
-        fcg_cols<T><<<dim3(blkB, g), p.thrB, smB, stream>>>(Tt, p.t_img, p.n0, p.m, p.cpb, p.radB, p.strB, twB, C,
-                                                              p.c_img);
-        fcg_rows_inv<T><<<dim3(blkC, g), p.thrC, smC, stream>>>(C, p.c_img, p.n0, p.n1, p.rpb, p.radC, p.strC, twC,
-                                                                  norm, mode, (T)threshold, out + b0 * out_img);
+        if (p.oned) {
+            fcg_rows_inv<T, true><<<dim3(blkC, g), p.thrC, smC, stream>>>(
+                Tt, p.t_img, p.n0, p.n1, p.rpb, p.radC, p.strC, twC, norm, mode, (T)threshold, out + b0 * out_img);
+        } else {
+            fcg_cols<T><<<dim3(blkB, g), p.thrB, smB, stream>>>(Tt, p.t_img, p.n0, p.m, p.cpb, p.radB, p.strB, twB,
+                                                                  C, p.c_img);
+            fcg_rows_inv<T, false><<<dim3(blkC, g), p.thrC, smC, stream>>>(
+                C, p.c_img, p.n0, p.n1, p.rpb, p.radC, p.strC, twC, norm, mode, (T)threshold, out + b0 * out_img);
+        }
         IDIWF_CUDA_CHECK(cudaGetLastError());
     }
     return IDIWF_OK;
@@ -1251,4 +1281,69 @@ extern "C" idiwf_status idiwf_fft_autocorr(const void *x, int32_t dtype, int64_t
                               threshold, static_cast<double *>(out), ws, stream);
     return fc_run<float>(static_cast<const float *>(x), batch, p, static_cast<const float *>(norm), mode, threshold,
                          static_cast<float *>(out), ws, stream);
+}
+
+// ---- 1D: independent lines ----
+// Lines run as images of kFc1dLines rows (plus one image of the remainder).
+constexpr int kFc1dLines = 1024;
+static bool fc1d_plans(int64_t lines, int n, int dtype, FcgPlan &full, FcgPlan &rest, int64_t &nfull, int &nrest) {
+    if (lines <= 0 || (dtype != IDIWF_F64 && dtype != IDIWF_F32)) return false;
+    const int L = (int)std::min<int64_t>(lines, kFc1dLines);
+    nfull = lines / L;
+    nrest = (int)(lines - nfull * L);
+    if (!fcg_plan(nfull, L, n, dtype, full, true)) return false;
+    if (nrest && !fcg_plan(1, nrest, n, dtype, rest, true)) return false;
+    return true;
+}
+
+extern "C" size_t idiwf_fft_autocorr_1d_workspace_size(int64_t lines, int32_t n, int32_t dtype) {
+    FcgPlan full, rest;
+    int64_t nfull;
+    int nrest;
+    if (!fc1d_plans(lines, n, dtype, full, rest, nfull, nrest)) return 0;
+    // the remainder image reuses the same workspace (it is smaller)
+    return full.twA_bytes + full.twC_bytes + full.t_bytes;
+}
+
+extern "C" idiwf_status idiwf_fft_autocorr_1d(const void *x, int32_t dtype, int64_t lines, int32_t n,
+                                              const void *norm, int32_t mode, double threshold, void *out,
+                                              void *workspace, size_t workspace_bytes, cudaStream_t stream) {
+    if (!x || !out) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (lines <= 0) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "lines must be positive");
+    if (dtype != IDIWF_F64 && dtype != IDIWF_F32)
+        return set_error(IDIWF_ERR_INVALID_ARGUMENT, "dtype must be IDIWF_F64 or IDIWF_F32");
+    FcgPlan full, rest;
+    int64_t nfull;
+    int nrest;
+    if (!fc1d_plans(lines, n, dtype, full, rest, nfull, nrest))
+        return set_error(IDIWF_ERR_UNSUPPORTED,
+                         "length not supported by the hand-written autocorrelation (an even fastlen(2 n) <= 4096)");
+    if (mode < -1 || mode > 2) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "mode must be -1, 0, 1 or 2");
+    if ((mode == 0 || mode == 1) && !norm) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "modes 0 and 1 need norm");
+    const size_t need = idiwf_fft_autocorr_1d_workspace_size(lines, n, dtype);
+    if (!workspace || workspace_bytes < need)
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace smaller than idiwf_fft_autocorr_1d_workspace_size()");
+    if (reinterpret_cast<uintptr_t>(workspace) & 255)
+        return set_error(IDIWF_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    const size_t es = dtype == IDIWF_F64 ? 8 : 4;
+    const int64_t done = nfull * full.n0;
+    const unsigned char *xb = static_cast<const unsigned char *>(x);
+    unsigned char *ob = static_cast<unsigned char *>(out);
+    for (int part = 0; part < 2; ++part) {
+        const FcgPlan &p = part == 0 ? full : rest;
+        const int64_t images = part == 0 ? nfull : (nrest ? 1 : 0);
+        if (images == 0) continue;
+        const void *xp = xb + (part == 0 ? 0 : (size_t)done * n * es);
+        void *op = ob + (part == 0 ? 0 : (size_t)done * 2 * n * es);
+        idiwf_status st;
+        if (dtype == IDIWF_F64)
+            st = fcg_run<double>(static_cast<const double *>(xp), images, p, static_cast<const double *>(norm), mode,
+                                 threshold, static_cast<double *>(op), ws, stream);
+        else
+            st = fcg_run<float>(static_cast<const float *>(xp), images, p, static_cast<const float *>(norm), mode,
+                                threshold, static_cast<float *>(op), ws, stream);
+        if (st != IDIWF_OK) return st;
+    }
+    return IDIWF_OK;
 }

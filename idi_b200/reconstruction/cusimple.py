@@ -90,21 +90,32 @@ def _autocorr(x, nax, fftshape):
 
 
 def _hand_ok(shape, dtype):
-    """Whether ``idiwf_fft_autocorr`` takes these one or two correlated axes
-    (one axis of length n runs as a 1 x n image)."""
+    """Whether ``idiwf_fft_autocorr`` (two correlated axes) or
+    ``idiwf_fft_autocorr_1d`` (one) takes this shape."""
     if len(shape) not in (1, 2) or dtype not in (torch.float32, torch.float64):
         return False
-    n0, n1 = (1, int(shape[0])) if len(shape) == 1 else (int(shape[0]), int(shape[1]))
     code = nat.F64 if dtype == torch.float64 else nat.F32
-    return nat.load().idiwf_fft_autocorr_workspace_size(1, n0, n1, code) > 0
+    lib = nat.load()
+    if len(shape) == 1:
+        return lib.idiwf_fft_autocorr_1d_workspace_size(1, int(shape[0]), code) > 0
+    return lib.idiwf_fft_autocorr_workspace_size(1, int(shape[0]), int(shape[1]), code) > 0
 
 
 def _hand_autocorr_1d(x, mode=-1, threshold=0.0):
-    """Autocorrelation of the last axis (length n) as 1 x n images: row 1 of
-    the (2, 2n) result is the zero row shift."""
+    """Autocorrelation of every line of the last axis (length n) by
+    ``idiwf_fft_autocorr_1d``; ``mode`` -1 or 2 (pair count n - |j - n|)."""
     n = int(x.shape[-1])
-    out = _hand_autocorr(x.reshape(-1, 1, n), mode=mode, threshold=threshold)
-    return out[:, 1, :].reshape(tuple(x.shape[:-1]) + (2 * n,))
+    x = x.contiguous()
+    lines = x.numel() // n
+    out = torch.empty(tuple(x.shape[:-1]) + (2 * n,), dtype=x.dtype, device=x.device)
+    lib = nat.load()
+    code = _code(x)
+    nbytes = lib.idiwf_fft_autocorr_1d_workspace_size(lines, n, code)
+    ws = _core.WORKSPACES.get(nbytes, x.device, "fftcorr")
+    nat.check(lib.idiwf_fft_autocorr_1d(
+        ctypes.c_void_p(x.data_ptr()), code, lines, n, None, int(mode), float(threshold),
+        ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(), _stream(x.device)))
+    return out
 
 
 def _hand_autocorr(x, mode=-1, norm=None, threshold=0.0):

@@ -479,8 +479,7 @@ idiwf_status idiwf_qcorr_3d(const float *zd, const float *images, int32_t n_imag
  * G1 = fastlen(2 n1) (smallest products of 2, 3, 5, 7, 11, as
  * idi.util.fastlen) are at most 4096 with G1 even; out is then the centre
  * crop (i - n0) mod G0, (j - n1) mod G1 of the shifted array, as the
- * reference's slice.  Other shapes: IDIWF_ERR_UNSUPPORTED.  A 1D
- * autocorrelation of length n is row 1 of the 1 x n image's result.
+ * reference's slice.  Other shapes: IDIWF_ERR_UNSUPPORTED.
  * workspace: idiwf_fft_autocorr_workspace_size() bytes for this batch and
  * shape, 256-byte aligned (twiddle tables and the intermediates of one group
  * of images; groups run one after another; 0 for unsupported arguments).
@@ -489,6 +488,20 @@ size_t idiwf_fft_autocorr_workspace_size(int64_t batch, int32_t n0, int32_t n1, 
 idiwf_status idiwf_fft_autocorr(const void *x, int32_t dtype, int64_t batch, int32_t n0, int32_t n1,
                                 const void *norm, int32_t mode, double threshold, void *out, void *workspace,
                                 size_t workspace_bytes, cudaStream_t stream);
+
+/*
+ * The autocorrelation of each of `lines` independent lines (x: lines x n of
+ * dtype, contiguous) along its length, as cusimple.py:6-38 with one
+ * correlated axis: out (lines x 2n) = crop(fftshift(irfft(|rfft(x, G)|^2)))
+ * with G = fastlen(2 n), which must be even and at most 4096 (else
+ * IDIWF_ERR_UNSUPPORTED).  Modes as idiwf_fft_autocorr, with the pair count
+ * n - |j - n| and norm of 2n values.  workspace:
+ * idiwf_fft_autocorr_1d_workspace_size() bytes, 256-byte aligned.
+ */
+size_t idiwf_fft_autocorr_1d_workspace_size(int64_t lines, int32_t n, int32_t dtype);
+idiwf_status idiwf_fft_autocorr_1d(const void *x, int32_t dtype, int64_t lines, int32_t n, const void *norm,
+                                   int32_t mode, double threshold, void *out, void *workspace,
+                                   size_t workspace_bytes, cudaStream_t stream);
 
 /* Helpers around a library FFT (other shapes). */
 

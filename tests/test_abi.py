@@ -210,3 +210,30 @@ def test_fft_autocorr_shape_predicate():
     assert not cusimple._hand_ok((8, 8192), torch.float64)
     assert not cusimple._hand_ok((8, 8, 8), torch.float64)
     assert not cusimple._hand_ok((8, 8), torch.float16)
+
+
+def test_fft_autocorr_1d_validation(lib):
+    """``idiwf_fft_autocorr_1d``: lines run as images of up to 1024 rows;
+    the workspace holds two twiddle tables and T of one group of images."""
+    vp = ctypes.c_void_p
+    al = lambda b: (b + 255) // 256 * 256  # noqa: E731
+    # 3000 lines of 1000: images of 1024 rows (2 + a remainder of 952), G = 2000, m = 1001
+    assert lib.idiwf_fft_autocorr_1d_workspace_size(3000, 1000, nat.F64) == 2 * al(2000 * 16) + al(
+        2 * 1001 * 1024 * 16)
+    assert lib.idiwf_fft_autocorr_1d_workspace_size(10, 30, nat.F32) == 2 * al(60 * 16) + al(31 * 10 * 8)
+    assert lib.idiwf_fft_autocorr_1d_workspace_size(1, 13, nat.F64) == 0  # fastlen(26) = 27 is odd
+    assert lib.idiwf_fft_autocorr_1d_workspace_size(0, 30, nat.F64) == 0
+    assert lib.idiwf_fft_autocorr_1d_workspace_size(1, 30, 7) == 0
+    need = lib.idiwf_fft_autocorr_1d_workspace_size(4, 30, nat.F64)
+
+    def call(x=4096, dtype=nat.F64, lines=4, n=30, mode=-1, ws=4096, ws_bytes=need, out=8192):
+        return lib.idiwf_fft_autocorr_1d(vp(x), dtype, lines, n, None, mode, 0.5, vp(out), vp(ws), ws_bytes, None)
+
+    assert call(x=0) == nat.ERR_INVALID_ARGUMENT
+    assert call(lines=0) == nat.ERR_INVALID_ARGUMENT
+    assert call(dtype=9) == nat.ERR_INVALID_ARGUMENT
+    assert call(n=13) == nat.ERR_UNSUPPORTED
+    assert call(mode=5) == nat.ERR_INVALID_ARGUMENT
+    assert call(mode=1) == nat.ERR_INVALID_ARGUMENT  # no norm
+    assert call(ws_bytes=need - 1) == nat.ERR_WORKSPACE
+    assert call(ws=4096 + 64) == nat.ERR_WORKSPACE

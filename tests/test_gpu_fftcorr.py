@@ -160,14 +160,16 @@ def test_hand_fft_general_vs_cufft(shape, dtype):
     assert ((hn - rn).abs() * count)[ok].max().item() <= 2 * tol * ref.abs().max().item()
 
 
-@pytest.mark.parametrize("n", [4, 30, 1000, 1024, 1500])
-def test_hand_fft_1d_vs_cufft(n):
-    """One correlated axis as 1 x n images, against cuFFT's 1D transforms."""
+@pytest.mark.parametrize("lead,n", [((5, 2), 4), ((5, 2), 30), ((5, 2), 1000), ((5, 2), 1024), ((5, 2), 1500),
+                                    ((2500,), 100), ((1030,), 7)])
+def test_hand_fft_1d_vs_cufft(lead, n):
+    """One correlated axis (idiwf_fft_autocorr_1d; more than 1024 lines run as
+    several images plus a remainder) against cuFFT's 1D transforms."""
     g = torch.Generator(device="cuda").manual_seed(n)
-    x = torch.empty((5, 2, n), dtype=torch.float64, device="cuda").exponential_(1.0, generator=g)
+    x = torch.empty(lead + (n,), dtype=torch.float64, device="cuda").exponential_(1.0, generator=g)
     ref = cusimple._crop(cusimple._autocorr(x, 1, [cusimple.fastlen(2 * n)]), 1, [n])
     hand = cusimple._hand_autocorr_1d(x)
-    assert hand.shape == ref.shape == (5, 2, 2 * n)
+    assert hand.shape == ref.shape == lead + (2 * n,)
     assert (hand - ref).abs().max().item() <= 1e-12 * ref.abs().max().item()
     j = torch.arange(2 * n, dtype=torch.float64, device="cuda")
     count = n - (j - n).abs()
