@@ -736,6 +736,40 @@ __device__ __forceinline__ V *fcg_fft(V *A, V *B, int stride, const FcgRad &rad,
     return in;
 }
 
+// Bluestein's algorithm for the inverse along rows when L1/2 has a prime
+// factor above 11 (an odd G1, L1 = G1 - 1): with c_m = exp(pi i m^2 / N),
+//     sum_n Z_n exp(2 pi i k n / N) = c_k sum_n (Z_n c_n) conj(c_{k-n}),
+// a cyclic convolution of length M = fastlen(2N - 1) done with the FFTs
+// above; the filter's spectrum Bf = FFT(conj c, wrapped) / M is made once
+// per call.
+__global__ void fcg_chirp_kernel(double2 *c, int N) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= N) return;
+    const int64_t e = ((int64_t)m * m) % (2 * (int64_t)N);  // exact: the angle pi e / N
+    double sn, cs;
+    sincospi((double)e / (double)N, &sn, &cs);
+    c[m] = make_double2(cs, sn);
+}
+
+__global__ void __launch_bounds__(512) fcg_blue_filter_kernel(const double2 *__restrict__ c, int N, FcgRad radM,
+                                                              int stride, const double2 *__restrict__ twM,
+                                                              double2 *__restrict__ Bf) {
+    extern __shared__ __align__(16) unsigned char fsm[];
+    double2 *S = reinterpret_cast<double2 *>(fsm);
+    const int M = radM.n;
+    auto ld = [&](int, int i) -> double2 {
+        const int m = i < N ? i : (M - i < N ? M - i : -1);
+        if (m < 0) return make_double2(0.0, 0.0);
+        return make_double2(c[m].x, -c[m].y);
+    };
+    const double2 *F = fcg_fft<double2, false>(S, S + stride, stride, radM, 1, twM, M, ld, true);
+    const double inv = 1.0 / (double)M;
+    for (int i = threadIdx.x; i < M; i += blockDim.x) {
+        const double2 v = F[fcg_slot<double2>(0, i, stride)];
+        Bf[i] = make_double2(v.x * inv, v.y * inv);
+    }
+}
+
 // Pass A (general): ppb pairs of rows per block, one image per blockIdx.y;
 // rows 2p, 2p+1 as one complex sequence of length G1 (zero-padded from n1),
 // split by Hermitian symmetry into the two real spectra, columns k = 0..m-1
@@ -839,23 +873,28 @@ __global__ void __launch_bounds__(512) fcg_cols(const typename Cx<T>::t *__restr
 }
 
 // Pass C (general): rpb rows per block of rows 0..n0; the inverse real FFT
-// of length L1 = 2 rad.n through a complex inverse FFT of length rad.n (the
-// real parts only at frequencies 0 and L1/2, as a c2r transform), then the
+// of length L1 = 2 Hp through a complex inverse FFT of Hp values (the real
+// parts only at frequencies 0 and L1/2, as a c2r transform), then the
 // centre crop: output (i, j) of row r is column (j - n1) mod L1 for
 // i = n0 + r (r < n0), and by point symmetry column (n1 - j) mod L1 for the
 // mirrored row i = n0 - r.  Normalisation modes as fc_rows_inv.
 // ONED: the autocorrelation of each of n0 lines on its own -- the half
 // spectrum is the line's power |T[k][r]|^2 (C is pass A's T), and line r's
 // result is output row r (pair count n1 - |j - n1|, norm of 2 n1 values).
-template <typename T, bool ONED>
+// BLUE: the inverse of Hp values by Bluestein's algorithm through FFTs of
+// length rad.n = M (chirp c, filter spectrum Bf); otherwise rad.n = Hp.
+template <typename T, bool ONED, bool BLUE>
 __global__ void __launch_bounds__(512) fcg_rows_inv(const typename Cx<T>::t *__restrict__ C, size_t c_img, int n0,
-                                                    int n1, int rpb, FcgRad rad, int stride,
-                                                    const double2 *__restrict__ twl1, const T *__restrict__ norm,
+                                                    int n1, int Hp, int rpb, FcgRad rad, int stride,
+                                                    const double2 *__restrict__ twl1, const double2 *__restrict__ twm,
+                                                    const double2 *__restrict__ chirp,
+                                                    const double2 *__restrict__ Bf, const T *__restrict__ norm,
                                                     int mode, T threshold, T *__restrict__ out) {
     using V = typename Cx<T>::t;
     extern __shared__ __align__(16) unsigned char fsm[];
     V *S = reinterpret_cast<V *>(fsm);
-    const int Hp = rad.n, L1 = 2 * Hp, r0 = blockIdx.x * rpb, W = 2 * n1;
+    V *S2 = S + rpb * stride;
+    const int L1 = 2 * Hp, r0 = blockIdx.x * rpb, W = 2 * n1, NF = rad.n;
     const int rows = ONED ? n0 : n0 + 1, cst = ONED ? n0 : n0 + 1;
     C += (size_t)blockIdx.y * c_img;
     out += (size_t)blockIdx.y * (ONED ? n0 : 2 * n0) * W;
@@ -867,12 +906,19 @@ __global__ void __launch_bounds__(512) fcg_rows_inv(const typename Cx<T>::t *__r
         }
         return y;
     };
+    auto cvt = [](double2 d) -> V {
+        V v;
+        v.x = (T)d.x;
+        v.y = (T)d.y;
+        return v;
+    };
     // Z[k] = (Y[k] + conj Y[Hp-k]) + i W^-k (Y[k] - conj Y[Hp-k]); rows fastest
+    // (BLUE: times the chirp, zero-padded to M)
     FcgIdx it(threadIdx.x, blockDim.x, rpb);
-    for (int idx = threadIdx.x; idx < rpb * Hp; idx += blockDim.x, it.next()) {
+    for (int idx = threadIdx.x; idx < rpb * NF; idx += blockDim.x, it.next()) {
         const int k = it.a, rr = it.b, r = r0 + rr;
         V z = cx_zero<V>();
-        if (r < rows) {
+        if (r < rows && k < Hp) {
             V yk = spec(k, r), yc = cx_conj(spec(Hp - k, r));
             if (k == 0) {
                 yk.y = T(0);
@@ -886,14 +932,28 @@ __global__ void __launch_bounds__(512) fcg_rows_inv(const typename Cx<T>::t *__r
             const V wd = cx_mul(w, d);
             z.x = e.x - wd.y;
             z.y = e.y + wd.x;
+            if constexpr (BLUE) z = cx_mul(z, cvt(__ldg(&chirp[k])));
         }
         S[fcg_slot<V>(rr, k, stride)] = z;
     }
     __syncthreads();
-    const V *Z = fcg_fft<V, true>(S, S + rpb * stride, stride, rad, rpb, twl1, L1, FcNoLoad<V>{}, false);
+    const V *Z;
+    if constexpr (BLUE) {
+        V *F = fcg_fft<V, false>(S, S2, stride, rad, rpb, twm, NF, FcNoLoad<V>{}, false);
+        for (int idx = threadIdx.x; idx < rpb * NF; idx += blockDim.x) {
+            const int rr = idx / NF, i = idx - rr * NF;
+            V &v = F[fcg_slot<V>(rr, i, stride)];
+            v = cx_mul(v, cvt(__ldg(&Bf[i])));
+        }
+        __syncthreads();
+        Z = fcg_fft<V, true>(F, F == S ? S2 : S, stride, rad, rpb, twm, NF, FcNoLoad<V>{}, false);
+    } else {
+        Z = fcg_fft<V, true>(S, S2, stride, rad, rpb, twl1, L1, FcNoLoad<V>{}, false);
+    }
     const T scale = T(1) / (T)L1;
     auto val = [&](int rr, int c) -> T {
-        const V z = Z[fcg_slot<V>(rr, c >> 1, stride)];
+        V z = Z[fcg_slot<V>(rr, c >> 1, stride)];
+        if constexpr (BLUE) z = cx_mul(z, cvt(__ldg(&chirp[c >> 1])));
         return ((c & 1) ? z.y : z.x) * scale;
     };
     auto put = [&](int i, int j, T y) {
@@ -1089,18 +1149,40 @@ static int fcg_threads(int values, size_t smem) {
     const int cap = 2 * smem <= 227 * 1024 ? 256 : 512;
     return std::min(cap, std::max(32, (values / 4 + 31) / 32 * 32));
 }
+constexpr int kFcgMaxLen = 4096;  // G0, G1 and L1 of the general path
+// Bluestein's FFT length: any M >= need works; the one from need to
+// min(2 need, 4096) with the least estimated work, M times the per-value
+// cost of its passes (odd radices cost more than 8, 4, 2); 0 if none fits.
+static int fcg_blue_length(int need) {
+    int best = 0;
+    double best_cost = 0;
+    for (int M = need; M <= std::min(2 * need, kFcgMaxLen); ++M) {
+        FcgRad r;
+        if (!fcg_radices(M, r)) continue;
+        double c = 0;
+        for (int i = 0; i < r.np; ++i)
+            c += r.r[i] == 11 ? 4.0 : r.r[i] == 7 ? 2.8 : r.r[i] == 5 ? 2.0 : r.r[i] == 3 ? 1.4 : r.r[i] == 8 ? 1.5 : 1.1;
+        c *= M;
+        if (!best || c < best_cost) {
+            best = M;
+            best_cost = c;
+        }
+    }
+    return best;
+}
 static int fcg_stride(int n, int lkc) { return n + ((n - 1) >> lkc) + 1; }
 
-constexpr int kFcgMaxLen = 4096;  // G0, G1 and L1 of the general path
 struct FcgPlan {
-    int n0, n1, G0, G1, L1, m;
+    int n0, n1, G0, G1, L1, m, Hp;
     int ppb, cpb, rpb;  // row pairs (pass A), columns (B), rows (C) per block
-    FcgRad radA, radB, radC;
+    FcgRad radA, radB, radC;  // radC: Hp, or M with blue
     int thrA, thrB, thrC, strA, strB, strC;
     size_t vsz, t_img, c_img;
-    size_t twA_bytes, twB_bytes, twC_bytes, t_bytes, c_bytes;
+    size_t twA_bytes, twB_bytes, twC_bytes, blue_bytes, t_bytes, c_bytes;
     int64_t group;
     bool oned;  // n0 independent lines: no column pass, no C
+    bool blue;  // odd G1: the inverse of Hp = (G1 - 1) / 2 values by Bluestein
+    int M;      // Bluestein's FFT length
 };
 static bool fcg_plan(int64_t batch, int n0, int n1, int dtype, FcgPlan &p, bool oned = false) {
     if (n0 < 1 || n1 < 1 || (!oned && n0 > kFcgMaxLen) || n1 > kFcgMaxLen) return false;
@@ -1110,29 +1192,39 @@ static bool fcg_plan(int64_t batch, int n0, int n1, int dtype, FcgPlan &p, bool 
     p.n1 = n1;
     p.G0 = fcg_fastlen(2 * n0);
     p.G1 = fcg_fastlen(2 * n1);
-    p.L1 = p.G1;
+    // numpy's irfftn default along the last axis: 2 (G1/2 + 1 - 1) values
+    p.L1 = p.G1 % 2 ? p.G1 - 1 : p.G1;
     p.m = p.G1 / 2 + 1;
-    if (p.G0 > kFcgMaxLen || p.G1 > kFcgMaxLen || p.G1 % 2) return false;
+    p.Hp = p.L1 / 2;
+    if (p.G0 > kFcgMaxLen || p.G1 > kFcgMaxLen) return false;
     if (oned) p.G0 = 1;  // no column pass
-    if (!fcg_radices(p.G1, p.radA) || !fcg_radices(p.L1 / 2, p.radC)) return false;
+    if (!fcg_radices(p.G1, p.radA)) return false;
     if (!oned && !fcg_radices(p.G0, p.radB)) return false;
+    p.blue = !fcg_radices(p.Hp, p.radC);
+    if (p.blue) {
+        p.M = fcg_blue_length(2 * p.Hp - 1);
+        if (p.M == 0 || !fcg_radices(p.M, p.radC)) return false;
+    }
+    const int nC = p.radC.n;  // values per row in pass C
     p.vsz = dtype == IDIWF_F64 ? 16 : 8;
     const int lkc = p.vsz == 16 ? 3 : 4;
     p.ppb = std::max(1, std::min(kFcBlockElems / p.G1, (n0 + 1) / 2));
     p.cpb = std::max(1, std::min(kFcBlockElems / p.G0, p.m));
-    p.rpb = std::max(1, std::min(kFcBlockElems / (p.L1 / 2), oned ? n0 : n0 + 1));
+    p.rpb = std::max(1, std::min(kFcBlockElems / nC, oned ? n0 : n0 + 1));
     p.strA = fcg_stride(p.G1, lkc);
     p.strB = fcg_stride(p.G0, lkc);
-    p.strC = fcg_stride(p.L1 / 2, lkc);
+    p.strC = fcg_stride(nC, lkc);
     // ping-pong buffers of count sequences each
     p.thrA = fcg_threads(p.ppb * p.G1, 2 * (size_t)p.ppb * p.strA * p.vsz);
     p.thrB = fcg_threads(p.cpb * p.G0, 2 * (size_t)p.cpb * p.strB * p.vsz);
-    p.thrC = fcg_threads(p.rpb * (p.L1 / 2), 2 * (size_t)p.rpb * p.strC * p.vsz);
+    p.thrC = fcg_threads(p.rpb * nC, 2 * (size_t)p.rpb * p.strC * p.vsz);
     p.t_img = (size_t)p.m * n0;
     p.c_img = oned ? 0 : (size_t)p.m * (n0 + 1);
     p.twA_bytes = fc_align((size_t)p.G1 * sizeof(double2));
     p.twB_bytes = oned ? 0 : fc_align((size_t)p.G0 * sizeof(double2));
     p.twC_bytes = fc_align((size_t)p.L1 * sizeof(double2));
+    // chirp (Hp), filter spectrum (M), twiddles of M
+    p.blue_bytes = p.blue ? fc_align((size_t)p.Hp * sizeof(double2)) + 2 * fc_align((size_t)p.M * sizeof(double2)) : 0;
     const size_t per = (p.t_img + p.c_img) * p.vsz;
     const int64_t gmax = std::max<int64_t>(1, std::min<int64_t>(65535, (int64_t)((256u << 20) / per)));
     const int64_t ngroups = (std::max<int64_t>(batch, 1) + gmax - 1) / gmax;
@@ -1140,6 +1232,14 @@ static bool fcg_plan(int64_t batch, int n0, int n1, int dtype, FcgPlan &p, bool 
     p.t_bytes = fc_align(p.t_img * p.vsz * p.group);
     p.c_bytes = fc_align(p.c_img * p.vsz * p.group);
     return true;
+}
+// For an odd G1 the reference's inverse has G1 - 1 values and its pair count
+// (the same transform of ones) is not the closed form of mode 2.
+static const char *const kFcOddPairs =
+    "mode 2 (closed-form pair count) does not hold for an odd fastlen(2 n1); transform ones with mode -1 and pass "
+    "the result as norm with mode 0";
+static size_t fcg_ws_bytes(const FcgPlan &p) {
+    return p.twA_bytes + p.twB_bytes + p.twC_bytes + p.blue_bytes + p.t_bytes + p.c_bytes;
 }
 
 template <typename T>
@@ -1149,22 +1249,35 @@ static idiwf_status fcg_run(const T *x, int64_t batch, const FcgPlan &p, const T
     double2 *twA = reinterpret_cast<double2 *>(ws);
     double2 *twB = reinterpret_cast<double2 *>(ws + p.twA_bytes);
     double2 *twC = reinterpret_cast<double2 *>(ws + p.twA_bytes + p.twB_bytes);
-    unsigned char *rest = ws + p.twA_bytes + p.twB_bytes + p.twC_bytes;
+    unsigned char *bl = ws + p.twA_bytes + p.twB_bytes + p.twC_bytes;
+    double2 *chirp = p.blue ? reinterpret_cast<double2 *>(bl) : nullptr;
+    double2 *Bf = p.blue ? reinterpret_cast<double2 *>(bl + fc_align((size_t)p.Hp * sizeof(double2))) : nullptr;
+    double2 *twM = p.blue ? Bf + fc_align((size_t)p.M * sizeof(double2)) / sizeof(double2) : nullptr;
+    unsigned char *rest = bl + p.blue_bytes;
     V *Tt = reinterpret_cast<V *>(rest);
     V *C = reinterpret_cast<V *>(rest + p.t_bytes);
     fc_twiddle_kernel<<<(p.G1 + 255) / 256, 256, 0, stream>>>(twA, p.G1);
     if (!p.oned) fc_twiddle_kernel<<<(p.G0 + 255) / 256, 256, 0, stream>>>(twB, p.G0);
     fc_twiddle_kernel<<<(p.L1 + 255) / 256, 256, 0, stream>>>(twC, p.L1);
     IDIWF_CUDA_CHECK(cudaGetLastError());
+    if (p.blue) {
+        fc_twiddle_kernel<<<(p.M + 255) / 256, 256, 0, stream>>>(twM, p.M);
+        fcg_chirp_kernel<<<(p.Hp + 255) / 256, 256, 0, stream>>>(chirp, p.Hp);
+        const int strM = fcg_stride(p.M, 3);  // the filter is made in FP64
+        const size_t smF = 2 * (size_t)strM * sizeof(double2);
+        IDIWF_CUDA_CHECK(
+            cudaFuncSetAttribute(fcg_blue_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smF));
+        fcg_blue_filter_kernel<<<1, 512, smF, stream>>>(chirp, p.Hp, p.radC, strM, twM, Bf);
+        IDIWF_CUDA_CHECK(cudaGetLastError());
+    }
     const size_t smA = 2 * (size_t)p.ppb * p.strA * sizeof(V), smB = 2 * (size_t)p.cpb * p.strB * sizeof(V);
     const size_t smC = 2 * (size_t)p.rpb * p.strC * sizeof(V);
     IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fcg_rows_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
     if (!p.oned)
         IDIWF_CUDA_CHECK(cudaFuncSetAttribute(fcg_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
-    IDIWF_CUDA_CHECK(
-        cudaFuncSetAttribute(fcg_rows_inv<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
-    IDIWF_CUDA_CHECK(
-        cudaFuncSetAttribute(fcg_rows_inv<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
+    void *kC = p.oned ? (p.blue ? (void *)fcg_rows_inv<T, true, true> : (void *)fcg_rows_inv<T, true, false>)
+                      : (p.blue ? (void *)fcg_rows_inv<T, false, true> : (void *)fcg_rows_inv<T, false, false>);
+    IDIWF_CUDA_CHECK(cudaFuncSetAttribute(kC, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
     const int npairs = (p.n0 + 1) / 2;
     const unsigned blkA = (unsigned)((npairs + p.ppb - 1) / p.ppb), blkB = (unsigned)((p.m + p.cpb - 1) / p.cpb);
     const int rowsC = p.oned ? p.n0 : p.n0 + 1;
@@ -1174,16 +1287,18 @@ static idiwf_status fcg_run(const T *x, int64_t batch, const FcgPlan &p, const T
         const unsigned g = (unsigned)std::min<int64_t>(p.group, batch - b0);
         fcg_rows_fwd<T><<<dim3(blkA, g), p.thrA, smA, stream>>>(x + b0 * in_img, p.n0, p.n1, p.ppb, p.radA, p.strA,
                                                                   twA, p.m, Tt, p.t_img);
-        if (p.oned) {
-            fcg_rows_inv<T, true><<<dim3(blkC, g), p.thrC, smC, stream>>>(
-                Tt, p.t_img, p.n0, p.n1, p.rpb, p.radC, p.strC, twC, norm, mode, (T)threshold, out + b0 * out_img);
-        } else {
+        if (!p.oned)
             fcg_cols<T><<<dim3(blkB, g), p.thrB, smB, stream>>>(Tt, p.t_img, p.n0, p.m, p.cpb, p.radB, p.strB, twB,
                                                                   C, p.c_img);
-            fcg_rows_inv<T, false><<<dim3(blkC, g), p.thrC, smC, stream>>>(
-                C, p.c_img, p.n0, p.n1, p.rpb, p.radC, p.strC, twC, norm, mode, (T)threshold, out + b0 * out_img);
-        }
         IDIWF_CUDA_CHECK(cudaGetLastError());
+        const V *Csrc = p.oned ? Tt : C;
+        const size_t c_img = p.oned ? p.t_img : p.c_img;
+        T *o = out + b0 * out_img;
+        T thr = (T)threshold;
+        void *args[] = {(void *)&Csrc, (void *)&c_img, (void *)&p.n0, (void *)&p.n1, (void *)&p.Hp, (void *)&p.rpb,
+                        (void *)&p.radC, (void *)&p.strC, (void *)&twC, (void *)&twM, (void *)&chirp, (void *)&Bf,
+                        (void *)&norm, (void *)&mode, (void *)&thr, (void *)&o};
+        IDIWF_CUDA_CHECK(cudaLaunchKernel(kC, dim3(blkC, g), dim3(p.thrC), args, smC, stream));
     }
     return IDIWF_OK;
 }
@@ -1196,7 +1311,7 @@ extern "C" size_t idiwf_fft_autocorr_workspace_size(int64_t batch, int32_t n0, i
     }
     FcgPlan g;
     if (!fcg_plan(batch, n0, n1, dtype, g)) return 0;
-    return g.twA_bytes + g.twB_bytes + g.twC_bytes + g.t_bytes + g.c_bytes;
+    return fcg_ws_bytes(g);
 }
 
 template <typename T, int EA, int EB>
@@ -1252,7 +1367,7 @@ extern "C" idiwf_status idiwf_fft_autocorr(const void *x, int32_t dtype, int64_t
     if ((dtype == IDIWF_F64 || dtype == IDIWF_F32) && idiwf_fft_autocorr_workspace_size(batch, n0, n1, dtype) == 0)
         return set_error(IDIWF_ERR_UNSUPPORTED,
                          "shape not supported by the hand-written autocorrelation (powers of two from 4 to 4096, or "
-                         "fastlen(2 n0) <= 4096 and an even fastlen(2 n1) <= 4096)");
+                         "fastlen(2 n0), fastlen(2 n1) <= 4096)");
     if (mode < -1 || mode > 2) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "mode must be -1, 0, 1 or 2");
     if ((mode == 0 || mode == 1) && !norm) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "modes 0 and 1 need norm");
     const size_t need = idiwf_fft_autocorr_workspace_size(batch, n0, n1, dtype);
@@ -1265,6 +1380,8 @@ extern "C" idiwf_status idiwf_fft_autocorr(const void *x, int32_t dtype, int64_t
     if (!(fc_pow2(n0) && fc_pow2(n1))) {
         FcgPlan g;
         fcg_plan(batch, n0, n1, dtype, g);
+        if (g.blue && mode == 2)
+            return set_error(IDIWF_ERR_UNSUPPORTED, kFcOddPairs);
         if (dtype == IDIWF_F64)
             return fcg_run<double>(static_cast<const double *>(x), batch, g, static_cast<const double *>(norm), mode,
                                    threshold, static_cast<double *>(out), ws, stream);
@@ -1302,7 +1419,7 @@ extern "C" size_t idiwf_fft_autocorr_1d_workspace_size(int64_t lines, int32_t n,
     int nrest;
     if (!fc1d_plans(lines, n, dtype, full, rest, nfull, nrest)) return 0;
     // the remainder image reuses the same workspace (it is smaller)
-    return full.twA_bytes + full.twC_bytes + full.t_bytes;
+    return fcg_ws_bytes(full);
 }
 
 extern "C" idiwf_status idiwf_fft_autocorr_1d(const void *x, int32_t dtype, int64_t lines, int32_t n,
@@ -1317,7 +1434,8 @@ extern "C" idiwf_status idiwf_fft_autocorr_1d(const void *x, int32_t dtype, int6
     int nrest;
     if (!fc1d_plans(lines, n, dtype, full, rest, nfull, nrest))
         return set_error(IDIWF_ERR_UNSUPPORTED,
-                         "length not supported by the hand-written autocorrelation (an even fastlen(2 n) <= 4096)");
+                         "length not supported by the hand-written autocorrelation (fastlen(2 n) <= 4096)");
+    if (full.blue && mode == 2) return set_error(IDIWF_ERR_UNSUPPORTED, kFcOddPairs);
     if (mode < -1 || mode > 2) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "mode must be -1, 0, 1 or 2");
     if ((mode == 0 || mode == 1) && !norm) return set_error(IDIWF_ERR_INVALID_ARGUMENT, "modes 0 and 1 need norm");
     const size_t need = idiwf_fft_autocorr_1d_workspace_size(lines, n, dtype);

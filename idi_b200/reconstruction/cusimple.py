@@ -5,7 +5,8 @@ One or two correlated axes go through this library's own FFTs end to end
 (``idiwf_fft_autocorr``: the padded transform, the power spectrum, the
 inverse, the fftshift, the crop and the normalisation) whenever the library
 takes the shape: powers of two from 4 to 4096, or padded lengths
-``fastlen(2 n)`` up to 4096 with an even one along the last axis.
+``fastlen(2 n)`` up to 4096 (an odd last one by Bluestein's algorithm, for
+the reference's inverse of one value fewer).
 Other shapes (and three axes) use cuFFT's transforms (through ``torch.fft``)
 with this library's power-spectrum and crop kernels around them
 (``idiwf_power_spectrum``, ``idiwf_corr_crop``).  The correlator's running mean / variance is
@@ -101,11 +102,14 @@ def _hand_ok(shape, dtype):
     return lib.idiwf_fft_autocorr_workspace_size(1, int(shape[0]), int(shape[1]), code) > 0
 
 
-def _hand_autocorr_1d(x, mode=-1, threshold=0.0):
+def _hand_autocorr_1d(x, mode=-1, norm=None, threshold=0.0):
     """Autocorrelation of every line of the last axis (length n) by
-    ``idiwf_fft_autocorr_1d``; ``mode`` -1 or 2 (pair count n - |j - n|)."""
+    ``idiwf_fft_autocorr_1d``; ``mode`` as ``idiwf_fft_autocorr`` (norm: 2n
+    values)."""
     n = int(x.shape[-1])
     x = x.contiguous()
+    if norm is not None:
+        norm = norm.to(x.dtype).contiguous()
     lines = x.numel() // n
     out = torch.empty(tuple(x.shape[:-1]) + (2 * n,), dtype=x.dtype, device=x.device)
     lib = nat.load()
@@ -113,7 +117,8 @@ def _hand_autocorr_1d(x, mode=-1, threshold=0.0):
     nbytes = lib.idiwf_fft_autocorr_1d_workspace_size(lines, n, code)
     ws = _core.WORKSPACES.get(nbytes, x.device, "fftcorr")
     nat.check(lib.idiwf_fft_autocorr_1d(
-        ctypes.c_void_p(x.data_ptr()), code, lines, n, None, int(mode), float(threshold),
+        ctypes.c_void_p(x.data_ptr()), code, lines, n,
+        ctypes.c_void_p(norm.data_ptr()) if norm is not None else None, int(mode), float(threshold),
         ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(), _stream(x.device)))
     return out
 
@@ -159,10 +164,18 @@ def corr(input, axes=(-1, -2), norm=False, returngpu=False, **kwargs):
         x = x * (1 / x.mean(dim=others if others else None, keepdim=bool(others)))
     moved = torch.movedim(x, axes, list(range(x.ndim - len(axes), x.ndim))).contiguous()
     if _hand_ok(sizes, x.dtype):
-        # the pair count in closed form: the transform of ones in the
-        # reference rounds to the same integers, and the same < 0.9 positions
         f = _hand_autocorr if len(sizes) == 2 else _hand_autocorr_1d
-        ret = f(moved, mode=2 if norm else -1, threshold=0.9)
+        if not norm:
+            ret = f(moved, mode=-1)
+        elif fastlen(2 * sizes[-1]) % 2 == 0:
+            # the pair count in closed form: the transform of ones in the
+            # reference rounds to the same integers, and the same < 0.9 positions
+            ret = f(moved, mode=2, threshold=0.9)
+        else:
+            # an odd last padded length: the reference's inverse has one
+            # value fewer, and its pair count is the same transform of ones
+            pairs = f(torch.ones(sizes, dtype=x.dtype, device=x.device), mode=-1)
+            ret = f(moved, mode=0, norm=pairs, threshold=0.9)
     else:
         full = _autocorr(moved, len(axes), fftshape)
         pairs = None

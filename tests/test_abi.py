@@ -167,12 +167,14 @@ def test_fft_autocorr_validation(lib):
     # other lengths: padded to fastlen(2 n); tables of G1, G0 and L1 values,
     # T m x n0 and C m x (n0 + 1), m = G1 / 2 + 1.  6 x 8: G0 = 12, G1 = L1 = 16
     assert lib.idiwf_fft_autocorr_workspace_size(1, 6, 8, nat.F64) == 3 * 256 + al(9 * 6 * 16) + al(9 * 7 * 16)
-    # 5 x 13: G1 = 27 is odd, the inverse length L1 = 26 has the factor 13
-    for n0, n1 in ((5, 13), (8, 8192), (0, 8), (3000, 8), (8, 0)):
+    # padded lengths above 4096 (fastlen(4098) = 4116, fastlen(6000) = 6000)
+    for n0, n1 in ((8, 2049), (8, 8192), (0, 8), (3000, 8), (8, 0)):
         assert lib.idiwf_fft_autocorr_workspace_size(1, n0, n1, nat.F64) == 0, (n0, n1)
-    # 5 x 14: G1 = 28; 4 x 17: G1 = 35 odd, L1 = 34 -> inverse of 17 values: not taken
-    assert lib.idiwf_fft_autocorr_workspace_size(1, 5, 14, nat.F64) > 0
-    assert lib.idiwf_fft_autocorr_workspace_size(1, 4, 17, nat.F64) == 0
+    # 5 x 13: G1 = 27 is odd, the inverse has L1 = 26 values (Hp = 13 by
+    # Bluestein through FFTs of M = 32, the cheapest smooth length from
+    # 2 Hp - 1 = 25): tables of 27, 10, 26 and chirp 13, filter and twiddles 32
+    assert lib.idiwf_fft_autocorr_workspace_size(1, 5, 13, nat.F64) == (
+        al(27 * 16) + al(10 * 16) + al(26 * 16) + al(13 * 16) + 2 * al(32 * 16) + al(14 * 5 * 16) + al(14 * 6 * 16))
     assert lib.idiwf_fft_autocorr_workspace_size(1, 8, 8, 7) == 0
     assert lib.idiwf_fft_autocorr_workspace_size(0, 8, 8, nat.F64) == 0
 
@@ -183,8 +185,11 @@ def test_fft_autocorr_validation(lib):
     assert call(x=0) == nat.ERR_INVALID_ARGUMENT
     assert call(out=0) == nat.ERR_INVALID_ARGUMENT
     assert call(batch=0) == nat.ERR_INVALID_ARGUMENT
-    assert call(n1=13) == nat.ERR_UNSUPPORTED
+    assert call(n1=3000) == nat.ERR_UNSUPPORTED
     assert b"not supported" in lib.idiwf_last_error_string()
+    # the closed-form pair count does not hold for an odd padded width
+    ws_odd = lib.idiwf_fft_autocorr_workspace_size(1, 5, 13, nat.F64)
+    assert call(n0=5, n1=13, mode=2, ws_bytes=ws_odd) == nat.ERR_UNSUPPORTED
     assert call(mode=3) == nat.ERR_INVALID_ARGUMENT
     assert call(mode=0) == nat.ERR_INVALID_ARGUMENT  # no norm
     assert call(ws_bytes=need - 1) == nat.ERR_WORKSPACE
@@ -205,8 +210,9 @@ def test_fft_autocorr_shape_predicate():
     assert cusimple._hand_ok((2, 8), torch.float64)
     assert cusimple._hand_ok((15, 33), torch.float64)
     assert cusimple._hand_ok((30,), torch.float64)
-    assert not cusimple._hand_ok((13,), torch.float64)
-    assert not cusimple._hand_ok((8, 13), torch.float64)
+    assert cusimple._hand_ok((13,), torch.float64)
+    assert cusimple._hand_ok((8, 13), torch.float64)
+    assert not cusimple._hand_ok((8, 3000), torch.float64)
     assert not cusimple._hand_ok((8, 8192), torch.float64)
     assert not cusimple._hand_ok((8, 8, 8), torch.float64)
     assert not cusimple._hand_ok((8, 8), torch.float16)
@@ -221,7 +227,8 @@ def test_fft_autocorr_1d_validation(lib):
     assert lib.idiwf_fft_autocorr_1d_workspace_size(3000, 1000, nat.F64) == 2 * al(2000 * 16) + al(
         2 * 1001 * 1024 * 16)
     assert lib.idiwf_fft_autocorr_1d_workspace_size(10, 30, nat.F32) == 2 * al(60 * 16) + al(31 * 10 * 8)
-    assert lib.idiwf_fft_autocorr_1d_workspace_size(1, 13, nat.F64) == 0  # fastlen(26) = 27 is odd
+    assert lib.idiwf_fft_autocorr_1d_workspace_size(1, 13, nat.F64) > 0  # fastlen(26) = 27: Bluestein
+    assert lib.idiwf_fft_autocorr_1d_workspace_size(1, 3000, nat.F64) == 0
     assert lib.idiwf_fft_autocorr_1d_workspace_size(0, 30, nat.F64) == 0
     assert lib.idiwf_fft_autocorr_1d_workspace_size(1, 30, 7) == 0
     need = lib.idiwf_fft_autocorr_1d_workspace_size(4, 30, nat.F64)
@@ -232,7 +239,7 @@ def test_fft_autocorr_1d_validation(lib):
     assert call(x=0) == nat.ERR_INVALID_ARGUMENT
     assert call(lines=0) == nat.ERR_INVALID_ARGUMENT
     assert call(dtype=9) == nat.ERR_INVALID_ARGUMENT
-    assert call(n=13) == nat.ERR_UNSUPPORTED
+    assert call(n=3000) == nat.ERR_UNSUPPORTED
     assert call(mode=5) == nat.ERR_INVALID_ARGUMENT
     assert call(mode=1) == nat.ERR_INVALID_ARGUMENT  # no norm
     assert call(ws_bytes=need - 1) == nat.ERR_WORKSPACE

@@ -124,12 +124,11 @@ def test_hand_fft_vs_cufft(shape, dtype):
 
 
 def test_other_shapes_take_cufft():
-    # fastlen(26) = 27 is odd: the reference's inverse then has length 26,
-    # which the hand-written FFTs do not take; cuFFT does
-    assert not cusimple._hand_ok((12, 13), torch.float64)
-    x = torch.ones((12, 13), dtype=torch.float64, device="cuda")
+    # fastlen(6000) = 6000 is above the hand-written FFTs' 4096; cuFFT takes it
+    assert not cusimple._hand_ok((12, 3000), torch.float64)
+    x = torch.ones((12, 3000), dtype=torch.float64, device="cuda")
     c = cusimple.corr(x, returngpu=True)
-    assert c.shape == (24, 26)
+    assert c.shape == (24, 6000)
 
 
 @pytest.mark.parametrize("shape,dtype", [((15, 33), torch.float64), ((13, 10), torch.float64),
@@ -178,3 +177,55 @@ def test_hand_fft_1d_vs_cufft(lead, n):
     assert torch.equal(torch.isnan(hn), torch.isnan(rn))
     ok = ~torch.isnan(rn)
     assert ((hn - rn).abs() * count)[ok].max().item() <= 2e-12 * ref.abs().max().item()
+
+
+@pytest.mark.parametrize("shape,dtype", [((5, 13), torch.float64), ((9, 17), torch.float64),
+                                         ((12, 31), torch.float64), ((4, 38), torch.float64),
+                                         ((7, 61), torch.float64), ((300, 301), torch.float64),
+                                         ((1000, 344), torch.float64), ((64, 337), torch.float32)])
+def test_hand_fft_odd_width_vs_cufft(shape, dtype):
+    """An odd last padded length fastlen(2 n1): the reference's inverse has
+    one value fewer, which is never a product of 2, 3, 5, 7, 11 -- the
+    inverse by Bluestein's algorithm -- and norm=True divides by the same
+    transform of ones.  Against cuFFT's transforms with the same lengths."""
+    fs = [cusimple.fastlen(2 * s) for s in shape]
+    assert fs[1] % 2 == 1 and cusimple._hand_ok(shape, dtype)
+    g = torch.Generator(device="cuda").manual_seed(sum(shape) + 11)
+    x = torch.empty((3,) + shape, dtype=dtype, device="cuda").exponential_(1.0, generator=g)
+    tol = 1e-12 if dtype == torch.float64 else 2e-5
+    ref = cusimple._crop(cusimple._autocorr(x, 2, fs), 2, list(shape))
+    hand = cusimple._hand_autocorr(x)
+    assert hand.shape == ref.shape
+    assert (hand - ref).abs().max().item() <= tol * ref.abs().max().item()
+    ones = torch.ones(shape, dtype=dtype, device="cuda")
+    pairs = cusimple._crop(cusimple._autocorr(ones, 2, fs), 2, list(shape))
+    rn = cusimple._crop(cusimple._autocorr(x, 2, fs), 2, list(shape), norm=pairs, mode=0, threshold=0.9)
+    hn = cusimple.corr(x, axes=(1, 2), returngpu=True, norm=False)
+    assert torch.equal(hn, cusimple._hand_autocorr(x))
+    # corr(norm=True) divides by the mean first; compare on the same input
+    xm = x * (1 / x.mean(dim=0, keepdim=True))
+    hn = cusimple.corr(x, axes=(1, 2), norm=True, returngpu=True)
+    rn = cusimple._crop(cusimple._autocorr(xm, 2, fs), 2, list(shape), norm=pairs, mode=0, threshold=0.9)
+    assert torch.equal(torch.isnan(hn), torch.isnan(rn))
+    ok = ~torch.isnan(rn)
+    assert ((hn - rn).abs() * pairs)[ok].max().item() <= 4 * tol * (rn.abs() * pairs)[ok].max().item()
+
+
+@pytest.mark.parametrize("n", [13, 38, 301])
+def test_hand_fft_1d_odd_vs_cufft(n):
+    """One axis with an odd padded length, plain and divided by the
+    transform of ones."""
+    G = cusimple.fastlen(2 * n)
+    assert G % 2 == 1
+    g = torch.Generator(device="cuda").manual_seed(n)
+    x = torch.empty((7, n), dtype=torch.float64, device="cuda").exponential_(1.0, generator=g)
+    ref = cusimple._crop(cusimple._autocorr(x, 1, [G]), 1, [n])
+    hand = cusimple._hand_autocorr_1d(x)
+    assert (hand - ref).abs().max().item() <= 1e-12 * ref.abs().max().item()
+    ones = torch.ones((n,), dtype=torch.float64, device="cuda")
+    pairs = cusimple._crop(cusimple._autocorr(ones, 1, [G]), 1, [n])
+    hn = cusimple._hand_autocorr_1d(x, mode=0, norm=pairs, threshold=0.9)
+    rn = torch.where(pairs < 0.9, torch.full_like(ref, float("nan")), ref / pairs)
+    assert torch.equal(torch.isnan(hn), torch.isnan(rn))
+    ok = ~torch.isnan(rn)
+    assert ((hn - rn).abs() * pairs)[ok].max().item() <= 2e-12 * ref.abs().max().item()
