@@ -1150,26 +1150,6 @@ static int fcg_threads(int values, size_t smem) {
     return std::min(cap, std::max(32, (values / 4 + 31) / 32 * 32));
 }
 constexpr int kFcgMaxLen = 4096;  // G0, G1 and L1 of the general path
-// Bluestein's FFT length: any M >= need works; the one from need to
-// min(2 need, 4096) with the least estimated work, M times the per-value
-// cost of its passes (odd radices cost more than 8, 4, 2); 0 if none fits.
-static int fcg_blue_length(int need) {
-    int best = 0;
-    double best_cost = 0;
-    for (int M = need; M <= std::min(2 * need, kFcgMaxLen); ++M) {
-        FcgRad r;
-        if (!fcg_radices(M, r)) continue;
-        double c = 0;
-        for (int i = 0; i < r.np; ++i)
-            c += r.r[i] == 11 ? 4.0 : r.r[i] == 7 ? 2.8 : r.r[i] == 5 ? 2.0 : r.r[i] == 3 ? 1.4 : r.r[i] == 8 ? 1.5 : 1.1;
-        c *= M;
-        if (!best || c < best_cost) {
-            best = M;
-            best_cost = c;
-        }
-    }
-    return best;
-}
 static int fcg_stride(int n, int lkc) { return n + ((n - 1) >> lkc) + 1; }
 
 struct FcgPlan {
@@ -1202,8 +1182,10 @@ static bool fcg_plan(int64_t batch, int n0, int n1, int dtype, FcgPlan &p, bool 
     if (!oned && !fcg_radices(p.G0, p.radB)) return false;
     p.blue = !fcg_radices(p.Hp, p.radC);
     if (p.blue) {
-        p.M = fcg_blue_length(2 * p.Hp - 1);
-        if (p.M == 0 || !fcg_radices(p.M, p.radC)) return false;
+        // the shortest smooth length: measured faster than longer lengths with
+        // cheaper radices (2304 or 640 instead of 2079 or 605)
+        p.M = fcg_fastlen(2 * p.Hp - 1);
+        if (p.M > kFcgMaxLen || !fcg_radices(p.M, p.radC)) return false;
     }
     const int nC = p.radC.n;  // values per row in pass C
     p.vsz = dtype == IDIWF_F64 ? 16 : 8;

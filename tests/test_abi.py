@@ -171,10 +171,10 @@ def test_fft_autocorr_validation(lib):
     for n0, n1 in ((8, 2049), (8, 8192), (0, 8), (3000, 8), (8, 0)):
         assert lib.idiwf_fft_autocorr_workspace_size(1, n0, n1, nat.F64) == 0, (n0, n1)
     # 5 x 13: G1 = 27 is odd, the inverse has L1 = 26 values (Hp = 13 by
-    # Bluestein through FFTs of M = 32, the cheapest smooth length from
-    # 2 Hp - 1 = 25): tables of 27, 10, 26 and chirp 13, filter and twiddles 32
+    # Bluestein through FFTs of M = fastlen(2 Hp - 1) = 25): tables of 27, 10,
+    # 26 and chirp 13, filter and twiddles 25
     assert lib.idiwf_fft_autocorr_workspace_size(1, 5, 13, nat.F64) == (
-        al(27 * 16) + al(10 * 16) + al(26 * 16) + al(13 * 16) + 2 * al(32 * 16) + al(14 * 5 * 16) + al(14 * 6 * 16))
+        al(27 * 16) + al(10 * 16) + al(26 * 16) + al(13 * 16) + 2 * al(25 * 16) + al(14 * 5 * 16) + al(14 * 6 * 16))
     assert lib.idiwf_fft_autocorr_workspace_size(1, 8, 8, 7) == 0
     assert lib.idiwf_fft_autocorr_workspace_size(0, 8, 8, nat.F64) == 0
 
