@@ -477,9 +477,12 @@ idiwf_status idiwf_qcorr_3d(const float *zd, const float *images, int32_t n_imag
  * Shapes: n0, n1 powers of two from 4 to 4096 (x and out aligned to two
  * elements), or any n0, n1 >= 1 whose padded lengths G0 = fastlen(2 n0) and
  * G1 = fastlen(2 n1) (smallest products of 2, 3, 5, 7, 11, as
- * idi.util.fastlen) are at most 4096 with G1 even; out is then the centre
- * crop (i - n0) mod G0, (j - n1) mod G1 of the shifted array, as the
- * reference's slice.  Other shapes: IDIWF_ERR_UNSUPPORTED.
+ * idi.util.fastlen) are at most 4096; out is then the centre crop
+ * (i - n0) mod G0, (j - n1) mod L1 of the shifted array, as the reference's
+ * slice, with L1 = G1 for an even G1 and G1 - 1 for an odd one (numpy's
+ * default inverse length; mode 2 is then IDIWF_ERR_UNSUPPORTED, since the
+ * reference's pair count is the same transform of ones: pass it as norm with
+ * mode 0).  Other shapes: IDIWF_ERR_UNSUPPORTED.
  * workspace: idiwf_fft_autocorr_workspace_size() bytes for this batch and
  * shape, 256-byte aligned (twiddle tables and the intermediates of one group
  * of images; groups run one after another; 0 for unsupported arguments).
@@ -493,8 +496,8 @@ idiwf_status idiwf_fft_autocorr(const void *x, int32_t dtype, int64_t batch, int
  * The autocorrelation of each of `lines` independent lines (x: lines x n of
  * dtype, contiguous) along its length, as cusimple.py:6-38 with one
  * correlated axis: out (lines x 2n) = crop(fftshift(irfft(|rfft(x, G)|^2)))
- * with G = fastlen(2 n), which must be even and at most 4096 (else
- * IDIWF_ERR_UNSUPPORTED).  Modes as idiwf_fft_autocorr, with the pair count
+ * with G = fastlen(2 n) at most 4096 (else IDIWF_ERR_UNSUPPORTED; an odd G
+ * as for idiwf_fft_autocorr).  Modes as idiwf_fft_autocorr, with the pair count
  * n - |j - n| and norm of 2n values.  workspace:
  * idiwf_fft_autocorr_1d_workspace_size() bytes, 256-byte aligned.
  */
