@@ -1,9 +1,11 @@
-// FFT autocorrelation (idi/reconstruction/cusimple.py): for power-of-two
-// shapes the whole autocorrelation by hand-written shared-memory FFTs (three
-// passes per image, below); for other lengths the elementwise steps around
-// cuFFT's transforms -- the power spectrum in place, the fftshift + centre crop
-// fused with the normalisation -- and the correlator's running mean /
-// variance.
+// FFT autocorrelation (idi/reconstruction/cusimple.py) by hand-written
+// shared-memory FFTs, three passes per group of images: a tuned path for
+// power-of-two shapes (fc_*), and a mixed-radix path for the reference's
+// padded lengths fastlen(2 n) up to 4096 (fcg_*, with Bluestein's algorithm
+// for the inverse of an odd last padded length and a 1D form for independent
+// lines).  For larger shapes, the elementwise steps around cuFFT's transforms
+// -- the power spectrum in place, the fftshift + centre crop fused with the
+// normalisation -- and the correlator's running mean / variance.
 #include <cmath>
 #include <type_traits>
 
