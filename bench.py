@@ -210,7 +210,9 @@ def c2_oracle_windows(out, pos, ph, k, w=64, seed=9):
 
 
 def summarize_targets(line, t):
-    """The north-star figures in one compact object, last on the line."""
+    """The target figures (C2 rate, SFU fraction, split/FP64 speed-up and error,
+    end-to-end rate, forward+adjoint ratio, batched rate and balance, time
+    path) in one compact object, last on the line."""
     def r4(x):
         return None if x is None else float(f"{x:.4g}")
 
