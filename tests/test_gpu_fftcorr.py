@@ -137,7 +137,9 @@ def test_other_shapes_take_cufft():
                                          ((40, 12), torch.float64), ((100, 75), torch.float64),
                                          ((300, 500), torch.float64), ((1000, 1050), torch.float64),
                                          ((1500, 7), torch.float64), ((6, 2000), torch.float64),
-                                         ((100, 75), torch.float32), ((300, 500), torch.float32)])
+                                         ((100, 75), torch.float32), ((300, 500), torch.float32),
+                                         ((4, 1), torch.float64), ((1, 1), torch.float64), ((2, 2), torch.float64),
+                                         ((5, 1), torch.float32), ((1, 3), torch.float64)])
 def test_hand_fft_general_vs_cufft(shape, dtype):
     """Other lengths: mixed-radix passes (2, 3, 4, 5, 7, 8, 11) on the padded
     lengths fastlen(2 n), cropped, against cuFFT's transforms with the same
@@ -160,7 +162,7 @@ def test_hand_fft_general_vs_cufft(shape, dtype):
 
 
 @pytest.mark.parametrize("lead,n", [((5, 2), 4), ((5, 2), 30), ((5, 2), 1000), ((5, 2), 1024), ((5, 2), 1500),
-                                    ((2500,), 100), ((1030,), 7)])
+                                    ((2500,), 100), ((1030,), 7), ((3,), 1), ((3,), 2), ((4,), 3)])
 def test_hand_fft_1d_vs_cufft(lead, n):
     """One correlated axis (idiwf_fft_autocorr_1d; more than 1024 lines run as
     several images plus a remainder) against cuFFT's 1D transforms."""
