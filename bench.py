@@ -940,6 +940,13 @@ def qcorr_leg(torch, dev, args):
     out["fft_corr"] = {"ms": msf, "images_per_s": 8 / (msf * 1e-3), "cufft_path_ms": msc,
                        "workload": "cusimple.corr of 8 x 1024x1024 float64 (2048^2 transforms), on the device; "
                                    "hand-written FFTs (power-of-two shape)"}
+    # a general shape: fastlen(2000) = 2000 = 5^3 2^4, mixed-radix passes
+    stack_g = torch.from_numpy(g.exponential(1.0, (8, 1000, 1000))).to(dev)
+    msg = timed(lambda: cusimple.corr(stack_g, returngpu=True), reps=3)
+    msgc = timed(lambda: cusimple._crop(cusimple._autocorr(stack_g, 2, [2000, 2000]), 2, [1000, 1000]), reps=3)
+    out["fft_corr_general"] = {"ms": msg, "images_per_s": 8 / (msg * 1e-3), "cufft_path_ms": msgc,
+                               "workload": "cusimple.corr of 8 x 1000x1000 float64 (2000^2 transforms, radices "
+                                           "5, 8, 2), on the device; hand-written FFTs"}
     if not args.no_cpu_baseline:
         import oracle
 
