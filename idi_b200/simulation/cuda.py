@@ -182,7 +182,7 @@ def simulate(
 
     Mirrors ``idi/simulation/cuda.py:141-202``: images are drawn from
     ``simobject.get2()`` in order and run in batched persistent launches.
-    With host output, the images are processed in up to four chunks whose
+    With host output, the images are processed in up to eight chunks whose
     device-to-host copies (into pinned staging, on a second stream) overlap
     the next chunk's kernel.  Ctrl-C returns the images finished so far.
     Device-side errors (split-precision emitters out of range, a near-field
@@ -197,8 +197,7 @@ def simulate(
     elem = 8 if out_kind == nat.OUT_C64 else 16
     per_img = npix * elem
     cap = int(max(1, _MAX_OUT_BYTES // max(per_img, 1)))
-    # enough chunks to overlap copies with compute when the output is large
-    nchunks = 4 if (per_img * Nimg >= (64 << 20) and Nimg >= 4) else 1
+    nchunks = _nchunks(per_img * Nimg, Nimg)
     chunk = int(max(1, min(cap, -(-Nimg // nchunks))))
     done = 0
     if returngpu:
@@ -226,6 +225,25 @@ def simulate(
     dtype = torch.complex64 if out_kind == nat.OUT_C64 else torch.complex128
     return _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, dtype, amplitudes, verbose,
                       np.complex128)
+
+
+def _nchunks(out_bytes, Nimg):
+    """Chunks of the host-output pipeline: enough to overlap the copies with
+    the kernels, and the more the larger the output, since the first chunk's
+    upload and the last chunk's copies are not overlapped."""
+    if out_bytes >= (256 << 20) and Nimg >= 8:
+        return 8
+    if out_bytes >= (64 << 20) and Nimg >= 4:
+        return 4
+    return 1
+
+
+def _prefault(a):
+    """Touch one byte per 4 KiB page of a fresh host array, so that the page
+    faults happen now (while the GPU computes) and not in the copy of the
+    last chunk, which nothing overlaps."""
+    flat = a.reshape(-1).view(np.uint8)
+    flat[::4096] = 0
 
 
 def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, out_dtype, amplitudes, verbose,
@@ -257,6 +275,10 @@ def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, 
         ev_copied[ps].synchronize()
         if sink is not None:
             sink(pstart, h_out[ps][:pn].numpy())
+        elif result.dtype == h_out[ps].numpy().dtype:
+            # torch's CPU copy runs on several threads; the last chunk's copy
+            # is on the critical path
+            torch.from_numpy(result[pstart:pstart + pn]).copy_(h_out[ps][:pn])
         else:
             result[pstart:pstart + pn] = h_out[ps][:pn].numpy()
         finished[0] = pstart + pn
@@ -290,6 +312,8 @@ def _pipelined(Nimg, simobject, N, Ndet, chunk, dev, geom, precision, out_kind, 
             with torch.cuda.stream(copy):
                 h_out[slot][:nb].copy_(src, non_blocking=True)
             ev_copied[slot].record(copy)
+            if i == 0 and result is not None and Nimg > nb:
+                _prefault(result)  # overlaps the first chunk's kernels
             if pending is not None:
                 _collect(*pending)
             pending = (slot, done, nb)
@@ -344,7 +368,7 @@ def simulate_to_npz(
     Nimg = int(Nimg)
     per_img = Ndet[0] * Ndet[1] * 8
     cap = int(max(1, _MAX_OUT_BYTES // max(per_img, 1)))
-    nchunks = 4 if (per_img * Nimg >= (64 << 20) and Nimg >= 4) else 1
+    nchunks = _nchunks(per_img * Nimg, Nimg)
     chunk = int(max(1, min(cap, -(-Nimg // nchunks))))
     with NpzStream(outfile, compress=compress) as npz:
         member = npz.array("result", (Nimg, Ndet[0], Ndet[1]), np.float64)
@@ -404,7 +428,7 @@ def simulate_photons(
     else:
         final = tdt
     cap = int(max(1, _MAX_OUT_BYTES // max(npix * 16, 1)))
-    nchunks = 4 if (npix * 8 * Nimg >= (64 << 20) and Nimg >= 4) else 1
+    nchunks = _nchunks(npix * 8 * Nimg, Nimg)
     chunk = int(max(1, min(cap, -(-Nimg // nchunks))))
     counts = [None, None]
     shared = [None, None]
