@@ -772,9 +772,9 @@ __global__ void __launch_bounds__(512) fcg_blue_filter_kernel(const double2 *__r
     }
 }
 
-// Launch bounds of the general kernels: FP64 blocks take up to 512 threads
-// (one block per SM when two do not fit in shared memory); FP32 blocks always
-// fit two or more per SM, take at most 256 threads, and are held to 85
+// Launch bounds of the general kernels: FP64 blocks (2048 values) fit two
+// per SM and take 256 threads -- the bound of 512 leaves them 128 registers;
+// FP32 blocks (4096 values) take at most 256 threads and are held to 85
 // registers for three blocks per SM (measured 16-20 % faster than two).
 template <typename T> constexpr int kFcgMaxThreads = sizeof(T) == 8 ? 512 : 256;
 template <typename T> constexpr int kFcgMinBlocks = sizeof(T) == 8 ? 1 : 3;
